@@ -1,0 +1,448 @@
+/*
+ * warren_cuda.h — the C ABI of the B200 (sm_100a) backend for pg_warren's
+ * whole-graph compute path.
+ *
+ * pg_warren names a kernel seam between its SQL adapters and whatever runs a
+ * kernel (the `Kernels` trait of the reference's DESIGN.md:1208-1243, today
+ * the free functions of warren-core).  Every entry point below replaces one
+ * of those functions for one dense-id graph version; the comment on each
+ * names the reference function (path within the reference project, file:line)
+ * whose arguments, results and errors it keeps.
+ *
+ * Conventions shared by every call:
+ *  - Plain pointers and sizes only.  A pointer to an operand may be a host
+ *    pointer (pageable or pinned) or a device pointer of the handle's device;
+ *    the library tells them apart itself (cudaPointerGetAttributes).
+ *  - Dense ids are the reference's DenseId (u64 on the ABI); the device copy
+ *    stores them as u32, so an id space of 2^32 or more is not served
+ *    (WC_UNSUPPORTED, and the adapter keeps the native kernel: `serves`).
+ *  - Every call returns a wc_status mirroring the reference's error enums
+ *    1:1 (ComputeError in compute/error.rs:10-208, TraversalError in
+ *    traversal/error.rs, SpectralError in spectral/error.rs).  A call never
+ *    aborts; device-side arithmetic errors go to an error word that the call
+ *    turns into its status.
+ *  - Device memory (the version's copy and each call's scratch) is charged to
+ *    a wc_budget before it is allocated, as the reference charges its
+ *    ComputeMemory (compute/memory.rs:31-227); a refused charge is
+ *    WC_MEMORY_LIMIT with requested/in_use/limit in the detail.
+ *  - Cancellation: the call polls `wc_call.cancel` (a host word the caller
+ *    sets, e.g. from a signal handler) between launches and at least every
+ *    millisecond while it waits, and returns WC_CANCELLED.
+ */
+#ifndef WARREN_CUDA_H
+#define WARREN_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WC_ABI_VERSION 1
+
+/* ------------------------------------------------------------------ status */
+
+typedef enum wc_status {
+    WC_OK = 0,
+    /* ComputeError (compute/error.rs) */
+    WC_MEMORY_LIMIT = 1,          /* MemoryLimit {requested, in_use, limit} */
+    WC_OUT_OF_MEMORY = 2,         /* OutOfMemory {bytes} */
+    WC_DTYPE_MISMATCH = 3,        /* DtypeMismatch */
+    WC_ID_SPACE_MISMATCH = 4,     /* IdSpaceMismatch */
+    WC_WIDTH_MISMATCH = 5,        /* WidthMismatch */
+    WC_UNKNOWN_SEMIRING = 6,      /* UnknownSemiring */
+    WC_UNKNOWN_BINARY_OP = 7,     /* UnknownBinaryOp */
+    WC_ZERO_WIDTH = 8,            /* ZeroWidth */
+    WC_CANCELLED = 9,             /* Cancelled */
+    /* ArithmeticError (compute/error.rs:180-208) */
+    WC_BIGINT_OUT_OF_RANGE = 10,  /* BigintOutOfRange */
+    WC_FLOAT_OVERFLOW = 11,       /* FloatOverflow */
+    WC_FLOAT_UNDERFLOW = 12,      /* FloatUnderflow */
+    WC_DIVISION_BY_ZERO = 13,     /* DivisionByZero */
+    /* TraversalError (traversal/error.rs) */
+    WC_NODE_OUTSIDE_ID_SPACE = 20,  /* NodeOutsideIdSpace {node} */
+    WC_NODE_FILTER_ID_SPACE = 21,   /* NodeFilterIdSpace {expected, found} */
+    WC_REVERSE_CSR_MISSING = 22,    /* ReverseCsrMissing */
+    /* SpectralError (spectral/error.rs) */
+    WC_NOT_SYMMETRIC = 30,          /* NotSymmetric */
+    WC_NON_POSITIVE_DEGREE = 31,    /* NonPositiveDegree {node, degree} */
+    WC_EIGENPAIR_COUNT = 32,        /* EigenpairCount {k, dimension} */
+    WC_WORKING_SET = 33,            /* WorkingSet {bytes, in_use, limit} */
+    WC_NOT_FINITE = 34,             /* NotFinite */
+    /* the backend's own */
+    WC_INVALID_ARGUMENT = 40,       /* a null pointer, a bad enum value, ... */
+    WC_UNSUPPORTED = 41,            /* not served here: the adapter keeps the native kernel */
+    WC_CUDA_ERROR = 42,             /* a CUDA runtime error; detail.cuda_error */
+    WC_DEVICE_TIMEOUT = 43,         /* a bounded device-side wait ran out */
+    WC_NO_DEVICE = 44               /* no usable sm_100 device */
+} wc_status;
+
+/* What went wrong, beyond the status.  Any field may be zero. */
+typedef struct wc_error_detail {
+    uint64_t requested;  /* MemoryLimit / OutOfMemory / WorkingSet: bytes */
+    uint64_t in_use;
+    uint64_t limit;
+    uint64_t node;       /* NodeOutsideIdSpace / NonPositiveDegree: dense id */
+    uint64_t expected;   /* *Mismatch: expected / found */
+    uint64_t found;
+    double degree;       /* NonPositiveDegree */
+    int32_t cuda_error;  /* WC_CUDA_ERROR: the cudaError_t */
+    char message[200];   /* a one-line description */
+} wc_error_detail;
+
+/* The message of a status ("division by zero", ...), as the reference's
+ * Display impls word them. */
+const char* wc_status_name(wc_status status);
+
+/* ------------------------------------------------------------ element types */
+
+/* compute/dtype.rs:12-21, in the same order. */
+typedef enum wc_dtype { WC_F32 = 0, WC_F64 = 1, WC_I64 = 2, WC_BOOL = 3 } wc_dtype;
+
+/* compute/semiring.rs:15-38 (BinaryOp), in declaration order. */
+typedef enum wc_binary_op {
+    WC_OP_FIRST = 0, WC_OP_SECOND = 1, WC_OP_PAIR = 2, WC_OP_PLUS = 3, WC_OP_TIMES = 4,
+    WC_OP_MIN = 5, WC_OP_MAX = 6, WC_OP_LOR = 7, WC_OP_LAND = 8, WC_OP_ANY = 9,
+    WC_OP_NONE = -1 /* no accumulator */
+} wc_binary_op;
+
+/* compute/semiring.rs:118-146 (Semiring), in declaration order. */
+typedef enum wc_semiring {
+    WC_PLUS_TIMES = 0, WC_MIN_PLUS = 1, WC_MAX_PLUS = 2, WC_MAX_TIMES = 3, WC_MIN_TIMES = 4,
+    WC_LOR_LAND = 5, WC_ANY_PAIR = 6, WC_PLUS_PAIR = 7, WC_PLUS_FIRST = 8, WC_PLUS_SECOND = 9,
+    WC_MIN_FIRST = 10, WC_MIN_SECOND = 11, WC_MAX_SECOND = 12
+} wc_semiring;
+
+/* graph/direction.rs:6-13. */
+typedef enum wc_direction { WC_OUT = 0, WC_IN = 1, WC_BOTH = 2 } wc_direction;
+
+/* ----------------------------------------------------------- runtime handles */
+
+typedef struct wc_budget wc_budget;     /* device memory budget (ComputeMemory) */
+typedef struct wc_version wc_version;   /* a version's device CSR + CSC */
+
+/* A budget of `limit` bytes of device memory (ComputeMemory::new,
+ * compute/memory.rs).  Thread-safe. */
+wc_status wc_budget_create(uint64_t limit, wc_budget** out);
+void wc_budget_destroy(wc_budget* budget);
+uint64_t wc_budget_in_use(const wc_budget* budget);
+uint64_t wc_budget_peak(const wc_budget* budget);
+
+/* Progress (progress.rs:9-16): a phase starting with an optional total, then
+ * units done.  `total` is UINT64_MAX when unknown. */
+typedef void (*wc_progress_fn)(void* context, const char* phase, uint64_t done, uint64_t total);
+
+/* What a call is given besides its operands: the seam's `Call`
+ * (DESIGN.md:1213-1220) plus the stream the work goes on. */
+typedef struct wc_call {
+    wc_budget* memory;             /* scratch is charged here; NULL: the version's budget */
+    volatile const int32_t* cancel; /* non-zero: stop (WC_CANCELLED); may be NULL */
+    wc_progress_fn progress;       /* may be NULL */
+    void* progress_context;
+    void* stream;                  /* cudaStream_t; NULL: the version's own stream */
+    uint32_t flags;                /* WC_CALL_* */
+    uint32_t timeout_ms;           /* bound on any wait for the device; 0: 600000 */
+    wc_error_detail* detail;       /* filled on error; may be NULL */
+} wc_call;
+
+/* With device operands only: return once the work is queued on the stream,
+ * without waiting for it; errors found on the device are reported by the next
+ * call on the version, or by wc_version_sync. */
+#define WC_CALL_ASYNC 1u
+
+/* -------------------------------------------------------------- versions */
+
+/* A built version's adjacency as the reference holds it (graph/csr/mod.rs:
+ * 38-237): offsets u64[n+1], targets u32[m] ascending and distinct within a
+ * row, weights f64[m] or NULL (every weight 1).  The reverse CSR
+ * (graph/csr/graph_csr.rs:15-55, transpose.rs:1-30) may be given; without it
+ * the device builds its own by transposing, counted in the budget.  Only a
+ * single merged CSR is uploaded: the relation selection "all relations" of
+ * every call reads it (product/matrix.rs:126-157). */
+typedef struct wc_csr_host {
+    uint64_t id_space;
+    uint64_t edges;
+    const uint64_t* offsets;
+    const uint32_t* targets;
+    const double* weights;
+    const uint64_t* reverse_offsets;  /* NULL: built on the device */
+    const uint32_t* reverse_targets;
+    const double* reverse_weights;
+} wc_csr_host;
+
+typedef struct wc_version_info {
+    uint64_t id_space;
+    uint64_t edges;
+    uint64_t device_bytes;     /* charged to the budget */
+    int32_t weighted;          /* the CSR has weights */
+    int32_t integral_weights;  /* every weight is an integer in int32 range: an int32 copy is kept */
+    int32_t device;            /* CUDA ordinal */
+    int32_t symmetric;         /* the CSR equals its transpose (values included) */
+} wc_version_info;
+
+/* Uploads `csr` for (graph_id, version) to the current device: the derived
+ * device copy the seam keys by version (DESIGN.md:1240).  Charged to
+ * `budget` (which must outlive the handle). */
+wc_status wc_version_upload(uint64_t graph_id, uint64_t version, const wc_csr_host* csr,
+                            wc_budget* budget, const wc_call* call, wc_version** out);
+wc_status wc_version_release(wc_version* version);
+wc_status wc_version_info_get(const wc_version* version, wc_version_info* info);
+/* Waits for the version's stream and reports a pending device error. */
+wc_status wc_version_sync(wc_version* version, const wc_call* call);
+
+/* Whether this backend serves `operation` over `dtype` (the seam's
+ * `Kernels::serves`, DESIGN.md:1224).  Operations: "spmv", "spmm", "pagerank",
+ * "bfs", "reachable_set", "eigen", "vector_topk". */
+int32_t wc_serves(const char* operation, wc_dtype dtype);
+
+/* -------------------------------------------------------------- products */
+
+/* A value mask (compute/mask.rs:11-45): row i is written when mask[i] is
+ * non-zero (NaN included), or zero with `complement`. */
+typedef struct wc_mask {
+    const void* values;   /* id_space elements of `dtype` */
+    wc_dtype dtype;
+    int32_t complement;
+} wc_mask;
+
+/* compute/product/mod.rs:31-56 (Product), for the all-relations selection. */
+typedef struct wc_product {
+    wc_semiring semiring;
+    int32_t transpose;       /* y = Aᵀ ⊗ x */
+    int32_t weighted;        /* -1: if the graph has weights; 0: every weight 1; 1: weights */
+    const wc_mask* mask;     /* NULL: every row */
+    int32_t replace;
+    wc_binary_op accumulate; /* WC_OP_NONE: overwrite */
+} wc_product;
+
+/* SpMV y = A ⊗ x (or Aᵀ ⊗ x) over width-1 vectors of `dtype`:
+ * compute/product/mod.rs:77-92 (spmv).  `y` holds the values kept where the
+ * mask leaves rows unwritten or `accumulate` combines (compute_sql/product.rs:
+ * 101-109 fills it). */
+wc_status wc_spmv(wc_version* version, const wc_call* call, const wc_product* product,
+                  wc_dtype dtype, const void* x, void* y);
+
+/* SpMM Y = A ⊗ X for row-major id_space × width matrices:
+ * compute/product/mod.rs:97-110 (spmm). */
+wc_status wc_spmm(wc_version* version, const wc_call* call, const wc_product* product,
+                  wc_dtype dtype, uint32_t width, const void* x, void* y);
+
+/* -------------------------------------------------------------- pagerank */
+
+/* compute/pagerank/mod.rs:27-47 (PageRank), all relations. */
+typedef struct wc_pagerank_opts {
+    double damping;
+    double tol;              /* used when has_tol */
+    int32_t has_tol;         /* 0: run every iteration */
+    int32_t weighted;        /* -1 / 0 / 1 as wc_product.weighted */
+    uint32_t max_iter;
+    const double* seed;      /* personalisation (width-1 f64); NULL: uniform */
+} wc_pagerank_opts;
+
+/* compute/pagerank/mod.rs:96-151 (pagerank): ranks over the live nodes
+ * (`tombstones`, graph/tombstones.rs: bit i of word i/64 marks dense id i
+ * deleted; NULL: none), zero at tombstoned rows. */
+wc_status wc_pagerank(wc_version* version, const wc_call* call, const wc_pagerank_opts* opts,
+                      const uint64_t* tombstones, double* ranks, uint32_t* iterations);
+
+/* The stop test's margin of the last iteration run: delta / (live × tol).
+ * Available after wc_pagerank on the same version (diagnostics). */
+double wc_pagerank_last_margin(const wc_version* version);
+
+/* ------------------------------------------------------------- traversal */
+
+/* traversal/stats.rs:12-23 (TraversalStats). */
+typedef struct wc_traversal_stats {
+    uint64_t nodes_visited;
+    uint64_t edges_traversed;
+    int32_t truncated;
+    uint32_t levels;         /* levels expanded */
+    uint32_t pulled_levels;  /* of which pulled (reachable_set) */
+} wc_traversal_stats;
+
+/* traversal/limits.rs:4-12 (Limits); UINT32_MAX / UINT64_MAX: unbounded. */
+typedef struct wc_limits {
+    uint32_t max_depth;
+    uint64_t max_results;
+} wc_limits;
+
+#define WC_UNREACHED UINT32_MAX
+#define WC_NO_VIA UINT64_MAX
+
+/* traversal/bfs.rs:34-60 (bfs / bfs_each) over the all-relations adjacency
+ * read in `direction`, node filter `filter` (NodeSet bitmap words; NULL:
+ * none).  Per node: depth_out[i] its depth (WC_UNREACHED if not visited) and
+ * via_out[i] the node it was first reached from (WC_NO_VIA for a start or an
+ * unvisited node) — the same (node, depth, via) the reference's visits carry.
+ * Either output may be NULL. */
+wc_status wc_bfs(wc_version* version, const wc_call* call, wc_direction direction,
+                 const uint64_t* starts, uint64_t start_count, const wc_limits* limits,
+                 const uint64_t* filter, uint32_t* depth_out, uint64_t* via_out,
+                 wc_traversal_stats* stats);
+
+/* The visits of wc_bfs in the reference's order (by depth; within a depth,
+ * the previous depth's nodes expanded in ascending dense id, each row in
+ * ascending target order), truncated at max_results as bfs truncates:
+ * visits_out[3*r .. 3*r+2] = (node, depth, via).  `capacity` rows;
+ * *count gets the number written. */
+wc_status wc_bfs_visits(wc_version* version, const wc_call* call, wc_direction direction,
+                        const uint64_t* starts, uint64_t start_count, const wc_limits* limits,
+                        const uint64_t* filter, uint64_t* visits_out, uint64_t capacity,
+                        uint64_t* count, wc_traversal_stats* stats);
+
+/* traversal/reachable.rs:48-90 (reachable_set / reachable_set_each): the
+ * nodes within max_depth of `starts` in the reference's order (by depth;
+ * pushed levels in the order reached, pulled levels ascending), with the
+ * reference's direction switch (Beamer, α = 1, β = 24, level.rs:19-29) so
+ * stats.edges_traversed matches.  `capacity` entries; *count written. */
+wc_status wc_reachable_set(wc_version* version, const wc_call* call, wc_direction direction,
+                           const uint64_t* starts, uint64_t start_count, uint32_t max_depth,
+                           uint64_t* nodes_out, uint64_t capacity, uint64_t* count,
+                           wc_traversal_stats* stats);
+
+/* traversal/reachable.rs:18-43 (reachable). */
+wc_status wc_reachable(wc_version* version, const wc_call* call, wc_direction direction,
+                       uint64_t start, uint64_t target, uint32_t max_depth, int32_t* reached,
+                       wc_traversal_stats* stats);
+
+/* ------------------------------------------------- batched (no reference
+ * counterpart: many searches as one semiring SpMM in a persistent kernel
+ * under a captured CUDA graph) */
+
+/* A schedule for the batched SpMM: columns per pass and rows per work unit,
+ * chosen by wc_autotune for (version, kind, width) and cached in the handle. */
+typedef struct wc_schedule {
+    uint32_t columns_per_pass;
+    uint32_t rows_per_unit;
+    uint32_t blocks_per_sm;
+    uint32_t reserved;
+} wc_schedule;
+
+typedef enum wc_batch_kind { WC_BATCH_BFS = 0, WC_BATCH_MINPLUS = 1, WC_BATCH_PPR = 2 } wc_batch_kind;
+
+/* Times the candidate schedules for `kind` at `width` columns on this version
+ * and keeps the fastest; `chosen` may be NULL. */
+wc_status wc_autotune(wc_version* version, const wc_call* call, wc_batch_kind kind,
+                      uint32_t width, wc_schedule* chosen);
+
+/* `width` BFS searches, source s from sources[s] to depth max_depths[s]
+ * (out-edges), as one boolean SpMM over bit-packed frontiers.  depth_out is
+ * source-major: depth_out[s * id_space + i] = depth of i from sources[s]
+ * (255 if not reached within the cap).  Identical to `width` calls of
+ * wc_bfs (node, depth).  edges_traversed_out[s] (may be NULL) gets the edges
+ * a push-only bfs from that source would scan. */
+wc_status wc_bfs_batched(wc_version* version, const wc_call* call, const uint64_t* sources,
+                         const uint32_t* max_depths, uint32_t width, uint8_t* depth_out,
+                         uint64_t* edges_traversed_out);
+
+/* `width` hop-bounded shortest-path searches (the sssp_vector loop,
+ * compute_sql/library/sssp_vector.sql:14-66, with max_iter = max_hops[s]):
+ * dist_out[s * id_space + i] = the i64 min-plus distance (INT64_MAX:
+ * unreached) over transpose min_plus with accumulate min; iterations_out[s]
+ * (may be NULL) the iterations that loop runs.  Weights are cast as
+ * SemiringElement::from_weight casts them (semiring.rs:365-367). */
+wc_status wc_minplus_batched(wc_version* version, const wc_call* call, const uint64_t* sources,
+                             const uint32_t* max_hops, uint32_t width, int64_t* dist_out,
+                             uint32_t* iterations_out);
+
+/* `width` personalised PageRanks (pagerank/mod.rs:96-199 with a seed): seed
+ * set c is seed_nodes[seed_offsets[c] .. seed_offsets[c+1]), each node's
+ * seed value 1, so p = 1/|set| on the set.  Each column stops at its own
+ * iterate (delta < live × tol).  ranks_out is column-major:
+ * ranks_out[c * id_space + i]; iterations_out[c] per column. */
+wc_status wc_ppr_batched(wc_version* version, const wc_call* call, const wc_pagerank_opts* opts,
+                         const uint64_t* seed_nodes, const uint64_t* seed_offsets, uint32_t width,
+                         double* ranks_out, uint32_t* iterations_out);
+
+/* ------------------------------------------------------------- spectral */
+
+/* spectral/operator.rs:33-44 (Operator) and lanczos.rs:69-74 (Which). */
+typedef enum wc_operator {
+    WC_ADJACENCY = 0, WC_LAPLACIAN = 1, WC_NORMALIZED_LAPLACIAN = 2, WC_RANDOM_WALK = 3
+} wc_operator;
+typedef enum wc_which { WC_LARGEST = 0, WC_SMALLEST = 1 } wc_which;
+
+/* spectral/lanczos.rs:136-168 (EigenOptions) with GraphMatrix
+ * (operator.rs:77-93); f64 precision only. */
+typedef struct wc_eigen_opts {
+    uint32_t k;
+    wc_which which;
+    wc_operator op;
+    int32_t symmetrize;
+    int32_t weighted;        /* -1 / 0 / 1 */
+    double tol;
+    uint64_t max_iter;       /* 0: 1,000 × the basis size */
+    uint64_t seed;
+} wc_eigen_opts;
+
+typedef struct wc_eigen_stats {
+    uint64_t iterations;
+    uint64_t components;
+    uint32_t exact;
+    int32_t converged;
+} wc_eigen_stats;
+
+/* spectral/lanczos.rs:206-224 (eigen): values[k], residuals[k] and the unit
+ * eigenvectors vectors[j * id_space + i] (may be NULL), in `which` order. */
+wc_status wc_eigen(wc_version* version, const wc_call* call, const wc_eigen_opts* opts,
+                   double* values, double* residuals, double* vectors, wc_eigen_stats* stats);
+
+/* ------------------------------------------------------------- adjoint
+ * (no reference counterpart) */
+
+/* ∂L_c/∂w for `losses` losses L_c = Σ_{t in targets of c} x_t, x the
+ * uniform PageRank of the weighted graph (recomputed, not stored):
+ * targets of loss c are loss_targets[loss_offsets[c] .. loss_offsets[c+1]).
+ * grad_out is loss-major over the forward CSR's edge order:
+ * grad_out[c * edges + e].  The forward runs opts->max_iter iterations or
+ * stops at opts->tol as wc_pagerank does; the adjoint solve runs to
+ * adjoint_tol (L1 of the adjoint change) or opts->max_iter. */
+wc_status wc_pagerank_adjoint(wc_version* version, const wc_call* call,
+                              const wc_pagerank_opts* opts, const uint64_t* loss_targets,
+                              const uint64_t* loss_offsets, uint32_t losses, double adjoint_tol,
+                              double* grad_out, double* ranks_out, uint32_t* iterations_out);
+
+/* ------------------------------------------------------------- ranking */
+
+/* compute/ranking.rs:52 (top_k): the k live rows with the largest
+ * (`descending`) or smallest values of width-1 `x`, best first, ties to the
+ * smaller dense id, SQL order (NaN above every number). */
+wc_status wc_topk(wc_version* version, const wc_call* call, wc_dtype dtype, const void* x,
+                  const uint64_t* tombstones, uint64_t k, int32_t descending,
+                  uint64_t* nodes_out, double* values_out, uint64_t* count);
+
+/* ------------------------------------------------- graph synthesis (host)
+ * Deterministic synthetic inputs for tests and benchmarks; not part of the
+ * seam.  Both return a CSR built as the reference builds one (rows sorted,
+ * parallel edges folded, self-loops dropped) with node ids relabelled by a
+ * random bijection of distinct int64 external ids ranked in sorted order
+ * (graph/id_map/mod.rs:38-49). */
+
+typedef struct wc_host_csr {
+    uint64_t id_space;
+    uint64_t edges;
+    uint64_t* offsets;   /* id_space + 1, owned by the library */
+    uint32_t* targets;   /* edges */
+    int64_t* external_ids; /* id_space: the external id of each dense id */
+} wc_host_csr;
+
+/* R-MAT (a, b, c, 1-a-b-c) at `scale` with edge_factor·2^scale generated
+ * edges, seed `seed`.  `undirected`: each edge stored both ways. */
+wc_status wc_graph_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double c,
+                        uint64_t seed, int32_t undirected, wc_host_csr* out);
+/* Erdős–Rényi G(n, m): `edges` edges drawn uniformly (then folded). */
+wc_status wc_graph_gnm(uint64_t id_space, uint64_t edges, uint64_t seed, int32_t undirected,
+                       wc_host_csr* out);
+void wc_host_csr_free(wc_host_csr* csr);
+/* The transpose of a host CSR (reverse CSR), rows ascending. */
+wc_status wc_host_transpose(uint64_t id_space, uint64_t edges, const uint64_t* offsets,
+                            const uint32_t* targets, const double* weights,
+                            uint64_t* reverse_offsets, uint32_t* reverse_targets,
+                            double* reverse_weights);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WARREN_CUDA_H */
