@@ -1,0 +1,777 @@
+"""The host-side mirror of warren-core's compute interface, over the C ABI.
+
+Names, argument meanings and errors follow the reference's functions
+(paths within the reference project):
+
+- ``spmv`` / ``spmm`` with ``Product``: compute/product/mod.rs:31-110;
+- ``pagerank`` with ``PageRank`` -> ``Ranks``: compute/pagerank/mod.rs:27-151;
+- ``bfs`` / ``reachable_set`` / ``reachable`` with ``Limits`` ->
+  ``Traversed``: traversal/bfs.rs:14-60, reachable.rs:18-90, limits.rs,
+  stats.rs;
+- ``eigen`` with ``EigenOptions`` -> ``Eigen``: spectral/lanczos.rs:136-224;
+- ``top_k``: compute/ranking.rs:52.
+
+Operands are numpy arrays (host) or torch CUDA tensors (device); the
+library tells them apart.  Errors raise the ``ComputeError`` /
+``TraversalError`` / ``SpectralError`` subclasses named as the reference's
+variants.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _abi as A
+
+# ----------------------------------------------------------------- errors
+
+
+class WarrenError(Exception):
+    """A non-OK wc_status, with the library's detail."""
+
+    def __init__(self, status: int, detail: Optional[A.ErrorDetail] = None):
+        self.status = status
+        self.detail = detail
+        msg = A.load().wc_status_name(status).decode()
+        if detail is not None and detail.message:
+            msg = f"{msg}: {detail.message.decode(errors='replace')}"
+        super().__init__(msg)
+
+
+class ComputeError(WarrenError):
+    pass
+
+
+class MemoryLimit(ComputeError):
+    pass
+
+
+class OutOfMemory(ComputeError):
+    pass
+
+
+class DtypeMismatch(ComputeError):
+    pass
+
+
+class IdSpaceMismatch(ComputeError):
+    pass
+
+
+class WidthMismatch(ComputeError):
+    pass
+
+
+class UnknownSemiring(ComputeError):
+    pass
+
+
+class UnknownBinaryOp(ComputeError):
+    pass
+
+
+class ZeroWidth(ComputeError):
+    pass
+
+
+class Cancelled(ComputeError):
+    pass
+
+
+class ArithmeticError_(ComputeError):
+    """ComputeError::Arithmetic (compute/error.rs:150-152)."""
+
+
+class BigintOutOfRange(ArithmeticError_):
+    pass
+
+
+class FloatOverflow(ArithmeticError_):
+    pass
+
+
+class FloatUnderflow(ArithmeticError_):
+    pass
+
+
+class DivisionByZero(ArithmeticError_):
+    pass
+
+
+class TraversalError(WarrenError):
+    pass
+
+
+class NodeOutsideIdSpace(TraversalError):
+    pass
+
+
+class NodeFilterIdSpace(TraversalError):
+    pass
+
+
+class ReverseCsrMissing(TraversalError):
+    pass
+
+
+class SpectralError(WarrenError):
+    pass
+
+
+class NotSymmetric(SpectralError):
+    pass
+
+
+class NonPositiveDegree(SpectralError):
+    pass
+
+
+class EigenpairCount(SpectralError):
+    pass
+
+
+class WorkingSet(SpectralError):
+    pass
+
+
+class NotFinite(SpectralError):
+    pass
+
+
+class BackendError(WarrenError):
+    pass
+
+
+class InvalidArgument(BackendError):
+    pass
+
+
+class Unsupported(BackendError):
+    pass
+
+
+class CudaError(BackendError):
+    pass
+
+
+class DeviceTimeout(BackendError):
+    pass
+
+
+class NoDevice(BackendError):
+    pass
+
+
+_ERRORS = {
+    1: MemoryLimit, 2: OutOfMemory, 3: DtypeMismatch, 4: IdSpaceMismatch, 5: WidthMismatch,
+    6: UnknownSemiring, 7: UnknownBinaryOp, 8: ZeroWidth, 9: Cancelled, 10: BigintOutOfRange,
+    11: FloatOverflow, 12: FloatUnderflow, 13: DivisionByZero, 20: NodeOutsideIdSpace,
+    21: NodeFilterIdSpace, 22: ReverseCsrMissing, 30: NotSymmetric, 31: NonPositiveDegree,
+    32: EigenpairCount, 33: WorkingSet, 34: NotFinite, 40: InvalidArgument, 41: Unsupported,
+    42: CudaError, 43: DeviceTimeout, 44: NoDevice,
+}
+
+
+def _raise(status: int, detail: A.ErrorDetail):
+    if status != 0:
+        raise _ERRORS.get(status, WarrenError)(status, detail)
+
+
+# ----------------------------------------------------------------- operands
+
+_DTYPES = {np.dtype(np.float64): A.F64, np.dtype(np.float32): A.F32, np.dtype(np.int64): A.I64,
+           np.dtype(np.uint8): A.BOOL, np.dtype(np.bool_): A.BOOL}
+_TORCH_DTYPES = {"torch.float64": A.F64, "torch.float32": A.F32, "torch.int64": A.I64,
+                 "torch.uint8": A.BOOL, "torch.bool": A.BOOL}
+
+
+def _ptr(a) -> Optional[int]:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("operands must be C-contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("operands must be contiguous")
+        return a.data_ptr()
+    raise TypeError(f"unsupported operand {type(a)}")
+
+
+def _dtype(a) -> int:
+    if isinstance(a, np.ndarray):
+        return _DTYPES[a.dtype]
+    return _TORCH_DTYPES[str(a.dtype)]
+
+
+def _len(a) -> int:
+    return a.shape[0] if len(a.shape) else 1
+
+
+# ----------------------------------------------------------------- runtime
+
+
+class Budget:
+    """compute/memory.rs (ComputeMemory): device bytes charged before use."""
+
+    def __init__(self, limit: int = 1 << 62):
+        h = A.P()
+        _raise(A.load().wc_budget_create(limit, C.byref(h)), A.ErrorDetail())
+        self.handle = h
+        self.limit = limit
+
+    @property
+    def in_use(self) -> int:
+        return A.load().wc_budget_in_use(self.handle)
+
+    @property
+    def peak(self) -> int:
+        return A.load().wc_budget_peak(self.handle)
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            A.load().wc_budget_destroy(h)
+            self.handle = None
+
+
+class Interrupts:
+    """A host cancel word and a progress hook (interrupts.rs, progress.rs)."""
+
+    def __init__(self, progress=None):
+        self.word = C.c_int32(0)
+        self.progress = progress
+        self.phases: list = []
+
+    def cancel(self):
+        self.word.value = 1
+
+
+def _call(interrupts: Optional[Interrupts] = None, stream=None, flags: int = 0,
+          memory: Optional[Budget] = None):
+    detail = A.ErrorDetail()
+    call = A.Call()
+    call.detail = C.pointer(detail)
+    if memory is not None:
+        call.memory = memory.handle
+    if interrupts is not None:
+        call.cancel = C.pointer(interrupts.word)
+        if interrupts.progress is not None:
+            cb = A.PROGRESS_FN(lambda ctx, phase, done, total: interrupts.progress(
+                phase.decode(), done, None if total == 2**64 - 1 else total))
+            call.progress = cb
+            call._keep = cb  # noqa: keep the callback alive for the call
+    if stream is not None:
+        call.stream = stream if isinstance(stream, int) else getattr(stream, "cuda_stream", None)
+    call.flags = flags
+    return call, detail
+
+
+class GraphVersion:
+    """A version's device copy: the CSR and reverse CSR of a built version
+    (graph/csr/mod.rs:38-237), keyed by (graph, version)."""
+
+    def __init__(self, offsets, targets, weights=None, reverse=True, budget: Budget = None,
+                 graph_id: int = 0, version: int = 0):
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        targets = np.ascontiguousarray(targets, dtype=np.uint32)
+        n = len(offsets) - 1
+        m = len(targets)
+        csr = A.CsrHost(n, m, offsets.ctypes.data, targets.ctypes.data, None, None, None, None)
+        self._keep = [offsets, targets]
+        if weights is not None:
+            weights = np.ascontiguousarray(weights, dtype=np.float64)
+            csr.weights = weights.ctypes.data
+            self._keep.append(weights)
+        if reverse is True:
+            roff = np.zeros(n + 1, np.uint64)
+            rtgt = np.zeros(max(m, 1), np.uint32)
+            rw = np.zeros(max(m, 1), np.float64) if weights is not None else None
+            _raise(A.load().wc_host_transpose(n, m, offsets.ctypes.data, targets.ctypes.data,
+                                              _ptr(weights), roff.ctypes.data, rtgt.ctypes.data,
+                                              _ptr(rw)), A.ErrorDetail())
+            csr.reverse_offsets, csr.reverse_targets = roff.ctypes.data, rtgt.ctypes.data
+            csr.reverse_weights = _ptr(rw)
+            self._keep += [roff, rtgt, rw]
+        elif reverse:
+            roff, rtgt, rw = reverse
+            roff = np.ascontiguousarray(roff, dtype=np.uint64)
+            rtgt = np.ascontiguousarray(rtgt, dtype=np.uint32)
+            rw = None if rw is None else np.ascontiguousarray(rw, dtype=np.float64)
+            csr.reverse_offsets, csr.reverse_targets = roff.ctypes.data, rtgt.ctypes.data
+            csr.reverse_weights = _ptr(rw)
+            self._keep += [roff, rtgt, rw]
+        self.budget = budget or Budget()
+        call, detail = _call()
+        h = A.P()
+        _raise(A.load().wc_version_upload(graph_id, version, C.byref(csr), self.budget.handle,
+                                          C.byref(call), C.byref(h)), detail)
+        self._keep = None
+        self.handle = h
+        self.id_space = n
+        self.edges = m
+        self.weighted = weights is not None
+
+    def info(self) -> A.VersionInfo:
+        info = A.VersionInfo()
+        _raise(A.load().wc_version_info_get(self.handle, C.byref(info)), A.ErrorDetail())
+        return info
+
+    def sync(self, interrupts=None):
+        call, detail = _call(interrupts)
+        _raise(A.load().wc_version_sync(self.handle, C.byref(call)), detail)
+
+    def release(self):
+        h = getattr(self, "handle", None)
+        if h:
+            A.load().wc_version_release(h)
+            self.handle = None
+
+    def __del__(self):
+        self.release()
+
+
+# ----------------------------------------------------------------- products
+
+
+@dataclass
+class Product:
+    """compute/product/mod.rs:31-56."""
+
+    semiring: str = "plus_times"
+    transpose: bool = False
+    weighted: Optional[bool] = None
+    mask: object = None
+    complement: bool = False
+    replace: bool = False
+    accumulate: Optional[str] = None
+
+
+def _product_c(p: Product):
+    name = {"or_and": "lor_land"}.get(p.semiring, p.semiring)
+    if name not in A.SEMIRINGS:
+        raise UnknownSemiring(6)
+    acc = A.OP_NONE
+    if p.accumulate is not None:
+        if p.accumulate not in A.BINARY_OPS:
+            raise UnknownBinaryOp(7)
+        acc = A.BINARY_OPS.index(p.accumulate)
+    pc = A.ProductC(A.SEMIRINGS.index(name), int(p.transpose),
+                    -1 if p.weighted is None else int(p.weighted), None, int(p.replace), acc)
+    mask = None
+    if p.mask is not None:
+        mask = A.Mask(_ptr(p.mask), _dtype(p.mask), int(p.complement))
+        pc.mask = C.pointer(mask)
+    return pc, mask
+
+
+def _check_operands(graph: GraphVersion, x, y, width: Optional[int]):
+    if _dtype(x) != _dtype(y):
+        raise DtypeMismatch(3)
+    for v in (x, y):
+        if _len(v) != graph.id_space:
+            raise IdSpaceMismatch(4)
+    wx = 1 if len(x.shape) == 1 else x.shape[1]
+    wy = 1 if len(y.shape) == 1 else y.shape[1]
+    if width == 1 and (wx != 1 or wy != 1):
+        raise WidthMismatch(5)
+    if wx != wy:
+        raise WidthMismatch(5)
+    return wx
+
+
+def spmv(graph: GraphVersion, product: Product, x, y, interrupts=None, stream=None,
+         asynchronous=False):
+    """y = A ⊗ x (or Aᵀ ⊗ x), y updated in place (product/mod.rs:77-92)."""
+    _check_operands(graph, x, y, 1)
+    pc, mask = _product_c(product)
+    call, detail = _call(interrupts, stream, 1 if asynchronous else 0)
+    _raise(A.load().wc_spmv(graph.handle, C.byref(call), C.byref(pc), _dtype(y), _ptr(x), _ptr(y)),
+           detail)
+
+
+def spmm(graph: GraphVersion, product: Product, x, y, interrupts=None, stream=None):
+    """Y = A ⊗ X over row-major id_space × width matrices (product/mod.rs:97-110)."""
+    width = _check_operands(graph, x, y, None)
+    pc, mask = _product_c(product)
+    call, detail = _call(interrupts, stream)
+    _raise(A.load().wc_spmm(graph.handle, C.byref(call), C.byref(pc), _dtype(y), width, _ptr(x),
+                            _ptr(y)), detail)
+
+
+# ----------------------------------------------------------------- pagerank
+
+
+@dataclass
+class PageRank:
+    """compute/pagerank/mod.rs:27-47 (all relations)."""
+
+    damping: float = 0.85
+    tol: Optional[float] = 1e-6
+    max_iter: int = 100
+    weighted: Optional[bool] = None
+    seed: object = None
+
+
+@dataclass
+class Ranks:
+    values: object
+    iterations: int
+
+
+def _pr_opts(p: PageRank):
+    seed = None
+    if p.seed is not None:
+        seed = p.seed if not isinstance(p.seed, np.ndarray) else np.ascontiguousarray(
+            p.seed, dtype=np.float64)
+        if isinstance(seed, np.ndarray) and seed.dtype == np.bool_:
+            raise DtypeMismatch(3)
+    o = A.PageRankOpts(p.damping, 0.0 if p.tol is None else p.tol, int(p.tol is not None),
+                       -1 if p.weighted is None else int(p.weighted), p.max_iter, _ptr(seed))
+    return o, seed
+
+
+def pagerank(graph: GraphVersion, tombstones=None, pagerank: PageRank = PageRank(), out=None,
+             interrupts=None, stream=None) -> Ranks:
+    """compute/pagerank/mod.rs:96-151; `tombstones` are NodeSet words."""
+    o, seed = _pr_opts(pagerank)
+    ranks = out if out is not None else np.zeros(graph.id_space, np.float64)
+    it = C.c_uint32(0)
+    call, detail = _call(interrupts, stream)
+    _raise(A.load().wc_pagerank(graph.handle, C.byref(call), C.byref(o), _ptr(tombstones),
+                                _ptr(ranks), C.byref(it)), detail)
+    return Ranks(ranks, it.value)
+
+
+def last_margin(graph: GraphVersion) -> float:
+    return A.load().wc_pagerank_last_margin(graph.handle)
+
+
+def node_set(id_space: int, ids) -> np.ndarray:
+    """NodeSet bitmap words (traversal/node_set.rs, graph/tombstones.rs)."""
+    words = np.zeros((id_space + 63) // 64, np.uint64)
+    ids = np.asarray(list(ids), dtype=np.uint64)
+    if len(ids):
+        np.bitwise_or.at(words, (ids // 64).astype(np.int64),
+                         np.left_shift(np.uint64(1), ids % np.uint64(64)))
+    return words
+
+
+# ----------------------------------------------------------------- traversal
+
+
+@dataclass
+class Limits:
+    """traversal/limits.rs:4-12."""
+
+    max_depth: Optional[int] = None
+    max_results: Optional[int] = None
+
+
+@dataclass
+class Visit:
+    node: int
+    depth: int
+    via: Optional[int]
+
+
+@dataclass
+class TraversalStats:
+    nodes_visited: int = 0
+    edges_traversed: int = 0
+    truncated: bool = False
+    levels: int = 0
+    pulled_levels: int = 0
+
+
+@dataclass
+class Traversed:
+    result: object
+    stats: TraversalStats
+
+
+_DIRECTIONS = {"out": A.OUT, "in": A.IN, "both": A.BOTH}
+
+
+def _stats(s: A.TraversalStats) -> TraversalStats:
+    return TraversalStats(s.nodes_visited, s.edges_traversed, bool(s.truncated), s.levels,
+                          s.pulled_levels)
+
+
+def _limits(limits: Limits) -> A.Limits:
+    return A.Limits(A.UNREACHED if limits.max_depth is None else limits.max_depth,
+                    2**64 - 1 if limits.max_results is None else limits.max_results)
+
+
+def bfs(graph: GraphVersion, starts: Sequence[int], filter=None, limits: Limits = Limits(),
+        direction: str = "out", interrupts=None) -> Traversed:
+    """traversal/bfs.rs:34-45: every node reached, once, in BFS order."""
+    st = np.ascontiguousarray(np.asarray(starts, dtype=np.uint64))
+    filt = None
+    if filter is not None:
+        filt = node_set(graph.id_space, filter) if not isinstance(filter, np.ndarray) else filter
+    rows = np.zeros(3 * (graph.id_space + 1), np.uint64)
+    count = C.c_uint64(0)
+    stats = A.TraversalStats()
+    lim = _limits(limits)
+    call, detail = _call(interrupts)
+    _raise(A.load().wc_bfs_visits(graph.handle, C.byref(call), _DIRECTIONS[direction], _ptr(st),
+                                  len(st), C.byref(lim), _ptr(filt), _ptr(rows),
+                                  graph.id_space + 1, C.byref(count), C.byref(stats)), detail)
+    r = rows[: 3 * count.value].reshape(-1, 3)
+    visits = [Visit(int(a), int(b), None if int(c) == A.NO_VIA else int(c)) for a, b, c in r]
+    return Traversed(visits, _stats(stats))
+
+
+def bfs_depths(graph: GraphVersion, starts, max_depth=None, direction="out", filter=None,
+               depth_out=None, via_out=None):
+    """The per-node form of bfs: (depth u32[n], via u64[n], stats)."""
+    st = np.ascontiguousarray(np.asarray(starts, dtype=np.uint64))
+    d = depth_out if depth_out is not None else np.zeros(graph.id_space, np.uint32)
+    v = via_out if via_out is not None else np.zeros(graph.id_space, np.uint64)
+    stats = A.TraversalStats()
+    lim = _limits(Limits(max_depth, None))
+    call, detail = _call()
+    _raise(A.load().wc_bfs(graph.handle, C.byref(call), _DIRECTIONS[direction], _ptr(st), len(st),
+                           C.byref(lim), _ptr(filter), _ptr(d), _ptr(v), C.byref(stats)), detail)
+    return d, v, _stats(stats)
+
+
+def reachable_set(graph: GraphVersion, starts, max_depth=None, direction="out",
+                  interrupts=None) -> Traversed:
+    """traversal/reachable.rs:48-58."""
+    st = np.ascontiguousarray(np.asarray(starts, dtype=np.uint64))
+    nodes = np.zeros(graph.id_space + 1, np.uint64)
+    count = C.c_uint64(0)
+    stats = A.TraversalStats()
+    call, detail = _call(interrupts)
+    _raise(A.load().wc_reachable_set(graph.handle, C.byref(call), _DIRECTIONS[direction], _ptr(st),
+                                     len(st), A.UNREACHED if max_depth is None else max_depth,
+                                     _ptr(nodes), len(nodes), C.byref(count), C.byref(stats)),
+           detail)
+    return Traversed([int(v) for v in nodes[: count.value]], _stats(stats))
+
+
+def reachable(graph: GraphVersion, start: int, target: int, max_depth=None,
+              direction="out") -> Traversed:
+    """traversal/reachable.rs:18-43."""
+    r = C.c_int32(0)
+    stats = A.TraversalStats()
+    call, detail = _call()
+    _raise(A.load().wc_reachable(graph.handle, C.byref(call), _DIRECTIONS[direction], start,
+                                 target, A.UNREACHED if max_depth is None else max_depth,
+                                 C.byref(r), C.byref(stats)), detail)
+    return Traversed(bool(r.value), _stats(stats))
+
+
+# ----------------------------------------------------------------- batched
+
+
+def bfs_batched(graph: GraphVersion, sources, max_depths, depth_out=None, edges_out=None):
+    """`len(sources)` BFS searches as one bit-packed boolean SpMM: depths
+    u8[k, n] (255: not reached within the source's cap)."""
+    src = np.ascontiguousarray(np.asarray(sources, dtype=np.uint64))
+    caps = np.ascontiguousarray(np.asarray(max_depths, dtype=np.uint32))
+    k = len(src)
+    d = depth_out if depth_out is not None else np.zeros((k, graph.id_space), np.uint8)
+    e = edges_out if edges_out is not None else np.zeros(k, np.uint64)
+    call, detail = _call()
+    _raise(A.load().wc_bfs_batched(graph.handle, C.byref(call), _ptr(src), _ptr(caps), k, _ptr(d),
+                                   _ptr(e)), detail)
+    return d, e
+
+
+def minplus_batched(graph: GraphVersion, sources, max_hops, dist_out=None, iterations_out=None):
+    """`len(sources)` hop-bounded min-plus searches (the sssp_vector loop)."""
+    src = np.ascontiguousarray(np.asarray(sources, dtype=np.uint64))
+    hops = np.ascontiguousarray(np.asarray(max_hops, dtype=np.uint32))
+    k = len(src)
+    d = dist_out if dist_out is not None else np.zeros((k, graph.id_space), np.int64)
+    it = iterations_out if iterations_out is not None else np.zeros(k, np.uint32)
+    call, detail = _call()
+    _raise(A.load().wc_minplus_batched(graph.handle, C.byref(call), _ptr(src), _ptr(hops), k,
+                                       _ptr(d), _ptr(it)), detail)
+    return d, it
+
+
+def ppr_batched(graph: GraphVersion, seed_sets, pagerank: PageRank = PageRank(), ranks_out=None,
+                iterations_out=None):
+    """Personalised PageRank per seed set, each column stopping on its own."""
+    offs = np.zeros(len(seed_sets) + 1, np.uint64)
+    for i, s in enumerate(seed_sets):
+        offs[i + 1] = offs[i] + len(s)
+    nodes = np.ascontiguousarray(np.concatenate([np.asarray(s, np.uint64) for s in seed_sets])
+                                 if len(seed_sets) else np.zeros(0, np.uint64))
+    k = len(seed_sets)
+    o, _ = _pr_opts(PageRank(pagerank.damping, pagerank.tol, pagerank.max_iter, pagerank.weighted))
+    r = ranks_out if ranks_out is not None else np.zeros((k, graph.id_space), np.float64)
+    it = iterations_out if iterations_out is not None else np.zeros(k, np.uint32)
+    call, detail = _call()
+    _raise(A.load().wc_ppr_batched(graph.handle, C.byref(call), C.byref(o), _ptr(nodes), _ptr(offs),
+                                   k, _ptr(r), _ptr(it)), detail)
+    return r, it
+
+
+def autotune(graph: GraphVersion, kind: str, width: int) -> A.Schedule:
+    s = A.Schedule()
+    call, detail = _call()
+    _raise(A.load().wc_autotune(graph.handle, C.byref(call), {"bfs": 0, "minplus": 1, "ppr": 2}[kind],
+                                width, C.byref(s)), detail)
+    return s
+
+
+# ----------------------------------------------------------------- spectral
+
+
+@dataclass
+class EigenOptions:
+    """spectral/lanczos.rs:136-168 with GraphMatrix (operator.rs:77-93)."""
+
+    k: int
+    which: str = "largest"
+    operator: str = "adjacency"
+    symmetrize: bool = True
+    weighted: Optional[bool] = None
+    tol: float = 1e-6
+    max_iter: Optional[int] = None
+    seed: int = 0
+
+
+@dataclass
+class Eigen:
+    values: np.ndarray
+    residuals: np.ndarray
+    vectors: Optional[np.ndarray]
+    iterations: int
+    converged: bool
+    components: int
+    exact: int
+
+
+_OPERATORS = ["adjacency", "laplacian", "normalized_laplacian", "random_walk"]
+
+
+def eigen(graph: GraphVersion, options: EigenOptions, vectors=True) -> Eigen:
+    """spectral/lanczos.rs:206-224 (f64 precision)."""
+    o = A.EigenOpts(options.k, {"largest": 0, "smallest": 1}[options.which],
+                    _OPERATORS.index(options.operator), int(options.symmetrize),
+                    -1 if options.weighted is None else int(options.weighted), options.tol,
+                    options.max_iter or 0, options.seed)
+    k = options.k
+    vals = np.zeros(k, np.float64)
+    res = np.zeros(k, np.float64)
+    vecs = np.zeros((k, graph.id_space), np.float64) if vectors else None
+    st = A.EigenStats()
+    call, detail = _call()
+    _raise(A.load().wc_eigen(graph.handle, C.byref(call), C.byref(o), _ptr(vals), _ptr(res),
+                             _ptr(vecs), C.byref(st)), detail)
+    return Eigen(vals, res, vecs, st.iterations, bool(st.converged), st.components, st.exact)
+
+
+# ----------------------------------------------------------------- adjoint
+
+
+def pagerank_adjoint(graph: GraphVersion, loss_targets: Sequence[Sequence[int]],
+                     pagerank: PageRank = PageRank(), adjoint_tol: float = 1e-14, grad_out=None):
+    """∂L_c/∂w for L_c = Σ_{t in loss_targets[c]} x_t over every edge of the
+    forward CSR: (grad[losses, edges], ranks, iterations)."""
+    offs = np.zeros(len(loss_targets) + 1, np.uint64)
+    for i, s in enumerate(loss_targets):
+        offs[i + 1] = offs[i] + len(s)
+    nodes = np.ascontiguousarray(np.concatenate([np.asarray(s, np.uint64) for s in loss_targets]))
+    k = len(loss_targets)
+    o, _ = _pr_opts(pagerank)
+    g = grad_out if grad_out is not None else np.zeros((k, graph.edges), np.float64)
+    ranks = np.zeros(graph.id_space, np.float64)
+    it = np.zeros(2, np.uint32)
+    call, detail = _call()
+    _raise(A.load().wc_pagerank_adjoint(graph.handle, C.byref(call), C.byref(o), _ptr(nodes),
+                                        _ptr(offs), k, adjoint_tol, _ptr(g), _ptr(ranks),
+                                        _ptr(it)), detail)
+    return g, ranks, it
+
+
+# ----------------------------------------------------------------- ranking
+
+
+def top_k(graph: GraphVersion, x, k: int, descending: bool = True, tombstones=None):
+    """compute/ranking.rs:52: [(dense id, value)] best first."""
+    nodes = np.zeros(max(k, 1), np.uint64)
+    vals = np.zeros(max(k, 1), np.float64)
+    count = C.c_uint64(0)
+    call, detail = _call()
+    _raise(A.load().wc_topk(graph.handle, C.byref(call), _dtype(x), _ptr(x), _ptr(tombstones), k,
+                            int(descending), _ptr(nodes), _ptr(vals), C.byref(count)), detail)
+    c = count.value
+    return [(int(a), float(b)) for a, b in zip(nodes[:c], vals[:c])]
+
+
+# ----------------------------------------------------------------- synthesis
+
+
+@dataclass
+class HostGraph:
+    """A synthetic built version: CSR arrays and external ids by dense id."""
+
+    offsets: np.ndarray
+    targets: np.ndarray
+    external_ids: np.ndarray
+    weights: Optional[np.ndarray] = None
+
+    @property
+    def id_space(self) -> int:
+        return len(self.offsets) - 1
+
+    @property
+    def edges(self) -> int:
+        return len(self.targets)
+
+    def upload(self, reverse=True, budget=None) -> GraphVersion:
+        return GraphVersion(self.offsets, self.targets, self.weights, reverse, budget)
+
+
+def _take(csr: A.HostCsr) -> HostGraph:
+    n, m = csr.id_space, csr.edges
+    off = np.ctypeslib.as_array(csr.offsets, shape=(n + 1,)).copy()
+    tgt = np.ctypeslib.as_array(csr.targets, shape=(max(m, 1),))[:m].copy()
+    ext = np.ctypeslib.as_array(csr.external_ids, shape=(max(n, 1),))[:n].copy()
+    A.load().wc_host_csr_free(C.byref(csr))
+    return HostGraph(off, tgt, ext)
+
+
+def rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+         seed: int = 1, undirected: bool = False) -> HostGraph:
+    csr = A.HostCsr()
+    _raise(A.load().wc_graph_rmat(scale, edge_factor, a, b, c, seed, int(undirected), C.byref(csr)),
+           A.ErrorDetail())
+    return _take(csr)
+
+
+def gnm(n: int, m: int, seed: int = 1, undirected: bool = False) -> HostGraph:
+    csr = A.HostCsr()
+    _raise(A.load().wc_graph_gnm(n, m, seed, int(undirected), C.byref(csr)), A.ErrorDetail())
+    return _take(csr)
+
+
+def edge_weights(g: HostGraph, kind: str, seed: int = 7) -> np.ndarray:
+    """Seeded per-edge weights as the benchmark configs define them:
+    'uniform' U(0, 1]; 'int' integers U{1..100}; 'lognormal' exp(N(0, 1))
+    row-normalised so each row sums to 1."""
+    rng = np.random.default_rng(seed)
+    m = g.edges
+    if kind == "uniform":
+        return 1.0 - rng.random(m)
+    if kind == "int":
+        return rng.integers(1, 101, m).astype(np.float64)
+    if kind == "lognormal":
+        w = np.exp(rng.standard_normal(m))
+        deg = np.diff(g.offsets).astype(np.int64)
+        rows = np.repeat(np.arange(g.id_space), deg)
+        sums = np.bincount(rows, weights=w, minlength=g.id_space)
+        return w / sums[rows]
+    raise ValueError(kind)

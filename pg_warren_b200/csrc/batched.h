@@ -1,0 +1,18 @@
+// batched.h — buffers and entry points shared by the batched searches.
+#pragma once
+
+#include "runtime.cuh"
+
+namespace wc {
+
+struct BatchBuffers {
+  DevBuf *V = nullptr, *F = nullptr, *bits = nullptr, *masks = nullptr, *counts = nullptr;
+  wc_status reserve(Ctx& ctx, uint32_t words, uint32_t levels);
+};
+
+wc_schedule default_bfs_schedule(uint32_t width);
+wc_status bfs_batched_run(Ctx& ctx, const wc_schedule& sched, const uint64_t* sources_dev,
+                          const uint32_t* caps_dev, const uint32_t* caps_host, uint32_t width,
+                          uint8_t* depth_dev, unsigned long long* edges_dev);
+
+}  // namespace wc

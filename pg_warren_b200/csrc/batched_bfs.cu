@@ -1,0 +1,404 @@
+// batched_bfs.cu — wc_bfs_batched and wc_autotune: many BFS searches as one
+// boolean SpMM over bit-packed frontiers (no reference counterpart; its CPU
+// prior art is compute/centrality/multi_source.rs, 64 sources per word).
+//
+// A pass takes up to 1,024 sources, one bit each in a row of W 32-bit words
+// per node (W = columns / 32).  Level L pulls over the reverse CSR: node i
+// ORs the frontier rows F_L[j] of its in-neighbours j (only those whose row
+// is non-zero for a source still expanding, read from a frontier bitmap),
+// keeps the bits it has not seen, and writes them as its row of F_{L+1}.  A
+// source with depth cap c expands levels 0 .. c-1, as the reference's
+// LevelSearch stops at max_depth (traversal/level.rs:119-123), so its bits
+// are masked out of the frontier from level c on.  Every F_L is kept (the
+// kernel writes each row, new bits or zero), and a last kernel turns them
+// into per-source depths, source-major, while summing the out-degree of each
+// node a source expands: the row entries a push-only bfs from that source
+// scans (its edges_traversed).
+//
+// Every level's launches are queued without a host round trip: a level whose
+// frontier is empty returns at once, reading the count the previous level
+// wrote.  The pass is therefore a fixed launch sequence, captured once per
+// (version, pass shape) into a CUDA graph and replayed.
+#include <algorithm>
+
+#include "batched.h"
+#include "operand.h"
+#include "semiring.cuh"
+
+namespace wc {
+
+__device__ inline bool nbit(const uint32_t* b, uint32_t i) { return (b[i >> 5] >> (i & 31)) & 1; }
+
+// Seeds: F_0 and V get bit s at node sources[s]; the level masks A_L (bits
+// of sources with cap > L) are built for every level.
+template <int W>
+__global__ void msbfs_seed_kernel(const uint64_t* sources, const uint32_t* caps, uint32_t k,
+                                  uint32_t levels, uint32_t n, uint32_t* V, uint32_t* F0,
+                                  uint32_t* fbits0, uint32_t* masks, uint32_t* counts) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < k) {
+    const uint32_t node = (uint32_t)sources[t];
+    atomicOr(V + (size_t)node * W + (t >> 5), 1u << (t & 31));
+    atomicOr(F0 + (size_t)node * W + (t >> 5), 1u << (t & 31));
+    if (caps[t] > 0) atomicOr(fbits0 + (node >> 5), 1u << (node & 31));
+  }
+  // masks[L * W + w]: bit b set if source 32w+b exists and cap > L.
+  for (uint32_t x = t; x < levels * W; x += gridDim.x * blockDim.x) {
+    const uint32_t L = x / W, w = x % W;
+    uint32_t m = 0;
+    for (uint32_t b = 0; b < 32; b++) {
+      const uint32_t s = 32 * w + b;
+      if (s < k && caps[s] > L) m |= 1u << b;
+    }
+    masks[x] = m;
+  }
+  if (t == 0) counts[0] = 1;  // level 0's frontier is non-empty (or harmlessly so)
+}
+
+// Level L: F_{L+1}[i] = (OR over in-neighbours j in the frontier of
+// F_L[j] & A_L) & ~V[i]; V[i] |= F_{L+1}[i].  A group of W lanes per node.
+template <int W>
+__global__ void __launch_bounds__(256)
+    msbfs_level_kernel(uint32_t n, const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,
+                       uint32_t* V, const uint32_t* __restrict__ Fcur, uint32_t* Fnext,
+                       const uint32_t* __restrict__ fbits, uint32_t* fbits_next,
+                       const uint32_t* masks, uint32_t L, uint32_t* counts,
+                       const int32_t* cancel) {
+  if (counts[L] == 0) return;  // nothing expands: F_{L+1} is not read
+  constexpr uint32_t G = 32 / W;  // nodes per warp
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned sub = lane / W, w = lane % W;
+  const unsigned gmask = (W == 32) ? 0xffffffffu : (((1u << W) - 1) << (sub * W));
+  const uint32_t a = masks[L * W + w];
+  const uint32_t a_next = masks[(L + 1) * W + w];
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  uint32_t admitted = 0;
+  const uint32_t groups = (n + G - 1) / G;
+  for (uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < groups; g += warps) {
+    const uint32_t i = g * G + sub;
+    const bool valid = i < n;
+    uint32_t v = valid ? V[(size_t)i * W + w] : 0xffffffffu;
+    const uint32_t target = ~v & a;
+    uint32_t acc = 0;
+    const bool work = __ballot_sync(gmask, target != 0) != 0;
+    if (valid && work) {
+      const uint32_t lo = __ldg(off + i), hi = __ldg(off + i + 1);
+      if (W == 32) {
+        // The warp loads 32 targets at once, then ORs the frontier rows.
+        for (uint32_t base = lo; base < hi; base += 32) {
+          const uint32_t e = base + lane;
+          uint32_t j = 0;
+          bool f = false;
+          if (e < hi) {
+            j = __ldcs(tgt + e);
+            f = nbit(fbits, j);
+          }
+          uint32_t hits = __ballot_sync(0xffffffffu, f);
+          while (hits) {
+            const int k = __ffs(hits) - 1;
+            hits &= hits - 1;
+            const uint32_t jj = __shfl_sync(0xffffffffu, j, k);
+            acc |= __ldg(Fcur + (size_t)jj * W + w) & a;
+          }
+          if (__all_sync(0xffffffffu, (acc & target) == target)) break;
+        }
+      } else {
+        for (uint32_t e = lo; e < hi; e++) {
+          const uint32_t j = __ldg(tgt + e);
+          if (nbit(fbits, j)) acc |= __ldg(Fcur + (size_t)j * W + w) & a;
+          if (__all_sync(gmask, (acc & target) == target)) break;
+        }
+      }
+    }
+    const uint32_t fresh = acc & target;
+    if (valid) {
+      if (fresh) V[(size_t)i * W + w] = v | fresh;
+      Fnext[(size_t)i * W + w] = fresh;
+    }
+    const bool expands = __ballot_sync(gmask, (fresh & a_next) != 0) != 0;
+    if (valid && expands && w == 0) {
+      atomicOr(fbits_next + (i >> 5), 1u << (i & 31));
+      admitted++;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) admitted += __shfl_down_sync(0xffffffffu, admitted, o);
+  if (lane == 0 && admitted) atomicAdd(counts + L + 1, admitted);
+  (void)cancel;
+}
+
+// Depths from the kept frontiers, source-major, and each source's
+// edges_traversed: Σ out-degree over the nodes it reached at a depth below
+// its cap.  A block takes 64 nodes at a time; the depths of all sources of
+// the pass for them are assembled in shared memory ([source][node]) and
+// written out 16 bytes at a time.
+template <int W>
+__global__ void __launch_bounds__(256)
+    msbfs_depth_kernel(uint32_t n, uint32_t k, uint32_t levels, const uint32_t* F, uint64_t fstride,
+                       const uint32_t* caps, const uint32_t* off, const uint32_t* counts,
+                       uint8_t* depth_out, unsigned long long* edges) {
+  constexpr uint32_t P = 32 * W;
+  constexpr uint32_t T = 64;
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint8_t* tile = smem;                                               // [P][T]
+  uint32_t* esum = reinterpret_cast<uint32_t*>(smem + P * T);          // [P]
+  uint32_t* scap = esum + P;                                           // [P]
+  for (uint32_t s = threadIdx.x; s < P; s += blockDim.x) {
+    esum[s] = 0;
+    scap[s] = s < k ? caps[s] : 0;
+  }
+  const uint32_t tiles = (n + T - 1) / T;
+  for (uint32_t tt = blockIdx.x; tt < tiles; tt += gridDim.x) {
+    const uint32_t i0 = tt * T;
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < P * T / 16; x += blockDim.x)
+      reinterpret_cast<uint4*>(tile)[x] = make_uint4(~0u, ~0u, ~0u, ~0u);
+    __syncthreads();
+    for (uint32_t L = 0; L < levels; L++) {
+      // F_L was written only if level L-1 had a frontier to expand.
+      if (L > 0 && counts[L - 1] == 0) break;
+      const uint32_t* FL = F + L * fstride;
+      for (uint32_t x = threadIdx.x; x < T * W; x += blockDim.x) {
+        const uint32_t node = x / W, w = x % W;
+        const uint32_t i = i0 + node;
+        if (i >= n) continue;
+        uint32_t bits = FL[(size_t)i * W + w];
+        if (!bits) continue;
+        const uint32_t deg = __ldg(off + i + 1) - __ldg(off + i);
+        while (bits) {
+          const uint32_t b = __ffs(bits) - 1;
+          bits &= bits - 1;
+          const uint32_t s = 32 * w + b;
+          tile[s * T + node] = (uint8_t)L;
+          if (L < scap[s] && deg) atomicAdd(esum + s, deg);
+        }
+      }
+    }
+    __syncthreads();
+    // Write the tile: source s's depths for nodes i0 .. i0+63, 16 bytes a
+    // thread.
+    for (uint32_t x = threadIdx.x; x < k * (T / 16); x += blockDim.x) {
+      const uint32_t s = x / (T / 16), q = x % (T / 16);
+      const uint32_t i = i0 + q * 16;
+      uint8_t* dst = depth_out + (size_t)s * n + i;
+      const uint4 val = reinterpret_cast<const uint4*>(tile + s * T)[q];
+      if (i + 16 <= n && (((uintptr_t)dst) & 15) == 0) {
+        *reinterpret_cast<uint4*>(dst) = val;
+      } else {
+        const uint8_t* src = reinterpret_cast<const uint8_t*>(&val);
+        for (uint32_t b = 0; b < 16 && i + b < n; b++) dst[b] = src[b];
+      }
+    }
+  }
+  __syncthreads();
+  for (uint32_t s = threadIdx.x; s < k; s += blockDim.x)
+    if (esum[s]) atomicAdd(edges + s, (unsigned long long)esum[s]);
+}
+
+// One pass of up to 32·W sources.
+template <int W>
+wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const uint32_t* caps_dev,
+                   uint32_t k, uint32_t levels, uint8_t* depth_dev, unsigned long long* edges_dev,
+                   uint32_t blocks_per_sm) {
+  wc_version* v = ctx.v;
+  const uint32_t n = (uint32_t)v->n;
+  const uint64_t row_words = (uint64_t)n * W;
+  const uint64_t fstride = row_words;
+  cudaStream_t st = ctx.stream;
+  // Zero V, F_0, the bitmaps and the counts (rows of later levels are
+  // written whole by the level kernel).
+  WC_CUDA(cudaMemsetAsync(b.V->ptr, 0, row_words * 4, st), ctx.detail);
+  WC_CUDA(cudaMemsetAsync(b.F->ptr, 0, row_words * 4, st), ctx.detail);
+  const uint64_t bitmap_words = (n + 31) / 32;
+  WC_CUDA(cudaMemsetAsync(b.bits->ptr, 0, (uint64_t)(levels + 1) * bitmap_words * 4, st), ctx.detail);
+  WC_CUDA(cudaMemsetAsync(b.counts->ptr, 0, (levels + 2) * 4, st), ctx.detail);
+  uint32_t* V = b.V->as<uint32_t>();
+  uint32_t* F = b.F->as<uint32_t>();
+  uint32_t* bits = b.bits->as<uint32_t>();
+  uint32_t* masks = b.masks->as<uint32_t>();
+  uint32_t* counts = b.counts->as<uint32_t>();
+  msbfs_seed_kernel<W><<<std::max<uint32_t>(1, (std::max(k, (levels + 1) * W) + 255) / 256), 256, 0,
+                         st>>>(sources_dev, caps_dev, k, levels + 1, n, V, F, bits, masks, counts);
+  const uint32_t grid = max_blocks((int)blocks_per_sm);
+  const DevCsr& csc = v->rev;
+  for (uint32_t L = 0; L < levels; L++) {
+    msbfs_level_kernel<W><<<grid, 256, 0, st>>>(
+        n, csc.offsets.as<uint32_t>(), csc.targets.as<uint32_t>(), V, F + L * fstride,
+        F + (L + 1) * fstride, bits + L * bitmap_words, bits + (L + 1) * bitmap_words, masks, L,
+        counts, v->cancel_dev);
+  }
+  const size_t smem = 32 * W * 64 + 2 * 32 * W * 4;
+  if (smem > 48 * 1024)
+    WC_CUDA(cudaFuncSetAttribute(msbfs_depth_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem), ctx.detail);
+  msbfs_depth_kernel<W><<<max_blocks(2), 256, smem, st>>>(
+      n, k, levels + 1, F, fstride, caps_dev, v->fwd.offsets.as<uint32_t>(), counts, depth_dev,
+      edges_dev);
+  return cuda_status(cudaGetLastError(), ctx.detail, "batched bfs pass");
+}
+
+wc_status BatchBuffers::reserve(Ctx& ctx, uint32_t words, uint32_t levels) {
+  const uint64_t n = ctx.v->n;
+  WC_TRY(ctx.scratch(POOL_BATCH_0, n * words * 4, &V));
+  WC_TRY(ctx.scratch(POOL_BATCH_1, n * words * 4 * (uint64_t)(levels + 1), &F));
+  WC_TRY(ctx.scratch(POOL_BATCH_2, ((n + 31) / 32) * 4 * (uint64_t)(levels + 2), &bits));
+  WC_TRY(ctx.scratch(POOL_BATCH_3, (uint64_t)(levels + 2) * words * 4, &masks));
+  WC_TRY(ctx.scratch(POOL_BATCH_4, (uint64_t)(levels + 2) * 4, &counts));
+  return WC_OK;
+}
+
+typedef wc_status (*PassFn)(Ctx&, BatchBuffers&, const uint64_t*, const uint32_t*, uint32_t,
+                            uint32_t, uint8_t*, unsigned long long*, uint32_t);
+
+static PassFn pass_for(uint32_t columns) {
+  switch (columns) {
+    case 32: return run_pass<1>;
+    case 64: return run_pass<2>;
+    case 128: return run_pass<4>;
+    case 256: return run_pass<8>;
+    case 512: return run_pass<16>;
+    default: return run_pass<32>;
+  }
+}
+
+static uint32_t round_columns(uint32_t k) {
+  uint32_t c = 32;
+  while (c < k && c < 1024) c <<= 1;
+  return c;
+}
+
+wc_schedule default_bfs_schedule(uint32_t width) {
+  return wc_schedule{round_columns(width), 1, 4, 0};
+}
+
+// The whole batch on the call's stream: passes of `columns` sources.
+wc_status bfs_batched_run(Ctx& ctx, const wc_schedule& sched, const uint64_t* sources_dev,
+                          const uint32_t* caps_dev, const uint32_t* caps_host, uint32_t width,
+                          uint8_t* depth_dev, unsigned long long* edges_dev) {
+  const uint32_t columns = std::max<uint32_t>(32, std::min<uint32_t>(1024, sched.columns_per_pass));
+  BatchBuffers b;
+  uint32_t max_levels = 0;
+  for (uint32_t s = 0; s < width; s++) max_levels = std::max(max_levels, caps_host[s]);
+  max_levels = std::min<uint32_t>(max_levels, 254);
+  WC_TRY(b.reserve(ctx, columns / 32, max_levels));
+  WC_CUDA(cudaMemsetAsync(edges_dev, 0, width * 8, ctx.stream), ctx.detail);
+  for (uint32_t s0 = 0; s0 < width; s0 += columns) {
+    const uint32_t k = std::min(columns, width - s0);
+    uint32_t levels = 0;
+    for (uint32_t s = s0; s < s0 + k; s++) levels = std::max(levels, caps_host[s]);
+    levels = std::min<uint32_t>(levels, 254);
+    WC_TRY(pass_for(columns)(ctx, b, sources_dev + s0, caps_dev + s0, k, levels,
+                             depth_dev + (uint64_t)s0 * ctx.v->n, edges_dev + s0,
+                             sched.blocks_per_sm ? sched.blocks_per_sm : 4));
+  }
+  return WC_OK;
+}
+
+// Times `candidates` on a seeded sample batch of `width` sources (caps 16,
+// the deepest the benchmark asks) and returns the fastest.
+wc_status tune_bfs(Ctx& ctx, uint32_t width, wc_schedule* best) {
+  wc_version* v = ctx.v;
+  const uint32_t n = (uint32_t)v->n;
+  std::vector<uint64_t> src(width);
+  std::vector<uint32_t> caps(width, 16);
+  uint64_t z = 0x7e57u;
+  for (uint32_t s = 0; s < width; s++) {
+    z = z * 6364136223846793005ull + 1442695040888963407ull;
+    src[s] = (z >> 17) % n;
+  }
+  DevBuf *S, *C, *D, *E;
+  WC_TRY(ctx.scratch(POOL_BATCH_5, width * 8, &S));
+  WC_TRY(ctx.scratch(POOL_BATCH_6, width * 4, &C));
+  WC_TRY(ctx.scratch(POOL_BATCH_7, (uint64_t)width * n, &D));
+  WC_TRY(ctx.scratch(POOL_BATCH_9, width * 8, &E));
+  WC_CUDA(cudaMemcpyAsync(S->ptr, src.data(), width * 8, cudaMemcpyHostToDevice, ctx.stream), ctx.detail);
+  WC_CUDA(cudaMemcpyAsync(C->ptr, caps.data(), width * 4, cudaMemcpyHostToDevice, ctx.stream), ctx.detail);
+  std::vector<wc_schedule> candidates;
+  const uint32_t top = round_columns(width);
+  for (uint32_t cols = top; cols >= 32 && cols * 4 >= top; cols >>= 1)
+    for (uint32_t bps : {2u, 4u, 8u}) candidates.push_back(wc_schedule{cols, 1, bps, 0});
+  cudaEvent_t a, b;
+  WC_CUDA(cudaEventCreate(&a), ctx.detail);
+  WC_CUDA(cudaEventCreate(&b), ctx.detail);
+  float best_ms = 1e30f;
+  for (const wc_schedule& c : candidates) {
+    float ms = 0;
+    for (int rep = 0; rep < 2; rep++) {  // the first run warms up
+      WC_CUDA(cudaEventRecord(a, ctx.stream), ctx.detail);
+      WC_TRY(bfs_batched_run(ctx, c, S->as<uint64_t>(), C->as<uint32_t>(), caps.data(), width,
+                             D->as<uint8_t>(), E->as<unsigned long long>()));
+      WC_CUDA(cudaEventRecord(b, ctx.stream), ctx.detail);
+      WC_CUDA(cudaEventSynchronize(b), ctx.detail);
+      WC_CUDA(cudaEventElapsedTime(&ms, a, b), ctx.detail);
+    }
+    if (ms < best_ms) {
+      best_ms = ms;
+      *best = c;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return WC_OK;
+}
+
+}  // namespace wc
+
+using namespace wc;
+
+extern "C" {
+
+wc_status wc_autotune(wc_version* v, const wc_call* call, wc_batch_kind kind, uint32_t width,
+                      wc_schedule* chosen) {
+  if (!v || width == 0) return WC_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lock(v->mu);
+  WC_CUDA(cudaSetDevice(v->device), call ? call->detail : nullptr);
+  Ctx ctx(v, call);
+  WC_TRY(ctx.begin());
+  wc_schedule best{};
+  switch (kind) {
+    case WC_BATCH_BFS: WC_TRY(tune_bfs(ctx, width, &best)); break;
+    default: return WC_UNSUPPORTED;
+  }
+  WC_TRY(ctx.finish());
+  v->tuned[((uint64_t)kind << 32) | width] = best;
+  if (chosen) *chosen = best;
+  return WC_OK;
+}
+
+wc_status wc_bfs_batched(wc_version* v, const wc_call* call, const uint64_t* sources,
+                         const uint32_t* max_depths, uint32_t width, uint8_t* depth_out,
+                         uint64_t* edges_traversed_out) {
+  if (!v || (width && (!sources || !max_depths || !depth_out))) return WC_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lock(v->mu);
+  WC_CUDA(cudaSetDevice(v->device), call ? call->detail : nullptr);
+  Ctx ctx(v, call);
+  if (ctx.cancelled()) return WC_CANCELLED;
+  if (width == 0) return WC_OK;
+  std::vector<uint64_t> src(width);
+  std::vector<uint32_t> caps(width);
+  WC_CUDA(cudaMemcpy(src.data(), sources, width * 8, cudaMemcpyDefault), ctx.detail);
+  WC_CUDA(cudaMemcpy(caps.data(), max_depths, width * 4, cudaMemcpyDefault), ctx.detail);
+  for (uint64_t s : src)
+    if (s >= v->n) {
+      if (ctx.detail) ctx.detail->node = s;
+      return WC_NODE_OUTSIDE_ID_SPACE;
+    }
+  WC_TRY(ctx.begin());
+  Operand S(POOL_BATCH_5), C(POOL_BATCH_6), D(POOL_BATCH_7), E(POOL_BATCH_8);
+  WC_TRY(S.in(ctx, sources, width * 8));
+  WC_TRY(C.in(ctx, max_depths, width * 4));
+  WC_TRY(D.output(ctx, depth_out, (uint64_t)width * v->n));
+  DevBuf* edges;
+  WC_TRY(ctx.scratch(POOL_BATCH_9, (uint64_t)width * 8, &edges));
+  auto key = ((uint64_t)WC_BATCH_BFS << 32) | width;
+  wc_schedule sched = v->tuned.count(key) ? v->tuned[key] : default_bfs_schedule(width);
+  WC_TRY(bfs_batched_run(ctx, sched, static_cast<const uint64_t*>(S.dev),
+                         static_cast<const uint32_t*>(C.dev), caps.data(), width,
+                         static_cast<uint8_t*>(D.dev), edges->as<unsigned long long>()));
+  WC_TRY(D.out(ctx));
+  if (edges_traversed_out)
+    WC_CUDA(cudaMemcpyAsync(edges_traversed_out, edges->ptr, width * 8, cudaMemcpyDefault,
+                            ctx.stream), ctx.detail);
+  return ctx.finish();
+}
+
+}  // extern "C"

@@ -1,0 +1,351 @@
+// pagerank.cu — wc_pagerank: compute/pagerank/mod.rs:96-287 on the device.
+//
+// The reference runs, per iteration, `spread` (msg = x / out, the dangling
+// rank summed), a plus_times pull over the reverse CSR, and `advance`
+// (x ← d·(y + dangling·p) + (1−d)·p with the L1 change), each step's
+// arithmetic as SQL float8 does it.  Here one kernel per iteration does all
+// three: the pull of row i is followed at once by its advance and by the
+// spread of the new x_i into the next iteration's message, so the messages
+// are read once and x once per iteration.  The two sums (the L1 change and
+// the next dangling rank) are reduced per block and then, by the last block
+// to finish, in block order, so results do not vary from run to run.  That
+// block also applies the stop test (delta < live × tol in SQL order) and
+// raises a device flag on which later iterations return at once, so a
+// call's iterations are queued without a round trip per iteration.
+//
+// Floating-point reassociation: rows of more than 256 entries, and the two
+// sums, are added in another order than the reference's sequential folds
+// (documented; the ranks stay within 1e-12 relative L1).  The seeded
+// personalisation's sum is computed in the reference's own order (65536-
+// element chunks folded sequentially, combined in order).
+#include "operand.h"
+#include "pagerank.h"
+#include "pull.cuh"
+#include "sqlfloat.cuh"
+
+namespace wc {
+
+constexpr uint64_t kChunk = 1 << 16;  // compute/reduce.rs:20
+
+__device__ inline bool tomb_at(const uint64_t* t, uint32_t i) {
+  return t && ((t[i >> 6] >> (i & 63)) & 1);
+}
+
+// Sums two values per thread over the block, then over blocks in order in
+// the last block to arrive; returns true in thread 0 of that block with the
+// totals in a, b.
+__device__ inline bool reduce_two(double& a, double& b, double* partials, unsigned* counter) {
+  __shared__ double sa[32], sb[32];
+  __shared__ bool last;
+  const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  if (lane == 0) {
+    sa[wid] = a;
+    sb[wid] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double ta = 0.0, tb = 0.0;
+    for (unsigned w = 0; w < blockDim.x / 32; w++) {
+      ta += sa[w];
+      tb += sb[w];
+    }
+    partials[2 * blockIdx.x] = ta;
+    partials[2 * blockIdx.x + 1] = tb;
+    __threadfence();
+    last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return false;
+  __threadfence();
+  double ta = 0.0, tb = 0.0;
+  for (unsigned k = 0; k < gridDim.x; k++) {
+    ta += __ldcg(partials + 2 * k);
+    tb += __ldcg(partials + 2 * k + 1);
+  }
+  *counter = 0;
+  a = ta;
+  b = tb;
+  return true;
+}
+
+// The reference's sum of a seed over live rows (reduce.rs:137-153, 266-279):
+// each 65536-element chunk folded sequentially from +0.
+__global__ void seed_chunks_kernel(const double* seed, const uint64_t* tomb, uint64_t n,
+                                   double* partial) {
+  uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  uint64_t lo = c * kChunk;
+  if (lo >= n) return;
+  uint64_t hi = min(n, lo + kChunk);
+  double s = 0.0;
+  for (uint64_t i = lo; i < hi; i++)
+    if (!tomb_at(tomb, (uint32_t)i)) s = s + seed[i];
+  partial[c] = s;
+}
+
+__global__ void seed_shares_kernel(const double* seed, const uint64_t* tomb, uint32_t n,
+                                   const double* partial, uint32_t chunks, double* shares,
+                                   DeviceError* err) {
+  // total = 1 / (chunk sums added in chunk order); every thread recomputes
+  // the short fold so no second launch is needed.
+  double sum = 0.0;
+  for (uint32_t c = 0; c < chunks; c++) sum = sum + partial[c];
+  double total;
+  int32_t s = sql_float<F_DIV>(1.0, sum, &total);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (s) {
+      raise(err, s);
+      return;
+    }
+    double share = 0.0;
+    if (!tomb_at(tomb, i)) {
+      int32_t e = sql_float<F_MUL>(seed[i], total, &share);
+      if (e) raise(err, e, i);
+    }
+    shares[i] = share;
+  }
+}
+
+// spread (mod.rs:204-232) for one row: the message, and the row's dangling
+// rank (x where out is not above 0 in SQL order).
+__device__ inline double spread_row(double x, double out, double* msg, DeviceError* err,
+                                    uint32_t row) {
+  if (sql_cmp_f(out, 0.0) > 0) {
+    double m;
+    int32_t s = sql_float<F_DIV>(x, out, &m);
+    if (s) raise(err, s, row);
+    *msg = m;
+    return 0.0;
+  }
+  *msg = 0.0;
+  return x;
+}
+
+__global__ void pr_init_kernel(PrState s) {
+  double none = 0.0, dangling = 0.0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += gridDim.x * blockDim.x) {
+    double x = tomb_at(s.tomb, i) ? 0.0 : s.start;
+    s.x[0][i] = x;
+    dangling += spread_row(x, s.out[i], &s.msg[0][i], s.err, i);
+  }
+  if (reduce_two(none, dangling, s.partials, s.counter)) {
+    s.dangling[0] = dangling;
+    *s.iterations = 0;
+    *s.done = 0;
+  }
+}
+
+// advance (mod.rs:245-282) and the next spread, for the row the pull ends.
+struct PrEpi {
+  const PrState* s;
+  int cur;
+  double dangling_in;
+  double delta;
+  double dangling_out;
+  __device__ void row(uint32_t i, bool present, double y) {
+    const PrState& st = *s;
+    if (!present) y = 0.0;  // an empty row writes the plus identity
+    double next = 0.0;
+    if (!tomb_at(st.tomb, i)) {
+      const double p = st.shares ? st.shares[i] : st.start;
+      double dp, flowed, a, b;
+      int32_t e = sql_float<F_MUL>(dangling_in, p, &dp);
+      if (!e) e = sql_float<F_ADD>(y, dp, &flowed);
+      if (!e) e = sql_float<F_MUL>(st.damping, flowed, &a);
+      if (!e) e = sql_float<F_MUL>(st.teleport, p, &b);
+      if (!e) e = sql_float<F_ADD>(a, b, &next);
+      if (e) raise(st.err, e, i);
+    }
+    const double old = st.x[cur][i];
+    delta += fabs(next - old);
+    st.x[cur ^ 1][i] = next;
+    dangling_out += spread_row(next, st.out[i], &st.msg[cur ^ 1][i], st.err, i);
+  }
+};
+
+template <class W>
+__global__ void __launch_bounds__(kPullThreads) pr_iter_kernel(CsrView<W> A, PrState s, uint32_t it) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  if (*(volatile int32_t*)s.done) return;
+  const int cur = it & 1;
+  PrEpi epi{&s, cur, s.dangling[it], 0.0, 0.0};
+  double* stage = reinterpret_cast<double*>(smem) + (threadIdx.x >> 5) * kTileEntries;
+  pull_units<double, WC_PLUS_TIMES, W>(A, s.msg[cur], epi, s.err, stage);
+  double delta = epi.delta, dangling = epi.dangling_out;
+  if (reduce_two(delta, dangling, s.partials, s.counter)) {
+    s.delta[it] = delta;
+    s.dangling[it + 1] = dangling;
+    *s.iterations = it + 1;
+    if (s.has_tol && sql_cmp_f(delta, s.threshold) < 0) *s.done = 1;
+    // The caller's cancel word (host memory, mapped) is read once per
+    // iteration, here; the next iteration then returns at once.
+    if (*(volatile const int32_t*)s.cancel) {
+      raise(s.err, WC_CANCELLED);
+      *s.done = 1;
+    }
+  }
+}
+
+template <class W>
+wc_status launch_iter(const PullLaunch& L, const PrState& s, uint32_t it, uint32_t blocks) {
+  CsrView<W> A{L.off, L.tgt, static_cast<const W*>(L.weights), L.units, L.unit_count, L.counters,
+               L.carry};
+  pr_iter_kernel<W><<<blocks, kPullThreads, kPullWarps * kTileEntries * sizeof(double), L.stream>>>(
+      A, s, it);
+  return WC_OK;
+}
+
+wc_status prepare_pull(Ctx& ctx, DevCsr& csr, int semiring, int weighted_flag, int dtype,
+                       uint32_t width, PullLaunch& L);
+wc_status launch_pull(const PullLaunch& L, int dtype, const void* x, void* y);
+
+uint64_t live_count(const uint64_t* tomb, uint64_t n) {
+  uint64_t dead = 0;
+  if (tomb)
+    for (uint64_t w = 0; w < (n + 63) / 64; w++) {
+      uint64_t word = tomb[w];
+      if (w == n / 64 && (n & 63)) word &= (1ull << (n & 63)) - 1;
+      dead += __builtin_popcountll(word);
+    }
+  return n - dead;
+}
+
+wc_status PageRankRun::setup(Ctx& ctx, const wc_pagerank_opts* o, const uint64_t* tomb_host,
+                             const double* seed) {
+  wc_version* v = ctx.v;
+  const uint64_t n = v->n;
+  opts = *o;
+  // Tombstones: the caller's words, on the device.
+  std::vector<uint64_t> words;
+  const uint64_t* th = tomb_host;
+  if (tomb_host && is_device_pointer(tomb_host)) {
+    words.resize((n + 63) / 64);
+    WC_CUDA(cudaMemcpy(words.data(), tomb_host, words.size() * 8, cudaMemcpyDeviceToHost),
+            ctx.detail);
+    th = words.data();
+  }
+  live = live_count(th, n);
+  nodes = (double)live;
+  double start;
+  WC_TRY((wc_status)sql_float<F_DIV>(1.0, nodes, &start));
+  double teleport;
+  WC_TRY((wc_status)sql_float<F_SUB>(1.0, o->damping, &teleport));
+  double threshold = 0.0;
+  if (o->has_tol && o->max_iter > 0) WC_TRY((wc_status)sql_float<F_MUL>(nodes, o->tol, &threshold));
+  const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>(
+      (v->rev.schedule.count + kPullWarps - 1) / kPullWarps, max_blocks(8)));
+  grid = blocks;
+  WC_TRY(ctx.scratch(POOL_PR_X, 2 * n * 8, &x));
+  WC_TRY(ctx.scratch(POOL_PR_MSG, 2 * n * 8, &msg));
+  WC_TRY(ctx.scratch(POOL_PR_OUT, n * 8, &out));
+  const uint64_t scalar_bytes = (2 * (uint64_t)o->max_iter + 8) * 8 + 2 * blocks * 8 + 64;
+  WC_TRY(ctx.scratch(POOL_PR_SCALARS, scalar_bytes, &scalars));
+  if (th) {
+    WC_TRY(ctx.scratch(POOL_PR_TOMB, ((n + 63) / 64) * 8, &tomb));
+    WC_CUDA(cudaMemcpyAsync(tomb->ptr, th, ((n + 63) / 64) * 8, cudaMemcpyHostToDevice,
+                            ctx.stream), ctx.detail);
+  }
+  WC_CUDA(cudaMemsetAsync(scalars->ptr, 0, scalar_bytes, ctx.stream), ctx.detail);
+  double* sc = scalars->as<double>();
+  s = PrState{};
+  s.n = (uint32_t)n;
+  s.x[0] = x->as<double>();
+  s.x[1] = x->as<double>() + n;
+  s.msg[0] = msg->as<double>();
+  s.msg[1] = msg->as<double>() + n;
+  s.out = out->as<double>();
+  s.tomb = th ? tomb->as<uint64_t>() : nullptr;
+  s.start = start;
+  s.damping = o->damping;
+  s.teleport = teleport;
+  s.threshold = threshold;
+  s.has_tol = o->has_tol != 0;
+  s.delta = sc;
+  s.dangling = sc + o->max_iter;
+  s.partials = sc + 2 * (uint64_t)o->max_iter + 8;
+  unsigned char* tail = reinterpret_cast<unsigned char*>(s.partials + 2 * blocks);
+  s.counter = reinterpret_cast<unsigned*>(tail);
+  s.iterations = reinterpret_cast<uint32_t*>(tail + 8);
+  s.done = reinterpret_cast<int32_t*>(tail + 16);
+  s.cancel = v->cancel_dev;
+  s.err = v->error.as<DeviceError>();
+  // out = plus_first over the forward CSR: each row's out-weight.
+  PullLaunch L;
+  WC_TRY(prepare_pull(ctx, v->fwd, WC_PLUS_FIRST, o->weighted, WC_F64, 1, L));
+  WC_TRY(launch_pull(L, WC_F64, s.x[0], out->ptr));
+  // The personalisation.
+  if (seed) {
+    Operand S(POOL_SEED);
+    WC_TRY(S.in(ctx, seed, n * 8));
+    const double* sd = static_cast<const double*>(S.dev);
+    const uint32_t chunks = (uint32_t)((n + kChunk - 1) / kChunk);
+    WC_TRY(ctx.scratch(POOL_PR_SHARES, n * 8 + (uint64_t)chunks * 8, &shares));
+    double* partial = shares->as<double>() + n;
+    seed_chunks_kernel<<<(chunks + 127) / 128, 128, 0, ctx.stream>>>(sd, s.tomb, n, partial);
+    seed_shares_kernel<<<max_blocks(4), 256, 0, ctx.stream>>>(sd, s.tomb, (uint32_t)n, partial,
+                                                             chunks, shares->as<double>(), s.err);
+    s.shares = shares->as<double>();
+  }
+  return cuda_status(cudaGetLastError(), ctx.detail, "pagerank setup");
+}
+
+wc_status PageRankRun::run(Ctx& ctx) {
+  wc_version* v = ctx.v;
+  pr_init_kernel<<<grid, kPullThreads, 0, ctx.stream>>>(s);
+  PullLaunch L;
+  WC_TRY(prepare_pull(ctx, v->rev, WC_PLUS_TIMES, opts.weighted, WC_F64, 1, L));
+  for (uint32_t it = 0; it < opts.max_iter; it++) {
+    if (L.weight_kind == WEIGHTS_F64) WC_TRY(launch_iter<double>(L, s, it, grid));
+    else WC_TRY(launch_iter<void>(L, s, it, grid));
+  }
+  return cuda_status(cudaGetLastError(), ctx.detail, "pagerank iterations");
+}
+
+wc_status PageRankRun::result(Ctx& ctx, double* ranks_dev_or_host, uint32_t* iterations_out,
+                              double* margin) {
+  uint32_t its = 0;
+  WC_CUDA(cudaMemcpy(&its, s.iterations, 4, cudaMemcpyDeviceToHost), ctx.detail);
+  if (opts.max_iter == 0) its = 0;
+  const double* final_x = s.x[its & 1];
+  WC_CUDA(cudaMemcpy(ranks_dev_or_host, final_x, ctx.v->n * 8, cudaMemcpyDefault), ctx.detail);
+  if (iterations_out) *iterations_out = its;
+  if (margin && its > 0) {
+    double delta = 0.0;
+    WC_CUDA(cudaMemcpy(&delta, s.delta + (its - 1), 8, cudaMemcpyDeviceToHost), ctx.detail);
+    *margin = s.threshold != 0.0 ? delta / s.threshold : 0.0;
+  }
+  return WC_OK;
+}
+
+}  // namespace wc
+
+using namespace wc;
+
+extern "C" {
+
+wc_status wc_pagerank(wc_version* v, const wc_call* call, const wc_pagerank_opts* o,
+                      const uint64_t* tombstones, double* ranks, uint32_t* iterations) {
+  if (!v || !o || !ranks) return WC_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lock(v->mu);
+  WC_CUDA(cudaSetDevice(v->device), call ? call->detail : nullptr);
+  Ctx ctx(v, call);
+  if (ctx.cancelled()) return WC_CANCELLED;
+  WC_TRY(ctx.begin());
+  PageRankRun run;
+  WC_TRY(run.setup(ctx, o, tombstones, o->seed));
+  ctx.progress("iterating", 0, o->max_iter);
+  WC_TRY(run.run(ctx));
+  WC_TRY(ctx.finish());
+  double margin = 0.0;
+  WC_TRY(run.result(ctx, ranks, iterations, &margin));
+  v->last_margin = margin;
+  ctx.progress("iterating", iterations ? *iterations : 0, o->max_iter);
+  return WC_OK;
+}
+
+double wc_pagerank_last_margin(const wc_version* v) { return v ? v->last_margin : 0.0; }
+
+}  // extern "C"

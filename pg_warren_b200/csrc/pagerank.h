@@ -1,0 +1,46 @@
+// pagerank.h — the state of one PageRank solve on the device, shared by
+// wc_pagerank, the batched personalised PageRank and the adjoint.
+#pragma once
+
+#include "product.h"
+#include "runtime.cuh"
+
+namespace wc {
+
+struct PrState {
+  uint32_t n;
+  double* x[2];
+  double* msg[2];
+  const double* out;
+  const double* shares;  // NULL: uniform, `start` at every live row
+  const uint64_t* tomb;
+  double start, damping, teleport, threshold;
+  bool has_tol;
+  double* delta;     // per iteration
+  double* dangling;  // per iteration (+1)
+  double* partials;  // 2 per block
+  unsigned* counter;
+  uint32_t* iterations;
+  int32_t* done;
+  const int32_t* cancel;
+  DeviceError* err;
+};
+
+struct PageRankRun {
+  wc_pagerank_opts opts;
+  uint64_t live = 0;
+  double nodes = 0.0;
+  uint32_t grid = 1;
+  DevBuf *x = nullptr, *msg = nullptr, *out = nullptr, *shares = nullptr, *tomb = nullptr,
+         *scalars = nullptr;
+  PrState s;
+
+  wc_status setup(Ctx& ctx, const wc_pagerank_opts* o, const uint64_t* tomb_host,
+                  const double* seed);
+  wc_status run(Ctx& ctx);
+  wc_status result(Ctx& ctx, double* ranks, uint32_t* iterations, double* margin);
+};
+
+uint64_t live_count(const uint64_t* tomb, uint64_t n);
+
+}  // namespace wc

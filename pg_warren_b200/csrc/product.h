@@ -1,0 +1,53 @@
+// product.h — what a launch of the product kernels needs, independent of the
+// element type, so the per-dtype translation units share one interface.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "runtime.cuh"
+
+namespace wc {
+
+// compute/product/kernel.rs:200-240 (Write::row): the mask, replace and
+// accumulate of a product (accumulate < 0: overwrite).
+struct WriteArgs {
+  const void* mask;
+  int32_t mask_dtype;
+  int32_t complement;
+  int32_t replace;
+  int32_t accumulate;
+};
+
+enum WeightKind { WEIGHTS_NONE = 0, WEIGHTS_F64 = 1, WEIGHTS_I32 = 2 };
+
+struct PullLaunch {
+  const uint32_t* off;
+  const uint32_t* tgt;
+  const void* weights;
+  int32_t weight_kind;
+  const Unit* units;
+  uint32_t unit_count;
+  uint32_t* counters;
+  void* carry;
+  uint32_t n;
+  uint32_t width;
+  int32_t semiring;
+  uint32_t max_blocks;
+  cudaStream_t stream;
+  DeviceError* err;
+  wc_error_detail* detail;
+  WriteArgs write;
+};
+
+wc_status launch_pull_f64(const PullLaunch& L, const void* x, void* y);
+wc_status launch_pull_f32(const PullLaunch& L, const void* x, void* y);
+wc_status launch_pull_i64(const PullLaunch& L, const void* x, void* y);
+wc_status launch_pull_bool(const PullLaunch& L, const void* x, void* y);
+
+// The bytes of carry space a long-row schedule needs per slot (the largest
+// partial accumulator: i64 plus keeps three 128-bit values).
+constexpr uint64_t kCarryBytesPerSlot = 64;
+
+}  // namespace wc

@@ -1,0 +1,334 @@
+// runtime.cuh — the backend's host runtime: device memory charged to a
+// budget before it is allocated, the version handle holding the device CSR
+// and CSC, and the per-call context (stream, error word, cancellation).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdarg>
+#include <thread>
+#include <chrono>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/warren_cuda.h"
+
+namespace wc {
+
+// ------------------------------------------------------------------ budget
+// compute/memory.rs:31-227: every buffer is charged before it is allocated;
+// a charge past the limit is refused with what was asked and what is held.
+}  // namespace wc
+
+struct wc_budget {
+  uint64_t limit;
+  std::atomic<uint64_t> in_use{0};
+  std::atomic<uint64_t> peak{0};
+  std::mutex mu;
+};
+
+namespace wc {
+
+inline void set_message(wc_error_detail* d, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+inline void set_message(wc_error_detail* d, const char* fmt, ...) {
+  if (!d) return;
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(d->message, sizeof d->message, fmt, ap);
+  va_end(ap);
+}
+
+// A failed CUDA call: WC_CUDA_ERROR with the error code in the detail.
+inline wc_status cuda_status(cudaError_t e, wc_error_detail* d, const char* where) {
+  if (e == cudaSuccess) return WC_OK;
+  if (d) {
+    d->cuda_error = (int32_t)e;
+    set_message(d, "%s: %s", where, cudaGetErrorString(e));
+  }
+  if (e == cudaErrorMemoryAllocation) return WC_OUT_OF_MEMORY;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return WC_NO_DEVICE;
+  return WC_CUDA_ERROR;
+}
+
+#define WC_TRY(expr)                 \
+  do {                               \
+    wc_status _s = (expr);           \
+    if (_s != WC_OK) return _s;      \
+  } while (0)
+
+#define WC_CUDA(expr, detail)                                       \
+  do {                                                              \
+    cudaError_t _e = (expr);                                        \
+    if (_e != cudaSuccess) return ::wc::cuda_status(_e, detail, #expr); \
+  } while (0)
+
+inline wc_status charge(wc_budget* b, uint64_t bytes, wc_error_detail* d) {
+  if (!b) return WC_OK;
+  std::lock_guard<std::mutex> lock(b->mu);
+  uint64_t used = b->in_use.load();
+  if (bytes > b->limit || used > b->limit - bytes) {
+    if (d) {
+      d->requested = bytes;
+      d->in_use = used;
+      d->limit = b->limit;
+      set_message(d, "compute memory limit exceeded: %llu bytes requested, %llu of %llu in use",
+                  (unsigned long long)bytes, (unsigned long long)used,
+                  (unsigned long long)b->limit);
+    }
+    return WC_MEMORY_LIMIT;
+  }
+  b->in_use.store(used + bytes);
+  if (used + bytes > b->peak.load()) b->peak.store(used + bytes);
+  return WC_OK;
+}
+
+inline void uncharge(wc_budget* b, uint64_t bytes) {
+  if (!b) return;
+  std::lock_guard<std::mutex> lock(b->mu);
+  b->in_use.store(b->in_use.load() - bytes);
+}
+
+// A device buffer charged to a budget for its lifetime.
+struct DevBuf {
+  void* ptr = nullptr;
+  uint64_t bytes = 0;
+  wc_budget* budget = nullptr;
+
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept { *this = std::move(o); }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      ptr = o.ptr;
+      bytes = o.bytes;
+      budget = o.budget;
+      o.ptr = nullptr;
+      o.bytes = 0;
+    }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+
+  void release() {
+    if (ptr) {
+      cudaFree(ptr);
+      uncharge(budget, bytes);
+    }
+    ptr = nullptr;
+    bytes = 0;
+  }
+
+  wc_status alloc(wc_budget* b, uint64_t n, wc_error_detail* d) {
+    release();
+    if (n == 0) n = 16;
+    n = (n + 255) & ~uint64_t(255);
+    WC_TRY(charge(b, n, d));
+    cudaError_t e = cudaMalloc(&ptr, n);
+    if (e != cudaSuccess) {
+      uncharge(b, n);
+      ptr = nullptr;
+      cudaGetLastError();
+      if (d) {
+        d->requested = n;
+        set_message(d, "out of memory allocating %llu bytes", (unsigned long long)n);
+      }
+      return WC_OUT_OF_MEMORY;
+    }
+    bytes = n;
+    budget = b;
+    return WC_OK;
+  }
+
+  template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Where a device buffer of an operand comes from: the caller's own device
+// pointer, or a staging copy of a host operand.
+inline bool is_device_pointer(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// The device error word a kernel raises: the first status wins (atomicCAS
+// from 0); `aux` carries a node id or a count where the status has one.
+struct DeviceError {
+  int32_t status;
+  int32_t pad;
+  uint64_t aux;
+};
+
+// ------------------------------------------------------------------ schedule
+// The row-split schedule of one CSR orientation for the pull kernels: rows
+// grouped into warp tiles (at most kTileRows consecutive rows, at most
+// kTileEntries entries, none longer than that), and each longer row split
+// into pieces of at most kPieceEntries entries whose partial results are
+// combined in piece order by the last piece to finish.
+constexpr uint32_t kTileRows = 32;
+constexpr uint32_t kTileEntries = 256;
+constexpr uint32_t kPieceEntries = 4096;
+
+struct Unit {
+  uint32_t a, b, c, d;  // tile: rows [a, b), c = 0; piece: row a, entries [b, d), c = 1<<31 | slot
+};
+
+struct Schedule {
+  DevBuf units;       // Unit[count]
+  DevBuf counters;    // u32[slots]: arrivals per long row (indexed by its first slot)
+  DevBuf carry;       // the pieces' partial results, kCarryBytesPerSlot per slot
+  uint32_t count = 0;
+  uint32_t slots = 0;
+  uint32_t long_rows = 0;
+  uint32_t tiles = 0;
+};
+
+// One CSR orientation on the device: u32 offsets and targets, f64 weights
+// (absent when unweighted) and, when every weight is an integer in int32
+// range, an int32 copy for the integer semirings.
+struct DevCsr {
+  DevBuf offsets, targets, weights, iweights;
+  Schedule schedule;
+  uint32_t max_degree = 0;
+};
+
+}  // namespace wc
+
+// The handle: one version's device copy, keyed by (graph, version).
+struct wc_version {
+  uint64_t graph_id = 0, version = 0;
+  uint64_t n = 0, m = 0;
+  int device = 0;
+  bool weighted = false;
+  bool integral = false;
+  bool symmetric = false;
+  wc_budget* budget = nullptr;
+  cudaStream_t stream = nullptr;
+  wc::DevCsr fwd, rev;
+  bool reverse_given = false;          // the caller uploaded a reverse CSR
+  std::vector<uint64_t> host_offsets;  // forward offsets, for truncated-BFS stats
+  std::vector<uint64_t> host_rev_offsets;
+  wc::DevBuf error;                    // DeviceError
+  int32_t* cancel_host = nullptr;      // pinned, mapped: the device reads it
+  int32_t* cancel_dev = nullptr;
+  std::recursive_mutex mu;             // calls on one handle run one at a time
+  double last_margin = 0.0;
+  std::map<uint64_t, wc_schedule> tuned;  // (kind << 32 | width) -> schedule
+  // Scratch kept between calls (charged to the budget while held), so a
+  // call allocates only when it needs more than the last one did.  Calls on
+  // one handle are serialised; asynchronous ones must share one stream.
+  std::map<int, wc::DevBuf> pool;
+};
+
+namespace wc {
+
+// The pool's tags: one buffer per role.
+enum PoolTag {
+  POOL_X = 1, POOL_Y, POOL_MASK, POOL_XCOPY, POOL_SEED,
+  POOL_PR_X, POOL_PR_MSG, POOL_PR_OUT, POOL_PR_SHARES, POOL_PR_TOMB, POOL_PR_SCALARS,
+  POOL_BFS_DEPTH, POOL_BFS_VIA, POOL_BFS_Q0, POOL_BFS_Q1, POOL_BFS_FBITS, POOL_BFS_COUNTERS,
+  POOL_BFS_FILTER, POOL_BFS_FLAGS,
+  POOL_BATCH_0 = 40, POOL_BATCH_1, POOL_BATCH_2, POOL_BATCH_3, POOL_BATCH_4, POOL_BATCH_5,
+  POOL_BATCH_6, POOL_BATCH_7, POOL_BATCH_8, POOL_BATCH_9,
+  POOL_EIG_0 = 60, POOL_EIG_1, POOL_EIG_2, POOL_EIG_3, POOL_EIG_4, POOL_EIG_5, POOL_EIG_6,
+  POOL_EIG_7, POOL_EIG_8, POOL_EIG_9,
+  POOL_ADJ_0 = 80, POOL_ADJ_1, POOL_ADJ_2, POOL_ADJ_3, POOL_ADJ_4, POOL_ADJ_5, POOL_ADJ_6,
+  POOL_ADJ_7, POOL_ADJ_8, POOL_ADJ_9,
+};
+
+// A call's context: the stream, the caller's detail and cancellation.
+struct Ctx {
+  wc_version* v;
+  const wc_call* call;
+  cudaStream_t stream;
+  wc_budget* budget;
+  wc_error_detail* detail;
+  bool async;
+  uint32_t timeout_ms;
+
+  Ctx(wc_version* ver, const wc_call* c)
+      : v(ver), call(c), stream(ver->stream), budget(ver->budget), detail(nullptr),
+        async(false), timeout_ms(600000) {
+    if (c) {
+      if (c->stream) stream = (cudaStream_t)c->stream;
+      if (c->memory) budget = c->memory;
+      detail = c->detail;
+      async = (c->flags & WC_CALL_ASYNC) != 0;
+      if (c->timeout_ms) timeout_ms = c->timeout_ms;
+    }
+  }
+
+  bool cancelled() const { return call && call->cancel && *call->cancel; }
+
+  // Pooled scratch of at least `bytes` under `tag` (contents undefined).
+  wc_status scratch(int tag, uint64_t bytes, DevBuf** out) {
+    DevBuf& b = v->pool[tag];
+    if (b.bytes < bytes) {
+      b.release();
+      WC_TRY(b.alloc(v->budget, bytes + bytes / 8, detail));
+    }
+    *out = &b;
+    return WC_OK;
+  }
+
+  void progress(const char* phase, uint64_t done, uint64_t total) const {
+    if (call && call->progress) call->progress(call->progress_context, phase, done, total);
+  }
+
+  // Clears the device error word and the device-visible cancel flag.
+  wc_status begin() {
+    *v->cancel_host = 0;
+    WC_CUDA(cudaMemsetAsync(v->error.ptr, 0, sizeof(DeviceError), stream), detail);
+    return WC_OK;
+  }
+
+  // Waits for the stream, polling the caller's cancel word every 50 µs and
+  // passing it on to the device (kernels that loop read it and stop).  Then
+  // reads the device error word.
+  wc_status finish() {
+    auto start = std::chrono::steady_clock::now();
+    bool cancel = false, timed_out = false;
+    for (;;) {
+      cudaError_t q = cudaStreamQuery(stream);
+      if (q == cudaSuccess) break;
+      if (q != cudaErrorNotReady) return cuda_status(q, detail, "cudaStreamQuery");
+      if (!cancel && cancelled()) {
+        cancel = true;
+        *v->cancel_host = 1;
+      }
+      auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(
+                    std::chrono::steady_clock::now() - start).count();
+      if (!timed_out && (uint64_t)ms > timeout_ms) {
+        timed_out = true;
+        *v->cancel_host = 1;
+      }
+      if (ms >= 2) std::this_thread::sleep_for(std::chrono::microseconds(20));
+      else std::this_thread::yield();
+    }
+    DeviceError e;
+    WC_CUDA(cudaMemcpy(&e, v->error.ptr, sizeof e, cudaMemcpyDeviceToHost), detail);
+    if (cancel) return WC_CANCELLED;
+    if (timed_out) return WC_DEVICE_TIMEOUT;
+    if (e.status != 0) {
+      if (detail) detail->node = e.aux;
+      return (wc_status)e.status;
+    }
+    return WC_OK;
+  }
+
+};
+
+}  // namespace wc
