@@ -326,6 +326,11 @@ typedef enum wc_batch_kind { WC_BATCH_BFS = 0, WC_BATCH_MINPLUS = 1, WC_BATCH_PP
 wc_status wc_autotune(wc_version* version, const wc_call* call, wc_batch_kind kind,
                       uint32_t width, wc_schedule* chosen);
 
+/* Pins the schedule used for `kind` at `width` columns on this version (as
+ * wc_autotune would keep its choice), for reproducible runs. */
+wc_status wc_schedule_set(wc_version* version, wc_batch_kind kind, uint32_t width,
+                          const wc_schedule* schedule);
+
 /* `width` BFS searches, source s from sources[s] to depth max_depths[s]
  * (out-edges), as one boolean SpMM over bit-packed frontiers.  depth_out is
  * source-major: depth_out[s * id_space + i] = depth of i from sources[s]

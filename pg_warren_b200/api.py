@@ -617,10 +617,20 @@ def ppr_batched(graph: GraphVersion, seed_sets, pagerank: PageRank = PageRank(),
     return r, it
 
 
+_KINDS = {"bfs": 0, "minplus": 1, "ppr": 2}
+
+
+def set_schedule(graph: GraphVersion, kind: str, width: int, columns_per_pass: int,
+                 blocks_per_sm: int = 4):
+    s = A.Schedule(columns_per_pass, 1, blocks_per_sm, 0)
+    _raise(A.load().wc_schedule_set(graph.handle, _KINDS[kind], width, C.byref(s)),
+           A.ErrorDetail())
+
+
 def autotune(graph: GraphVersion, kind: str, width: int) -> A.Schedule:
     s = A.Schedule()
     call, detail = _call()
-    _raise(A.load().wc_autotune(graph.handle, C.byref(call), {"bfs": 0, "minplus": 1, "ppr": 2}[kind],
+    _raise(A.load().wc_autotune(graph.handle, C.byref(call), _KINDS[kind],
                                 width, C.byref(s)), detail)
     return s
 

@@ -6,7 +6,8 @@
 namespace wc {
 
 struct BatchBuffers {
-  DevBuf *V = nullptr, *F = nullptr, *bits = nullptr, *masks = nullptr, *counts = nullptr;
+  DevBuf *V = nullptr, *F = nullptr, *bits = nullptr, *masks = nullptr, *counts = nullptr,
+         *nacc = nullptr;
   wc_status reserve(Ctx& ctx, uint32_t words, uint32_t levels);
 };
 

@@ -56,74 +56,209 @@ __global__ void msbfs_seed_kernel(const uint64_t* sources, const uint32_t* caps,
 }
 
 // Level L: F_{L+1}[i] = (OR over in-neighbours j in the frontier of
-// F_L[j] & A_L) & ~V[i]; V[i] |= F_{L+1}[i].  A group of W lanes per node.
+// F_L[j] & A_L) & ~V[i]; V[i] |= F_{L+1}[i].  Warps walk the reverse CSR's
+// row-split schedule (units of at most 256 entries).  In a tile of rows the
+// warp first finds which rows still lack a source (the rest are skipped),
+// loads the tile's targets and their frontier bits with eight loads in
+// flight a lane, lists the hits, then gathers the hit rows of F_L, several
+// at once, OR-ing them into per-row accumulators in shared memory.  A long
+// row's pieces OR into a per-row accumulator in global memory, and the last
+// piece to arrive writes the row.
+struct MsLevel {
+  uint32_t n;
+  const uint32_t* off;
+  const uint32_t* tgt;
+  const Unit* units;
+  uint32_t unit_count;
+  uint32_t* counters;  // per long row (first slot), left zero
+  uint32_t* nacc;      // W words per long row (first slot), left zero
+  uint32_t* V;
+  const uint32_t* Fcur;
+  uint32_t* Fnext;
+  const uint32_t* fbits;
+  uint32_t* fbits_next;
+  const uint32_t* masks;
+  uint32_t L;
+  uint32_t* counts;
+};
+
+template <int W> struct MsWarpSmem {
+  uint32_t acc[32 * W];
+  uint32_t hitj[kTileEntries];
+  uint8_t hitr[kTileEntries];
+  uint8_t rowof[kTileEntries];  // the tile row of each entry
+};
+
 template <int W>
-__global__ void __launch_bounds__(256)
-    msbfs_level_kernel(uint32_t n, const uint32_t* __restrict__ off, const uint32_t* __restrict__ tgt,
-                       uint32_t* V, const uint32_t* __restrict__ Fcur, uint32_t* Fnext,
-                       const uint32_t* __restrict__ fbits, uint32_t* fbits_next,
-                       const uint32_t* masks, uint32_t L, uint32_t* counts,
-                       const int32_t* cancel) {
-  if (counts[L] == 0) return;  // nothing expands: F_{L+1} is not read
-  constexpr uint32_t G = 32 / W;  // nodes per warp
+__global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
+  if (P.counts[P.L] == 0) return;  // nothing expands: F_{L+1} is not read
+  constexpr uint32_t G = 32 / W;     // lane groups: rows or hits handled at once
+  constexpr int Q = kTileEntries / 32;
+  constexpr int U = 8;               // gathers in flight per lane
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  MsWarpSmem<W>& sm = reinterpret_cast<MsWarpSmem<W>*>(smem_raw)[threadIdx.x >> 5];
   const unsigned lane = threadIdx.x & 31;
   const unsigned sub = lane / W, w = lane % W;
   const unsigned gmask = (W == 32) ? 0xffffffffu : (((1u << W) - 1) << (sub * W));
-  const uint32_t a = masks[L * W + w];
-  const uint32_t a_next = masks[(L + 1) * W + w];
+  const uint32_t a = P.masks[P.L * W + w];
+  const uint32_t a_next = P.masks[(P.L + 1) * W + w];
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   uint32_t admitted = 0;
-  const uint32_t groups = (n + G - 1) / G;
-  for (uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < groups; g += warps) {
-    const uint32_t i = g * G + sub;
-    const bool valid = i < n;
-    uint32_t v = valid ? V[(size_t)i * W + w] : 0xffffffffu;
-    const uint32_t target = ~v & a;
-    uint32_t acc = 0;
-    const bool work = __ballot_sync(gmask, target != 0) != 0;
-    if (valid && work) {
-      const uint32_t lo = __ldg(off + i), hi = __ldg(off + i + 1);
-      if (W == 32) {
-        // The warp loads 32 targets at once, then ORs the frontier rows.
-        for (uint32_t base = lo; base < hi; base += 32) {
-          const uint32_t e = base + lane;
-          uint32_t j = 0;
-          bool f = false;
-          if (e < hi) {
-            j = __ldcs(tgt + e);
-            f = nbit(fbits, j);
-          }
-          uint32_t hits = __ballot_sync(0xffffffffu, f);
-          while (hits) {
-            const int k = __ffs(hits) - 1;
-            hits &= hits - 1;
-            const uint32_t jj = __shfl_sync(0xffffffffu, j, k);
-            acc |= __ldg(Fcur + (size_t)jj * W + w) & a;
-          }
-          if (__all_sync(0xffffffffu, (acc & target) == target)) break;
+
+  for (uint32_t u = warp; u < P.unit_count; u += warps) {
+    const Unit unit = P.units[u];
+    const bool tile = (unit.c >> 31) == 0;
+    const uint32_t r0 = unit.a;
+    const uint32_t R = tile ? unit.b - unit.a : 1;
+    // Which rows still lack an active source: the rows' V words are all
+    // loaded first (kept for the write at the end), then tested.
+    constexpr uint32_t VR = kTileRows / G;
+    uint32_t vrow[VR];
+#pragma unroll
+    for (uint32_t x = 0; x < VR; x++) {
+      const uint32_t r = x * G + sub;
+      vrow[x] = r < R ? P.V[(size_t)(r0 + r) * W + w] : 0xffffffffu;
+    }
+    uint32_t needy = 0;
+#pragma unroll
+    for (uint32_t x = 0; x < VR; x++) {
+      if (x * G >= R) break;
+      const uint32_t gb = __ballot_sync(0xffffffffu, (~vrow[x] & a) != 0);
+#pragma unroll
+      for (uint32_t g = 0; g < G; g++)
+        if ((gb >> (g * W)) & (W == 32 ? 0xffffffffu : ((1u << W) - 1))) needy |= 1u << (x * G + g);
+    }
+    needy &= R == 32 ? 0xffffffffu : ((1u << R) - 1);
+    uint32_t base, count;
+    if (tile) {
+      uint32_t lo = 0, hi = 0;
+      if (lane < R) {
+        lo = __ldg(P.off + r0 + lane);
+        hi = __ldg(P.off + r0 + lane + 1);
+      }
+      base = __shfl_sync(0xffffffffu, lo, 0);
+      const uint32_t end = __shfl_sync(0xffffffffu, hi, R - 1);
+      count = end - base;
+      if (needy)
+        for (uint32_t k = lo - base; k < hi - base; k++) sm.rowof[k] = (uint8_t)lane;
+      for (uint32_t x = lane; x < R * W; x += 32) sm.acc[x] = 0;
+    } else {
+      base = unit.b;
+      count = unit.d - unit.b;
+    }
+    __syncwarp();
+    // The hits: entries whose source row is in the frontier, in needy rows.
+    uint32_t H = 0;
+    if (needy) {
+      uint32_t jv[Q];
+#pragma unroll
+      for (int q = 0; q < Q; q++) {
+        const uint32_t k = lane + 32 * q;
+        jv[q] = k < count ? __ldcs(P.tgt + base + k) : 0u;
+      }
+      bool fb[Q];
+#pragma unroll
+      for (int q = 0; q < Q; q++) fb[q] = (lane + 32 * q) < count && nbit(P.fbits, jv[q]);
+#pragma unroll
+      for (int q = 0; q < Q; q++) {
+        const uint32_t k = lane + 32 * q;
+        const uint32_t row = (tile && fb[q]) ? sm.rowof[k] : 0u;
+        const bool hit = fb[q] && ((needy >> row) & 1);
+        const uint32_t m = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+          const uint32_t pos = H + __popc(m & ((1u << lane) - 1));
+          sm.hitj[pos] = jv[q];
+          sm.hitr[pos] = (uint8_t)row;
         }
-      } else {
-        for (uint32_t e = lo; e < hi; e++) {
-          const uint32_t j = __ldg(tgt + e);
-          if (nbit(fbits, j)) acc |= __ldg(Fcur + (size_t)j * W + w) & a;
-          if (__all_sync(gmask, (acc & target) == target)) break;
+        H += __popc(m);
+      }
+    }
+    __syncwarp();
+    // Gather the hit rows, G at a time, U deep.
+    uint32_t racc = 0;
+    for (uint32_t h0 = 0; h0 < H; h0 += G * U) {
+      uint32_t val[U];
+      uint32_t rr[U];
+#pragma unroll
+      for (int x = 0; x < U; x++) {
+        const uint32_t h = h0 + x * G + sub;
+        val[x] = 0;
+        rr[x] = 0;
+        if (h < H) {
+          val[x] = __ldg(P.Fcur + (size_t)sm.hitj[h] * W + w);
+          rr[x] = sm.hitr[h];
+        }
+      }
+#pragma unroll
+      for (int x = 0; x < U; x++) {
+        const uint32_t bits = val[x] & a;
+        if (!bits) continue;
+        if (tile) atomicOr(&sm.acc[rr[x] * W + w], bits);
+        else racc |= bits;
+      }
+    }
+    __syncwarp();
+    if (tile) {
+#pragma unroll
+      for (uint32_t x = 0; x < VR; x++) {
+        if (x * G >= R) break;
+        const uint32_t r = x * G + sub;
+        uint32_t fresh = 0;
+        if (r < R) {
+          const uint32_t i = r0 + r;
+          if ((needy >> r) & 1) {
+            fresh = sm.acc[r * W + w] & ~vrow[x];
+            if (fresh) P.V[(size_t)i * W + w] = vrow[x] | fresh;
+          }
+          P.Fnext[(size_t)i * W + w] = fresh;
+        }
+        const bool expands = __ballot_sync(0xffffffffu, (fresh & a_next) != 0) & gmask;
+        if (r < R && expands && w == 0) {
+          atomicOr(P.fbits_next + ((r0 + r) >> 5), 1u << ((r0 + r) & 31));
+          admitted++;
+        }
+      }
+      __syncwarp();
+    } else {
+      // OR the lane groups' words together, then into the row's accumulator.
+#pragma unroll
+      for (uint32_t o = W; o < 32; o <<= 1) racc |= __shfl_xor_sync(0xffffffffu, racc, o);
+      const uint32_t row = unit.a, slot = unit.c & 0x7fffffffu;
+      const uint32_t row_lo = __ldg(P.off + row);
+      const uint32_t deg = __ldg(P.off + row + 1) - row_lo;
+      const uint32_t pieces = (deg + kPieceEntries - 1) / kPieceEntries;
+      const uint32_t first = slot - (unit.b - row_lo) / kPieceEntries;
+      if (sub == 0 && racc) atomicOr(P.nacc + (size_t)first * W + w, racc);
+      __threadfence();
+      __syncwarp();
+      uint32_t arrived = 0;
+      if (lane == 0) arrived = atomicAdd(P.counters + first, 1u);
+      arrived = __shfl_sync(0xffffffffu, arrived, 0);
+      if (arrived == pieces - 1) {
+        __threadfence();
+        uint32_t fresh = 0;
+        if (sub == 0) {
+          const uint32_t tot = __ldcg(P.nacc + (size_t)first * W + w);
+          P.nacc[(size_t)first * W + w] = 0;
+          const uint32_t v = vrow[0];
+          fresh = tot & ~v & a;
+          if (fresh) P.V[(size_t)row * W + w] = v | fresh;
+          P.Fnext[(size_t)row * W + w] = fresh;
+        }
+        const bool expands = __ballot_sync(0xffffffffu, sub == 0 && (fresh & a_next) != 0) != 0;
+        if (lane == 0) {
+          P.counters[first] = 0;
+          if (expands) {
+            atomicOr(P.fbits_next + (row >> 5), 1u << (row & 31));
+            admitted++;
+          }
         }
       }
     }
-    const uint32_t fresh = acc & target;
-    if (valid) {
-      if (fresh) V[(size_t)i * W + w] = v | fresh;
-      Fnext[(size_t)i * W + w] = fresh;
-    }
-    const bool expands = __ballot_sync(gmask, (fresh & a_next) != 0) != 0;
-    if (valid && expands && w == 0) {
-      atomicOr(fbits_next + (i >> 5), 1u << (i & 31));
-      admitted++;
-    }
   }
   for (int o = 16; o > 0; o >>= 1) admitted += __shfl_down_sync(0xffffffffu, admitted, o);
-  if (lane == 0 && admitted) atomicAdd(counts + L + 1, admitted);
-  (void)cancel;
+  if (lane == 0 && admitted) atomicAdd(P.counts + P.L + 1, admitted);
 }
 
 // Depths from the kept frontiers, source-major, and each source's
@@ -218,13 +353,19 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
   uint32_t* counts = b.counts->as<uint32_t>();
   msbfs_seed_kernel<W><<<std::max<uint32_t>(1, (std::max(k, (levels + 1) * W) + 255) / 256), 256, 0,
                          st>>>(sources_dev, caps_dev, k, levels + 1, n, V, F, bits, masks, counts);
-  const uint32_t grid = max_blocks((int)blocks_per_sm);
   const DevCsr& csc = v->rev;
+  const size_t level_smem = 8 * sizeof(MsWarpSmem<W>);
+  if (level_smem > 48 * 1024)
+    WC_CUDA(cudaFuncSetAttribute(msbfs_level_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)level_smem), ctx.detail);
+  const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(
+      max_blocks((int)blocks_per_sm), (csc.schedule.count + 7) / 8));
   for (uint32_t L = 0; L < levels; L++) {
-    msbfs_level_kernel<W><<<grid, 256, 0, st>>>(
-        n, csc.offsets.as<uint32_t>(), csc.targets.as<uint32_t>(), V, F + L * fstride,
-        F + (L + 1) * fstride, bits + L * bitmap_words, bits + (L + 1) * bitmap_words, masks, L,
-        counts, v->cancel_dev);
+    MsLevel P{n, csc.offsets.as<uint32_t>(), csc.targets.as<uint32_t>(), csc.schedule.units.as<Unit>(),
+              csc.schedule.count, csc.schedule.counters.as<uint32_t>(), b.nacc->as<uint32_t>(), V,
+              F + L * fstride, F + (L + 1) * fstride, bits + L * bitmap_words,
+              bits + (L + 1) * bitmap_words, masks, L, counts};
+    msbfs_level_kernel<W><<<grid, 256, level_smem, st>>>(P);
   }
   const size_t smem = 32 * W * 64 + 2 * 32 * W * 4;
   if (smem > 48 * 1024)
@@ -243,6 +384,11 @@ wc_status BatchBuffers::reserve(Ctx& ctx, uint32_t words, uint32_t levels) {
   WC_TRY(ctx.scratch(POOL_BATCH_2, ((n + 31) / 32) * 4 * (uint64_t)(levels + 2), &bits));
   WC_TRY(ctx.scratch(POOL_BATCH_3, (uint64_t)(levels + 2) * words * 4, &masks));
   WC_TRY(ctx.scratch(POOL_BATCH_4, (uint64_t)(levels + 2) * 4, &counts));
+  // The long rows' accumulators start zero and are left zero by each level.
+  const uint64_t nacc_bytes = (uint64_t)std::max<uint32_t>(ctx.v->rev.schedule.slots, 1) * words * 4;
+  const bool fresh = ctx.v->pool[POOL_BATCH_10].bytes < nacc_bytes;
+  WC_TRY(ctx.scratch(POOL_BATCH_10, nacc_bytes, &nacc));
+  if (fresh) WC_CUDA(cudaMemsetAsync(nacc->ptr, 0, nacc->bytes, ctx.stream), ctx.detail);
   return WC_OK;
 }
 
@@ -292,6 +438,9 @@ wc_status bfs_batched_run(Ctx& ctx, const wc_schedule& sched, const uint64_t* so
   }
   return WC_OK;
 }
+
+wc_status tune_minplus(Ctx& ctx, uint32_t width, wc_schedule* best);
+wc_status tune_ppr(Ctx& ctx, uint32_t width, wc_schedule* best);
 
 // Times `candidates` on a seeded sample batch of `width` sources (caps 16,
 // the deepest the benchmark asks) and returns the fastest.
@@ -346,6 +495,18 @@ using namespace wc;
 
 extern "C" {
 
+wc_status wc_schedule_set(wc_version* v, wc_batch_kind kind, uint32_t width,
+                          const wc_schedule* schedule) {
+  if (!v || !schedule || kind < WC_BATCH_BFS || kind > WC_BATCH_PPR) return WC_INVALID_ARGUMENT;
+  const uint32_t c = schedule->columns_per_pass;
+  if (c == 0 || c > 1024 || (c & (c - 1)) || (kind != WC_BATCH_BFS && (c > 32)) ||
+      (kind == WC_BATCH_BFS && c < 32))
+    return WC_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lock(v->mu);
+  v->tuned[((uint64_t)kind << 32) | width] = *schedule;
+  return WC_OK;
+}
+
 wc_status wc_autotune(wc_version* v, const wc_call* call, wc_batch_kind kind, uint32_t width,
                       wc_schedule* chosen) {
   if (!v || width == 0) return WC_INVALID_ARGUMENT;
@@ -356,7 +517,9 @@ wc_status wc_autotune(wc_version* v, const wc_call* call, wc_batch_kind kind, ui
   wc_schedule best{};
   switch (kind) {
     case WC_BATCH_BFS: WC_TRY(tune_bfs(ctx, width, &best)); break;
-    default: return WC_UNSUPPORTED;
+    case WC_BATCH_MINPLUS: WC_TRY(tune_minplus(ctx, width, &best)); break;
+    case WC_BATCH_PPR: WC_TRY(tune_ppr(ctx, width, &best)); break;
+    default: return WC_INVALID_ARGUMENT;
   }
   WC_TRY(ctx.finish());
   v->tuned[((uint64_t)kind << 32) | width] = best;

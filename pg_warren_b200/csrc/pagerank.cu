@@ -31,17 +31,16 @@ __device__ inline bool tomb_at(const uint64_t* t, uint32_t i) {
   return t && ((t[i >> 6] >> (i & 63)) & 1);
 }
 
-// Sums two values per thread over the block, then over blocks in order in
-// the last block to arrive; returns true in thread 0 of that block with the
-// totals in a, b.
-__device__ inline bool reduce_two(double& a, double& b, double* partials, unsigned* counter) {
+// A fixed-order sum of two values over the block: lanes, then warps in
+// order.  The result is in thread 0.
+__device__ inline void block_sum_two(double& a, double& b) {
   __shared__ double sa[32], sb[32];
-  __shared__ bool last;
   const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int o = 16; o > 0; o >>= 1) {
     a += __shfl_down_sync(0xffffffffu, a, o);
     b += __shfl_down_sync(0xffffffffu, b, o);
   }
+  __syncthreads();
   if (lane == 0) {
     sa[wid] = a;
     sb[wid] = b;
@@ -53,19 +52,35 @@ __device__ inline bool reduce_two(double& a, double& b, double* partials, unsign
       ta += sa[w];
       tb += sb[w];
     }
-    partials[2 * blockIdx.x] = ta;
-    partials[2 * blockIdx.x + 1] = tb;
+    a = ta;
+    b = tb;
+  }
+}
+
+// Sums two values per thread over the block, then over the blocks' sums
+// in the last block to arrive (each of its threads folding a fixed stride
+// of them, then the block in fixed order), so the totals do not depend on
+// which block arrives last.  Returns true in thread 0 of that block, with
+// the totals in a, b.
+__device__ inline bool reduce_two(double& a, double& b, double* partials, unsigned* counter) {
+  __shared__ bool last;
+  block_sum_two(a, b);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = a;
+    partials[2 * blockIdx.x + 1] = b;
     __threadfence();
     last = atomicAdd(counter, 1u) == gridDim.x - 1;
   }
   __syncthreads();
-  if (!last || threadIdx.x != 0) return false;
+  if (!last) return false;
   __threadfence();
   double ta = 0.0, tb = 0.0;
-  for (unsigned k = 0; k < gridDim.x; k++) {
+  for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
     ta += __ldcg(partials + 2 * k);
     tb += __ldcg(partials + 2 * k + 1);
   }
+  block_sum_two(ta, tb);
+  if (threadIdx.x != 0) return false;
   *counter = 0;
   a = ta;
   b = tb;

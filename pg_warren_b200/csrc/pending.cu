@@ -5,14 +5,6 @@
 
 extern "C" {
 
-wc_status wc_minplus_batched(wc_version*, const wc_call*, const uint64_t*, const uint32_t*,
-                             uint32_t, int64_t*, uint32_t*) {
-  return WC_UNSUPPORTED;
-}
-wc_status wc_ppr_batched(wc_version*, const wc_call*, const wc_pagerank_opts*, const uint64_t*,
-                         const uint64_t*, uint32_t, double*, uint32_t*) {
-  return WC_UNSUPPORTED;
-}
 wc_status wc_eigen(wc_version*, const wc_call*, const wc_eigen_opts*, double*, double*, double*,
                    wc_eigen_stats*) {
   return WC_UNSUPPORTED;

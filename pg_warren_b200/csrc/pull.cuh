@@ -48,24 +48,33 @@ template <> struct CsrView<void> {
   void* carry;
 };
 
-template <class E, int S, class W> struct EntryOf {
-  __device__ static int32_t get(const CsrView<W>& A, uint32_t e, E xv, E* o);
-};
+// An entry's weight as stored (WT), loaded apart from its product so the
+// loads of a tile can all be in flight at once.
+template <class E, int S, class W> struct EntryOf;
 template <class E, int S> struct EntryOf<E, S, double> {
+  typedef double WT;
+  __device__ static WT load(const CsrView<double>& A, uint32_t e) { return __ldcs(A.w + e); }
+  __device__ static int32_t product(WT w, E xv, E* o) { return Entry<E, S, double>::product(w, xv, o); }
   __device__ static int32_t get(const CsrView<double>& A, uint32_t e, E xv, E* o) {
-    return Entry<E, S, double>::product(__ldcs(A.w + e), xv, o);
+    return product(load(A, e), xv, o);
   }
 };
 template <class E, int S> struct EntryOf<E, S, int32_t> {
+  typedef int32_t WT;
+  __device__ static WT load(const CsrView<int32_t>& A, uint32_t e) { return __ldcs(A.w + e); }
+  __device__ static int32_t product(WT w, E xv, E* o) {
+    return Entry<E, S, int32_t>::product_int(w, xv, o);
+  }
   __device__ static int32_t get(const CsrView<int32_t>& A, uint32_t e, E xv, E* o) {
-    return Entry<E, S, int32_t>::product_int(__ldcs(A.w + e), xv, o);
+    return product(load(A, e), xv, o);
   }
 };
 template <class E, int S> struct EntryOf<E, S, void> {
-  __device__ static int32_t get(const CsrView<void>& A, uint32_t e, E xv, E* o) {
-    (void)A;
-    (void)e;
-    return Entry<E, S, void>::product(1.0, xv, o);
+  typedef char WT;
+  __device__ static WT load(const CsrView<void>&, uint32_t) { return 0; }
+  __device__ static int32_t product(WT, E xv, E* o) { return Entry<E, S, void>::product(1.0, xv, o); }
+  __device__ static int32_t get(const CsrView<void>&, uint32_t, E xv, E* o) {
+    return product(0, xv, o);
   }
 };
 
@@ -106,6 +115,43 @@ __device__ inline Partial<E, ADD> shfl_partial(const Partial<E, ADD>& p, unsigne
   return r;
 }
 
+// Stages the products of entries [base, base + count) (count <= 256) in
+// `stage`: every lane first issues its (up to 8) target loads, then its
+// weight loads and x gathers, then forms the products, so each lane has
+// eight independent loads in flight instead of a chain.
+template <class E, int S, class W>
+__device__ inline void stage_products(const CsrView<W>& A, const E* __restrict__ x, uint32_t base,
+                                      uint32_t count, E* stage, DeviceError* err, uint32_t row) {
+  const unsigned lane = threadIdx.x & 31;
+  constexpr int Q = kTileEntries / 32;
+  uint32_t j[Q];
+#pragma unroll
+  for (int q = 0; q < Q; q++) {
+    const uint32_t k = lane + 32 * q;
+    j[q] = k < count ? __ldcs(A.tgt + base + k) : 0u;
+  }
+  E xv[Q];
+  typename EntryOf<E, S, W>::WT wv[Q];
+#pragma unroll
+  for (int q = 0; q < Q; q++) {
+    const uint32_t k = lane + 32 * q;
+    if (k < count) {
+      xv[q] = load_x(x, j[q]);
+      wv[q] = EntryOf<E, S, W>::load(A, base + k);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < Q; q++) {
+    const uint32_t k = lane + 32 * q;
+    if (k < count) {
+      E p;
+      int32_t s = EntryOf<E, S, W>::product(wv[q], xv[q], &p);
+      if (s) raise(err, s, row);
+      stage[k] = p;
+    }
+  }
+}
+
 // Walks the schedule.  `epi.row(row, present, value)` is called exactly
 // once per row, by one lane.  Products are staged in `stage`
 // (kTileEntries elements per warp).
@@ -119,7 +165,7 @@ __device__ inline void pull_units(const CsrView<W>& A, const E* __restrict__ x, 
   Partial<E, ADD>* carry = static_cast<Partial<E, ADD>*>(A.carry);
 
   for (uint32_t u = warp; u < A.unit_count; u += warps) {
-    Unit unit = A.units[u];
+    const Unit unit = A.units[u];
     if ((unit.c >> 31) == 0) {
       // A tile of rows [a, b): stage every product, then one lane per row.
       const uint32_t r0 = unit.a, rows = unit.b - unit.a;
@@ -130,15 +176,7 @@ __device__ inline void pull_units(const CsrView<W>& A, const E* __restrict__ x, 
       }
       const uint32_t base = __shfl_sync(0xffffffffu, lo, 0);
       const uint32_t end = __shfl_sync(0xffffffffu, hi, rows - 1);
-      const uint32_t count = end - base;
-      for (uint32_t k = lane; k < count; k += 32) {
-        uint32_t e = base + k;
-        uint32_t j = __ldcs(A.tgt + e);
-        E p;
-        int32_t s = EntryOf<E, S, W>::get(A, e, load_x(x, j), &p);
-        if (s) raise(err, s, r0);
-        stage[k] = p;
-      }
+      stage_products<E, S, W>(A, x, base, end - base, stage, err, r0);
       __syncwarp();
       if (lane < rows) {
         E sum{};
@@ -159,56 +197,39 @@ __device__ inline void pull_units(const CsrView<W>& A, const E* __restrict__ x, 
       }
       __syncwarp();
     } else {
-      // A piece [b, d) of row a.
+      // A piece [b, d) (at most 256 entries) of row a: each lane folds a
+      // contiguous run of 8, then the lanes combine left to right.
       const uint32_t row = unit.a, e0 = unit.b, e1 = unit.d;
       const uint32_t slot = unit.c & 0x7fffffffu;
-      Partial<E, ADD> piece{Acc<E, ADD>::of(E{}), false};
-      for (uint32_t c0 = e0; c0 < e1; c0 += kTileEntries) {
-        const uint32_t count = min(kTileEntries, e1 - c0);
-        for (uint32_t k = lane; k < count; k += 32) {
-          uint32_t e = c0 + k;
-          uint32_t j = __ldcs(A.tgt + e);
-          E p;
-          int32_t s = EntryOf<E, S, W>::get(A, e, load_x(x, j), &p);
-          if (s) raise(err, s, row);
-          stage[k] = p;
-        }
-        __syncwarp();
-        Partial<E, ADD> mine{Acc<E, ADD>::of(E{}), false};
-        const uint32_t per = kTileEntries / 32;
-        for (uint32_t k = lane * per; k < min(count, lane * per + per); k++)
-          mine = join(mine, Partial<E, ADD>{Acc<E, ADD>::of(stage[k]), true});
-        for (unsigned o = 1; o < 32; o <<= 1) {
-          Partial<E, ADD> other = shfl_partial(mine, o);
-          if ((lane & (2 * o - 1)) == 0) mine = join(mine, other);
-        }
-        if (lane == 0) piece = join(piece, mine);
-        __syncwarp();
+      const uint32_t count = e1 - e0;
+      stage_products<E, S, W>(A, x, e0, count, stage, err, row);
+      __syncwarp();
+      Partial<E, ADD> mine{Acc<E, ADD>::of(E{}), false};
+      constexpr uint32_t per = kTileEntries / 32;
+      for (uint32_t k = lane * per; k < min(count, lane * per + per); k++)
+        mine = join(mine, Partial<E, ADD>{Acc<E, ADD>::of(stage[k]), true});
+      for (unsigned o = 1; o < 32; o <<= 1) {
+        Partial<E, ADD> other = shfl_partial(mine, o);
+        if ((lane & (2 * o - 1)) == 0) mine = join(mine, other);
       }
-      const uint32_t deg = __ldg(A.off + row + 1) - __ldg(A.off + row);
-      const uint32_t pieces = (deg + kPieceEntries - 1) / kPieceEntries;
-      const uint32_t index = (e0 - __ldg(A.off + row)) / kPieceEntries;
+      __syncwarp();
       if (lane == 0) {
-        if (pieces == 1) {
+        const uint32_t row_lo = __ldg(A.off + row);
+        const uint32_t deg = __ldg(A.off + row + 1) - row_lo;
+        const uint32_t pieces = (deg + kPieceEntries - 1) / kPieceEntries;
+        const uint32_t first = slot - (e0 - row_lo) / kPieceEntries;
+        carry[slot] = mine;
+        __threadfence();
+        const uint32_t arrived = atomicAdd(A.counters + first, 1u);
+        if (arrived == pieces - 1) {
+          __threadfence();
+          Partial<E, ADD> total = load_cg(carry + first);
+          for (uint32_t p = 1; p < pieces; p++) total = join(total, load_cg(carry + first + p));
+          A.counters[first] = 0;
           E v;
-          int32_t s = piece.acc.value(&v);
+          int32_t s = total.acc.value(&v);
           if (s) raise(err, s, row);
           epi.row(row, true, v);
-        } else {
-          const uint32_t first = slot - index;
-          carry[slot] = piece;
-          __threadfence();
-          uint32_t arrived = atomicAdd(A.counters + first, 1u);
-          if (arrived == pieces - 1) {
-            __threadfence();
-            Partial<E, ADD> total = load_cg(carry + first);
-            for (uint32_t p = 1; p < pieces; p++) total = join(total, load_cg(carry + first + p));
-            A.counters[first] = 0;
-            E v;
-            int32_t s = total.acc.value(&v);
-            if (s) raise(err, s, row);
-            epi.row(row, true, v);
-          }
         }
       }
     }

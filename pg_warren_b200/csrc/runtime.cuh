@@ -177,10 +177,11 @@ struct DeviceError {
 // grouped into warp tiles (at most kTileRows consecutive rows, at most
 // kTileEntries entries, none longer than that), and each longer row split
 // into pieces of at most kPieceEntries entries whose partial results are
-// combined in piece order by the last piece to finish.
+// combined in piece order by the last piece to finish.  Every unit is at
+// most 256 entries, so warps taking units round-robin stay balanced.
 constexpr uint32_t kTileRows = 32;
 constexpr uint32_t kTileEntries = 256;
-constexpr uint32_t kPieceEntries = 4096;
+constexpr uint32_t kPieceEntries = 256;
 
 struct Unit {
   uint32_t a, b, c, d;  // tile: rows [a, b), c = 0; piece: row a, entries [b, d), c = 1<<31 | slot
@@ -242,7 +243,7 @@ enum PoolTag {
   POOL_BFS_DEPTH, POOL_BFS_VIA, POOL_BFS_Q0, POOL_BFS_Q1, POOL_BFS_FBITS, POOL_BFS_COUNTERS,
   POOL_BFS_FILTER, POOL_BFS_FLAGS,
   POOL_BATCH_0 = 40, POOL_BATCH_1, POOL_BATCH_2, POOL_BATCH_3, POOL_BATCH_4, POOL_BATCH_5,
-  POOL_BATCH_6, POOL_BATCH_7, POOL_BATCH_8, POOL_BATCH_9,
+  POOL_BATCH_6, POOL_BATCH_7, POOL_BATCH_8, POOL_BATCH_9, POOL_BATCH_10, POOL_BATCH_11,
   POOL_EIG_0 = 60, POOL_EIG_1, POOL_EIG_2, POOL_EIG_3, POOL_EIG_4, POOL_EIG_5, POOL_EIG_6,
   POOL_EIG_7, POOL_EIG_8, POOL_EIG_9,
   POOL_ADJ_0 = 80, POOL_ADJ_1, POOL_ADJ_2, POOL_ADJ_3, POOL_ADJ_4, POOL_ADJ_5, POOL_ADJ_6,

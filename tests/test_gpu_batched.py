@@ -52,3 +52,62 @@ def test_bfs_batched_device_outputs():
     do, eo = O.bfs_depths(og, src, caps)
     assert np.array_equal(d.cpu().numpy(), do)
     assert np.array_equal(e.cpu().numpy().astype(np.uint64), eo)
+
+
+def weighted_graph(scale, kind, seed=1):
+    g = W.rmat(scale, seed=seed)
+    w = W.edge_weights(g, kind)
+    og = O.Graph.from_csr(g.id_space, g.offsets, g.targets, w)
+    return g, w, og, W.GraphVersion(g.offsets, g.targets, w)
+
+
+@pytest.mark.parametrize("columns", [1, 4, 32])
+def test_minplus_batched_equals_the_sssp_loop_per_source(columns):
+    g, w, og, gv = weighted_graph(13, "int")
+    rng = np.random.default_rng(columns)
+    width = 70
+    src = rng.integers(0, g.id_space, width).astype(np.uint64)
+    hops = rng.integers(0, 17, width).astype(np.uint32)
+    W.set_schedule(gv, "minplus", width, columns)
+    d, it = W.minplus_batched(gv, src, hops)
+    do, ito = O.sssp_i64(og, src, hops)
+    assert np.array_equal(d, do)
+    assert np.array_equal(it, ito)
+
+
+def test_minplus_batched_unweighted_and_capped():
+    g = W.rmat(12, seed=4)
+    og = O.Graph.from_csr(g.id_space, g.offsets, g.targets)
+    gv = W.GraphVersion(g.offsets, g.targets)
+    src = np.arange(40, dtype=np.uint64) * 13
+    hops = np.array([0, 1, 2, 3, 16] * 8, np.uint32)
+    d, it = W.minplus_batched(gv, src, hops)
+    do, ito = O.sssp_i64(og, src, hops)
+    assert np.array_equal(d, do) and np.array_equal(it, ito)
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_ppr_batched_matches_seeded_pagerank_per_column(weighted):
+    g = W.rmat(14, seed=2)
+    w = W.edge_weights(g, "uniform") if weighted else None
+    og = O.Graph.from_csr(g.id_space, g.offsets, g.targets, w)
+    gv = W.GraphVersion(g.offsets, g.targets, w)
+    rng = np.random.default_rng(7)
+    sets = [rng.choice(g.id_space, int(np.exp(rng.uniform(0, np.log(300)))), replace=False)
+            for _ in range(19)]
+    W.set_schedule(gv, "ppr", len(sets), 8 if weighted else 2)
+    r, it = W.ppr_batched(gv, sets, W.PageRank(0.85, 1e-10, 100))
+    for c, s in enumerate(sets):
+        seed = np.zeros(g.id_space)
+        seed[s] = 1.0
+        ro, ito, _, _ = O.pagerank(og, 0.85, 1e-10, 100, seed=seed)
+        assert it[c] == ito
+        assert np.abs(r[c] - ro).sum() / np.abs(ro).sum() <= 1e-12
+
+
+def test_autotuners_pick_valid_schedules():
+    g, w, og, gv = weighted_graph(12, "int")
+    s = W.autotune(gv, "minplus", 100)
+    assert s.columns_per_pass in (4, 8, 16, 32)
+    s = W.autotune(gv, "ppr", 100)
+    assert s.columns_per_pass in (1, 2, 4, 8, 16, 32)
