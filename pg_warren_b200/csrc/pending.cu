@@ -5,10 +5,6 @@
 
 extern "C" {
 
-wc_status wc_eigen(wc_version*, const wc_call*, const wc_eigen_opts*, double*, double*, double*,
-                   wc_eigen_stats*) {
-  return WC_UNSUPPORTED;
-}
 wc_status wc_pagerank_adjoint(wc_version*, const wc_call*, const wc_pagerank_opts*,
                               const uint64_t*, const uint64_t*, uint32_t, double, double*, double*,
                               uint32_t*) {
