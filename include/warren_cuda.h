@@ -402,7 +402,10 @@ wc_status wc_eigen(wc_version* version, const wc_call* call, const wc_eigen_opts
  * grad_out is loss-major over the forward CSR's edge order:
  * grad_out[c * edges + e].  The forward runs opts->max_iter iterations or
  * stops at opts->tol as wc_pagerank does; the adjoint solve runs to
- * adjoint_tol (L1 of the adjoint change) or opts->max_iter. */
+ * adjoint_tol (L1 of the adjoint change) or opts->max_iter.
+ * iterations_out (2 entries, may be NULL): the forward iterations, and the
+ * most adjoint iterations any loss took.  Uniform personalisation, no
+ * tombstones. */
 wc_status wc_pagerank_adjoint(wc_version* version, const wc_call* call,
                               const wc_pagerank_opts* opts, const uint64_t* loss_targets,
                               const uint64_t* loss_offsets, uint32_t losses, double adjoint_tol,

@@ -36,7 +36,7 @@ def build(force: bool = False) -> str:
         if all(os.path.getmtime(d) <= built for d in deps):
             return LIBRARY
     sources = [d for d in deps if d.endswith(".cpp")]
-    cmd = ["g++", "-O3", "-std=c++17", "-shared", "-fPIC", "-Wall", "-o", LIBRARY + ".tmp",
+    cmd = ["g++", "-O3", "-std=c++17", "-shared", "-fPIC", "-Wall", "-Wno-maybe-uninitialized", "-o", LIBRARY + ".tmp",
            *sources, "-lpthread"]
     subprocess.run(cmd, check=True)
     os.replace(LIBRARY + ".tmp", LIBRARY)
@@ -107,9 +107,8 @@ def _declare(L):
     if hasattr(L, "wo_eigen"):
         L.wo_eigen.restype = I32
         L.wo_eigen.argtypes = [P, I, I, I, I, D, U64, U64, P, P, P, P]
-    if hasattr(L, "wo_pagerank_adjoint"):
-        L.wo_pagerank_adjoint.restype = I32
-        L.wo_pagerank_adjoint.argtypes = [P, D, I, D, U32, P, P, U32, D, P, P, P]
+    L.wo_pagerank_adjoint.restype = I32
+    L.wo_pagerank_adjoint.argtypes = [P, D, I, D, U32, P, P, U32, D, P, P, P]
 
 
 def _ptr(a):
@@ -301,3 +300,19 @@ def float_op(op, a, b):
     out = D(0.0)
     st = lib().wo_float(op, a, b, C.byref(out))
     return st, out.value
+
+
+def pagerank_adjoint(g, loss_targets, damping=0.85, tol=1e-10, max_iter=100, adjoint_tol=1e-14):
+    """The FP64 CPU adjoint: (grad[losses, edges], ranks, (forward, adjoint) iterations)."""
+    offs = np.zeros(len(loss_targets) + 1, np.uint64)
+    for i, t in enumerate(loss_targets):
+        offs[i + 1] = offs[i] + len(t)
+    nodes = np.ascontiguousarray(np.concatenate([np.asarray(t, np.uint64) for t in loss_targets]))
+    grad = np.zeros((len(loss_targets), g.m), np.float64)
+    ranks = np.zeros(g.n, np.float64)
+    its = np.zeros(2, np.uint32)
+    _check(lib().wo_pagerank_adjoint(g.handle, damping, int(tol is not None),
+                                     0.0 if tol is None else tol, max_iter, _ptr(nodes),
+                                     _ptr(offs), len(loss_targets), adjoint_tol, _ptr(grad),
+                                     _ptr(ranks), _ptr(its)))
+    return grad, ranks, its

@@ -993,3 +993,73 @@ int32_t wo_topk_f64(const double* x, uint64_t n, const uint64_t* tomb, uint64_t 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- adjoint
+// An FP64 CPU adjoint of the uniform PageRank above (no reference
+// counterpart: the reference has no derivative).  At the fixed point
+// x = d·(Aᵀ D⁻¹ x + (uᵀx)·p) + (1 − d)·p (D = diag(out), u the dangling
+// rows, p = 1/live), a loss L = cᵀx has the adjoint λ = d·(D⁻¹Aλ + u·(pᵀλ))
+// + c, solved here by the same power iteration, and
+//   ∂L/∂w_ij = d · x_i / out_i · (λ_j − Σ_k (w_ik / out_i) λ_k).
+// The forward solve is wo_pagerank's.
+extern "C" int32_t wo_pagerank_adjoint(const wo_graph* gp, double damping, int has_tol, double tol,
+                                       uint32_t max_iter, const uint64_t* targets,
+                                       const uint64_t* offsets, uint32_t losses, double adjoint_tol,
+                                       double* grad, double* ranks, uint32_t* iterations) {
+  const Graph& g = *(const Graph*)gp;
+  const uint64_t n = g.fwd.n, m = g.fwd.tgt.size();
+  PageRankOpts o;
+  o.damping = damping;
+  o.has_tol = has_tol != 0;
+  o.tol = tol;
+  o.max_iter = max_iter;
+  std::vector<double> x(n);
+  uint32_t it = 0;
+  Status s = pagerank(g, nullptr, o, x.data(), &it, nullptr, nullptr);
+  if (s) return s;
+  if (ranks) std::copy(x.begin(), x.end(), ranks);
+  if (iterations) iterations[0] = it;
+  std::vector<double> out(n, 0.0);
+  for (uint64_t i = 0; i < n; i++)
+    for (uint64_t e = g.fwd.off[i]; e < g.fwd.off[i + 1]; e++)
+      out[i] = (e == g.fwd.off[i]) ? (g.fwd.weighted() ? g.fwd.w[e] : 1.0)
+                                   : out[i] + (g.fwd.weighted() ? g.fwd.w[e] : 1.0);
+  const double p = 1.0 / (double)n;
+  uint32_t max_adj = 0;
+  for (uint32_t c = 0; c < losses; c++) {
+    std::vector<double> cvec(n, 0.0), lam(n), next(n), srow(n);
+    for (uint64_t q = offsets[c]; q < offsets[c + 1]; q++) cvec[targets[q]] += 1.0;
+    lam = cvec;
+    uint32_t t = 0;
+    for (; t < max_iter; t++) {
+      double pl = 0.0;
+      for (uint64_t i = 0; i < n; i++) pl += p * lam[i];
+      double change = 0.0;
+      for (uint64_t i = 0; i < n; i++) {
+        double z = 0.0;
+        for (uint64_t e = g.fwd.off[i]; e < g.fwd.off[i + 1]; e++)
+          z += (g.fwd.weighted() ? g.fwd.w[e] : 1.0) * lam[g.fwd.tgt[e]];
+        const double si = out[i] > 0.0 ? z / out[i] : 0.0;
+        next[i] = damping * (si + (out[i] > 0.0 ? 0.0 : pl)) + cvec[i];
+        change += std::fabs(next[i] - lam[i]);
+      }
+      lam.swap(next);
+      if (change < adjoint_tol) {
+        t++;
+        break;
+      }
+    }
+    max_adj = std::max(max_adj, t);
+    for (uint64_t i = 0; i < n; i++) {
+      double z = 0.0;
+      for (uint64_t e = g.fwd.off[i]; e < g.fwd.off[i + 1]; e++)
+        z += (g.fwd.weighted() ? g.fwd.w[e] : 1.0) * lam[g.fwd.tgt[e]];
+      srow[i] = out[i] > 0.0 ? z / out[i] : 0.0;
+    }
+    for (uint64_t i = 0; i < n; i++)
+      for (uint64_t e = g.fwd.off[i]; e < g.fwd.off[i + 1]; e++)
+        grad[(uint64_t)c * m + e] = damping * x[i] / out[i] * (lam[g.fwd.tgt[e]] - srow[i]);
+  }
+  if (iterations) iterations[1] = max_adj;
+  return WC_OK;
+}
