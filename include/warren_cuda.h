@@ -150,6 +150,9 @@ typedef struct wc_call {
  * without waiting for it; errors found on the device are reported by the next
  * call on the version, or by wc_version_sync. */
 #define WC_CALL_ASYNC 1u
+/* Record CUDA events around the call's kernel groups ("level", "depth",
+ * "iteration", ...) on its stream; read them with wc_version_timing. */
+#define WC_CALL_TIMING 2u
 
 /* -------------------------------------------------------------- versions */
 
@@ -190,6 +193,15 @@ wc_status wc_version_release(wc_version* version);
 wc_status wc_version_info_get(const wc_version* version, wc_version_info* info);
 /* Waits for the version's stream and reports a pending device error. */
 wc_status wc_version_sync(wc_version* version, const wc_call* call);
+
+/* The device time (ms, CUDA events on the call's stream) of kernel group
+ * `phase` in the last call made with WC_CALL_TIMING, and in *launches the
+ * kernels it launched in that group (may be NULL); 0 if not recorded. */
+double wc_version_timing(const wc_version* version, const char* phase, uint32_t* launches);
+
+/* The number of kernels this library has launched since it was loaded
+ * (a diagnostic: the count a benchmark reports for its timed region). */
+uint64_t wc_kernel_launches(void);
 
 /* Whether this backend serves `operation` over `dtype` (the seam's
  * `Kernels::serves`, DESIGN.md:1224).  Operations: "spmv", "spmm", "pagerank",

@@ -111,6 +111,8 @@ SIGNATURES = [
     ("wc_version_info_get", I32, [P, C.POINTER(VersionInfo)]),
     ("wc_version_sync", I32, [P, C.POINTER(Call)]),
     ("wc_serves", I32, [C.c_char_p, I32]),
+    ("wc_kernel_launches", U64, []),
+    ("wc_version_timing", D, [P, C.c_char_p, C.POINTER(U32)]),
     ("wc_spmv", I32, [P, C.POINTER(Call), C.POINTER(ProductC), I32, P, P]),
     ("wc_spmm", I32, [P, C.POINTER(Call), C.POINTER(ProductC), I32, U32, P, P]),
     ("wc_pagerank", I32, [P, C.POINTER(Call), C.POINTER(PageRankOpts), P, P, C.POINTER(U32)]),

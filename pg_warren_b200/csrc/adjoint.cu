@@ -185,11 +185,11 @@ static wc_status adjoint_pass(Ctx& ctx, AdjState& s, const DevCsr& fwd, const vo
   CsrView<W> A{fwd.offsets.as<uint32_t>(), fwd.targets.as<uint32_t>(),
                static_cast<const W*>(weights), fwd.schedule.units.as<Unit>(), fwd.schedule.count,
                fwd.schedule.counters.as<uint32_t>(), nullptr};
-  adj_init_kernel<kAdjP><<<grid, 256, 0, ctx.stream>>>(s);
+  note_launch(), adj_init_kernel<kAdjP><<<grid, 256, 0, ctx.stream>>>(s);
   for (uint32_t it = 0; it < max_iter; it++)
-    adj_iter_kernel<kAdjP, W><<<grid, 256, 0, ctx.stream>>>(A, s, it, carry, max_iter);
-  adj_rows_kernel<kAdjP, W><<<grid, 256, 0, ctx.stream>>>(A, s, carry);
-  adj_scatter_kernel<kAdjP><<<max_blocks(8), 256, 0, ctx.stream>>>(
+    note_launch(), adj_iter_kernel<kAdjP, W><<<grid, 256, 0, ctx.stream>>>(A, s, it, carry, max_iter);
+  note_launch(), adj_rows_kernel<kAdjP, W><<<grid, 256, 0, ctx.stream>>>(A, s, carry);
+  note_launch(), adj_scatter_kernel<kAdjP><<<max_blocks(8), 256, 0, ctx.stream>>>(
       fwd.offsets.as<uint32_t>(), fwd.targets.as<uint32_t>(), fwd.schedule.units.as<Unit>(),
       fwd.schedule.count, s, grad);
   return cuda_status(cudaGetLastError(), ctx.detail, "adjoint pass");
@@ -270,7 +270,7 @@ wc_status wc_pagerank_adjoint(wc_version* v, const wc_call* call, const wc_pager
     s.iterations = itb->as<uint32_t>() + c0;
     WC_CUDA(cudaMemsetAsync(sc->ptr, 0, 4096, ctx.stream), ctx.detail);
     WC_CUDA(cudaMemsetAsync(Cb->ptr, 0, n * P * 8, ctx.stream), ctx.detail);
-    adj_targets_kernel<<<k, 128, 0, ctx.stream>>>(static_cast<const uint64_t*>(T.dev),
+    note_launch(), adj_targets_kernel<<<k, 128, 0, ctx.stream>>>(static_cast<const uint64_t*>(T.dev),
                                                   static_cast<const uint64_t*>(F.dev), c0, k,
                                                   Cb->as<double>());
     double* g = static_cast<double*>(G.dev) + (uint64_t)c0 * m;

@@ -351,7 +351,7 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
   uint32_t* bits = b.bits->as<uint32_t>();
   uint32_t* masks = b.masks->as<uint32_t>();
   uint32_t* counts = b.counts->as<uint32_t>();
-  msbfs_seed_kernel<W><<<std::max<uint32_t>(1, (std::max(k, (levels + 1) * W) + 255) / 256), 256, 0,
+  note_launch(), msbfs_seed_kernel<W><<<std::max<uint32_t>(1, (std::max(k, (levels + 1) * W) + 255) / 256), 256, 0,
                          st>>>(sources_dev, caps_dev, k, levels + 1, n, V, F, bits, masks, counts);
   const DevCsr& csc = v->rev;
   const size_t level_smem = 8 * sizeof(MsWarpSmem<W>);
@@ -360,20 +360,24 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
                                  (int)level_smem), ctx.detail);
   const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(
       max_blocks((int)blocks_per_sm), (csc.schedule.count + 7) / 8));
+  ctx.phase_begin("level");
   for (uint32_t L = 0; L < levels; L++) {
     MsLevel P{n, csc.offsets.as<uint32_t>(), csc.targets.as<uint32_t>(), csc.schedule.units.as<Unit>(),
               csc.schedule.count, csc.schedule.counters.as<uint32_t>(), b.nacc->as<uint32_t>(), V,
               F + L * fstride, F + (L + 1) * fstride, bits + L * bitmap_words,
               bits + (L + 1) * bitmap_words, masks, L, counts};
-    msbfs_level_kernel<W><<<grid, 256, level_smem, st>>>(P);
+    note_launch(), msbfs_level_kernel<W><<<grid, 256, level_smem, st>>>(P);
   }
+  ctx.phase_end();
   const size_t smem = 32 * W * 64 + 2 * 32 * W * 4;
   if (smem > 48 * 1024)
     WC_CUDA(cudaFuncSetAttribute(msbfs_depth_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem), ctx.detail);
-  msbfs_depth_kernel<W><<<max_blocks(2), 256, smem, st>>>(
+  ctx.phase_begin("depth");
+  note_launch(), msbfs_depth_kernel<W><<<max_blocks(2), 256, smem, st>>>(
       n, k, levels + 1, F, fstride, caps_dev, v->fwd.offsets.as<uint32_t>(), counts, depth_dev,
       edges_dev);
+  ctx.phase_end();
   return cuda_status(cudaGetLastError(), ctx.detail, "batched bfs pass");
 }
 

@@ -159,25 +159,25 @@ wc_status mp_pass(Ctx& ctx, const uint64_t* sources, const uint32_t* caps_dev, u
   s.executed = s.running + 2;
   s.iterations = iterations_dev;
   s.err = v->error.as<DeviceError>();
-  mp_seed_kernel<P><<<max_blocks(4), 256, 0, ctx.stream>>>(s, sources);
-  mp_sources_kernel<P><<<1, 32, 0, ctx.stream>>>(s, sources);
+  note_launch(), mp_seed_kernel<P><<<max_blocks(4), 256, 0, ctx.stream>>>(s, sources);
+  note_launch(), mp_sources_kernel<P><<<1, 32, 0, ctx.stream>>>(s, sources);
   const bool weighted = v->weighted;
   const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(
       max_blocks((int)blocks_per_sm), (v->rev.schedule.count + 7) / 8));
   auto* carry = cb->as<Partial<int64_t, WC_OP_MIN>>();
   for (uint32_t it = 0; it < max_cap; it++) {
     if (weighted && v->integral)
-      mp_iter_kernel<P, int32_t><<<grid, 256, 0, ctx.stream>>>(
+      note_launch(), mp_iter_kernel<P, int32_t><<<grid, 256, 0, ctx.stream>>>(
           view_of<int32_t>(v->rev, v->rev.iweights.ptr), s, it, carry);
     else if (weighted)
-      mp_iter_kernel<P, double><<<grid, 256, 0, ctx.stream>>>(
+      note_launch(), mp_iter_kernel<P, double><<<grid, 256, 0, ctx.stream>>>(
           view_of<double>(v->rev, v->rev.weights.ptr), s, it, carry);
     else
-      mp_iter_kernel<P, void><<<grid, 256, 0, ctx.stream>>>(view_of<void>(v->rev, nullptr), s, it,
+      note_launch(), mp_iter_kernel<P, void><<<grid, 256, 0, ctx.stream>>>(view_of<void>(v->rev, nullptr), s, it,
                                                             carry);
-    mp_control_kernel<<<1, 32, 0, ctx.stream>>>(s, it);
+    note_launch(), mp_control_kernel<<<1, 32, 0, ctx.stream>>>(s, it);
   }
-  columns_out_kernel<P, int64_t><<<max_blocks(4), 256, 0, ctx.stream>>>(s.x[0], s.x[1], s.executed,
+  note_launch(), columns_out_kernel<P, int64_t><<<max_blocks(4), 256, 0, ctx.stream>>>(s.x[0], s.x[1], s.executed,
                                                                          n, k, out);
   return cuda_status(cudaGetLastError(), ctx.detail, "batched min-plus pass");
 }
@@ -337,7 +337,7 @@ wc_status ppr_pass(Ctx& ctx, const PageRankRun& base_run, const uint64_t* nodes,
                          sizeof(Partial<double, WC_OP_PLUS>), &cb));
   WC_CUDA(cudaMemsetAsync(memb->ptr, 0, (uint64_t)n * 4, ctx.stream), ctx.detail);
   WC_CUDA(cudaMemsetAsync(sb->ptr, 0, sb->bytes, ctx.stream), ctx.detail);
-  ppr_member_kernel<<<k, 128, 0, ctx.stream>>>(nodes, offsets, k, c0, memb->as<uint32_t>());
+  note_launch(), ppr_member_kernel<<<k, 128, 0, ctx.stream>>>(nodes, offsets, k, c0, memb->as<uint32_t>());
   unsigned char* sc = sb->as<unsigned char>();
   PprState s{};
   s.n = n;
@@ -365,18 +365,18 @@ wc_status ppr_pass(Ctx& ctx, const PageRankRun& base_run, const uint64_t* nodes,
   s.iterations = iterations_dev;
   s.partials = reinterpret_cast<double*>(sc + 4096);
   s.err = v->error.as<DeviceError>();
-  ppr_init_kernel<P><<<grid, 256, 0, ctx.stream>>>(s);
+  note_launch(), ppr_init_kernel<P><<<grid, 256, 0, ctx.stream>>>(s);
   auto* carry = cb->as<Partial<double, WC_OP_PLUS>>();
   const uint32_t max_iter = base_run.opts.max_iter;
   for (uint32_t it = 0; it < max_iter; it++) {
     if (base_run.opts.weighted != 0 && v->weighted)
-      ppr_iter_kernel<P, double><<<grid, 256, 0, ctx.stream>>>(
+      note_launch(), ppr_iter_kernel<P, double><<<grid, 256, 0, ctx.stream>>>(
           view_of<double>(v->rev, v->rev.weights.ptr), s, it, carry, max_iter);
     else
-      ppr_iter_kernel<P, void><<<grid, 256, 0, ctx.stream>>>(view_of<void>(v->rev, nullptr), s, it,
+      note_launch(), ppr_iter_kernel<P, void><<<grid, 256, 0, ctx.stream>>>(view_of<void>(v->rev, nullptr), s, it,
                                                              carry, max_iter);
   }
-  columns_out_kernel<P, double><<<max_blocks(4), 256, 0, ctx.stream>>>(s.x[0], s.x[1], s.executed,
+  note_launch(), columns_out_kernel<P, double><<<max_blocks(4), 256, 0, ctx.stream>>>(s.x[0], s.x[1], s.executed,
                                                                         n, k, out);
   return cuda_status(cudaGetLastError(), ctx.detail, "batched pagerank pass");
 }

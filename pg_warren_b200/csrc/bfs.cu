@@ -259,7 +259,7 @@ wc_status Search::run(Ctx& ctx, int dir, const uint64_t* starts_in, uint64_t sta
   if (count0) {
     WC_CUDA(cudaMemcpyAsync(queue[0]->ptr, seeds.data(), count0 * 4, cudaMemcpyHostToDevice,
                             ctx.stream), ctx.detail);
-    seed_kernel<<<(count0 + 255) / 256, 256, 0, ctx.stream>>>(queue[0]->as<uint32_t>(), count0,
+    note_launch(), seed_kernel<<<(count0 + 255) / 256, 256, 0, ctx.stream>>>(queue[0]->as<uint32_t>(), count0,
                                                              depth->as<uint32_t>());
   }
   const Rows adj = rows_of(v, dir);
@@ -292,13 +292,13 @@ wc_status Search::run(Ctx& ctx, int dir, const uint64_t* starts_in, uint64_t sta
     uint32_t* next = queue[cur ^ 1]->as<uint32_t>();
     if (pull) {
       WC_CUDA(cudaMemsetAsync(fbits->ptr, 0, ((n + 31) / 32) * 4, ctx.stream), ctx.detail);
-      set_bits_kernel<<<std::min<uint32_t>((count + 255) / 256, blocks), 256, 0, ctx.stream>>>(
+      note_launch(), set_bits_kernel<<<std::min<uint32_t>((count + 255) / 256, blocks), 256, 0, ctx.stream>>>(
           frontier, count, fbits->as<uint32_t>());
-      pull_kernel<<<std::min<uint32_t>((uint32_t)((n + 255) / 256), blocks), 256, 0, ctx.stream>>>(
+      note_launch(), pull_kernel<<<std::min<uint32_t>((uint32_t)((n + 255) / 256), blocks), 256, 0, ctx.stream>>>(
           adj, radj, (uint32_t)n, fbits->as<uint32_t>(), d + 1, depth->as<uint32_t>(),
           via->as<unsigned long long>(), filter_dev, next, c, 1);
     } else {
-      push_kernel<<<std::min<uint32_t>((count + 7) / 8, blocks), 256, 0, ctx.stream>>>(
+      note_launch(), push_kernel<<<std::min<uint32_t>((count + 7) / 8, blocks), 256, 0, ctx.stream>>>(
           adj, radj, frontier, count, d + 1, depth->as<uint32_t>(), via->as<unsigned long long>(),
           filter_dev, next, c);
     }
@@ -335,7 +335,7 @@ wc_status Search::ordered(Ctx& ctx, std::vector<uint64_t>& rows, bool with_via) 
   if (direction == WC_BOTH && n) {
     DevBuf* flags;
     WC_TRY(ctx.scratch(POOL_BFS_FLAGS, n, &flags));
-    in_forward_row_kernel<<<max_blocks(4), 256, 0, ctx.stream>>>(
+    note_launch(), in_forward_row_kernel<<<max_blocks(4), 256, 0, ctx.stream>>>(
         (uint32_t)n, depth->as<uint32_t>(), via->as<unsigned long long>(),
         ctx.v->fwd.offsets.as<uint32_t>(), ctx.v->fwd.targets.as<uint32_t>(), flags->as<uint8_t>());
     WC_CUDA(cudaMemcpyAsync(second_row.data(), flags->ptr, n, cudaMemcpyDeviceToHost, ctx.stream),

@@ -516,7 +516,7 @@ struct Eigensolver {
   cudaStream_t st() const { return ctx.stream; }
 
   wc_status sum_final(uint32_t count, uint32_t columns, double* out_host) {
-    sum_final_kernel<<<(columns + 63) / 64, 64, 0, st()>>>(partial->as<double>(), count, columns,
+    note_launch(), sum_final_kernel<<<(columns + 63) / 64, 64, 0, st()>>>(partial->as<double>(), count, columns,
                                                          coefbuf->as<double>());
     WC_CUDA(cudaMemcpyAsync(out_host, coefbuf->ptr, columns * 8, cudaMemcpyDeviceToHost, st()),
             ctx.detail);
@@ -526,7 +526,7 @@ struct Eigensolver {
 
   wc_status dot_self(const double* x, double* out) {
     auto f = [x] __device__(uint32_t i) { return x[i] * x[i]; };
-    sum_partial_kernel<<<grid, 256, 0, st()>>>(n, f, partial->as<double>());
+    note_launch(), sum_partial_kernel<<<grid, 256, 0, st()>>>(n, f, partial->as<double>());
     return sum_final(grid, 1, out);
   }
 
@@ -539,7 +539,7 @@ struct Eigensolver {
       PullLaunch R;
       WC_TRY(prepare_pull(ctx, v->rev, WC_PLUS_TIMES, weighted, WC_F64, 1, R));
       WC_TRY(launch_pull(R, WC_F64, x, scratch->ptr));
-      average_kernel<<<grid, 256, 0, st()>>>(y, scratch->as<double>(), n);
+      note_launch(), average_kernel<<<grid, 256, 0, st()>>>(y, scratch->as<double>(), n);
     }
     return WC_OK;
   }
@@ -548,11 +548,11 @@ struct Eigensolver {
   wc_status apply(const double* x, double* out) {
     const double* src = x;
     if (normalized) {
-      scale_kernel<<<grid, 256, 0, st()>>>(x, scale->as<double>(), scaled->as<double>(), n);
+      note_launch(), scale_kernel<<<grid, 256, 0, st()>>>(x, scale->as<double>(), scaled->as<double>(), n);
       src = scaled->as<double>();
     }
     WC_TRY(multiply(src, out, o.weighted));
-    finish_apply_kernel<<<grid, 256, 0, st()>>>(op, x, out);
+    note_launch(), finish_apply_kernel<<<grid, 256, 0, st()>>>(op, x, out);
     return WC_OK;
   }
 
@@ -571,7 +571,7 @@ struct Eigensolver {
                  degrees->as<double>(), scale->as<double>()};
     // Freivalds' check when not symmetrising (operator.rs:371-395).
     if (!o.symmetrize && !v->symmetric) {
-      random_kernel<<<grid, 256, 0, st()>>>(input->as<double>(), nullptr, n, kSymmetrySeed, 0, 1);
+      note_launch(), random_kernel<<<grid, 256, 0, st()>>>(input->as<double>(), nullptr, n, kSymmetrySeed, 0, 1);
       PullLaunch L, R;
       WC_TRY(prepare_pull(ctx, v->fwd, WC_PLUS_TIMES, o.weighted, WC_F64, 1, L));
       WC_TRY(launch_pull(L, WC_F64, input->ptr, output->ptr));
@@ -591,11 +591,11 @@ struct Eigensolver {
       if (nan || diff > kSymmetryTolerance * size) return WC_NOT_SYMMETRIC;
     }
     // Active nodes and degrees (operator.rs:336-369).
-    fill_kernel<<<grid, 256, 0, st()>>>(input->as<double>(), n, 1.0);
+    note_launch(), fill_kernel<<<grid, 256, 0, st()>>>(input->as<double>(), n, 1.0);
     WC_TRY(multiply(input->as<double>(), output->as<double>(), 0));
     WC_CUDA(cudaMemcpyAsync(scaled->ptr, output->ptr, nb, cudaMemcpyDeviceToDevice, st()), ctx.detail);
     WC_TRY(multiply(input->as<double>(), degrees->as<double>(), o.weighted));
-    measure_kernel<<<grid, 256, 0, st()>>>(scaled->as<double>(), degrees->as<double>(), n,
+    note_launch(), measure_kernel<<<grid, 256, 0, st()>>>(scaled->as<double>(), degrees->as<double>(), n,
                                            active->as<uint8_t>(), scale->as<double>(), normalized,
                                            v->error.as<DeviceError>());
     DeviceError e;
@@ -620,14 +620,14 @@ struct Eigensolver {
     DevBuf* flag;
     WC_TRY(ctx.scratch(POOL_ADJ_1, 16, &flag));
     uint32_t* par = parent->as<uint32_t>();
-    cc_init_kernel<<<grid, 256, 0, st()>>>(par, active->as<uint8_t>(), n);
+    note_launch(), cc_init_kernel<<<grid, 256, 0, st()>>>(par, active->as<uint8_t>(), n);
     int* changed = flag->as<int>();
     for (int round = 0; round < 1000; round++) {
       WC_CUDA(cudaMemsetAsync(changed, 0, 4, st()), ctx.detail);
-      cc_hook_kernel<<<max_blocks(8), 256, 0, st()>>>(v->fwd.offsets.as<uint32_t>(),
+      note_launch(), cc_hook_kernel<<<max_blocks(8), 256, 0, st()>>>(v->fwd.offsets.as<uint32_t>(),
                                                       v->fwd.targets.as<uint32_t>(),
                                                       active->as<uint8_t>(), n, par, changed);
-      cc_compress_kernel<<<grid, 256, 0, st()>>>(par, n);
+      note_launch(), cc_compress_kernel<<<grid, 256, 0, st()>>>(par, n);
       int h = 0;
       WC_CUDA(cudaMemcpyAsync(&h, changed, 4, cudaMemcpyDeviceToHost, st()), ctx.detail);
       WC_CUDA(cudaStreamSynchronize(st()), ctx.detail);
@@ -720,10 +720,10 @@ struct Eigensolver {
     WC_TRY(ctx.scratch(POOL_ADJ_4, (uint64_t)n * 8, &unit));
     WC_TRY(ctx.scratch(POOL_ADJ_5, std::max<uint64_t>(components, 1) * 16, &dcoef));
     WC_CUDA(cudaMemsetAsync(dcoef->ptr, 0, std::max<uint64_t>(components, 1) * 16, st()), ctx.detail);
-    unit_kernel<<<grid, 256, 0, st()>>>(n, active->as<uint8_t>(), comp->as<uint32_t>(),
+    note_launch(), unit_kernel<<<grid, 256, 0, st()>>>(n, active->as<uint8_t>(), comp->as<uint32_t>(),
                                         degrees->as<double>(), normalized, unit->as<double>(),
                                         dcoef->as<double>());
-    unit_normalize_kernel<<<grid, 256, 0, st()>>>(n, active->as<uint8_t>(), comp->as<uint32_t>(),
+    note_launch(), unit_normalize_kernel<<<grid, 256, 0, st()>>>(n, active->as<uint8_t>(), comp->as<uint32_t>(),
                                                   dcoef->as<double>(), unit->as<double>());
     return cuda_status(cudaGetLastError(), ctx.detail, "deflation");
   }
@@ -732,9 +732,9 @@ struct Eigensolver {
   wc_status project_out(double* x, double* norm) {
     WC_CUDA(cudaMemsetAsync(dcoef->ptr, 0, std::max<uint64_t>(components, 1) * 16, st()), ctx.detail);
     const uint8_t* col = colour ? colour->as<uint8_t>() : nullptr;
-    deflate_coef_kernel<<<grid, 256, 0, st()>>>(n, active->as<uint8_t>(), comp->as<uint32_t>(), col,
+    note_launch(), deflate_coef_kernel<<<grid, 256, 0, st()>>>(n, active->as<uint8_t>(), comp->as<uint32_t>(), col,
                                                 unit->as<double>(), x, dcoef->as<double>());
-    deflate_apply_kernel<<<grid, 256, 0, st()>>>(n, active->as<uint8_t>(), comp->as<uint32_t>(), col,
+    note_launch(), deflate_apply_kernel<<<grid, 256, 0, st()>>>(n, active->as<uint8_t>(), comp->as<uint32_t>(), col,
                                                  bip ? bip->as<uint8_t>() : nullptr,
                                                  unit->as<double>(), dcoef->as<double>(),
                                                  connected_flag, alternating_flag, x);
@@ -753,7 +753,7 @@ struct Eigensolver {
   wc_status project(double* w, int pending, double c, std::vector<double>& out) {
     out.assign(len, 0.0);
     for (uint32_t j0 = 0; j0 < len || (j0 == 0 && pending >= 0); j0 += 8) {
-      project_kernel<<<grid, 256, 0, st()>>>(n, Q->as<double>(), len, j0, w, pending, c,
+      note_launch(), project_kernel<<<grid, 256, 0, st()>>>(n, Q->as<double>(), len, j0, w, pending, c,
                                              partial->as<double>());
       std::vector<double> part(8);
       WC_TRY(sum_final(grid, 8, part.data()));
@@ -767,7 +767,7 @@ struct Eigensolver {
     if (!c.empty())
       WC_CUDA(cudaMemcpyAsync(coefbuf->ptr, c.data(), c.size() * 8, cudaMemcpyHostToDevice, st()),
               ctx.detail);
-    subtract_kernel<<<grid, 256, 0, st()>>>(n, Q->as<double>(), coefbuf->as<double>(), len, w,
+    note_launch(), subtract_kernel<<<grid, 256, 0, st()>>>(n, Q->as<double>(), coefbuf->as<double>(), len, w,
                                             partial->as<double>());
     double s;
     WC_TRY(sum_final(grid, 1, &s));
@@ -783,7 +783,7 @@ struct Eigensolver {
     double pending_c = 0.0;
     if (has_previous && len >= 2) {
       const uint32_t j = len - 1;
-      recurrence_kernel<<<grid, 256, 0, st()>>>(n, col(j - 1), col(j), previous, w,
+      note_launch(), recurrence_kernel<<<grid, 256, 0, st()>>>(n, col(j - 1), col(j), previous, w,
                                                 partial->as<double>());
       double alpha;
       WC_TRY(sum_final(grid, 1, &alpha));
@@ -807,8 +807,8 @@ struct Eigensolver {
 
   wc_status push(const double* w, double norm) {
     if (len == size) return WC_OK;
-    copy_kernel<<<grid, 256, 0, st()>>>(w, col(len), n);
-    scale_vec_kernel<<<grid, 256, 0, st()>>>(col(len), n, 1.0 / norm);
+    note_launch(), copy_kernel<<<grid, 256, 0, st()>>>(w, col(len), n);
+    note_launch(), scale_vec_kernel<<<grid, 256, 0, st()>>>(col(len), n, 1.0 / norm);
     len++;
     return cuda_status(cudaGetLastError(), ctx.detail, "push");
   }
@@ -822,7 +822,7 @@ struct Eigensolver {
   wc_status extend_randomly(bool* ok) {
     streams++;
     double* x = input->as<double>();
-    random_kernel<<<grid, 256, 0, st()>>>(x, active->as<uint8_t>(), n, o.seed, streams - 1, 0);
+    note_launch(), random_kernel<<<grid, 256, 0, st()>>>(x, active->as<uint8_t>(), n, o.seed, streams - 1, 0);
     double before;
     WC_TRY(dot_self(x, &before));
     before = std::sqrt(before);
@@ -904,7 +904,7 @@ struct Eigensolver {
     std::vector<double> vl(len);
     for (uint32_t i = 0; i < len; i++) vl[i] = r.vectors[(size_t)i * len + l];
     WC_CUDA(cudaMemcpy(vbuf->ptr, vl.data(), len * 8, cudaMemcpyHostToDevice), ctx.detail);
-    rotate_kernel<<<grid, 256, 0, st()>>>(n, Q->as<double>(), vbuf->as<double>(), len, 1, 1, out);
+    note_launch(), rotate_kernel<<<grid, 256, 0, st()>>>(n, Q->as<double>(), vbuf->as<double>(), len, 1, 1, out);
     return cuda_status(cudaGetLastError(), ctx.detail, "combine");
   }
 
@@ -912,15 +912,15 @@ struct Eigensolver {
   wc_status eigenpair(double value, double* x, Pair& p, bool keep_vector) {
     WC_TRY(settle(x));
     WC_TRY(apply(x, output->as<double>()));
-    residual_terms_kernel<<<grid, 256, 0, st()>>>(x, output->as<double>(), value, n,
+    note_launch(), residual_terms_kernel<<<grid, 256, 0, st()>>>(x, output->as<double>(), value, n,
                                                   partial->as<double>());
     double s;
     WC_TRY(sum_final(grid, 1, &s));
     p.residual = std::sqrt(s);
     p.value = value;
     if (o.op == WC_RANDOM_WALK) {
-      scale_kernel<<<grid, 256, 0, st()>>>(x, scale->as<double>(), scratch->as<double>(), n);
-      copy_kernel<<<grid, 256, 0, st()>>>(scratch->as<double>(), x, n);
+      note_launch(), scale_kernel<<<grid, 256, 0, st()>>>(x, scale->as<double>(), scratch->as<double>(), n);
+      note_launch(), copy_kernel<<<grid, 256, 0, st()>>>(scratch->as<double>(), x, n);
       WC_TRY(settle(x));
     }
     if (keep_vector) {
@@ -934,7 +934,7 @@ struct Eigensolver {
     double s;
     WC_TRY(dot_self(x, &s));
     const double norm = std::sqrt(s);
-    max_abs_kernel<<<grid, 256, 0, st()>>>(x, n, partial->as<double>());
+    note_launch(), max_abs_kernel<<<grid, 256, 0, st()>>>(x, n, partial->as<double>());
     std::vector<double> part(grid);
     WC_CUDA(cudaMemcpyAsync(part.data(), partial->ptr, grid * 8, cudaMemcpyDeviceToHost, st()),
             ctx.detail);
@@ -945,7 +945,7 @@ struct Eigensolver {
     if (m > 0.0) {
       unsigned* idx = reinterpret_cast<unsigned*>(coefbuf->as<char>() + 8 * 60);
       WC_CUDA(cudaMemsetAsync(idx, 0xff, 4, st()), ctx.detail);
-      first_at_kernel<<<grid, 256, 0, st()>>>(x, n, m, idx);
+      note_launch(), first_at_kernel<<<grid, 256, 0, st()>>>(x, n, m, idx);
       unsigned at = 0;
       WC_CUDA(cudaMemcpyAsync(&at, idx, 4, cudaMemcpyDeviceToHost, st()), ctx.detail);
       WC_CUDA(cudaStreamSynchronize(st()), ctx.detail);
@@ -953,7 +953,7 @@ struct Eigensolver {
       WC_CUDA(cudaMemcpy(&xv, x + at, 8, cudaMemcpyDeviceToHost), ctx.detail);
       sign = xv < 0 ? -1.0 : 1.0;
     }
-    scale_vec_kernel<<<grid, 256, 0, st()>>>(x, n, sign / norm);
+    note_launch(), scale_vec_kernel<<<grid, 256, 0, st()>>>(x, n, sign / norm);
     return cuda_status(cudaGetLastError(), ctx.detail, "settle");
   }
 
@@ -1000,7 +1000,7 @@ struct Eigensolver {
       for (uint32_t i = 0; i < len; i++)
         for (uint32_t l = 0; l < kept; l++) vk[(size_t)i * kept + l] = r.vectors[(size_t)i * len + l];
       WC_CUDA(cudaMemcpy(vbuf->ptr, vk.data(), vk.size() * 8, cudaMemcpyHostToDevice), ctx.detail);
-      rotate_kernel<<<grid, 256, 0, st()>>>(n, Q->as<double>(), vbuf->as<double>(), len, kept, kept,
+      note_launch(), rotate_kernel<<<grid, 256, 0, st()>>>(n, Q->as<double>(), vbuf->as<double>(), len, kept, kept,
                                             Q2->as<double>());
       WC_CUDA(cudaMemcpyAsync(Q->ptr, Q2->ptr, (uint64_t)kept * n * 8, cudaMemcpyDeviceToDevice, st()),
               ctx.detail);
@@ -1095,7 +1095,7 @@ wc_status wc_eigen(wc_version* v, const wc_call* call, const wc_eigen_opts* opts
     if (kp.size() > k) kp.resize(k);
     for (auto& q : kp) {
       double* x = es.input->as<double>();
-      known_vector_kernel<<<es.grid, 256, 0, ctx.stream>>>(
+      note_launch(), known_vector_kernel<<<es.grid, 256, 0, ctx.stream>>>(
           es.n, es.active->as<uint8_t>(), es.comp->as<uint32_t>(),
           es.colour ? es.colour->as<uint8_t>() : nullptr, es.unit->as<double>(),
           (uint32_t)q.second.first, q.second.second, x);

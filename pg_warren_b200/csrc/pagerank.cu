@@ -208,7 +208,7 @@ template <class W>
 wc_status launch_iter(const PullLaunch& L, const PrState& s, uint32_t it, uint32_t blocks) {
   CsrView<W> A{L.off, L.tgt, static_cast<const W*>(L.weights), L.units, L.unit_count, L.counters,
                L.carry};
-  pr_iter_kernel<W><<<blocks, kPullThreads, kPullWarps * kTileEntries * sizeof(double), L.stream>>>(
+  note_launch(), pr_iter_kernel<W><<<blocks, kPullThreads, kPullWarps * kTileEntries * sizeof(double), L.stream>>>(
       A, s, it);
   return WC_OK;
 }
@@ -299,8 +299,8 @@ wc_status PageRankRun::setup(Ctx& ctx, const wc_pagerank_opts* o, const uint64_t
     const uint32_t chunks = (uint32_t)((n + kChunk - 1) / kChunk);
     WC_TRY(ctx.scratch(POOL_PR_SHARES, n * 8 + (uint64_t)chunks * 8, &shares));
     double* partial = shares->as<double>() + n;
-    seed_chunks_kernel<<<(chunks + 127) / 128, 128, 0, ctx.stream>>>(sd, s.tomb, n, partial);
-    seed_shares_kernel<<<max_blocks(4), 256, 0, ctx.stream>>>(sd, s.tomb, (uint32_t)n, partial,
+    note_launch(), seed_chunks_kernel<<<(chunks + 127) / 128, 128, 0, ctx.stream>>>(sd, s.tomb, n, partial);
+    note_launch(), seed_shares_kernel<<<max_blocks(4), 256, 0, ctx.stream>>>(sd, s.tomb, (uint32_t)n, partial,
                                                              chunks, shares->as<double>(), s.err);
     s.shares = shares->as<double>();
   }
@@ -309,13 +309,15 @@ wc_status PageRankRun::setup(Ctx& ctx, const wc_pagerank_opts* o, const uint64_t
 
 wc_status PageRankRun::run(Ctx& ctx) {
   wc_version* v = ctx.v;
-  pr_init_kernel<<<grid, kPullThreads, 0, ctx.stream>>>(s);
+  note_launch(), pr_init_kernel<<<grid, kPullThreads, 0, ctx.stream>>>(s);
   PullLaunch L;
   WC_TRY(prepare_pull(ctx, v->rev, WC_PLUS_TIMES, opts.weighted, WC_F64, 1, L));
+  ctx.phase_begin("iteration");
   for (uint32_t it = 0; it < opts.max_iter; it++) {
     if (L.weight_kind == WEIGHTS_F64) WC_TRY(launch_iter<double>(L, s, it, grid));
     else WC_TRY(launch_iter<void>(L, s, it, grid));
   }
+  ctx.phase_end();
   return cuda_status(cudaGetLastError(), ctx.detail, "pagerank iterations");
 }
 

@@ -22,6 +22,11 @@
 
 namespace wc {
 
+// Every kernel launch of the library is counted (wc_kernel_launches), so a
+// caller can see that its work ran here and how many launches it took.
+extern std::atomic<uint64_t> g_launches;
+inline void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
 // ------------------------------------------------------------------ budget
 // compute/memory.rs:31-227: every buffer is charged before it is allocated;
 // a charge past the limit is refused with what was asked and what is held.
@@ -232,6 +237,8 @@ struct wc_version {
   // call allocates only when it needs more than the last one did.  Calls on
   // one handle are serialised; asynchronous ones must share one stream.
   std::map<int, wc::DevBuf> pool;
+  // Kernel-group timings of the last call made with WC_CALL_TIMING.
+  std::map<std::string, std::pair<double, uint32_t>> timings;
 };
 
 namespace wc {
@@ -260,6 +267,14 @@ struct Ctx {
   bool async;
   uint32_t timeout_ms;
 
+  bool timing = false;
+  struct Timer {
+    std::string name;
+    cudaEvent_t a, b;
+    uint64_t launches;
+  };
+  std::vector<Timer> timers;
+
   Ctx(wc_version* ver, const wc_call* c)
       : v(ver), call(c), stream(ver->stream), budget(ver->budget), detail(nullptr),
         async(false), timeout_ms(600000) {
@@ -268,7 +283,42 @@ struct Ctx {
       if (c->memory) budget = c->memory;
       detail = c->detail;
       async = (c->flags & WC_CALL_ASYNC) != 0;
+      timing = (c->flags & WC_CALL_TIMING) != 0;
       if (c->timeout_ms) timeout_ms = c->timeout_ms;
+    }
+  }
+  ~Ctx() {
+    for (Timer& t : timers) {
+      cudaEventDestroy(t.a);
+      cudaEventDestroy(t.b);
+    }
+  }
+
+  // Brackets a kernel group with events when the caller asked for timing.
+  void phase_begin(const char* name) {
+    if (!timing) return;
+    Timer t{name, nullptr, nullptr, g_launches.load()};
+    cudaEventCreate(&t.a);
+    cudaEventCreate(&t.b);
+    cudaEventRecord(t.a, stream);
+    timers.push_back(t);
+  }
+  void phase_end() {
+    if (!timing || timers.empty()) return;
+    Timer& t = timers.back();
+    cudaEventRecord(t.b, stream);
+    t.launches = g_launches.load() - t.launches;
+  }
+  void collect_timings() {
+    if (!timing) return;
+    v->timings.clear();
+    for (Timer& t : timers) {
+      float ms = 0.0f;
+      if (cudaEventSynchronize(t.b) == cudaSuccess && cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess) {
+        auto& slot = v->timings[t.name];
+        slot.first += ms;
+        slot.second += (uint32_t)t.launches;
+      }
     }
   }
 
@@ -319,6 +369,7 @@ struct Ctx {
       if (ms >= 2) std::this_thread::sleep_for(std::chrono::microseconds(20));
       else std::this_thread::yield();
     }
+    collect_timings();
     DeviceError e;
     WC_CUDA(cudaMemcpy(&e, v->error.ptr, sizeof e, cudaMemcpyDeviceToHost), detail);
     if (cancel) return WC_CANCELLED;

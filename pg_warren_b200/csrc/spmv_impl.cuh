@@ -73,12 +73,12 @@ wc_status launch_one(const PullLaunch& L, const void* x, void* y) {
     size_t smem = kPullWarps * kTileEntries * sizeof(E);
     uint32_t blocks = (L.unit_count + kPullWarps - 1) / kPullWarps;
     blocks = blocks < 1 ? 1 : (blocks > L.max_blocks ? L.max_blocks : blocks);
-    spmv_pull_kernel<E, S, W><<<blocks, kPullThreads, smem, L.stream>>>(
+    note_launch(), spmv_pull_kernel<E, S, W><<<blocks, kPullThreads, smem, L.stream>>>(
         A, static_cast<const E*>(x), epi, L.err);
   } else {
     uint32_t blocks = (L.n + 7) / 8;
     blocks = blocks < 1 ? 1 : (blocks > L.max_blocks ? L.max_blocks : blocks);
-    spmm_rows_kernel<E, S, W><<<blocks, 256, 0, L.stream>>>(
+    note_launch(), spmm_rows_kernel<E, S, W><<<blocks, 256, 0, L.stream>>>(
         A, L.n, L.width, static_cast<const E*>(x), static_cast<E*>(y), L.write, L.err);
   }
   return cuda_status(cudaGetLastError(), L.detail, "product kernel launch");

@@ -47,7 +47,7 @@ static wc_status topk_typed(Ctx& ctx, const void* x, const uint64_t* tomb, uint6
   WC_TRY(ctx.scratch(POOL_BATCH_3, (uint64_t)n * 8, &k2));
   WC_TRY(ctx.scratch(POOL_BATCH_4, (uint64_t)n * 4 * 2, &i2));
   WC_TRY(ctx.scratch(POOL_BATCH_11, 16, &num));
-  topk_keys_kernel<E><<<max_blocks(4), 256, 0, ctx.stream>>>(
+  note_launch(), topk_keys_kernel<E><<<max_blocks(4), 256, 0, ctx.stream>>>(
       static_cast<const E*>(x), tomb, n, desc, keys->as<uint64_t>(), ids->as<uint32_t>(),
       live->as<uint8_t>());
   // Compact the live rows (keys and ids), then sort by key, descending.

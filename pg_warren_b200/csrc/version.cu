@@ -9,6 +9,8 @@
 
 namespace wc {
 
+std::atomic<uint64_t> g_launches{0};
+
 // The reverse CSR by a counting transpose: in-degrees, then a scatter while
 // sources are scanned in order, so each reverse row comes out ascending
 // (graph/csr/transpose.rs:14-44).
@@ -258,6 +260,17 @@ wc_status wc_version_sync(wc_version* v, const wc_call* call) {
   std::lock_guard<std::recursive_mutex> lock(v->mu);
   Ctx ctx(v, call);
   return ctx.finish();
+}
+
+uint64_t wc_kernel_launches(void) { return g_launches.load(); }
+
+double wc_version_timing(const wc_version* v, const char* phase, uint32_t* launches) {
+  if (launches) *launches = 0;
+  if (!v || !phase) return 0.0;
+  auto it = v->timings.find(phase);
+  if (it == v->timings.end()) return 0.0;
+  if (launches) *launches = it->second.second;
+  return it->second.first;
 }
 
 int32_t wc_serves(const char* op, wc_dtype dtype) {
