@@ -258,6 +258,23 @@ typedef struct wc_pagerank_opts {
 wc_status wc_pagerank(wc_version* version, const wc_call* call, const wc_pagerank_opts* opts,
                       const uint64_t* tombstones, double* ranks, uint32_t* iterations);
 
+/* No reference counterpart.  wc_pagerank without any allocation: the call's
+ * working memory (ranks, messages, out-weights, tombstones, stop-test
+ * scalars; 40 bytes a node plus 16 an iteration) is a fixed 64 MiB array in
+ * the library's device globals, enough for about 1.67 million nodes at 100
+ * iterations; larger solves return WC_WORKING_SET with detail.requested and
+ * detail.limit set.  For callers that must not allocate while serving (device
+ * memory held by another allocator; no cudaMalloc/cudaFree on a latency
+ * budget).  Results equal wc_pagerank's.  Seeded (personalised) solves and
+ * WC_CALL_TIMING are not offered.  The array is shared by every call on a
+ * device: calls are serialised per device and return after their kernels
+ * finish, and any other use overlapping one on that device would race.  The
+ * first call on each device looks the array's address up with that device
+ * current; make it before any stream capture on that device. */
+wc_status wc_pagerank_noalloc(wc_version* version, const wc_call* call,
+                              const wc_pagerank_opts* opts, const uint64_t* tombstones,
+                              double* ranks, uint32_t* iterations);
+
 /* The stop test's margin of the last iteration run: delta / (live × tol).
  * Available after wc_pagerank on the same version (diagnostics). */
 double wc_pagerank_last_margin(const wc_version* version);

@@ -116,6 +116,8 @@ SIGNATURES = [
     ("wc_spmv", I32, [P, C.POINTER(Call), C.POINTER(ProductC), I32, P, P]),
     ("wc_spmm", I32, [P, C.POINTER(Call), C.POINTER(ProductC), I32, U32, P, P]),
     ("wc_pagerank", I32, [P, C.POINTER(Call), C.POINTER(PageRankOpts), P, P, C.POINTER(U32)]),
+    ("wc_pagerank_noalloc", I32, [P, C.POINTER(Call), C.POINTER(PageRankOpts), P, P,
+                             C.POINTER(U32)]),
     ("wc_pagerank_last_margin", D, [P]),
     ("wc_bfs", I32, [P, C.POINTER(Call), I32, P, U64, C.POINTER(Limits), P, P, P,
                      C.POINTER(TraversalStats)]),

@@ -448,6 +448,19 @@ def pagerank(graph: GraphVersion, tombstones=None, pagerank: PageRank = PageRank
     return Ranks(ranks, it.value)
 
 
+def pagerank_noalloc(graph: GraphVersion, tombstones=None, pagerank: PageRank = PageRank(),
+                     out=None, interrupts=None, stream=None) -> Ranks:
+    """pagerank() through wc_pagerank_noalloc: no allocation inside the call;
+    the working memory is the library's fixed 64 MiB device array."""
+    o, seed = _pr_opts(pagerank)
+    ranks = out if out is not None else np.zeros(graph.id_space, np.float64)
+    it = C.c_uint32(0)
+    call, detail = _call(interrupts, stream)
+    _raise(A.load().wc_pagerank_noalloc(graph.handle, C.byref(call), C.byref(o),
+                                        _ptr(tombstones), _ptr(ranks), C.byref(it)), detail)
+    return Ranks(ranks, it.value)
+
+
 def last_margin(graph: GraphVersion) -> float:
     return A.load().wc_pagerank_last_margin(graph.handle)
 
