@@ -160,12 +160,26 @@ struct PrEpi {
   double dangling_in;
   double delta;
   double dangling_out;
-  __device__ void row(uint32_t i, bool present, double y) {
+  // The row's operands, requested before its pull so they arrive with it.
+  struct Pre {
+    double old, out, share;
+    bool dead;
+  };
+  __device__ Pre pre(uint32_t i) const {
+    const PrState& st = *s;
+    Pre p;
+    p.dead = tomb_at(st.tomb, i);
+    p.share = st.shares ? st.shares[i] : st.start;
+    p.old = st.x[cur][i];
+    p.out = st.out[i];
+    return p;
+  }
+  __device__ void row(uint32_t i, bool present, double y, const Pre& pr) {
     const PrState& st = *s;
     if (!present) y = 0.0;  // an empty row writes the plus identity
     double next = 0.0;
-    if (!tomb_at(st.tomb, i)) {
-      const double p = st.shares ? st.shares[i] : st.start;
+    if (!pr.dead) {
+      const double p = pr.share;
       double dp, flowed, a, b;
       int32_t e = sql_float<F_MUL>(dangling_in, p, &dp);
       if (!e) e = sql_float<F_ADD>(y, dp, &flowed);
@@ -174,21 +188,20 @@ struct PrEpi {
       if (!e) e = sql_float<F_ADD>(a, b, &next);
       if (e) raise(st.err, e, i);
     }
-    const double old = st.x[cur][i];
-    delta += fabs(next - old);
+    delta += fabs(next - pr.old);
     st.x[cur ^ 1][i] = next;
-    dangling_out += spread_row(next, st.out[i], &st.msg[cur ^ 1][i], st.err, i);
+    dangling_out += spread_row(next, pr.out, &st.msg[cur ^ 1][i], st.err, i);
   }
 };
 
 template <class W>
-__global__ void __launch_bounds__(kPullThreads) pr_iter_kernel(CsrView<W> A, PrState s, uint32_t it) {
+__global__ void __launch_bounds__(kPullThreads, 3) pr_iter_kernel(CsrView<W> A, PrState s, uint32_t it) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (*(volatile int32_t*)s.done) return;
   const int cur = it & 1;
   PrEpi epi{&s, cur, s.dangling[it], 0.0, 0.0};
-  double* stage = reinterpret_cast<double*>(smem) + (threadIdx.x >> 5) * kTileEntries;
-  pull_units<double, WC_PLUS_TIMES, W>(A, s.msg[cur], epi, s.err, stage);
+  PullRing<double, W>* ring = reinterpret_cast<PullRing<double, W>*>(smem) + (threadIdx.x >> 5);
+  pull_units<double, WC_PLUS_TIMES, W>(A, s.msg[cur], epi, s.err, ring);
   double delta = epi.delta, dangling = epi.dangling_out;
   if (reduce_two(delta, dangling, s.partials, s.counter)) {
     s.delta[it] = delta;
@@ -208,8 +221,11 @@ template <class W>
 wc_status launch_iter(const PullLaunch& L, const PrState& s, uint32_t it, uint32_t blocks) {
   CsrView<W> A{L.off, L.tgt, static_cast<const W*>(L.weights), L.units, L.unit_count, L.counters,
                L.carry};
-  note_launch(), pr_iter_kernel<W><<<blocks, kPullThreads, kPullWarps * kTileEntries * sizeof(double), L.stream>>>(
-      A, s, it);
+  constexpr size_t smem = pull_smem_bytes<double, W>();
+  static const cudaError_t attr = cudaFuncSetAttribute(
+      pr_iter_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (attr != cudaSuccess) return cuda_status(attr, L.detail, "pagerank kernel attributes");
+  note_launch(), pr_iter_kernel<W><<<blocks, kPullThreads, smem, L.stream>>>(A, s, it);
   return WC_OK;
 }
 

@@ -5,20 +5,23 @@
 // The reference folds each row sequentially in ascending column order, the
 // first entry setting the sum (compute/product/kernel.rs:84-121).  Here a
 // warp takes one unit of the schedule at a time:
-//  - a tile of up to 32 consecutive rows holding at most 256 entries: the
-//    warp stages the tile's products in shared memory with coalesced loads
-//    (targets and weights streamed with an evict-first hint, x gathered
-//    through the read-only path), then each lane folds one row sequentially
-//    from shared memory — the reference's order exactly;
-//  - a piece of up to 4096 entries of a longer row: the warp folds chunks of
-//    256 staged products, each lane a contiguous run of 8, then combines the
-//    lanes left to right; pieces of one row are combined in piece order by
+//  - a tile of up to 32 consecutive rows holding at most 256 entries (its
+//    first entry and entry count are in the descriptor): the tile's
+//    targets, weights and row offsets arrive in the warp's shared-memory
+//    ring by bulk copies issued a few units ahead, the warp gathers x
+//    through the read-only path and stages the products, then each lane
+//    folds one row sequentially from shared memory — the reference's order
+//    exactly;
+//  - a piece of up to 256 entries of a longer row: the warp stages its
+//    products, each lane folds a contiguous run of 8, then the lanes combine
+//    left to right; pieces of one row are combined in piece order by
 //    whichever warp finishes the row's last piece.  Order-preserving
 //    combines keep min/max (first on a tie), lor, any and the i64 checked
 //    sum exactly what a sequential fold gives; only floating-point plus is
 //    reassociated, and only in rows longer than 256 entries.
 #pragma once
 
+#include "bulk.cuh"
 #include "product.h"
 #include "semiring.cuh"
 
@@ -115,75 +118,201 @@ __device__ inline Partial<E, ADD> shfl_partial(const Partial<E, ADD>& p, unsigne
   return r;
 }
 
-// Stages the products of entries [base, base + count) (count <= 256) in
-// `stage`: every lane first issues its (up to 8) target loads, then its
-// weight loads and x gathers, then forms the products, so each lane has
-// eight independent loads in flight instead of a chain.
+// Counts a piece in: the release publishes this thread's carry store, the
+// acquire (for the last to arrive) makes the other pieces' carries visible.
+// Cheaper than a full fence before a relaxed atomic.
+__device__ inline uint32_t arrive_acq_rel(uint32_t* counter) {
+  uint32_t old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(counter) : "memory");
+  return old;
+}
+
+// The combine of a long row's piece partials, in piece order, by the warp
+// that brings the row's last piece: the warp's G = 32 / P lane groups (lane
+// = g·P + c for column c) each fold a contiguous run of the pieces, then the
+// groups combine left to right, so a row of many pieces costs about
+// pieces / G dependent loads instead of `pieces`.  Group 0 holds the total.
+template <class E, int ADD, int P>
+__device__ inline Partial<E, ADD> combine_pieces(const Partial<E, ADD>* carry, uint32_t first,
+                                                 uint32_t pieces, uint32_t c, uint32_t g) {
+  constexpr uint32_t G = 32 / P;
+  const uint32_t per = (pieces + G - 1) / G;
+  const uint32_t p0 = min(pieces, g * per), p1 = min(pieces, g * per + per);
+  Partial<E, ADD> mine{Acc<E, ADD>::of(E{}), false};
+#pragma unroll 4
+  for (uint32_t p = p0; p < p1; p++)
+    mine = join(mine, load_cg(carry + (size_t)(first + p) * P + c));
+  for (uint32_t o = P; o < 32; o <<= 1) {  // groups o/P apart: left to right
+    Partial<E, ADD> other = shfl_partial(mine, o);
+    if ((g & (2 * (o / P) - 1)) == 0) mine = join(mine, other);
+  }
+  return mine;
+}
+
+// ------------------------------------------------- the warp's staging ring
+// Each warp keeps a ring of R buffers in shared memory.  Lane 0 fills a
+// buffer with one unit's targets, weights and (for a tile) row offsets by
+// bulk copies completed on the buffer's mbarrier, R units ahead of the unit
+// the warp is folding, so the stream of the CSR is always in flight and a
+// unit's critical path is one x gather.  Spans are widened to 16-byte
+// boundaries (kSpan, kOffSpan); the CSR arrays carry 16 bytes of padding.
+
+constexpr uint32_t kSpan = kTileEntries + 8;
+constexpr uint32_t kOffSpan = kTileRows + 8;
+
+template <class W> struct WSize { static constexpr int v = sizeof(W); };
+template <> struct WSize<void> { static constexpr int v = 0; };
+template <class W> struct alignas(16) WSpan { W v[kSpan]; };
+template <> struct alignas(16) WSpan<void> {};
+
+template <class E, class W> struct alignas(16) PullRing {
+  static constexpr int R = WSize<W>::v == 0 ? 3 : 2;
+  uint32_t tgt[R][kSpan];
+  WSpan<W> w[R];
+  uint32_t off[R][kOffSpan];
+  Unit desc[R];
+  E stage[kTileEntries];
+  uint64_t bar[R];
+};
+
+template <class E, class W> constexpr size_t pull_smem_bytes() {
+  return kPullWarps * sizeof(PullRing<E, W>);
+}
+
+// The first entry and entry count of a unit.
+__device__ inline uint32_t unit_first(const Unit& d) { return (d.c >> 31) == 0 ? d.d : d.b; }
+__device__ inline uint32_t unit_count(const Unit& d) { return (d.c >> 31) == 0 ? d.c : d.d - d.b; }
+
+// Lane 0: fills buffer b with unit d.
+template <class E, class W>
+__device__ inline void issue_unit(const CsrView<W>& A, PullRing<E, W>* ring, int b, const Unit& d) {
+  ring->desc[b] = d;
+  const uint32_t e0 = unit_first(d), cnt = unit_count(d);
+  const uint32_t ta = e0 & ~3u, tb = cnt ? (e0 + cnt + 3) & ~3u : ta;
+  uint32_t bytes = (tb - ta) * 4;
+  uint32_t wa = 0, wb = 0;
+  if constexpr (WSize<W>::v == 8) {
+    wa = e0 & ~1u;
+    wb = cnt ? (e0 + cnt + 1) & ~1u : wa;
+    bytes += (wb - wa) * 8;
+  } else if constexpr (WSize<W>::v == 4) {
+    wa = ta;
+    wb = tb;
+    bytes += (wb - wa) * 4;
+  }
+  const bool tile = (d.c >> 31) == 0;
+  const uint32_t oa = d.a & ~3u, ob = (d.b + 1 + 3) & ~3u;
+  if (tile) bytes += (ob - oa) * 4;
+  mbar_arrive_expect(&ring->bar[b], bytes);
+  if (tb > ta) bulk_load(ring->tgt[b], A.tgt + ta, (tb - ta) * 4, &ring->bar[b]);
+  if constexpr (WSize<W>::v != 0) {
+    if (wb > wa) bulk_load(ring->w[b].v, A.w + wa, (wb - wa) * WSize<W>::v, &ring->bar[b]);
+  }
+  if (tile) bulk_load(ring->off[b], A.off + oa, (ob - oa) * 4, &ring->bar[b]);
+}
+
+// The weight of the k-th entry of the unit in buffer b.
 template <class E, int S, class W>
-__device__ inline void stage_products(const CsrView<W>& A, const E* __restrict__ x, uint32_t base,
-                                      uint32_t count, E* stage, DeviceError* err, uint32_t row) {
+__device__ inline typename EntryOf<E, S, W>::WT ring_weight(const PullRing<E, W>* ring, int b,
+                                                            uint32_t e0, uint32_t k) {
+  if constexpr (WSize<W>::v == 8) return ring->w[b].v[(e0 & 1u) + k];
+  else if constexpr (WSize<W>::v == 4) return ring->w[b].v[(e0 & 3u) + k];
+  else return 0;
+}
+
+// Stages the products of the unit in buffer b (count <= 256 entries) in the
+// warp's stage: each lane gathers its (up to 8) x values at once, then forms
+// the products.
+template <class E, int S, class W>
+__device__ inline void stage_products(const PullRing<E, W>* ring, int b, const E* __restrict__ x,
+                                      uint32_t e0, uint32_t count, E* stage, DeviceError* err,
+                                      uint32_t row) {
   const unsigned lane = threadIdx.x & 31;
   constexpr int Q = kTileEntries / 32;
-  uint32_t j[Q];
-#pragma unroll
-  for (int q = 0; q < Q; q++) {
-    const uint32_t k = lane + 32 * q;
-    j[q] = k < count ? __ldcs(A.tgt + base + k) : 0u;
-  }
+  const uint32_t* tg = ring->tgt[b] + (e0 & 3u);
   E xv[Q];
-  typename EntryOf<E, S, W>::WT wv[Q];
 #pragma unroll
   for (int q = 0; q < Q; q++) {
     const uint32_t k = lane + 32 * q;
-    if (k < count) {
-      xv[q] = load_x(x, j[q]);
-      wv[q] = EntryOf<E, S, W>::load(A, base + k);
-    }
+    if (k < count) xv[q] = load_x(x, tg[k]);
   }
 #pragma unroll
   for (int q = 0; q < Q; q++) {
     const uint32_t k = lane + 32 * q;
     if (k < count) {
       E p;
-      int32_t s = EntryOf<E, S, W>::product(wv[q], xv[q], &p);
+      int32_t s = EntryOf<E, S, W>::product(ring_weight<E, S, W>(ring, b, e0, k), xv[q], &p);
       if (s) raise(err, s, row);
       stage[k] = p;
     }
   }
 }
 
-// Walks the schedule.  `epi.row(row, present, value)` is called exactly
-// once per row, by one lane.  Products are staged in `stage`
-// (kTileEntries elements per warp).
+// Walks the schedule, a warp per unit, the units of a warp strided by the
+// grid's warp count, through the warp's staging ring.  The epilogue's
+// per-row operands (`epi.pre(row)`) are requested as a unit starts, so they
+// arrive with its gathers.  `epi.row(row, present, value, pre)` is called
+// exactly once per row, by one lane.  A ring wait that runs out (about 2 s)
+// raises WC_DEVICE_TIMEOUT and ends the walk after the copies in flight.
 template <class E, int S, class W, class Epi>
 __device__ inline void pull_units(const CsrView<W>& A, const E* __restrict__ x, Epi& epi,
-                                  DeviceError* err, E* stage) {
+                                  DeviceError* err, PullRing<E, W>* ring) {
+  constexpr int R = PullRing<E, W>::R;
   constexpr int ADD = semiring_add(S);
   const unsigned lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   Partial<E, ADD>* carry = static_cast<Partial<E, ADD>*>(A.carry);
+  if (warp >= A.unit_count) return;
 
+  if (lane == 0)
+    for (int b = 0; b < R; b++) mbar_init(&ring->bar[b], 1);
+  __syncwarp();
+  Unit ahead{0u, 0u, 0u, 0u};  // lane 0: the next unit to issue
+  uint32_t pending = 0;        // buffers with a copy in flight (uniform)
+  for (int b = 0; b < R; b++) {
+    const uint32_t u = warp + b * warps;
+    if (u < A.unit_count) {
+      if (lane == 0) issue_unit(A, ring, b, A.units[u]);
+      pending |= 1u << b;
+    }
+  }
+  if (lane == 0 && warp + R * warps < A.unit_count) ahead = A.units[warp + R * warps];
+  __syncwarp();
+
+  uint32_t phase = 0;
+  int b = 0;
   for (uint32_t u = warp; u < A.unit_count; u += warps) {
-    const Unit unit = A.units[u];
+    const bool ok = mbar_wait(&ring->bar[b], (phase >> b) & 1u);
+    if (!__all_sync(0xffffffffu, ok)) {
+      if (lane == 0) raise(err, WC_DEVICE_TIMEOUT);
+      for (int q = 0; q < R; q++)
+        if (pending & (1u << q)) mbar_wait(&ring->bar[q], (phase >> q) & 1u);
+      break;
+    }
+    phase ^= 1u << b;
+    pending &= ~(1u << b);
+    const Unit unit = ring->desc[b];
     if ((unit.c >> 31) == 0) {
-      // A tile of rows [a, b): stage every product, then one lane per row.
-      const uint32_t r0 = unit.a, rows = unit.b - unit.a;
+      // A tile of rows [a, b) holding c entries from d: stage every
+      // product, then one lane per row folds its run in column order.
+      const uint32_t r0 = unit.a, rows = unit.b - unit.a, e0 = unit.d, count = unit.c;
+      const uint32_t* soff = ring->off[b] + (r0 & 3u);
       uint32_t lo = 0, hi = 0;
+      typename Epi::Pre pre{};
       if (lane < rows) {
-        lo = __ldg(A.off + r0 + lane);
-        hi = __ldg(A.off + r0 + lane + 1);
+        lo = soff[lane];
+        hi = soff[lane + 1];
+        pre = epi.pre(r0 + lane);
       }
-      const uint32_t base = __shfl_sync(0xffffffffu, lo, 0);
-      const uint32_t end = __shfl_sync(0xffffffffu, hi, rows - 1);
-      stage_products<E, S, W>(A, x, base, end - base, stage, err, r0);
+      stage_products<E, S, W>(ring, b, x, e0, count, ring->stage, err, r0);
       __syncwarp();
       if (lane < rows) {
         E sum{};
         bool present = false;
         int32_t bad = 0;
-        for (uint32_t k = lo - base; k < hi - base; k++) {
-          E p = stage[k];
+        for (uint32_t k = lo - e0; k < hi - e0; k++) {
+          E p = ring->stage[k];
           if (present) {
             int32_t s = Apply<E, ADD>::go(sum, p, &sum);
             if (s) bad = s;
@@ -193,46 +322,60 @@ __device__ inline void pull_units(const CsrView<W>& A, const E* __restrict__ x, 
           }
         }
         if (bad) raise(err, bad, r0 + lane);
-        epi.row(r0 + lane, present, sum);
+        epi.row(r0 + lane, present, sum, pre);
       }
-      __syncwarp();
     } else {
       // A piece [b, d) (at most 256 entries) of row a: each lane folds a
       // contiguous run of 8, then the lanes combine left to right.
       const uint32_t row = unit.a, e0 = unit.b, e1 = unit.d;
       const uint32_t slot = unit.c & 0x7fffffffu;
       const uint32_t count = e1 - e0;
-      stage_products<E, S, W>(A, x, e0, count, stage, err, row);
+      stage_products<E, S, W>(ring, b, x, e0, count, ring->stage, err, row);
       __syncwarp();
       Partial<E, ADD> mine{Acc<E, ADD>::of(E{}), false};
       constexpr uint32_t per = kTileEntries / 32;
       for (uint32_t k = lane * per; k < min(count, lane * per + per); k++)
-        mine = join(mine, Partial<E, ADD>{Acc<E, ADD>::of(stage[k]), true});
+        mine = join(mine, Partial<E, ADD>{Acc<E, ADD>::of(ring->stage[k]), true});
       for (unsigned o = 1; o < 32; o <<= 1) {
         Partial<E, ADD> other = shfl_partial(mine, o);
         if ((lane & (2 * o - 1)) == 0) mine = join(mine, other);
       }
-      __syncwarp();
+      const uint32_t row_lo = __ldg(A.off + row);
+      const uint32_t deg = __ldg(A.off + row + 1) - row_lo;
+      const uint32_t pieces = (deg + kPieceEntries - 1) / kPieceEntries;
+      const uint32_t first = slot - (e0 - row_lo) / kPieceEntries;
+      uint32_t arrived = 0;
       if (lane == 0) {
-        const uint32_t row_lo = __ldg(A.off + row);
-        const uint32_t deg = __ldg(A.off + row + 1) - row_lo;
-        const uint32_t pieces = (deg + kPieceEntries - 1) / kPieceEntries;
-        const uint32_t first = slot - (e0 - row_lo) / kPieceEntries;
         carry[slot] = mine;
+        arrived = arrive_acq_rel(A.counters + first);
+      }
+      arrived = __shfl_sync(0xffffffffu, arrived, 0);
+      if (arrived == pieces - 1) {
         __threadfence();
-        const uint32_t arrived = atomicAdd(A.counters + first, 1u);
-        if (arrived == pieces - 1) {
-          __threadfence();
-          Partial<E, ADD> total = load_cg(carry + first);
-          for (uint32_t p = 1; p < pieces; p++) total = join(total, load_cg(carry + first + p));
+        typename Epi::Pre pre{};
+        if (lane == 0) pre = epi.pre(row);
+        Partial<E, ADD> total = combine_pieces<E, ADD, 1>(carry, first, pieces, 0, lane);
+        if (lane == 0) {
           A.counters[first] = 0;
           E v;
           int32_t s = total.acc.value(&v);
           if (s) raise(err, s, row);
-          epi.row(row, true, v);
+          epi.row(row, true, v, pre);
         }
       }
     }
+    __syncwarp();
+    // Refill this buffer with the unit R ahead.
+    const uint32_t un = u + R * warps;
+    if (un < A.unit_count) {
+      if (lane == 0) {
+        issue_unit(A, ring, b, ahead);
+        if (un + warps < A.unit_count) ahead = A.units[un + warps];
+      }
+      pending |= 1u << b;
+    }
+    __syncwarp();
+    b = b + 1 == R ? 0 : b + 1;
   }
 }
 
@@ -255,9 +398,20 @@ template <class E, int S> struct WriteEpi {
   WriteArgs w;
   E* y;
   DeviceError* err;
-  __device__ void row(uint32_t row, bool present, E t) {
+  // Whether the mask selects the row, and y's old value when it is
+  // accumulated into.
+  struct Pre {
+    bool selected;
+    E old;
+  };
+  __device__ Pre pre(uint32_t row) const {
+    Pre p{mask_selects(w, row), E{}};
+    if (w.accumulate >= 0 && p.selected) p.old = y[row];
+    return p;
+  }
+  __device__ void row(uint32_t row, bool present, E t, const Pre& p) {
     const E identity = Identity<E>::of(semiring_add(S));
-    if (!mask_selects(w, row)) {
+    if (!p.selected) {
       if (w.replace) y[row] = identity;
       return;
     }
@@ -265,7 +419,7 @@ template <class E, int S> struct WriteEpi {
       y[row] = present ? t : identity;
     } else if (present) {
       E out;
-      int32_t s = apply_rt<E>(w.accumulate, y[row], t, &out);
+      int32_t s = apply_rt<E>(w.accumulate, p.old, t, &out);
       if (s) raise(err, s, row);
       else y[row] = out;
     }

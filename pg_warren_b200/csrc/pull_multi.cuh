@@ -109,10 +109,8 @@ __device__ inline void pull_multi(const CsrView<W>& A, const E* __restrict__ X, 
       arrived = __shfl_sync(0xffffffffu, arrived, 0);
       if (arrived == pieces - 1) {
         __threadfence();
+        Partial<E, ADD> total = combine_pieces<E, ADD, P>(carry, first, pieces, c, g);
         if (g == 0) {
-          Partial<E, ADD> total = load_cg(carry + (size_t)first * P + c);
-          for (uint32_t p = 1; p < pieces; p++)
-            total = join(total, load_cg(carry + (size_t)(first + p) * P + c));
           E v;
           int32_t s = total.acc.value(&v);
           if (s) raise(err, s, row);

@@ -187,9 +187,14 @@ struct DeviceError {
 constexpr uint32_t kTileRows = 32;
 constexpr uint32_t kTileEntries = 256;
 constexpr uint32_t kPieceEntries = 256;
+// Tail padding of the device CSR arrays (bulk copies read up to 16-byte
+// boundaries).
+constexpr uint64_t kBulkPad = 16;
 
 struct Unit {
-  uint32_t a, b, c, d;  // tile: rows [a, b), c = 0; piece: row a, entries [b, d), c = 1<<31 | slot
+  // tile: rows [a, b) holding c (<= 256) entries from entry d;
+  // piece: row a, entries [b, d), c = 1<<31 | slot.
+  uint32_t a, b, c, d;
 };
 
 struct Schedule {

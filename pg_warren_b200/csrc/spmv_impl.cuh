@@ -8,11 +8,11 @@
 namespace wc {
 
 template <class E, int S, class W>
-__global__ void __launch_bounds__(kPullThreads)
+__global__ void __launch_bounds__(kPullThreads, 3)
     spmv_pull_kernel(CsrView<W> A, const E* __restrict__ x, WriteEpi<E, S> epi, DeviceError* err) {
   extern __shared__ __align__(16) unsigned char smem[];
-  E* stage = reinterpret_cast<E*>(smem) + (threadIdx.x >> 5) * kTileEntries;
-  pull_units<E, S, W>(A, x, epi, err, stage);
+  PullRing<E, W>* ring = reinterpret_cast<PullRing<E, W>*>(smem) + (threadIdx.x >> 5);
+  pull_units<E, S, W>(A, x, epi, err, ring);
 }
 
 // SpMM, width > 1: a warp per row, each lane folding columns lane, lane+32,
@@ -70,7 +70,10 @@ wc_status launch_one(const PullLaunch& L, const void* x, void* y) {
                L.counters, L.carry};
   if (L.width == 1) {
     WriteEpi<E, S> epi{L.write, static_cast<E*>(y), L.err};
-    size_t smem = kPullWarps * kTileEntries * sizeof(E);
+    constexpr size_t smem = pull_smem_bytes<E, W>();
+    static const cudaError_t attr = cudaFuncSetAttribute(
+        spmv_pull_kernel<E, S, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (attr != cudaSuccess) return cuda_status(attr, L.detail, "product kernel attributes");
     uint32_t blocks = (L.unit_count + kPullWarps - 1) / kPullWarps;
     blocks = blocks < 1 ? 1 : (blocks > L.max_blocks ? L.max_blocks : blocks);
     note_launch(), spmv_pull_kernel<E, S, W><<<blocks, kPullThreads, smem, L.stream>>>(

@@ -56,7 +56,7 @@ static void build_units(uint64_t n, const uint64_t* off, std::vector<Unit>& unit
       entries += d;
       r++;
     }
-    units.push_back(Unit{(uint32_t)start, (uint32_t)r, 0u, 0u});
+    units.push_back(Unit{(uint32_t)start, (uint32_t)r, (uint32_t)entries, (uint32_t)off[start]});
     tiles++;
   }
 }
@@ -66,17 +66,19 @@ static wc_status upload_csr(wc_version* v, DevCsr& d, const uint64_t* off, const
   const uint64_t n = v->n, m = v->m;
   std::vector<uint32_t> off32(n + 1);
   for (uint64_t i = 0; i <= n; i++) off32[i] = (uint32_t)off[i];
-  WC_TRY(d.offsets.alloc(v->budget, (n + 1) * 4, detail));
-  WC_TRY(d.targets.alloc(v->budget, m * 4, detail));
+  // 16 bytes of tail padding on each array: the pull's bulk copies widen
+  // their spans to 16-byte boundaries.
+  WC_TRY(d.offsets.alloc(v->budget, (n + 1) * 4 + kBulkPad, detail));
+  WC_TRY(d.targets.alloc(v->budget, m * 4 + kBulkPad, detail));
   WC_CUDA(cudaMemcpy(d.offsets.ptr, off32.data(), (n + 1) * 4, cudaMemcpyHostToDevice), detail);
   WC_CUDA(cudaMemcpy(d.targets.ptr, tgt, m * 4, cudaMemcpyHostToDevice), detail);
   if (w) {
-    WC_TRY(d.weights.alloc(v->budget, m * 8, detail));
+    WC_TRY(d.weights.alloc(v->budget, m * 8 + kBulkPad, detail));
     WC_CUDA(cudaMemcpy(d.weights.ptr, w, m * 8, cudaMemcpyHostToDevice), detail);
     if (integral) {
       std::vector<int32_t> wi(m);
       for (uint64_t e = 0; e < m; e++) wi[e] = (int32_t)w[e];
-      WC_TRY(d.iweights.alloc(v->budget, m * 4, detail));
+      WC_TRY(d.iweights.alloc(v->budget, m * 4 + kBulkPad, detail));
       WC_CUDA(cudaMemcpy(d.iweights.ptr, wi.data(), m * 4, cudaMemcpyHostToDevice), detail);
     }
   }
