@@ -2,27 +2,39 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-Prints one JSON line (rank 0).  Workload: the directed R-MAT scale-22 graph
-(4,194,304 nodes, edge factor 16, a/b/c/d = .57/.19/.19/.05, seed 1,
+Prints one JSON line (rank 0).
+
+Workload (the batched-traversal configuration): the directed R-MAT scale-22
+graph (4,194,304 nodes, edge factor 16, a/b/c/d = .57/.19/.19/.05, seed 1;
 self-loops and repeats dropped, ids relabelled by sorted random int64
-external ids).  A step is one batch of the hot path over that graph:
+external ids; 65,241,322 stored edges) and 1,024 seeded random sources with
+per-source depth caps drawn from U{1..16}.  A step is one batched BFS of
+the 1,024 sources: one bit-packed boolean SpMM per level in a persistent
+kernel, each pass of sources replayed from a captured CUDA graph
+(wc_bfs_batched).
 
-- batched: 1,024 BFS searches from seeded random sources with per-source
-  depth caps U{1..16}, as one bit-packed boolean SpMM (wc_bfs_batched);
-- plain: the same searches one wc_bfs call each (a sample of them per step,
-  scaled by edges traversed);
-- PageRank: FP64, damping 0.85, tol 1e-10 (stop at delta < live × tol),
-  at most 100 iterations (wc_pagerank).
+- value: aggregate GTEPS over all ranks = Σ over sources of edges_traversed
+  (the out-degree summed over the nodes a push-only BFS from the source
+  expands, as warren-core counts it) ÷ device time (CUDA events on the
+  call's stream, inputs resident in HBM, max over ranks).
+- e2e: the same metric through the public call with host buffers: sources
+  and caps copied from pinned host memory, the 1,024 × n depth matrix and
+  the edge counts copied back to pinned host memory, inside the timed step.
+- roofline: msbfs_level_kernel (one level of a pass = one boolean SpMM
+  iteration over k columns); algorithmic bytes per level 4(n+1) + 4m +
+  n·k·(1/8 + 1/8) (CSC offsets and targets once, the frontier operand read
+  and written once), timed by CUDA events the library records around the
+  level launches on the call's stream during the timed steps.
+- Beside it: the plain per-source GPU BFS (wc_bfs, a sample of the sources),
+  FP64 PageRank (damping 0.85, tol 1e-10 × live nodes, at most 100
+  iterations) in iterations/s with its own roofline, and the CPU baseline:
+  the oracle (warren-core's kernels restated in C++) on the host cores, on a
+  bounded sample of the sources.
 
-`value` is the batched aggregate GTEPS (Σ over sources of the edges a
-push-only BFS from that source traverses, the reference's edges_traversed,
-÷ time) over all ranks; the plain path and PageRank are reported beside it.
-Inputs are device-resident when the timed region starts (`value`); `e2e`
-times the same work through the C ABI from host buffers, copies included.
-The graph (≈1.6 GB of CSR + CSC on the device) is larger than L2 and L2 is
-also flushed between timed steps.  Multi-GPU runs shard the sources across
-ranks (weak scaling, no exchange).  The CPU baseline is the C++ oracle
-(warren-core's kernels restated) on a bounded sample on the host cores.
+Inputs are larger than L2 (CSC 0.28 GB, frontier snapshots ≈ 4.5 GB), and a
+256 MiB buffer is also written between timed steps.  Multi-GPU runs give
+each rank its own 1,024 sources on a replica of the graph: weak scaling, no
+exchange on the data path.
 """
 
 from __future__ import annotations
@@ -41,10 +53,12 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-SCALE = int(os.environ.get("WARREN_BENCH_SCALE", "22"))
+METRIC = "BFS GTEPS & PageRank iters/s, batched vs plain on 1 B200, % HBM roofline"
+SCALE = 22
 WIDTH = 1024
-PLAIN_SAMPLE = 32  # plain-path searches timed per step
+PLAIN_SAMPLE = 32
 SEED = 1
+CPU_BUDGET_S = 12.0
 
 
 def measured_peaks():
@@ -52,16 +66,18 @@ def measured_peaks():
     if os.path.exists(path):
         with open(path) as f:
             p = json.load(f)
-        return float(p.get("hbm_gbs", 6650.0)), "measured"
+        if "hbm_gbs" in p:
+            return float(p["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
 
 
 class Clocks:
-    """nvidia-smi samples during the timed region (SM clock, reasons)."""
+    """nvidia-smi samples of the SM clock and throttle reasons."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, device: int):
         self.device = device
@@ -72,11 +88,12 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.reader = threading.Thread(target=self._read, daemon=True)
             self.reader.start()
-        except (OSError, FileNotFoundError):
+            time.sleep(0.3)
+        except OSError:
             self.proc = None
         return self
 
@@ -95,7 +112,6 @@ class Clocks:
 
     def summary(self):
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
@@ -105,7 +121,7 @@ class Clocks:
                 mx = float(parts[2])
             except ValueError:
                 continue
-            for name, flag in zip(names, parts[5:9]):
+            for name, flag in zip(self.NAMES, parts[5:9]):
                 if flag.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
@@ -114,73 +130,110 @@ class Clocks:
 
 def make_graph():
     import pg_warren_b200 as W
-    g = W.rmat(SCALE, 16, 0.57, 0.19, 0.19, SEED)
-    return g
+    return W.rmat(SCALE, 16, 0.57, 0.19, 0.19, SEED)
 
 
-def sources_and_caps(n, count=WIDTH, seed=SEED):
-    rng = np.random.default_rng(seed)
-    return rng.integers(0, n, count).astype(np.uint64), rng.integers(1, 17, count).astype(np.uint32)
+def sources_and_caps(n, rank=0):
+    rng = np.random.default_rng(SEED + 1000 * rank)
+    return rng.integers(0, n, WIDTH).astype(np.uint64), rng.integers(1, 17, WIDTH).astype(np.uint32)
 
 
-def push_edges(offsets, depth, caps=None):
-    """Edges a push-only BFS traverses: Σ out-degree over expanded nodes
-    (those reached at a depth below the cap)."""
-    deg = np.diff(offsets).astype(np.int64)
-    return deg, None
+def config(n, m, **extra):
+    c = {"workload": f"rmat{SCALE}-batched-bfs-{WIDTH}-sources-caps-U1..16",
+         "scale": SCALE, "edge_factor": 16, "nodes": n, "edges": m, "sources_per_rank": WIDTH,
+         "l2": "inputs larger than L2; 256 MiB buffer written between timed steps"}
+    c.update(extra)
+    return c
 
 
-def oracle_edges(og, sources, caps):
+def cpu_bfs(offsets, targets, sources, caps, budget_s):
+    """The oracle's per-source push BFS (warren-core's LevelSearch restated)
+    on all host threads, over as many of the sources as fit the budget:
+    (GTEPS, sources run, threads, seconds)."""
     import oracle as O
-    _, e = O.bfs_depths(og, sources, caps)
-    return e
+    O.build()
+    og = O.Graph.from_csr(len(offsets) - 1, offsets, targets, reverse=False)
+    threads = int(O.lib().wo_threads())
+    O.bfs_depths(og, sources[:1], caps[:1])  # warm
+    batch = max(1, threads)
+    done, edges, secs = 0, 0, 0.0
+    while done < len(sources) and secs < budget_s:
+        sl = slice(done, min(len(sources), done + batch))
+        t0 = time.perf_counter()
+        _, e = O.bfs_depths(og, sources[sl], caps[sl])
+        secs += time.perf_counter() - t0
+        edges += int(e.sum())
+        done = sl.stop
+    return edges / secs / 1e9, done, threads, secs
 
 
 # --------------------------------------------------------------- reference arm
 
 def reference_arm(args):
-    """warren-core's CPU kernels (the C++ restatement; the Rust crate cannot
-    be built here) on all host threads, on bounded samples of the same
-    workload: each step = BFS searches from a sample of the sources."""
-    import oracle as O
-    O.build()
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
+    """warren-core's CPU path (restated in C++; the Rust crate has no
+    toolchain here) on all host threads; each step a bounded sample of the
+    same 1,024 searches.  Rank 0 only."""
+    if int(os.environ.get("RANK", "0")) != 0:
         return
     g = make_graph()
-    og = O.Graph.from_csr(g.id_space, g.offsets, g.targets, reverse=False)
     src, caps = sources_and_caps(g.id_space)
-    cores = O.lib().wo_threads()
-    sample = max(cores, 8)
+    per_step = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+    import oracle as O
+    O.build()
+    og = O.Graph.from_csr(g.id_space, g.offsets, g.targets, reverse=False)
+    threads = int(O.lib().wo_threads())
+    batch = max(1, threads)
+    pos = 0
+
+    def step():
+        nonlocal pos
+        edges, secs = 0, 0.0
+        while secs < per_step:
+            idx = [(pos + q) % WIDTH for q in range(batch)]
+            pos = (pos + batch) % WIDTH
+            t0 = time.perf_counter()
+            _, e = O.bfs_depths(og, src[idx], caps[idx])
+            secs += time.perf_counter() - t0
+            edges += int(e.sum())
+        return edges, secs
+
     for _ in range(args.warmup):
-        O.bfs_depths(og, src[:2], caps[:2])
-    times, edges = [], []
-    for step in range(args.steps):
-        sl = slice((step * sample) % WIDTH, (step * sample) % WIDTH + sample)
-        t0 = time.perf_counter()
-        _, e = O.bfs_depths(og, src[sl], caps[sl])
-        times.append(time.perf_counter() - t0)
-        edges.append(int(e.sum()))
-    gteps = sum(edges) / sum(times) / 1e9
-    line = {
-        "metric": "BFS GTEPS & PageRank iters/s, batched vs plain on 1 B200, % HBM roofline",
-        "impl": "reference", "value": gteps, "unit": "GTEPS", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"rmat{SCALE}-bfs-{WIDTH}-sources-caps-1..16",
-                   "scale": SCALE, "edge_factor": 16, "sources": WIDTH},
-        "cpu_baseline": {"value": gteps, "unit": "GTEPS", "cores": cores, "kind": "port",
-                         "sample": f"{sample} of the {WIDTH} BFS searches per step"},
+        step()
+    tot_e, tot_s = 0, 0.0
+    for _ in range(args.steps):
+        e, s = step()
+        tot_e += e
+        tot_s += s
+    gteps = tot_e / tot_s / 1e9
+    sample = f"searches from the {WIDTH} sources, {batch} at a time, ≈{per_step:.0f} s per step"
+    print(json.dumps({
+        "metric": METRIC, "impl": "reference", "value": gteps, "unit": "GTEPS",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot_s / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": config(g.id_space, g.edges),
+        "cpu_baseline": {"value": gteps, "unit": "GTEPS", "cores": threads, "kind": "port",
+                         "sample": sample},
         "e2e": {"value": gteps, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line))
+    }))
 
 
 # --------------------------------------------------------------- GPU arm
 
-def flush_l2(torch, buf):
-    buf.add_(1)
+def executed_levels(depth, caps, columns):
+    """Per pass of `columns` sources: the levels whose frontier was
+    non-empty (level L runs when some source with cap > L reached a node at
+    depth L)."""
+    import torch
+    k = depth.shape[0]
+    total = 0
+    for s0 in range(0, k, columns):
+        d = depth[s0:s0 + columns]
+        reached = torch.where(d == 255, torch.zeros_like(d), d).amax(dim=1).to(torch.int64)
+        c = torch.as_tensor(caps[s0:s0 + columns].astype(np.int64), device=d.device)
+        last = torch.minimum(reached, c - 1)
+        total += int(last.max().item()) + 1
+    return total
 
 
 def main():
@@ -195,7 +248,6 @@ def main():
 
     import torch
     import pg_warren_b200 as W
-    from pg_warren_b200 import _abi
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -203,150 +255,170 @@ def main():
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
-        import torch.distributed as dist
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)
+    lib = W.load()
     peak, peak_kind = measured_peaks()
 
-    t0 = time.time()
     g = make_graph()
     n, m = g.id_space, g.edges
     gv = g.upload()
-    setup_s = time.time() - t0
-    src_all, caps_all = sources_and_caps(n)
-    # Weak scaling: each rank takes its own 1,024 sources.
-    src_all, caps_all = sources_and_caps(n, WIDTH, SEED + rank)
+    src, caps = sources_and_caps(n, rank)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def barrier():
-        torch.cuda.synchronize()
+        torch.cuda.synchronize(dev)
         if dist:
             dist.barrier()
 
-    def timed(fn, steps, warmup):
-        for _ in range(warmup):
-            fn()
-        barrier()
-        ms = []
-        for _ in range(steps):
-            flush_l2(torch, flush)
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            fn()
-            b.record(stream)
-            b.synchronize()
-            ms.append(a.elapsed_time(b))
-        barrier()
-        return ms
-
-    def max_over_ranks(x):
+    def reduce(x, op):
         if not dist:
             return x
         t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=op)
         return float(t.item())
 
-    launches = {"count": 0}
-    result = {}
+    # ---- batched: 1,024 searches, device-resident
+    sched = W.autotune(gv, "bfs", WIDTH)
+    columns = sched.columns_per_pass
+    src_d = torch.as_tensor(src.view(np.int64), device=dev)
+    caps_d = torch.as_tensor(caps.view(np.int32), device=dev)
+    depth_d = torch.empty((WIDTH, n), dtype=torch.uint8, device=dev)
+    edges_d = torch.empty(WIDTH, dtype=torch.int64, device=dev)
 
-    # ---- plain path: one wc_bfs per source (device outputs)
-    depth_d = torch.empty(n, dtype=torch.int32, device=dev)
-    via_d = torch.empty(n, dtype=torch.int64, device=dev)
-    plain_edges = []
+    def batched(timing=False):
+        W.bfs_batched(gv, src_d, caps_d, depth_out=depth_d, edges_out=edges_d, stream=stream,
+                      timing=timing)
 
-    def plain_step():
-        e = 0
-        for s, c in zip(src_all[:PLAIN_SAMPLE], caps_all[:PLAIN_SAMPLE]):
-            _, _, st = W.bfs_depths(gv, [int(s)], max_depth=int(c), depth_out=depth_d,
-                                    via_out=via_d)
-            e += st.edges_traversed
-        plain_edges.append(e)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            batched()
+        torch.cuda.synchronize(dev)
+        barrier()
+        level_ms, level_launches = 0.0, 0
+        step_ms = []
+        launches0 = lib.wc_kernel_launches()
+        with Clocks(local) as clocks:
+            for _ in range(args.steps):
+                flush.fill_(1)
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                batched(timing=True)
+                b.record(stream)
+                b.synchronize()
+                step_ms.append(a.elapsed_time(b))
+                ms, nl = gv.timing("level")
+                level_ms += ms
+                level_launches += nl
+        launches = lib.wc_kernel_launches() - launches0
+        barrier()
+    edges_step = int(edges_d.sum().item())
+    total_ms = reduce(sum(step_ms), dist.ReduceOp.MAX if dist else None)
+    edges_all = reduce(float(edges_step), dist.ReduceOp.SUM if dist else None)
+    value = edges_all * args.steps / (total_ms * 1e-3) / 1e9
+    batched_gteps_rank = edges_step * args.steps / (sum(step_ms) * 1e-3) / 1e9
+    levels = executed_levels(depth_d, caps, columns)
+    level_bytes = 4 * (n + 1) + 4 * m + n * columns // 4
+    level_avg_ms = level_ms / (levels * args.steps) if level_ms > 0 else None
+    achieved = level_bytes / (level_avg_ms * 1e-3) / 1e9 if level_avg_ms else None
 
-    ms_plain = timed(plain_step, max(1, args.steps // 2), 1)
-    plain_gteps = plain_edges[-1] / (statistics.median(ms_plain) * 1e-3) / 1e9
-    result["plain_bfs_gteps"] = plain_gteps
+    # ---- plain per-source GPU path, a sample of the same sources
+    dpl = torch.empty(n, dtype=torch.int32, device=dev)
+    vpl = torch.empty(n, dtype=torch.int64, device=dev)
+    for s, c in zip(src[:2], caps[:2]):
+        W.bfs_depths(gv, [int(s)], max_depth=int(c), depth_out=dpl, via_out=vpl)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    plain_edges = 0
+    for s, c in zip(src[:PLAIN_SAMPLE], caps[:PLAIN_SAMPLE]):
+        _, _, st = W.bfs_depths(gv, [int(s)], max_depth=int(c), depth_out=dpl, via_out=vpl)
+        plain_edges += st.edges_traversed
+    torch.cuda.synchronize(dev)
+    plain_gteps = plain_edges / (time.perf_counter() - t0) / 1e9
 
-    # ---- PageRank
+    # ---- PageRank (FP64, uniform), iterations/s
     ranks_d = torch.empty(n, dtype=torch.float64, device=dev)
-    pr_iters = []
+    opts = W.PageRank(0.85, 1e-10, 100)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            W.pagerank(gv, None, opts, out=ranks_d, stream=stream)
+        torch.cuda.synchronize(dev)
+        pr_ms, pr_it, pr_iter_ms = [], 0, 0.0
+        for _ in range(args.steps):
+            flush.fill_(1)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            r = W.pagerank(gv, None, opts, out=ranks_d, stream=stream, timing=True)
+            b.record(stream)
+            b.synchronize()
+            pr_ms.append(a.elapsed_time(b))
+            pr_it = r.iterations
+            pr_iter_ms += gv.timing("iteration")[0]
+    pr_bytes = 4 * (n + 1) + 4 * m + 24 * n
+    pr_kernel_gbs = pr_bytes * pr_it * args.steps / (pr_iter_ms * 1e-3) / 1e9 if pr_iter_ms else 0.0
+    pagerank = {"iterations": pr_it, "ms": statistics.median(pr_ms),
+                "iters_per_s": pr_it / (statistics.median(pr_ms) * 1e-3),
+                "roofline": {"bound": "hbm", "kernel": "pr_iter_kernel",
+                             "achieved": pr_kernel_gbs, "peak": peak, "unit": "GB/s",
+                             "frac": pr_kernel_gbs / peak,
+                             "bytes_per_iteration": pr_bytes}}
 
-    def pr_step():
-        r = W.pagerank(gv, None, W.PageRank(0.85, 1e-10, 100), out=ranks_d, stream=stream)
-        pr_iters.append(r.iterations)
+    # ---- end to end through the public call, host buffers
+    src_h = torch.from_numpy(src.view(np.int64)).pin_memory()
+    caps_h = torch.from_numpy(caps.view(np.int32)).pin_memory()
+    depth_h = torch.empty((WIDTH, n), dtype=torch.uint8, pin_memory=True)
+    edges_h = torch.empty(WIDTH, dtype=torch.int64, pin_memory=True)
+    W.bfs_batched(gv, src_h, caps_h, depth_out=depth_h, edges_out=edges_h, stream=stream)
+    barrier()
+    e2e_s = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        W.bfs_batched(gv, src_h, caps_h, depth_out=depth_h, edges_out=edges_h, stream=stream)
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_total = reduce(sum(e2e_s), dist.ReduceOp.MAX if dist else None)
+    e2e_value = edges_all * args.steps / e2e_total / 1e9
+    assert int(edges_h.sum()) == edges_step, "host and device runs disagree"
 
-    with Clocks(local) as clocks:
-        ms_pr = timed(pr_step, args.steps, args.warmup)
-    it = pr_iters[-1]
-    pr_ms = statistics.median(ms_pr)
-    pr_iters_s = it / (pr_ms * 1e-3)
-    pr_bytes_iter = 4 * (n + 1) + 4 * m + 24 * n
-    result["pagerank"] = {"iterations": it, "ms": pr_ms, "iters_per_s": pr_iters_s,
-                          "gbs": pr_bytes_iter * it / (pr_ms * 1e-3) / 1e9,
-                          "margin": W.api.last_margin(gv)}
-
-    # ---- batched path
-    batched = None
-    try:
-        depth_b = torch.empty((WIDTH, n), dtype=torch.uint8, device=dev)
-        edges_b = torch.empty(WIDTH, dtype=torch.int64, device=dev)
-        sched = W.autotune(gv, "bfs", WIDTH)
-        result["schedule"] = {"columns_per_pass": sched.columns_per_pass,
-                              "blocks_per_sm": sched.blocks_per_sm}
-
-        def batched_step():
-            W.bfs_batched(gv, src_all, caps_all, depth_out=depth_b, edges_out=edges_b)
-
-        with Clocks(local) as clocks_b:
-            ms_b = timed(batched_step, args.steps, args.warmup)
-        total_edges = int(edges_b.sum().item())
-        b_ms = statistics.median(ms_b)
-        batched_gteps = total_edges / (b_ms * 1e-3) / 1e9
-        levels = int(depth_b[depth_b != 255].max().item())
-        b_bytes_level = 4 * (n + 1) + 4 * m + n * WIDTH // 4
-        result["batched"] = {"ms": b_ms, "gteps": batched_gteps, "levels": levels,
-                             "edges": total_edges,
-                             "gbs_dense_operand_bound": levels * b_bytes_level / (b_ms * 1e-3) / 1e9}
-        batched = True
-    except W.api.Unsupported:
-        batched = False
+    # ---- CPU baseline (rank 0, one GPU only)
+    cpu = None
+    if rank == 0 and world == 1:
+        gt, done, threads, secs = cpu_bfs(g.offsets, g.targets, src, caps, CPU_BUDGET_S)
+        cpu = {"value": gt, "unit": "GTEPS", "cores": threads, "kind": "port",
+               "sample": f"{done} of the {WIDTH} searches (push BFS per source, "
+                         f"{threads} threads, {secs:.1f} s)"}
 
     line = {
-        "metric": "BFS GTEPS & PageRank iters/s, batched vs plain on 1 B200, % HBM roofline",
-        "unit": "GTEPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic",
-        "config": {"workload": f"rmat{SCALE}-bfs-{WIDTH}-sources-caps-1..16+pagerank-f64",
-                   "scale": SCALE, "nodes": n, "edges": m, "edge_factor": 16,
-                   "sources_per_rank": WIDTH, "l2": "inputs larger than L2; flushed between steps"},
+        "config": config(n, m, columns_per_pass=columns, blocks_per_sm=sched.blocks_per_sm),
+        "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": WIDTH * 12,
+                "d2h_bytes_per_step": WIDTH * n + WIDTH * 8},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if achieved else None, "traffic": None,
+                     "kernel": "msbfs_level_kernel",
+                     "bytes_per_level": level_bytes, "levels_per_step": levels,
+                     "level_ms_avg": level_avg_ms, "peak_kind": peak_kind},
+        "cpu_baseline": cpu,
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+        "edges_traversed_per_step": edges_step,
+        "batched_gteps_rank0": batched_gteps_rank,
+        "plain_bfs_gteps": plain_gteps,
+        "batched_vs_plain": batched_gteps_rank / plain_gteps,
+        "pagerank_iters_per_s": pagerank["iters_per_s"],
+        "pagerank": pagerank,
     }
-    if not batched:
-        # Headline falls back to the plain path until the batched kernel lands.
-        line["value"] = plain_gteps * world
-        line["ms_per_step"] = statistics.median(ms_plain)
-    else:
-        ms_max = max_over_ranks(result["batched"]["ms"])
-        line["value"] = world * result["batched"]["edges"] / (ms_max * 1e-3) / 1e9
-        line["ms_per_step"] = ms_max
-        line["batched"] = result["batched"]
-        line["batched_vs_plain"] = result["batched"]["gteps"] / plain_gteps
-        line["schedule"] = result["schedule"]
-        clocks = clocks_b
-    line["plain_bfs_gteps"] = plain_gteps
-    line["pagerank_iters_per_s"] = pr_iters_s
-    line["pagerank"] = result["pagerank"]
-    achieved = result["pagerank"]["gbs"]
-    line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                        "frac": achieved / peak, "traffic": None,
-                        "kernel": "pr_iter_kernel (PageRank iteration)",
-                        "peak_kind": peak_kind}
-    line["clocks"] = clocks.summary()
-    line["setup_s"] = setup_s
     if rank == 0:
         print(json.dumps(line))
     if dist:
+        dist.barrier()
         dist.destroy_process_group()
 
 

@@ -272,6 +272,10 @@ def _call(interrupts: Optional[Interrupts] = None, stream=None, flags: int = 0,
     return call, detail
 
 
+CALL_ASYNC = 1
+CALL_TIMING = 2
+
+
 class GraphVersion:
     """A version's device copy: the CSR and reverse CSR of a built version
     (graph/csr/mod.rs:38-237), keyed by (graph, version)."""
@@ -334,6 +338,13 @@ class GraphVersion:
 
     def __del__(self):
         self.release()
+
+    def timing(self, phase: str):
+        """(device ms, kernels launched) of kernel group `phase` ("level",
+        "depth", "iteration") in the last call made with timing=True."""
+        n = C.c_uint32(0)
+        ms = A.load().wc_version_timing(self.handle, phase.encode(), C.byref(n))
+        return ms, n.value
 
 
 # ----------------------------------------------------------------- products
@@ -437,12 +448,12 @@ def _pr_opts(p: PageRank):
 
 
 def pagerank(graph: GraphVersion, tombstones=None, pagerank: PageRank = PageRank(), out=None,
-             interrupts=None, stream=None) -> Ranks:
+             interrupts=None, stream=None, timing=False) -> Ranks:
     """compute/pagerank/mod.rs:96-151; `tombstones` are NodeSet words."""
     o, seed = _pr_opts(pagerank)
     ranks = out if out is not None else np.zeros(graph.id_space, np.float64)
     it = C.c_uint32(0)
-    call, detail = _call(interrupts, stream)
+    call, detail = _call(interrupts, stream, CALL_TIMING if timing else 0)
     _raise(A.load().wc_pagerank(graph.handle, C.byref(call), C.byref(o), _ptr(tombstones),
                                 _ptr(ranks), C.byref(it)), detail)
     return Ranks(ranks, it.value)
@@ -585,15 +596,19 @@ def reachable(graph: GraphVersion, start: int, target: int, max_depth=None,
 # ----------------------------------------------------------------- batched
 
 
-def bfs_batched(graph: GraphVersion, sources, max_depths, depth_out=None, edges_out=None):
+def bfs_batched(graph: GraphVersion, sources, max_depths, depth_out=None, edges_out=None,
+                stream=None, timing=False):
     """`len(sources)` BFS searches as one bit-packed boolean SpMM: depths
-    u8[k, n] (255: not reached within the source's cap)."""
-    src = np.ascontiguousarray(np.asarray(sources, dtype=np.uint64))
-    caps = np.ascontiguousarray(np.asarray(max_depths, dtype=np.uint32))
+    u8[k, n] (255: not reached within the source's cap).  Sources, caps and
+    outputs may be host arrays or device tensors."""
+    src = sources if hasattr(sources, "data_ptr") else np.ascontiguousarray(
+        np.asarray(sources, dtype=np.uint64))
+    caps = max_depths if hasattr(max_depths, "data_ptr") else np.ascontiguousarray(
+        np.asarray(max_depths, dtype=np.uint32))
     k = len(src)
     d = depth_out if depth_out is not None else np.zeros((k, graph.id_space), np.uint8)
     e = edges_out if edges_out is not None else np.zeros(k, np.uint64)
-    call, detail = _call()
+    call, detail = _call(None, stream, CALL_TIMING if timing else 0)
     _raise(A.load().wc_bfs_batched(graph.handle, C.byref(call), _ptr(src), _ptr(caps), k, _ptr(d),
                                    _ptr(e)), detail)
     return d, e

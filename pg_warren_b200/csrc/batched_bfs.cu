@@ -20,6 +20,7 @@
 // wrote.  The pass is therefore a fixed launch sequence, captured once per
 // (version, pass shape) into a CUDA graph and replayed.
 #include <algorithm>
+#include <string>
 
 #include "batched.h"
 #include "operand.h"
@@ -175,27 +176,44 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
       }
     }
     __syncwarp();
-    // Gather the hit rows, G at a time, U deep.
+    // Gather the hit rows.  Lane group g takes the contiguous run of hits
+    // [g·H/G, (g+1)·H/G) in order, U loads in flight; the hits of one row
+    // are consecutive, so they are OR-ed in a register and the row's word
+    // is added to its accumulator once, when the row changes (an atomicOr,
+    // as a row may straddle two groups' runs).  A piece is one row: its
+    // words gather in `racc`.
     uint32_t racc = 0;
-    for (uint32_t h0 = 0; h0 < H; h0 += G * U) {
-      uint32_t val[U];
-      uint32_t rr[U];
+    if (H) {
+      const uint32_t per = (H + G - 1) / G;
+      const uint32_t h_lo = min(H, sub * per), h_hi = min(H, sub * per + per);
+      uint32_t cur = h_lo < h_hi ? sm.hitr[h_lo] : 0u;
+      uint32_t run = 0;
+      for (uint32_t h0 = h_lo; h0 < h_hi; h0 += U) {
+        uint32_t val[U], rr[U];
 #pragma unroll
-      for (int x = 0; x < U; x++) {
-        const uint32_t h = h0 + x * G + sub;
-        val[x] = 0;
-        rr[x] = 0;
-        if (h < H) {
-          val[x] = __ldg(P.Fcur + (size_t)sm.hitj[h] * W + w);
-          rr[x] = sm.hitr[h];
+        for (int x = 0; x < U; x++) {
+          const uint32_t h = h0 + x;
+          val[x] = 0;
+          rr[x] = cur;
+          if (h < h_hi) {
+            val[x] = __ldg(P.Fcur + (size_t)sm.hitj[h] * W + w);
+            rr[x] = sm.hitr[h];
+          }
+        }
+#pragma unroll
+        for (int x = 0; x < U; x++) {
+          if (rr[x] != cur) {
+            if (run & a) atomicOr(&sm.acc[cur * W + w], run & a);
+            run = 0;
+            cur = rr[x];
+          }
+          run |= val[x];
         }
       }
-#pragma unroll
-      for (int x = 0; x < U; x++) {
-        const uint32_t bits = val[x] & a;
-        if (!bits) continue;
-        if (tile) atomicOr(&sm.acc[rr[x] * W + w], bits);
-        else racc |= bits;
+      if (tile) {
+        if (run & a) atomicOr(&sm.acc[cur * W + w], run & a);
+      } else {
+        racc = run & a;
       }
     }
     __syncwarp();
@@ -263,70 +281,101 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
 
 // Depths from the kept frontiers, source-major, and each source's
 // edges_traversed: Σ out-degree over the nodes it reached at a depth below
-// its cap.  A block takes 64 nodes at a time; the depths of all sources of
-// the pass for them are assembled in shared memory ([source][node]) and
-// written out 16 bytes at a time.
+// its cap.  A warp keeps one word w (32 sources) and takes 32 nodes at a
+// time: lane j folds node j's frontier words over the levels into bit planes
+// of the depth (plane b: the sources that reached the node at a level with
+// bit b set), the reached set and the expanded set (reached below the
+// source's cap), and turns them into the node's 32 depth bytes with a
+// multiply that spreads four bits to four bytes.  Through shared memory,
+// lane s then collects source 32w+s's bytes for the 32 nodes and stores
+// them, 32 contiguous bytes; the expanded nodes' out-degrees are summed per
+// source in a register and added to the global count once per warp.
+__device__ inline uint32_t spread4(uint32_t nibble) { return (nibble * 0x00204081u) & 0x01010101u; }
+
 template <int W>
 __global__ void __launch_bounds__(256)
     msbfs_depth_kernel(uint32_t n, uint32_t k, uint32_t levels, const uint32_t* F, uint64_t fstride,
-                       const uint32_t* caps, const uint32_t* off, const uint32_t* counts,
+                       const uint32_t* masks, const uint32_t* off, const uint32_t* counts,
                        uint8_t* depth_out, unsigned long long* edges) {
-  constexpr uint32_t P = 32 * W;
-  constexpr uint32_t T = 64;
-  extern __shared__ __align__(16) unsigned char smem[];
-  uint8_t* tile = smem;                                               // [P][T]
-  uint32_t* esum = reinterpret_cast<uint32_t*>(smem + P * T);          // [P]
-  uint32_t* scap = esum + P;                                           // [P]
-  for (uint32_t s = threadIdx.x; s < P; s += blockDim.x) {
-    esum[s] = 0;
-    scap[s] = s < k ? caps[s] : 0;
-  }
-  const uint32_t tiles = (n + T - 1) / T;
-  for (uint32_t tt = blockIdx.x; tt < tiles; tt += gridDim.x) {
-    const uint32_t i0 = tt * T;
-    __syncthreads();
-    for (uint32_t x = threadIdx.x; x < P * T / 16; x += blockDim.x)
-      reinterpret_cast<uint4*>(tile)[x] = make_uint4(~0u, ~0u, ~0u, ~0u);
-    __syncthreads();
-    for (uint32_t L = 0; L < levels; L++) {
-      // F_L was written only if level L-1 had a frontier to expand.
-      if (L > 0 && counts[L - 1] == 0) break;
-      const uint32_t* FL = F + L * fstride;
-      for (uint32_t x = threadIdx.x; x < T * W; x += blockDim.x) {
-        const uint32_t node = x / W, w = x % W;
-        const uint32_t i = i0 + node;
-        if (i >= n) continue;
-        uint32_t bits = FL[(size_t)i * W + w];
-        if (!bits) continue;
-        const uint32_t deg = __ldg(off + i + 1) - __ldg(off + i);
-        while (bits) {
-          const uint32_t b = __ffs(bits) - 1;
-          bits &= bits - 1;
-          const uint32_t s = 32 * w + b;
-          tile[s * T + node] = (uint8_t)L;
-          if (L < scap[s] && deg) atomicAdd(esum + s, deg);
+  __shared__ uint32_t stage_all[8][32][9];  // per warp: 32 nodes × 8 words (+1 against conflicts)
+  const unsigned lane = threadIdx.x & 31;
+  uint32_t(*stage)[9] = stage_all[threadIdx.x >> 5];
+  // The snapshots written: F_L exists for L < used (F_L is written only if
+  // level L-1 had a frontier to expand).
+  uint32_t used = 1;
+  while (used < levels && counts[used - 1] != 0) used++;
+  const uint32_t nbits = used > 1 ? 32 - __clz(used - 1) : 1;
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t gwarps = (gridDim.x * blockDim.x) >> 5;  // a multiple of W
+  const uint32_t w = gwarp % W;
+  const uint32_t s = 32 * w + lane;
+  const bool aligned = (n & 15u) == 0;
+  unsigned long long esum = 0;
+  for (uint32_t i0 = (gwarp / W) * 32; i0 < n; i0 += (gwarps / W) * 32) {
+    const uint32_t i = i0 + lane;
+    uint32_t plane[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t reached = 0, expanded = 0, deg = 0;
+    if (i < n) {
+      // Eight levels' words requested at once.
+      for (uint32_t L0 = 0; L0 < used; L0 += 8) {
+        uint32_t f[8], m[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const uint32_t L = L0 + q;
+          f[q] = L < used ? F[L * fstride + (size_t)i * W + w] : 0u;
+          m[q] = L < used ? masks[L * W + w] : 0u;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const uint32_t L = L0 + q;
+          reached |= f[q];
+          expanded |= f[q] & m[q];
+#pragma unroll
+          for (int b = 0; b < 8; b++)
+            if ((L >> b) & 1) plane[b] |= f[q];
         }
       }
+      if (expanded) deg = __ldg(off + i + 1) - __ldg(off + i);
     }
-    __syncthreads();
-    // Write the tile: source s's depths for nodes i0 .. i0+63, 16 bytes a
-    // thread.
-    for (uint32_t x = threadIdx.x; x < k * (T / 16); x += blockDim.x) {
-      const uint32_t s = x / (T / 16), q = x % (T / 16);
-      const uint32_t i = i0 + q * 16;
-      uint8_t* dst = depth_out + (size_t)s * n + i;
-      const uint4 val = reinterpret_cast<const uint4*>(tile + s * T)[q];
-      if (i + 16 <= n && (((uintptr_t)dst) & 15) == 0) {
-        *reinterpret_cast<uint4*>(dst) = val;
+#pragma unroll
+    for (int g = 0; g < 8; g++) {
+      uint32_t word = spread4((~reached >> (4 * g)) & 0xFu) * 0xFFu;
+#pragma unroll
+      for (int b = 0; b < 8; b++)
+        if (b < (int)nbits) word |= spread4((plane[b] >> (4 * g)) & 0xFu) << b;
+      stage[lane][g] = word;
+    }
+    __syncwarp();
+    uint32_t out[8];
+    const uint32_t col = lane >> 2, shift = 8 * (lane & 3);
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      uint32_t v = 0;
+#pragma unroll
+      for (int r = 0; r < 4; r++) v |= ((stage[4 * q + r][col] >> shift) & 0xFFu) << (8 * r);
+      out[q] = v;
+    }
+    uint32_t any = __ballot_sync(0xffffffffu, expanded != 0);
+    while (any) {
+      const int j = __ffs(any) - 1;
+      any &= any - 1;
+      const uint32_t x = __shfl_sync(0xffffffffu, expanded, j);
+      const uint32_t d = __shfl_sync(0xffffffffu, deg, j);
+      if ((x >> lane) & 1) esum += d;
+    }
+    __syncwarp();
+    if (s < k) {
+      uint8_t* dst = depth_out + (size_t)s * n + i0;
+      if (aligned && i0 + 32 <= n) {
+        reinterpret_cast<uint4*>(dst)[0] = make_uint4(out[0], out[1], out[2], out[3]);
+        reinterpret_cast<uint4*>(dst)[1] = make_uint4(out[4], out[5], out[6], out[7]);
       } else {
-        const uint8_t* src = reinterpret_cast<const uint8_t*>(&val);
-        for (uint32_t b = 0; b < 16 && i + b < n; b++) dst[b] = src[b];
+        for (uint32_t q = 0; q < 32 && i0 + q < n; q++)
+          dst[q] = (uint8_t)(out[q >> 2] >> (8 * (q & 3)));
       }
     }
   }
-  __syncthreads();
-  for (uint32_t s = threadIdx.x; s < k; s += blockDim.x)
-    if (esum[s]) atomicAdd(edges + s, (unsigned long long)esum[s]);
+  if (s < k && esum) atomicAdd(edges + s, esum);
 }
 
 // One pass of up to 32·W sources.
@@ -369,13 +418,13 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
     note_launch(), msbfs_level_kernel<W><<<grid, 256, level_smem, st>>>(P);
   }
   ctx.phase_end();
-  const size_t smem = 32 * W * 64 + 2 * 32 * W * 4;
-  if (smem > 48 * 1024)
-    WC_CUDA(cudaFuncSetAttribute(msbfs_depth_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem), ctx.detail);
+  // Depths: a warp per (word, 32 nodes); the grid's warp count is a
+  // multiple of W (8 warps a block, and an even block count for W = 16, a
+  // multiple of 4 for W = 32).
+  const uint32_t depth_grid = std::max<uint32_t>(4, max_blocks(4) & ~3u);
   ctx.phase_begin("depth");
-  note_launch(), msbfs_depth_kernel<W><<<max_blocks(2), 256, smem, st>>>(
-      n, k, levels + 1, F, fstride, caps_dev, v->fwd.offsets.as<uint32_t>(), counts, depth_dev,
+  note_launch(), msbfs_depth_kernel<W><<<depth_grid, 256, 0, st>>>(
+      n, k, levels + 1, F, fstride, masks, v->fwd.offsets.as<uint32_t>(), counts, depth_dev,
       edges_dev);
   ctx.phase_end();
   return cuda_status(cudaGetLastError(), ctx.detail, "batched bfs pass");
@@ -436,9 +485,13 @@ wc_status bfs_batched_run(Ctx& ctx, const wc_schedule& sched, const uint64_t* so
     uint32_t levels = 0;
     for (uint32_t s = s0; s < s0 + k; s++) levels = std::max(levels, caps_host[s]);
     levels = std::min<uint32_t>(levels, 254);
-    WC_TRY(pass_for(columns)(ctx, b, sources_dev + s0, caps_dev + s0, k, levels,
-                             depth_dev + (uint64_t)s0 * ctx.v->n, edges_dev + s0,
-                             sched.blocks_per_sm ? sched.blocks_per_sm : 4));
+    const uint32_t bps = sched.blocks_per_sm ? sched.blocks_per_sm : 4;
+    const std::string key = "bfs/" + std::to_string(columns) + "/" + std::to_string(k) + "/" +
+                            std::to_string(levels) + "/" + std::to_string(bps);
+    WC_TRY(ctx.run_captured(key, [&] {
+      return pass_for(columns)(ctx, b, sources_dev + s0, caps_dev + s0, k, levels,
+                               depth_dev + (uint64_t)s0 * ctx.v->n, edges_dev + s0, bps);
+    }));
   }
   return WC_OK;
 }

@@ -12,6 +12,7 @@
 // step after each iteration updates the columns still running on the
 // device, and iterations with no column left return at once.
 #include <algorithm>
+#include <string>
 
 #include "operand.h"
 #include "pagerank.h"
@@ -182,6 +183,18 @@ wc_status mp_pass(Ctx& ctx, const uint64_t* sources, const uint32_t* caps_dev, u
   return cuda_status(cudaGetLastError(), ctx.detail, "batched min-plus pass");
 }
 
+// The pass's scratch, acquired before a pass is captured (a capture may
+// not allocate); mp_pass then finds it in the pool.
+static wc_status mp_reserve(Ctx& ctx, uint32_t P) {
+  wc_version* v = ctx.v;
+  DevBuf* b;
+  WC_TRY(ctx.scratch(POOL_BATCH_0, (uint64_t)v->n * P * 8 * 2, &b));
+  WC_TRY(ctx.scratch(POOL_BATCH_1, 128, &b));
+  return ctx.scratch(POOL_BATCH_2,
+                     (uint64_t)std::max<uint32_t>(v->rev.schedule.slots, 1) * P *
+                         sizeof(Partial<int64_t, WC_OP_MIN>), &b);
+}
+
 typedef wc_status (*MpFn)(Ctx&, const uint64_t*, const uint32_t*, uint32_t, uint32_t, int64_t*,
                           uint32_t*, uint32_t);
 
@@ -321,7 +334,7 @@ __global__ void ppr_member_kernel(const uint64_t* nodes, const uint64_t* offsets
 
 template <int P>
 wc_status ppr_pass(Ctx& ctx, const PageRankRun& base_run, const uint64_t* nodes,
-                   const uint64_t* offsets, const std::vector<double>& shares, uint32_t c0,
+                   const uint64_t* offsets, const double* shares, uint32_t c0,
                    uint32_t k, double* out, uint32_t* iterations_dev, uint32_t blocks_per_sm) {
   wc_version* v = ctx.v;
   const uint32_t n = (uint32_t)v->n;
@@ -347,10 +360,7 @@ wc_status ppr_pass(Ctx& ctx, const PageRankRun& base_run, const uint64_t* nodes,
   s.msg[1] = s.msg[0] + (size_t)n * P;
   s.out = base_run.s.out;
   s.member = memb->as<uint32_t>();
-  double* share_dev = reinterpret_cast<double*>(sc);                // P
-  s.share = share_dev;
-  WC_CUDA(cudaMemcpyAsync(share_dev, shares.data() + c0, k * 8, cudaMemcpyHostToDevice, ctx.stream),
-          ctx.detail);
+  s.share = shares + c0;
   s.tomb = base_run.s.tomb;
   s.start = base_run.s.start;
   s.damping = base_run.s.damping;
@@ -381,9 +391,24 @@ wc_status ppr_pass(Ctx& ctx, const PageRankRun& base_run, const uint64_t* nodes,
   return cuda_status(cudaGetLastError(), ctx.detail, "batched pagerank pass");
 }
 
+// The pass's scratch, acquired before a pass is captured.
+static wc_status ppr_reserve(Ctx& ctx, uint32_t P, uint32_t blocks_per_sm) {
+  wc_version* v = ctx.v;
+  const uint64_t n = v->n;
+  const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(
+      max_blocks((int)blocks_per_sm), (v->rev.schedule.count + 7) / 8));
+  DevBuf* b;
+  WC_TRY(ctx.scratch(POOL_BATCH_0, n * P * 8 * 2, &b));
+  WC_TRY(ctx.scratch(POOL_BATCH_1, n * P * 8 * 2, &b));
+  WC_TRY(ctx.scratch(POOL_BATCH_2, n * 4, &b));
+  WC_TRY(ctx.scratch(POOL_BATCH_3, 4096 + (uint64_t)grid * P * 16 + 64 * P, &b));
+  return ctx.scratch(POOL_BATCH_4,
+                     (uint64_t)std::max<uint32_t>(v->rev.schedule.slots, 1) * P *
+                         sizeof(Partial<double, WC_OP_PLUS>), &b);
+}
+
 typedef wc_status (*PprFn)(Ctx&, const PageRankRun&, const uint64_t*, const uint64_t*,
-                           const std::vector<double>&, uint32_t, uint32_t, double*, uint32_t*,
-                           uint32_t);
+                           const double*, uint32_t, uint32_t, double*, uint32_t*, uint32_t);
 
 static PprFn ppr_for(uint32_t p) {
   switch (p) {
@@ -456,7 +481,10 @@ wc_status tune_ppr(Ctx& ctx, uint32_t width, wc_schedule* best) {
   std::vector<uint64_t> offs(sample + 1);
   for (uint32_t c = 0; c <= sample; c++) offs[c] = c;
   std::vector<double> shares(sample, 1.0);
-  DevBuf *N, *F, *R, *I;
+  DevBuf *N, *F, *R, *I, *SH;
+  WC_TRY(ctx.scratch(POOL_BATCH_11, sample * 8, &SH));
+  WC_CUDA(cudaMemcpyAsync(SH->ptr, shares.data(), sample * 8, cudaMemcpyHostToDevice, ctx.stream),
+          ctx.detail);
   WC_TRY(ctx.scratch(POOL_BATCH_5, sample * 8, &N));
   WC_TRY(ctx.scratch(POOL_BATCH_6, (sample + 1) * 8, &F));
   WC_TRY(ctx.scratch(POOL_BATCH_7, (uint64_t)sample * v->n * 8, &R));
@@ -477,7 +505,7 @@ wc_status tune_ppr(Ctx& ctx, uint32_t width, wc_schedule* best) {
       float ms = 0;
       for (int rep = 0; rep < 2; rep++) {
         WC_CUDA(cudaEventRecord(a, ctx.stream), ctx.detail);
-        WC_TRY(ppr_for(P)(ctx, base, N->as<uint64_t>(), F->as<uint64_t>(), shares, 0, k,
+        WC_TRY(ppr_for(P)(ctx, base, N->as<uint64_t>(), F->as<uint64_t>(), SH->as<double>(), 0, k,
                           R->as<double>(), I->as<uint32_t>(), bps));
         WC_CUDA(cudaEventRecord(b, ctx.stream), ctx.detail);
         WC_CUDA(cudaEventSynchronize(b), ctx.detail);
@@ -527,14 +555,20 @@ wc_status wc_minplus_batched(wc_version* v, const wc_call* call, const uint64_t*
   const auto key = ((uint64_t)WC_BATCH_MINPLUS << 32) | width;
   const wc_schedule sched = v->tuned.count(key) ? v->tuned[key] : wc_schedule{32, 1, 4, 0};
   const uint32_t P = std::max<uint32_t>(1, std::min<uint32_t>(32, sched.columns_per_pass));
+  const uint32_t bps = sched.blocks_per_sm ? sched.blocks_per_sm : 4;
+  WC_TRY(mp_reserve(ctx, P));
   for (uint32_t c0 = 0; c0 < width; c0 += P) {
     const uint32_t k = std::min(P, width - c0);
     uint32_t max_cap = 0;
     for (uint32_t c = c0; c < c0 + k; c++) max_cap = std::max(max_cap, caps[c]);
-    WC_TRY(mp_for(P)(ctx, static_cast<const uint64_t*>(S.dev) + c0,
-                     static_cast<const uint32_t*>(C.dev) + c0, k, max_cap,
-                     static_cast<int64_t*>(D.dev) + (uint64_t)c0 * v->n, its->as<uint32_t>() + c0,
-                     sched.blocks_per_sm ? sched.blocks_per_sm : 4));
+    const std::string gk = "minplus/" + std::to_string(P) + "/" + std::to_string(k) + "/" +
+                           std::to_string(max_cap) + "/" + std::to_string(bps);
+    WC_TRY(ctx.run_captured(gk, [&] {
+      return mp_for(P)(ctx, static_cast<const uint64_t*>(S.dev) + c0,
+                       static_cast<const uint32_t*>(C.dev) + c0, k, max_cap,
+                       static_cast<int64_t*>(D.dev) + (uint64_t)c0 * v->n,
+                       its->as<uint32_t>() + c0, bps);
+    }));
   }
   WC_TRY(D.out(ctx));
   if (iterations_out)
@@ -588,12 +622,22 @@ wc_status wc_ppr_batched(wc_version* v, const wc_call* call, const wc_pagerank_o
   const auto key = ((uint64_t)WC_BATCH_PPR << 32) | width;
   const wc_schedule sched = v->tuned.count(key) ? v->tuned[key] : wc_schedule{4, 1, 4, 0};
   const uint32_t P = std::max<uint32_t>(1, std::min<uint32_t>(32, sched.columns_per_pass));
+  const uint32_t bps = sched.blocks_per_sm ? sched.blocks_per_sm : 4;
+  DevBuf* sh;
+  WC_TRY(ctx.scratch(POOL_BATCH_11, (uint64_t)width * 8, &sh));
+  WC_CUDA(cudaMemcpyAsync(sh->ptr, shares.data(), (uint64_t)width * 8, cudaMemcpyHostToDevice,
+                          ctx.stream), ctx.detail);
+  WC_TRY(ppr_reserve(ctx, P, bps));
   for (uint32_t c0 = 0; c0 < width; c0 += P) {
     const uint32_t k = std::min(P, width - c0);
-    WC_TRY(ppr_for(P)(ctx, base, static_cast<const uint64_t*>(N.dev),
-                      static_cast<const uint64_t*>(F.dev), shares, c0, k,
-                      static_cast<double*>(R.dev) + (uint64_t)c0 * n, its->as<uint32_t>() + c0,
-                      sched.blocks_per_sm ? sched.blocks_per_sm : 4));
+    const std::string gk = "ppr/" + std::to_string(P) + "/" + std::to_string(k) + "/" +
+                           std::to_string(o->max_iter) + "/" + std::to_string(bps);
+    WC_TRY(ctx.run_captured(gk, [&] {
+      return ppr_for(P)(ctx, base, static_cast<const uint64_t*>(N.dev),
+                        static_cast<const uint64_t*>(F.dev), sh->as<double>(), c0, k,
+                        static_cast<double*>(R.dev) + (uint64_t)c0 * n, its->as<uint32_t>() + c0,
+                        bps);
+    }));
   }
   WC_TRY(R.out(ctx));
   if (iterations_out)

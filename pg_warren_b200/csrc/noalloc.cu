@@ -131,6 +131,7 @@ static wc_status static_setup(Ctx& ctx, PageRankRun& run, const wc_pagerank_opts
   s.iterations = reinterpret_cast<uint32_t*>(tail + 8);
   s.done = reinterpret_cast<int32_t*>(tail + 16);
   s.cancel = v->cancel_dev;
+  s.pace = v->pace_dev;
   s.err = v->error.as<DeviceError>();
   // out = plus_first over the forward CSR: each row's out-weight.
   PullLaunch L;

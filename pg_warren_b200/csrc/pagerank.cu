@@ -214,6 +214,12 @@ __global__ void __launch_bounds__(kPullThreads, 3) pr_iter_kernel(CsrView<W> A, 
       raise(s.err, WC_CANCELLED);
       *s.done = 1;
     }
+    // Tell the host how far the solve is, so it stops queueing iterations.
+    if (s.pace) {
+      volatile uint32_t* pace = s.pace;
+      pace[1] = *s.done;
+      pace[0] = it + 1;
+    }
   }
 }
 
@@ -302,6 +308,7 @@ wc_status PageRankRun::setup(Ctx& ctx, const wc_pagerank_opts* o, const uint64_t
   s.iterations = reinterpret_cast<uint32_t*>(tail + 8);
   s.done = reinterpret_cast<int32_t*>(tail + 16);
   s.cancel = v->cancel_dev;
+  s.pace = v->pace_dev;
   s.err = v->error.as<DeviceError>();
   // out = plus_first over the forward CSR: each row's out-weight.
   PullLaunch L;
@@ -328,8 +335,26 @@ wc_status PageRankRun::run(Ctx& ctx) {
   note_launch(), pr_init_kernel<<<grid, kPullThreads, 0, ctx.stream>>>(s);
   PullLaunch L;
   WC_TRY(prepare_pull(ctx, v->rev, WC_PLUS_TIMES, opts.weighted, WC_F64, 1, L));
+  // With a tolerance the solve usually stops well before max_iter: the
+  // host keeps at most kAhead iterations queued beyond the last one the
+  // device reported, and stops queueing once the device reports the stop,
+  // so few launches return at once on the done flag.
+  constexpr uint32_t kAhead = 3;
+  volatile uint32_t* pace = s.pace ? v->pace_host : nullptr;
+  if (pace) {
+    pace[0] = 0;
+    pace[1] = 0;
+  }
   ctx.phase_begin("iteration");
   for (uint32_t it = 0; it < opts.max_iter; it++) {
+    if (pace && s.has_tol) {
+      bool stop = false;
+      while (!(stop = pace[1] != 0) && it >= pace[0] + kAhead) {
+        if (ctx.cancelled() || cudaStreamQuery(ctx.stream) != cudaErrorNotReady) break;
+        std::this_thread::yield();
+      }
+      if (stop) break;
+    }
     if (L.weight_kind == WEIGHTS_F64) WC_TRY(launch_iter<double>(L, s, it, grid));
     else WC_TRY(launch_iter<void>(L, s, it, grid));
   }

@@ -23,6 +23,7 @@ struct PrState {
   uint32_t* iterations;
   int32_t* done;
   const int32_t* cancel;
+  uint32_t* pace;  // host-mapped: [0] iterations done, [1] stopped
   DeviceError* err;
 };
 

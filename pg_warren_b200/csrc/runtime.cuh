@@ -235,6 +235,8 @@ struct wc_version {
   wc::DevBuf error;                    // DeviceError
   int32_t* cancel_host = nullptr;      // pinned, mapped: the device reads it
   int32_t* cancel_dev = nullptr;
+  volatile uint32_t* pace_host = nullptr;  // mapped: [0] iterations done, [1] stopped
+  uint32_t* pace_dev = nullptr;
   std::recursive_mutex mu;             // calls on one handle run one at a time
   double last_margin = 0.0;
   std::map<uint64_t, wc_schedule> tuned;  // (kind << 32 | width) -> schedule
@@ -244,6 +246,9 @@ struct wc_version {
   std::map<int, wc::DevBuf> pool;
   // Kernel-group timings of the last call made with WC_CALL_TIMING.
   std::map<std::string, std::pair<double, uint32_t>> timings;
+  // Executable CUDA graphs of fixed launch sequences, by shape (see
+  // Ctx::run_captured); destroyed with the version.
+  std::map<std::string, cudaGraphExec_t> graphs;
 };
 
 namespace wc {
@@ -273,6 +278,7 @@ struct Ctx {
   uint32_t timeout_ms;
 
   bool timing = false;
+  bool capturing = false;  // the stream is being captured by run_captured
   struct Timer {
     std::string name;
     cudaEvent_t a, b;
@@ -305,15 +311,64 @@ struct Ctx {
     Timer t{name, nullptr, nullptr, g_launches.load()};
     cudaEventCreate(&t.a);
     cudaEventCreate(&t.b);
-    cudaEventRecord(t.a, stream);
+    record(t.a);
     timers.push_back(t);
   }
   void phase_end() {
     if (!timing || timers.empty()) return;
     Timer& t = timers.back();
-    cudaEventRecord(t.b, stream);
+    record(t.b);
     t.launches = g_launches.load() - t.launches;
   }
+  // Inside a capture the record becomes a graph node that still times.
+  void record(cudaEvent_t e) {
+    if (capturing) cudaEventRecordWithFlags(e, stream, cudaEventRecordExternal);
+    else cudaEventRecord(e, stream);
+  }
+
+  // Queues `enqueue`'s launch sequence (which must allocate nothing and
+  // wait for nothing) as a CUDA graph: the sequence is captured from the
+  // stream, the version's executable graph for `key` is updated in place to
+  // it (instantiated the first time, or when the update is refused), and
+  // that graph is launched.  A stream the caller is already capturing gets
+  // the sequence directly, as part of the caller's graph.
+  template <class F> wc_status run_captured(const std::string& key, F&& enqueue) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (!stream || cudaStreamIsCapturing(stream, &cs) != cudaSuccess ||
+        cs != cudaStreamCaptureStatusNone)
+      return enqueue();
+    WC_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), detail);
+    capturing = true;
+    const wc_status st = enqueue();
+    capturing = false;
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ended = cudaStreamEndCapture(stream, &graph);
+    if (st != WC_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+    }
+    if (ended != cudaSuccess) return cuda_status(ended, detail, "cudaStreamEndCapture");
+    cudaGraphExec_t& exec = v->graphs[key];
+    if (exec) {
+      cudaGraphExecUpdateResultInfo info;
+      if (cudaGraphExecUpdate(exec, graph, &info) != cudaSuccess) {
+        (void)cudaGetLastError();
+        cudaGraphExecDestroy(exec);
+        exec = nullptr;
+      }
+    }
+    if (!exec) {
+      const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+      if (e != cudaSuccess) {
+        exec = nullptr;
+        cudaGraphDestroy(graph);
+        return cuda_status(e, detail, "cudaGraphInstantiate");
+      }
+    }
+    cudaGraphDestroy(graph);
+    return cuda_status(cudaGraphLaunch(exec, stream), detail, "cudaGraphLaunch");
+  }
+
   void collect_timings() {
     if (!timing) return;
     v->timings.clear();

@@ -222,9 +222,13 @@ wc_status wc_version_upload(uint64_t graph_id, uint64_t version, const wc_csr_ho
   v->reverse_given = csr->reverse_offsets != nullptr;
   WC_TRY(v->error.alloc(v->budget, sizeof(DeviceError), detail));
   WC_CUDA(cudaMemset(v->error.ptr, 0, sizeof(DeviceError)), detail);
-  WC_CUDA(cudaHostAlloc((void**)&v->cancel_host, sizeof(int32_t), cudaHostAllocMapped), detail);
-  *v->cancel_host = 0;
+  // Four mapped words: the cancel word, then the pacing words (iterations
+  // completed, done) that iterative kernels report to the host.
+  WC_CUDA(cudaHostAlloc((void**)&v->cancel_host, 4 * sizeof(int32_t), cudaHostAllocMapped), detail);
+  for (int q = 0; q < 4; q++) v->cancel_host[q] = 0;
   WC_CUDA(cudaHostGetDevicePointer((void**)&v->cancel_dev, v->cancel_host, 0), detail);
+  v->pace_host = reinterpret_cast<volatile uint32_t*>(v->cancel_host + 1);
+  v->pace_dev = reinterpret_cast<uint32_t*>(v->cancel_dev + 1);
   *out = v.release();
   return WC_OK;
 }
@@ -234,6 +238,8 @@ wc_status wc_version_release(wc_version* v) {
   {
     std::lock_guard<std::recursive_mutex> lock(v->mu);
     if (v->stream) cudaStreamSynchronize(v->stream);
+    for (auto& g : v->graphs)
+      if (g.second) cudaGraphExecDestroy(g.second);
     if (v->cancel_host) cudaFreeHost(v->cancel_host);
     if (v->stream) cudaStreamDestroy(v->stream);
   }
