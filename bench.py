@@ -236,15 +236,286 @@ def executed_levels(depth, caps, columns):
     return total
 
 
+# --------------------------------------------------------------- the suite
+# `python bench.py --suite c1,c2,c3,c4,c5` measures every configuration of
+# the path (one JSON object, legs by name); the default run above is the
+# batched-traversal line alone.
+
+def _events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def leg_c1(W, O, torch, dev, stream, peak):
+    """R-MAT 16: 64 separate BFS (depth cap 8) and FP64 PageRank (tol
+    1e-10), on the GPU and on the oracle, compared."""
+    g = W.rmat(16)
+    n, m = g.id_space, g.edges
+    gv = g.upload()
+    og = O.Graph.from_csr(n, g.offsets, g.targets)
+    rng = np.random.default_rng(SEED)
+    seeds = rng.integers(0, n, 64).astype(np.uint64)
+    caps = np.full(64, 8, np.uint32)
+    O.bfs_depths(og, seeds, caps)
+    t0 = time.perf_counter()
+    depth, edges = O.bfs_depths(og, seeds, caps)
+    cpu_bfs_s = time.perf_counter() - t0
+    dd = torch.empty(n, dtype=torch.int32, device=dev)
+    vv = torch.empty(n, dtype=torch.int64, device=dev)
+    gpu_edges = 0
+    t0 = time.perf_counter()
+    for s in seeds:
+        _, _, st = W.bfs_depths(gv, [int(s)], max_depth=8, depth_out=dd, via_out=vv)
+        gpu_edges += st.edges_traversed
+    torch.cuda.synchronize(dev)
+    gpu_bfs_s = time.perf_counter() - t0
+    exact = True
+    for q, s in enumerate(seeds):
+        W.bfs_depths(gv, [int(s)], max_depth=8, depth_out=dd, via_out=vv)
+        d = dd.cpu().numpy()
+        mine = np.where(d == -1, 255, d).astype(np.int64)
+        exact &= bool(np.array_equal(mine, depth[q].astype(np.int64)))
+    ro, ito = O.pagerank(og, 0.85, 1e-10, 100)[:2]
+    t0 = time.perf_counter()
+    O.pagerank(og, 0.85, 1e-10, 100)
+    cpu_pr_s = time.perf_counter() - t0
+    r = W.pagerank(gv, None, W.PageRank(0.85, 1e-10, 100))
+    reps = 20
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        r = W.pagerank(gv, None, W.PageRank(0.85, 1e-10, 100))
+    gpu_pr_s = (time.perf_counter() - t0) / reps
+    return {"graph": {"scale": 16, "nodes": n, "edges": m},
+            "bfs": {"searches": 64, "max_depth": 8, "gpu_gteps": gpu_edges / gpu_bfs_s / 1e9,
+                    "cpu_gteps": int(edges.sum()) / cpu_bfs_s / 1e9,
+                    "cpu_threads": int(O.lib().wo_threads()),
+                    "depths_equal_oracle": exact,
+                    "edges_equal_oracle": int(edges.sum()) == gpu_edges},
+            "pagerank": {"iterations": r.iterations, "oracle_iterations": int(ito),
+                         "rel_l1_vs_oracle": float(np.abs(r.values - ro).sum() / ro.sum()),
+                         "gpu_ms": gpu_pr_s * 1e3, "cpu_ms": cpu_pr_s * 1e3}}
+
+
+def _spmv_sweep(W, O, torch, dev, stream, peak, g, cpu):
+    n, m = g.id_space, g.edges
+    rng = np.random.default_rng(SEED)
+    out = {}
+    hot = rng.random(n) < 0.01
+    wf = 1.0 - rng.random(m)                         # U(0, 1]
+    wi = rng.integers(1, 101, m).astype(np.float64)  # U{1..100}
+    cases = [("plus_times", wf, 4 * (n + 1) + 12 * m + 16 * n),
+             ("min_plus", wi, 4 * (n + 1) + 8 * m + 8 * n),
+             ("lor_land", None, 4 * (n + 1) + 4 * m + 2 * n)]
+    for sr, w, bytes_it in cases:
+        gv = W.GraphVersion(g.offsets, g.targets, w)
+        if sr == "plus_times":
+            x0 = torch.as_tensor(np.where(hot, 1.0, 0.0), device=dev)
+        elif sr == "min_plus":
+            x0 = torch.as_tensor(np.where(hot, 0, np.iinfo(np.int64).max).astype(np.int64),
+                                 device=dev)
+        else:
+            x0 = torch.as_tensor(hot.astype(np.uint8), device=dev)
+        for transpose in (False, True):
+            prod = W.Product(sr, transpose=transpose)
+            x = x0.clone()
+            y = torch.empty_like(x)
+            for _ in range(3):
+                W.spmv(gv, prod, x, y, stream=stream.cuda_stream, asynchronous=True)
+            torch.cuda.synchronize(dev)
+            x = x0.clone()
+            a, b = _events(torch)
+            a.record(stream)
+            for _ in range(20):
+                W.spmv(gv, prod, x, y, stream=stream.cuda_stream, asynchronous=True)
+                x, y = y, x
+            b.record(stream)
+            b.synchronize()
+            W.load().wc_version_sync(gv.handle, None)
+            ms = a.elapsed_time(b) / 20
+            gbs = bytes_it / (ms * 1e-3) / 1e9
+            out[f"{sr}/{'csc' if transpose else 'csr'}"] = {
+                "us_per_iteration": ms * 1e3, "gbs": gbs, "frac": gbs / peak,
+                "ge_per_s": m / (ms * 1e-3) / 1e9}
+        if cpu:
+            og = O.Graph.from_csr(n, g.offsets, g.targets, w)
+            xs = x0.cpu().numpy()
+            ys = np.empty_like(xs)
+            sid = {"plus_times": 0, "min_plus": 1, "lor_land": 5}[sr]
+            t0 = time.perf_counter()
+            O.product(og, sid, xs, ys, transpose=True)
+            sec = time.perf_counter() - t0
+            out[f"{sr}/cpu"] = {"ge_per_s": m / sec / 1e9, "threads": int(O.lib().wo_threads()),
+                                "sample": "one iteration over the CSC"}
+        del gv
+    return out
+
+
+def leg_c2(W, O, torch, dev, stream, peak):
+    """Semiring SpMV sweep: R-MAT 22 and G(n,m) of the same n and m."""
+    g = W.rmat(22)
+    res = {"rmat22": _spmv_sweep(W, O, torch, dev, stream, peak, g, True)}
+    e = W.gnm(g.id_space, g.edges)
+    res["gnm"] = _spmv_sweep(W, O, torch, dev, stream, peak, e, False)
+    res["graphs"] = {"rmat22": {"nodes": g.id_space, "edges": g.edges},
+                     "gnm": {"nodes": e.id_space, "edges": e.edges}}
+    return res
+
+
+def leg_c3(W, O, torch, dev, stream, peak):
+    """Batched min-plus (1,024 sources, int32 weights 1..100, caps U{1..16})
+    and 256 personalised PageRank seed sets (sizes log-uniform 1..1000)."""
+    g = W.rmat(22)
+    n, m = g.id_space, g.edges
+    rng = np.random.default_rng(SEED)
+    wi = rng.integers(1, 101, m).astype(np.float64)
+    gv = W.GraphVersion(g.offsets, g.targets, wi)
+    src = rng.integers(0, n, 1024).astype(np.uint64)
+    caps = rng.integers(1, 17, 1024).astype(np.uint32)
+    sched = W.autotune(gv, "minplus", 1024)
+    d = torch.empty((1024, n), dtype=torch.int64, device=dev)
+    it = torch.empty(1024, dtype=torch.int32, device=dev)
+    W.minplus_batched(gv, src, caps, dist_out=d, iterations_out=it)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    W.minplus_batched(gv, src, caps, dist_out=d, iterations_out=it)
+    torch.cuda.synchronize(dev)
+    mp_s = time.perf_counter() - t0
+    iters = int(it.sum().item())
+    del d
+    gu = g.upload()
+    sizes = np.exp(rng.uniform(0, np.log(1000), 256)).astype(np.int64)
+    sets = [rng.choice(n, int(s), replace=False) for s in sizes]
+    psched = W.autotune(gu, "ppr", 256)
+    r = torch.empty((256, n), dtype=torch.float64, device=dev)
+    pit = torch.empty(256, dtype=torch.int32, device=dev)
+    W.ppr_batched(gu, sets, W.PageRank(0.85, 1e-10, 100), ranks_out=r, iterations_out=pit)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    W.ppr_batched(gu, sets, W.PageRank(0.85, 1e-10, 100), ranks_out=r, iterations_out=pit)
+    torch.cuda.synchronize(dev)
+    ppr_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for q in range(4):
+        seed = np.zeros(n)
+        seed[sets[q]] = 1.0
+        W.pagerank(gu, None, W.PageRank(0.85, 1e-10, 100, seed=seed))
+    plain_ppr_s = (time.perf_counter() - t0) / 4
+    return {"minplus": {"sources": 1024, "seconds": mp_s, "column_iterations": iters,
+                        "columns_per_pass": sched.columns_per_pass,
+                        "gteps_relaxations": iters * m / mp_s / 1e9},
+            "ppr": {"seed_sets": 256, "seconds": ppr_s, "iterations_max": int(pit.max().item()),
+                    "columns_per_pass": psched.columns_per_pass,
+                    "per_set_ms": ppr_s / 256 * 1e3,
+                    "plain_per_set_ms": plain_ppr_s * 1e3,
+                    "batched_vs_plain": plain_ppr_s * 256 / ppr_s}}
+
+
+def leg_c4(W, O, torch, dev, stream, peak):
+    """Lanczos: R-MAT 20 symmetrised, normalised Laplacian, 16 smallest;
+    then the largest connected component (the full graph deflates)."""
+    from scipy.sparse import csr_matrix
+    from scipy.sparse.csgraph import connected_components
+    g = W.rmat(20, undirected=True)
+    n, m = g.id_space, g.edges
+    gv = g.upload()
+    opts = W.EigenOptions(16, which="smallest", operator="normalized_laplacian", tol=1e-10,
+                          max_iter=200, seed=7)
+    W.eigen(gv, opts)
+    t0 = time.perf_counter()
+    e = W.eigen(gv, opts)
+    full_s = time.perf_counter() - t0
+    rows = np.repeat(np.arange(n), np.diff(g.offsets).astype(np.int64))
+    a = csr_matrix((np.ones(m), (rows, g.targets)), shape=(n, n))
+    _, labels = connected_components(a, directed=False)
+    keep = np.where(labels == np.bincount(labels).argmax())[0]
+    sub = a[keep][:, keep].tocsr()
+    sub.sort_indices()
+    gl = W.GraphVersion(sub.indptr.astype(np.uint64), sub.indices.astype(np.uint32))
+    lopts = W.EigenOptions(16, which="smallest", operator="normalized_laplacian", tol=1e-10,
+                           max_iter=4000, seed=7)
+    W.eigen(gl, lopts)
+    t0 = time.perf_counter()
+    el = W.eigen(gl, lopts)
+    lcc_s = time.perf_counter() - t0
+    return {"graph": {"scale": 20, "nodes": n, "stored_entries": m},
+            "full": {"components": e.components, "exact_zeros": e.exact, "steps": e.iterations,
+                     "seconds": full_s, "max_residual": float(e.residuals.max())},
+            "largest_component": {"nodes": int(len(keep)), "stored_entries": int(sub.nnz),
+                                  "steps": el.iterations, "converged": el.converged,
+                                  "seconds": lcc_s,
+                                  "ms_per_step": lcc_s / max(1, el.iterations) * 1e3,
+                                  "max_residual": float(el.residuals.max()),
+                                  "smallest": [float(v) for v in el.values[:4]]}}
+
+
+def leg_c5(W, O, torch, dev, stream, peak):
+    """PageRank adjoint: R-MAT 22, lognormal(0,1) row-normalised weights,
+    64 losses of 1,000 random targets; central differences on a few edges."""
+    g = W.rmat(22)
+    n, m = g.id_space, g.edges
+    w = W.edge_weights(g, "lognormal")
+    gv = W.GraphVersion(g.offsets, g.targets, w)
+    rng = np.random.default_rng(SEED)
+    losses = [rng.choice(n, 1000, replace=False) for _ in range(64)]
+    pr = W.PageRank(0.85, None, 100)
+    grad = torch.empty((64, m), dtype=torch.float64, device=dev)
+    W.pagerank_adjoint(gv, losses[:1], pr, adjoint_tol=1e-14, grad_out=grad[:1])
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    _, ranks, its = W.pagerank_adjoint(gv, losses, pr, adjoint_tol=1e-14, grad_out=grad)
+    torch.cuda.synchronize(dev)
+    adj_s = time.perf_counter() - t0
+    h = 1e-6
+    checks = []
+    for e in rng.choice(m, 3, replace=False):
+        vals = []
+        for sgn in (1, -1):
+            wp = w.copy()
+            wp[e] += sgn * h
+            r = W.pagerank(W.GraphVersion(g.offsets, g.targets, wp), None, pr)
+            vals.append(r.values[losses[0]].sum())
+        fd = (vals[0] - vals[1]) / (2 * h)
+        gd = float(grad[0, int(e)].item())
+        floor = 1e-16 * vals[0] / h
+        checks.append({"edge": int(e), "fd": fd, "adjoint": gd,
+                       "within": abs(fd - gd) <= 1e-6 * abs(gd) + 4 * floor,
+                       "rel": abs(fd - gd) / max(abs(gd), 1e-300), "fd_floor": floor})
+    return {"graph": {"scale": 22, "nodes": n, "edges": m}, "losses": 64,
+            "targets_per_loss": 1000, "seconds": adj_s, "forward_iterations": int(its[0]),
+            "adjoint_iterations": int(its[1]), "fd_checks": checks}
+
+
+def suite(args):
+    import torch
+    import pg_warren_b200 as W
+    import oracle as O
+    O.build()
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    peak, kind = measured_peaks()
+    legs = {"c1": leg_c1, "c2": leg_c2, "c3": leg_c3, "c4": leg_c4, "c5": leg_c5}
+    out = {"peak_gbs": peak, "peak_kind": kind}
+    for name in args.suite.split(","):
+        t0 = time.time()
+        out[name] = legs[name](W, O, torch, dev, stream, peak)
+        out[name]["wall_s"] = time.time() - t0
+        torch.cuda.empty_cache()
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="warren")
+    ap.add_argument("--suite", default=None,
+                    help="comma-separated configurations to measure instead: c1,c2,c3,c4,c5")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.suite:
+        return suite(args)
 
     import torch
     import pg_warren_b200 as W
