@@ -477,7 +477,7 @@ def leg_c5(W, O, torch, dev, stream, peak):
         gd = float(grad[0, int(e)].item())
         floor = 1e-16 * vals[0] / h
         checks.append({"edge": int(e), "fd": fd, "adjoint": gd,
-                       "within": abs(fd - gd) <= 1e-6 * abs(gd) + 4 * floor,
+                       "within": bool(abs(fd - gd) <= 1e-6 * abs(gd) + 4 * floor),
                        "rel": abs(fd - gd) / max(abs(gd), 1e-300), "fd_floor": floor})
     return {"graph": {"scale": 22, "nodes": n, "edges": m}, "losses": 64,
             "targets_per_loss": 1000, "seconds": adj_s, "forward_iterations": int(its[0]),
@@ -503,6 +503,45 @@ def suite(args):
     print(json.dumps(out))
 
 
+# --------------------------------------------------------------- profiler cases
+# `python bench.py --case batched|spmv --scale S`: one small workload per
+# kernel family, for ncu captures (a few GB on the device at most).
+
+def profile_case(args):
+    import torch
+    import pg_warren_b200 as W
+    g = W.rmat(args.scale)
+    gv = g.upload()
+    n = g.id_space
+    stream = torch.cuda.Stream()
+    if args.case == "batched":
+        # 1,024 sources, caps 16, one pass of 1,024 columns; two calls.
+        rng = np.random.default_rng(SEED)
+        src = torch.as_tensor(rng.integers(0, n, 1024).astype(np.int64), device="cuda")
+        caps = torch.full((1024,), 16, dtype=torch.int32, device="cuda")
+        W.set_schedule(gv, "bfs", 1024, columns_per_pass=1024, blocks_per_sm=8)
+        d = torch.empty((1024, n), dtype=torch.uint8, device="cuda")
+        e = torch.empty(1024, dtype=torch.int64, device="cuda")
+        for _ in range(2):
+            W.bfs_batched(gv, src, caps, depth_out=d, edges_out=e, stream=stream, timing=True)
+            print(json.dumps({"level": gv.timing("level"), "depth": gv.timing("depth")}))
+        torch.cuda.synchronize()
+        print(json.dumps({"case": "batched", "nodes": n, "edges": g.edges,
+                          "edges_traversed": int(e.sum())}))
+    else:
+        # SpMV plus_times (f64, unweighted) over the forward CSR three
+        # times, then a PageRank of three iterations.
+        x = torch.rand(n, dtype=torch.float64, device="cuda")
+        y = torch.zeros(n, dtype=torch.float64, device="cuda")
+        for _ in range(3):
+            W.spmv(gv, W.Product("plus_times"), x, y)
+        out = torch.empty(n, dtype=torch.float64, device="cuda")
+        r = W.pagerank(gv, None, W.PageRank(0.85, None, 3), out=out)
+        torch.cuda.synchronize()
+        print(json.dumps({"case": "spmv", "nodes": n, "edges": g.edges,
+                          "iterations": r.iterations}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -511,11 +550,16 @@ def main():
     ap.add_argument("--impl", default="warren")
     ap.add_argument("--suite", default=None,
                     help="comma-separated configurations to measure instead: c1,c2,c3,c4,c5")
+    ap.add_argument("--case", default=None, choices=["batched", "spmv"],
+                    help="a small workload for profilers instead")
+    ap.add_argument("--scale", type=int, default=20)
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
     if args.suite:
         return suite(args)
+    if args.case:
+        return profile_case(args)
 
     import torch
     import pg_warren_b200 as W
@@ -569,7 +613,7 @@ def main():
             batched()
         torch.cuda.synchronize(dev)
         barrier()
-        level_ms, level_launches = 0.0, 0
+        level_ms, level_launches, depth_ms = 0.0, 0, 0.0
         step_ms = []
         launches0 = lib.wc_kernel_launches()
         with Clocks(local) as clocks:
@@ -585,6 +629,7 @@ def main():
                 ms, nl = gv.timing("level")
                 level_ms += ms
                 level_launches += nl
+                depth_ms += gv.timing("depth")[0]
         launches = lib.wc_kernel_launches() - launches0
         barrier()
     edges_step = int(edges_d.sum().item())
@@ -675,7 +720,9 @@ def main():
                      "frac": achieved / peak if achieved else None, "traffic": None,
                      "kernel": "msbfs_level_kernel",
                      "bytes_per_level": level_bytes, "levels_per_step": levels,
-                     "level_ms_avg": level_avg_ms, "peak_kind": peak_kind},
+                     "level_ms_avg": level_avg_ms, "peak_kind": peak_kind,
+                     "level_ms_per_step": level_ms / args.steps,
+                     "depth_ms_per_step": depth_ms / args.steps},
         "cpu_baseline": cpu,
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),

@@ -236,7 +236,10 @@ class Budget:
     def __del__(self):
         h = getattr(self, "handle", None)
         if h:
-            A.load().wc_budget_destroy(h)
+            try:
+                A.load().wc_budget_destroy(h)
+            except Exception:  # interpreter shutdown
+                pass
             self.handle = None
 
 
@@ -337,7 +340,10 @@ class GraphVersion:
             self.handle = None
 
     def __del__(self):
-        self.release()
+        try:
+            self.release()
+        except Exception:  # interpreter shutdown: the library is already gone
+            pass
 
     def timing(self, phase: str):
         """(device ms, kernels launched) of kernel group `phase` ("level",

@@ -282,68 +282,80 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
 // Depths from the kept frontiers, source-major, and each source's
 // edges_traversed: Σ out-degree over the nodes it reached at a depth below
 // its cap.  A warp keeps one word w (32 sources) and takes 32 nodes at a
-// time: lane j folds node j's frontier words over the levels into bit planes
-// of the depth (plane b: the sources that reached the node at a level with
-// bit b set), the reached set and the expanded set (reached below the
-// source's cap), and turns them into the node's 32 depth bytes with a
-// multiply that spreads four bits to four bytes.  Through shared memory,
-// lane s then collects source 32w+s's bytes for the 32 nodes and stores
-// them, 32 contiguous bytes; the expanded nodes' out-degrees are summed per
-// source in a register and added to the global count once per warp.
+// time: lane j folds node j's frontier words over the levels into NB bit
+// planes of the depth (plane b: the sources that reached the node at a
+// level with bit b set) and the reached set, and turns them into the node's
+// 32 depth bytes with a multiply that spreads four bits to four bytes.
+// Through shared memory, lane s then collects source 32w+s's bytes for the
+// 32 nodes, stores them (32 contiguous bytes), and adds the out-degrees of
+// the nodes whose depth is below the source's cap (four bytes compared at
+// once) to a register sum, added to the global count once per warp.
 __device__ inline uint32_t spread4(uint32_t nibble) { return (nibble * 0x00204081u) & 0x01010101u; }
 
-template <int W>
-__global__ void __launch_bounds__(256)
+template <int W, int NB>
+__global__ void __launch_bounds__(256, 4)
     msbfs_depth_kernel(uint32_t n, uint32_t k, uint32_t levels, const uint32_t* F, uint64_t fstride,
-                       const uint32_t* masks, const uint32_t* off, const uint32_t* counts,
+                       const uint32_t* caps, const uint32_t* off, const uint32_t* counts,
                        uint8_t* depth_out, unsigned long long* edges) {
   __shared__ uint32_t stage_all[8][32][9];  // per warp: 32 nodes × 8 words (+1 against conflicts)
+  __shared__ uint32_t degs_all[8][32];
   const unsigned lane = threadIdx.x & 31;
   uint32_t(*stage)[9] = stage_all[threadIdx.x >> 5];
+  uint32_t* degs = degs_all[threadIdx.x >> 5];
   // The snapshots written: F_L exists for L < used (F_L is written only if
   // level L-1 had a frontier to expand).
   uint32_t used = 1;
   while (used < levels && counts[used - 1] != 0) used++;
-  const uint32_t nbits = used > 1 ? 32 - __clz(used - 1) : 1;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t gwarps = (gridDim.x * blockDim.x) >> 5;  // a multiple of W
   const uint32_t w = gwarp % W;
   const uint32_t s = 32 * w + lane;
+  // Depth bytes below the cap count as expanded; 255 marks "not reached".
+  const uint32_t cap = s < k ? min(caps[s], 255u) : 0u;
+  const uint32_t cap4 = cap * 0x01010101u;
   const bool aligned = (n & 15u) == 0;
   unsigned long long esum = 0;
   for (uint32_t i0 = (gwarp / W) * 32; i0 < n; i0 += (gwarps / W) * 32) {
     const uint32_t i = i0 + lane;
-    uint32_t plane[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    uint32_t reached = 0, expanded = 0, deg = 0;
+    uint32_t plane[NB];
+#pragma unroll
+    for (int b = 0; b < NB; b++) plane[b] = 0;
+    uint32_t reached = 0, deg = 0;
     if (i < n) {
-      // Eight levels' words requested at once.
+      // Eight levels' words requested at once; within a chunk the low three
+      // bits of the level are the position in the chunk.
       for (uint32_t L0 = 0; L0 < used; L0 += 8) {
-        uint32_t f[8], m[8];
+        uint32_t f[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+          f[q] = L0 + q < used ? F[(L0 + q) * fstride + (size_t)i * W + w] : 0u;
+        uint32_t chunk = 0;
 #pragma unroll
         for (int q = 0; q < 8; q++) {
-          const uint32_t L = L0 + q;
-          f[q] = L < used ? F[L * fstride + (size_t)i * W + w] : 0u;
-          m[q] = L < used ? masks[L * W + w] : 0u;
-        }
+          chunk |= f[q];
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
-          const uint32_t L = L0 + q;
-          reached |= f[q];
-          expanded |= f[q] & m[q];
-#pragma unroll
-          for (int b = 0; b < 8; b++)
-            if ((L >> b) & 1) plane[b] |= f[q];
+          for (int b = 0; b < 3 && b < NB; b++)
+            if ((q >> b) & 1) plane[b] |= f[q];
         }
+        reached |= chunk;
+#pragma unroll
+        for (int b = 3; b < NB; b++)
+          if ((L0 >> b) & 1) plane[b] |= chunk;
       }
-      if (expanded) deg = __ldg(off + i + 1) - __ldg(off + i);
+      deg = __ldg(off + i + 1) - __ldg(off + i);
     }
+    degs[lane] = deg;
+    if (reached == 0) {  // no source of the word reached the node
 #pragma unroll
-    for (int g = 0; g < 8; g++) {
-      uint32_t word = spread4((~reached >> (4 * g)) & 0xFu) * 0xFFu;
+      for (int g = 0; g < 8; g++) stage[lane][g] = 0xFFFFFFFFu;
+    } else {
 #pragma unroll
-      for (int b = 0; b < 8; b++)
-        if (b < (int)nbits) word |= spread4((plane[b] >> (4 * g)) & 0xFu) << b;
-      stage[lane][g] = word;
+      for (int g = 0; g < 8; g++) {
+        uint32_t word = spread4((~reached >> (4 * g)) & 0xFu) * 0xFFu;
+#pragma unroll
+        for (int b = 0; b < NB; b++) word |= spread4((plane[b] >> (4 * g)) & 0xFu) << b;
+        stage[lane][g] = word;
+      }
     }
     __syncwarp();
     uint32_t out[8];
@@ -354,14 +366,12 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
       for (int r = 0; r < 4; r++) v |= ((stage[4 * q + r][col] >> shift) & 0xFFu) << (8 * r);
       out[q] = v;
-    }
-    uint32_t any = __ballot_sync(0xffffffffu, expanded != 0);
-    while (any) {
-      const int j = __ffs(any) - 1;
-      any &= any - 1;
-      const uint32_t x = __shfl_sync(0xffffffffu, expanded, j);
-      const uint32_t d = __shfl_sync(0xffffffffu, deg, j);
-      if ((x >> lane) & 1) esum += d;
+      const uint32_t below = __vcmpltu4(v, cap4);
+      if (below) {
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+          if ((below >> (8 * r)) & 1) esum += degs[4 * q + r];
+      }
     }
     __syncwarp();
     if (s < k) {
@@ -423,9 +433,15 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
   // multiple of 4 for W = 32).
   const uint32_t depth_grid = std::max<uint32_t>(4, max_blocks(4) & ~3u);
   ctx.phase_begin("depth");
-  note_launch(), msbfs_depth_kernel<W><<<depth_grid, 256, 0, st>>>(
-      n, k, levels + 1, F, fstride, masks, v->fwd.offsets.as<uint32_t>(), counts, depth_dev,
-      edges_dev);
+  // Depths fit five bit planes up to level 31.
+  if (levels + 1 <= 32)
+    note_launch(), msbfs_depth_kernel<W, 5><<<depth_grid, 256, 0, st>>>(
+        n, k, levels + 1, F, fstride, caps_dev, v->fwd.offsets.as<uint32_t>(), counts, depth_dev,
+        edges_dev);
+  else
+    note_launch(), msbfs_depth_kernel<W, 8><<<depth_grid, 256, 0, st>>>(
+        n, k, levels + 1, F, fstride, caps_dev, v->fwd.offsets.as<uint32_t>(), counts, depth_dev,
+        edges_dev);
   ctx.phase_end();
   return cuda_status(cudaGetLastError(), ctx.detail, "batched bfs pass");
 }
