@@ -30,17 +30,31 @@ namespace wc {
 
 __device__ inline bool nbit(const uint32_t* b, uint32_t i) { return (b[i >> 5] >> (i & 31)) & 1; }
 
-// Seeds: F_0 and V get bit s at node sources[s]; the level masks A_L (bits
-// of sources with cap > L) are built for every level.
+// Zeroes the sources' rows of F_0 (the only rows of F_0 that are read).
+template <int W>
+__global__ void msbfs_clear_kernel(const uint64_t* sources, uint32_t k, uint32_t* F0) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < k) {
+    uint32_t* row = F0 + (size_t)sources[t] * W;
+    for (int w = 0; w < W; w++) row[w] = 0;
+  }
+}
+
+// Seeds: F_0 and V get bit s at node sources[s] (F_0's rows are marked
+// written); every source is live at level 0; the level masks A_L (bits of
+// sources with cap > L) are built for every level.
 template <int W>
 __global__ void msbfs_seed_kernel(const uint64_t* sources, const uint32_t* caps, uint32_t k,
                                   uint32_t levels, uint32_t n, uint32_t* V, uint32_t* F0,
-                                  uint32_t* fbits0, uint32_t* masks, uint32_t* counts) {
+                                  uint32_t* fbits0, uint32_t* wbits0, uint32_t* masks,
+                                  uint32_t* alive0, uint32_t* counts) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < k) {
     const uint32_t node = (uint32_t)sources[t];
     atomicOr(V + (size_t)node * W + (t >> 5), 1u << (t & 31));
     atomicOr(F0 + (size_t)node * W + (t >> 5), 1u << (t & 31));
+    atomicOr(wbits0 + (node >> 5), 1u << (node & 31));
+    atomicOr(alive0 + (t >> 5), 1u << (t & 31));
     if (caps[t] > 0) atomicOr(fbits0 + (node >> 5), 1u << (node & 31));
   }
   // masks[L * W + w]: bit b set if source 32w+b exists and cap > L.
@@ -78,7 +92,9 @@ struct MsLevel {
   uint32_t* Fnext;
   const uint32_t* fbits;
   uint32_t* fbits_next;
+  uint32_t* wbits_next;  // rows of F_{L+1} written (the others are zero)
   const uint32_t* masks;
+  uint32_t* alive;       // [level][W]: sources with a non-empty frontier
   uint32_t L;
   uint32_t* counts;
 };
@@ -101,11 +117,14 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
   const unsigned lane = threadIdx.x & 31;
   const unsigned sub = lane / W, w = lane % W;
   const unsigned gmask = (W == 32) ? 0xffffffffu : (((1u << W) - 1) << (sub * W));
-  const uint32_t a = P.masks[P.L * W + w];
+  // Sources still searching: cap above L and a non-empty frontier.  A row
+  // all of whose such sources have reached it needs nothing this level.
+  const uint32_t a = P.masks[P.L * W + w] & P.alive[P.L * W + w];
   const uint32_t a_next = P.masks[(P.L + 1) * W + w];
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   uint32_t admitted = 0;
+  uint32_t live = 0;  // this warp's fresh bits, for the next level's live set
 
   for (uint32_t u = warp; u < P.unit_count; u += warps) {
     const Unit unit = P.units[u];
@@ -223,14 +242,17 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
         if (x * G >= R) break;
         const uint32_t r = x * G + sub;
         uint32_t fresh = 0;
-        if (r < R) {
-          const uint32_t i = r0 + r;
-          if ((needy >> r) & 1) {
-            fresh = sm.acc[r * W + w] & ~vrow[x];
-            if (fresh) P.V[(size_t)i * W + w] = vrow[x] | fresh;
-          }
-          P.Fnext[(size_t)i * W + w] = fresh;
+        if (r < R && ((needy >> r) & 1)) {
+          fresh = sm.acc[r * W + w] & ~vrow[x];
+          if (fresh) P.V[(size_t)(r0 + r) * W + w] = vrow[x] | fresh;
         }
+        // Only rows with fresh bits are written (and marked so).
+        const bool written = __ballot_sync(0xffffffffu, fresh != 0) & gmask;
+        if (written) {
+          P.Fnext[(size_t)(r0 + r) * W + w] = fresh;
+          if (w == 0) atomicOr(P.wbits_next + ((r0 + r) >> 5), 1u << ((r0 + r) & 31));
+        }
+        live |= fresh;
         const bool expands = __ballot_sync(0xffffffffu, (fresh & a_next) != 0) & gmask;
         if (r < R && expands && w == 0) {
           atomicOr(P.fbits_next + ((r0 + r) >> 5), 1u << ((r0 + r) & 31));
@@ -262,8 +284,12 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
           const uint32_t v = vrow[0];
           fresh = tot & ~v & a;
           if (fresh) P.V[(size_t)row * W + w] = v | fresh;
-          P.Fnext[(size_t)row * W + w] = fresh;
         }
+        if (__ballot_sync(0xffffffffu, fresh != 0)) {
+          if (sub == 0) P.Fnext[(size_t)row * W + w] = fresh;
+          if (lane == 0) atomicOr(P.wbits_next + (row >> 5), 1u << (row & 31));
+        }
+        live |= fresh;
         const bool expands = __ballot_sync(0xffffffffu, sub == 0 && (fresh & a_next) != 0) != 0;
         if (lane == 0) {
           P.counters[first] = 0;
@@ -277,12 +303,16 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
   }
   for (int o = 16; o > 0; o >>= 1) admitted += __shfl_down_sync(0xffffffffu, admitted, o);
   if (lane == 0 && admitted) atomicAdd(P.counts + P.L + 1, admitted);
+#pragma unroll
+  for (uint32_t o = W; o < 32; o <<= 1) live |= __shfl_xor_sync(0xffffffffu, live, o);
+  if (sub == 0 && live) atomicOr(P.alive + (P.L + 1) * W + w, live);
 }
 
 // Depths from the kept frontiers, source-major, and each source's
 // edges_traversed: Σ out-degree over the nodes it reached at a depth below
 // its cap.  A warp keeps one word w (32 sources) and takes 32 nodes at a
-// time: lane j folds node j's frontier words over the levels into NB bit
+// time: lane j folds node j's frontier words (the rows marked written) over
+// the levels into NB bit
 // planes of the depth (plane b: the sources that reached the node at a
 // level with bit b set) and the reached set, and turns them into the node's
 // 32 depth bytes with a multiply that spreads four bits to four bytes.
@@ -295,8 +325,9 @@ __device__ inline uint32_t spread4(uint32_t nibble) { return (nibble * 0x0020408
 template <int W, int NB>
 __global__ void __launch_bounds__(256, 4)
     msbfs_depth_kernel(uint32_t n, uint32_t k, uint32_t levels, const uint32_t* F, uint64_t fstride,
-                       const uint32_t* caps, const uint32_t* off, const uint32_t* counts,
-                       uint8_t* depth_out, unsigned long long* edges) {
+                       const uint32_t* wbits, uint32_t bitmap_words, const uint32_t* caps,
+                       const uint32_t* off, const uint32_t* counts, uint8_t* depth_out,
+                       unsigned long long* edges) {
   __shared__ uint32_t stage_all[8][32][9];  // per warp: 32 nodes × 8 words (+1 against conflicts)
   __shared__ uint32_t degs_all[8][32];
   const unsigned lane = threadIdx.x & 31;
@@ -327,8 +358,13 @@ __global__ void __launch_bounds__(256, 4)
       for (uint32_t L0 = 0; L0 < used; L0 += 8) {
         uint32_t f[8];
 #pragma unroll
-        for (int q = 0; q < 8; q++)
-          f[q] = L0 + q < used ? F[(L0 + q) * fstride + (size_t)i * W + w] : 0u;
+        for (int q = 0; q < 8; q++) {
+          const uint32_t L = L0 + q;
+          // Rows of F_L not marked written are zero.
+          f[q] = L < used && ((wbits[L * bitmap_words + (i >> 5)] >> (i & 31)) & 1)
+                     ? F[L * fstride + (size_t)i * W + w]
+                     : 0u;
+        }
         uint32_t chunk = 0;
 #pragma unroll
         for (int q = 0; q < 8; q++) {
@@ -398,20 +434,25 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
   const uint64_t row_words = (uint64_t)n * W;
   const uint64_t fstride = row_words;
   cudaStream_t st = ctx.stream;
-  // Zero V, F_0, the bitmaps and the counts (rows of later levels are
-  // written whole by the level kernel).
+  // Zero V, the bitmaps, the live sets and the counts, and the sources'
+  // rows of F_0; only rows marked written are read from any F_L.
   WC_CUDA(cudaMemsetAsync(b.V->ptr, 0, row_words * 4, st), ctx.detail);
-  WC_CUDA(cudaMemsetAsync(b.F->ptr, 0, row_words * 4, st), ctx.detail);
   const uint64_t bitmap_words = (n + 31) / 32;
-  WC_CUDA(cudaMemsetAsync(b.bits->ptr, 0, (uint64_t)(levels + 1) * bitmap_words * 4, st), ctx.detail);
+  const uint64_t maps = (uint64_t)(levels + 2) * bitmap_words;
+  WC_CUDA(cudaMemsetAsync(b.bits->ptr, 0, 2 * maps * 4, st), ctx.detail);
   WC_CUDA(cudaMemsetAsync(b.counts->ptr, 0, (levels + 2) * 4, st), ctx.detail);
   uint32_t* V = b.V->as<uint32_t>();
   uint32_t* F = b.F->as<uint32_t>();
-  uint32_t* bits = b.bits->as<uint32_t>();
+  uint32_t* fbits = b.bits->as<uint32_t>();
+  uint32_t* wbits = fbits + maps;
   uint32_t* masks = b.masks->as<uint32_t>();
+  uint32_t* alive = masks + (levels + 2) * W;
   uint32_t* counts = b.counts->as<uint32_t>();
+  WC_CUDA(cudaMemsetAsync(alive, 0, (uint64_t)(levels + 2) * W * 4, st), ctx.detail);
+  note_launch(), msbfs_clear_kernel<W><<<(k + 255) / 256, 256, 0, st>>>(sources_dev, k, F);
   note_launch(), msbfs_seed_kernel<W><<<std::max<uint32_t>(1, (std::max(k, (levels + 1) * W) + 255) / 256), 256, 0,
-                         st>>>(sources_dev, caps_dev, k, levels + 1, n, V, F, bits, masks, counts);
+                         st>>>(sources_dev, caps_dev, k, levels + 1, n, V, F, fbits, wbits, masks,
+                               alive, counts);
   const DevCsr& csc = v->rev;
   const size_t level_smem = 8 * sizeof(MsWarpSmem<W>);
   if (level_smem > 48 * 1024)
@@ -423,8 +464,9 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
   for (uint32_t L = 0; L < levels; L++) {
     MsLevel P{n, csc.offsets.as<uint32_t>(), csc.targets.as<uint32_t>(), csc.schedule.units.as<Unit>(),
               csc.schedule.count, csc.schedule.counters.as<uint32_t>(), b.nacc->as<uint32_t>(), V,
-              F + L * fstride, F + (L + 1) * fstride, bits + L * bitmap_words,
-              bits + (L + 1) * bitmap_words, masks, L, counts};
+              F + L * fstride, F + (L + 1) * fstride, fbits + L * bitmap_words,
+              fbits + (L + 1) * bitmap_words, wbits + (L + 1) * bitmap_words, masks, alive, L,
+              counts};
     note_launch(), msbfs_level_kernel<W><<<grid, 256, level_smem, st>>>(P);
   }
   ctx.phase_end();
@@ -436,12 +478,12 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
   // Depths fit five bit planes up to level 31.
   if (levels + 1 <= 32)
     note_launch(), msbfs_depth_kernel<W, 5><<<depth_grid, 256, 0, st>>>(
-        n, k, levels + 1, F, fstride, caps_dev, v->fwd.offsets.as<uint32_t>(), counts, depth_dev,
-        edges_dev);
+        n, k, levels + 1, F, fstride, wbits, (uint32_t)bitmap_words, caps_dev,
+        v->fwd.offsets.as<uint32_t>(), counts, depth_dev, edges_dev);
   else
     note_launch(), msbfs_depth_kernel<W, 8><<<depth_grid, 256, 0, st>>>(
-        n, k, levels + 1, F, fstride, caps_dev, v->fwd.offsets.as<uint32_t>(), counts, depth_dev,
-        edges_dev);
+        n, k, levels + 1, F, fstride, wbits, (uint32_t)bitmap_words, caps_dev,
+        v->fwd.offsets.as<uint32_t>(), counts, depth_dev, edges_dev);
   ctx.phase_end();
   return cuda_status(cudaGetLastError(), ctx.detail, "batched bfs pass");
 }
@@ -450,8 +492,10 @@ wc_status BatchBuffers::reserve(Ctx& ctx, uint32_t words, uint32_t levels) {
   const uint64_t n = ctx.v->n;
   WC_TRY(ctx.scratch(POOL_BATCH_0, n * words * 4, &V));
   WC_TRY(ctx.scratch(POOL_BATCH_1, n * words * 4 * (uint64_t)(levels + 1), &F));
-  WC_TRY(ctx.scratch(POOL_BATCH_2, ((n + 31) / 32) * 4 * (uint64_t)(levels + 2), &bits));
-  WC_TRY(ctx.scratch(POOL_BATCH_3, (uint64_t)(levels + 2) * words * 4, &masks));
+  // The frontier bitmaps and the written-row bitmaps, per level.
+  WC_TRY(ctx.scratch(POOL_BATCH_2, ((n + 31) / 32) * 4 * (uint64_t)(levels + 2) * 2, &bits));
+  // The level masks and the live sets, per level.
+  WC_TRY(ctx.scratch(POOL_BATCH_3, (uint64_t)(levels + 2) * words * 4 * 2, &masks));
   WC_TRY(ctx.scratch(POOL_BATCH_4, (uint64_t)(levels + 2) * 4, &counts));
   // The long rows' accumulators start zero and are left zero by each level.
   const uint64_t nacc_bytes = (uint64_t)std::max<uint32_t>(ctx.v->rev.schedule.slots, 1) * words * 4;
