@@ -310,118 +310,120 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
 
 // Depths from the kept frontiers, source-major, and each source's
 // edges_traversed: Σ out-degree over the nodes it reached at a depth below
-// its cap.  A warp keeps one word w (32 sources) and takes 32 nodes at a
-// time: lane j folds node j's frontier words (the rows marked written) over
-// the levels into NB bit
-// planes of the depth (plane b: the sources that reached the node at a
-// level with bit b set) and the reached set, and turns them into the node's
-// 32 depth bytes with a multiply that spreads four bits to four bytes.
-// Through shared memory, lane s then collects source 32w+s's bytes for the
-// 32 nodes, stores them (32 contiguous bytes), and adds the out-degrees of
-// the nodes whose depth is below the source's cap (four bytes compared at
-// once) to a register sum, added to the global count once per warp.
+// its cap.  A block takes 32 nodes at a time, all sources of the pass.
+// Phase 1: a thread per (node, word) — the lanes of a warp cover whole node
+// rows, so each level's row is read coalesced (only rows marked written) —
+// folds the node's frontier words into NB bit planes of the depth (plane b:
+// the sources that reached it at a level with bit b set) and the reached
+// set, turns them into 32 depth bytes with a multiply that spreads four bits
+// to four bytes, and scatters them into a shared [source][node] tile (rows
+// of each 32-source block shifted by one word, which keeps the scatter free
+// of bank conflicts).  Phase 2: eight threads a source row store its 32
+// bytes, four each, and add the out-degrees of the nodes whose depth is
+// below the source's cap (four bytes compared at once) to the source's
+// shared sum; the sums go to the global counts once per block.
 __device__ inline uint32_t spread4(uint32_t nibble) { return (nibble * 0x00204081u) & 0x01010101u; }
 
 template <int W, int NB>
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256)
     msbfs_depth_kernel(uint32_t n, uint32_t k, uint32_t levels, const uint32_t* F, uint64_t fstride,
                        const uint32_t* wbits, uint32_t bitmap_words, const uint32_t* caps,
                        const uint32_t* off, const uint32_t* counts, uint8_t* depth_out,
                        unsigned long long* edges) {
-  __shared__ uint32_t stage_all[8][32][9];  // per warp: 32 nodes × 8 words (+1 against conflicts)
-  __shared__ uint32_t degs_all[8][32];
-  const unsigned lane = threadIdx.x & 31;
-  uint32_t(*stage)[9] = stage_all[threadIdx.x >> 5];
-  uint32_t* degs = degs_all[threadIdx.x >> 5];
+  constexpr uint32_t S = 32 * W;  // sources in the pass (k <= S)
+  __shared__ __align__(16) uint32_t tile[S * 8 + W];
+  __shared__ unsigned long long esum[S];
+  __shared__ uint32_t cap4s[S];
+  __shared__ uint32_t degs[32];
+  uint8_t* tbytes = reinterpret_cast<uint8_t*>(tile);
   // The snapshots written: F_L exists for L < used (F_L is written only if
   // level L-1 had a frontier to expand).
   uint32_t used = 1;
   while (used < levels && counts[used - 1] != 0) used++;
-  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t gwarps = (gridDim.x * blockDim.x) >> 5;  // a multiple of W
-  const uint32_t w = gwarp % W;
-  const uint32_t s = 32 * w + lane;
-  // Depth bytes below the cap count as expanded; 255 marks "not reached".
-  const uint32_t cap = s < k ? min(caps[s], 255u) : 0u;
-  const uint32_t cap4 = cap * 0x01010101u;
-  const bool aligned = (n & 15u) == 0;
-  unsigned long long esum = 0;
-  for (uint32_t i0 = (gwarp / W) * 32; i0 < n; i0 += (gwarps / W) * 32) {
-    const uint32_t i = i0 + lane;
-    uint32_t plane[NB];
+  for (uint32_t x = threadIdx.x; x < S; x += blockDim.x) {
+    esum[x] = 0;
+    // Depth bytes below the cap count as expanded; 255 marks "not reached".
+    cap4s[x] = (x < k ? min(caps[x], 255u) : 0u) * 0x01010101u;
+  }
+  const bool aligned = (n & 3u) == 0;
+  const uint32_t tiles = (n + 31) / 32;
+  for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const uint32_t i0 = t * 32;
+    for (uint32_t x = threadIdx.x; x < 32 * W; x += blockDim.x) {
+      const uint32_t j = x / W, w = x % W, i = i0 + j;
+      uint32_t plane[NB];
 #pragma unroll
-    for (int b = 0; b < NB; b++) plane[b] = 0;
-    uint32_t reached = 0, deg = 0;
-    if (i < n) {
-      // Eight levels' words requested at once; within a chunk the low three
-      // bits of the level are the position in the chunk.
-      for (uint32_t L0 = 0; L0 < used; L0 += 8) {
-        uint32_t f[8];
+      for (int b = 0; b < NB; b++) plane[b] = 0;
+      uint32_t reached = 0;
+      if (i < n) {
+        // Eight levels' words requested at once; within a chunk the low
+        // three bits of the level are the position in the chunk.
+        for (uint32_t L0 = 0; L0 < used; L0 += 8) {
+          uint32_t f[8];
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
-          const uint32_t L = L0 + q;
-          // Rows of F_L not marked written are zero.
-          f[q] = L < used && ((wbits[L * bitmap_words + (i >> 5)] >> (i & 31)) & 1)
-                     ? F[L * fstride + (size_t)i * W + w]
-                     : 0u;
+          for (int q = 0; q < 8; q++) {
+            const uint32_t L = L0 + q;
+            f[q] = L < used && ((wbits[L * bitmap_words + (i >> 5)] >> (i & 31)) & 1)
+                       ? F[L * fstride + (size_t)i * W + w]
+                       : 0u;
+          }
+          uint32_t chunk = 0;
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            chunk |= f[q];
+#pragma unroll
+            for (int b = 0; b < 3 && b < NB; b++)
+              if ((q >> b) & 1) plane[b] |= f[q];
+          }
+          reached |= chunk;
+#pragma unroll
+          for (int b = 3; b < NB; b++)
+            if ((L0 >> b) & 1) plane[b] |= chunk;
         }
-        uint32_t chunk = 0;
-#pragma unroll
-        for (int q = 0; q < 8; q++) {
-          chunk |= f[q];
-#pragma unroll
-          for (int b = 0; b < 3 && b < NB; b++)
-            if ((q >> b) & 1) plane[b] |= f[q];
-        }
-        reached |= chunk;
-#pragma unroll
-        for (int b = 3; b < NB; b++)
-          if ((L0 >> b) & 1) plane[b] |= chunk;
       }
-      deg = __ldg(off + i + 1) - __ldg(off + i);
-    }
-    degs[lane] = deg;
-    if (reached == 0) {  // no source of the word reached the node
-#pragma unroll
-      for (int g = 0; g < 8; g++) stage[lane][g] = 0xFFFFFFFFu;
-    } else {
+      if (w == 0) degs[j] = i < n ? __ldg(off + i + 1) - __ldg(off + i) : 0u;
+      // Source 32w + b's byte for node j: row 32w + b of the tile, which
+      // starts at word (32w + b)·8 + w.
+      uint8_t* col = tbytes + ((size_t)(32 * w) * 8 + w) * 4 + j;
 #pragma unroll
       for (int g = 0; g < 8; g++) {
-        uint32_t word = spread4((~reached >> (4 * g)) & 0xFu) * 0xFFu;
+        uint32_t word = 0xFFFFFFFFu;
+        if (reached) {
+          word = spread4((~reached >> (4 * g)) & 0xFu) * 0xFFu;
 #pragma unroll
-        for (int b = 0; b < NB; b++) word |= spread4((plane[b] >> (4 * g)) & 0xFu) << b;
-        stage[lane][g] = word;
+          for (int b = 0; b < NB; b++) word |= spread4((plane[b] >> (4 * g)) & 0xFu) << b;
+        }
+#pragma unroll
+        for (int r = 0; r < 4; r++) col[(4 * g + r) * 32] = (uint8_t)(word >> (8 * r));
       }
     }
-    __syncwarp();
-    uint32_t out[8];
-    const uint32_t col = lane >> 2, shift = 8 * (lane & 3);
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < S * 8; x += blockDim.x) {
+      const uint32_t s = x >> 3, q = x & 7;
+      const uint32_t word = tile[s * 8 + (s >> 5) + q];
+      const uint32_t below = __vcmpltu4(word, cap4s[s]);
+      uint32_t part = 0;
 #pragma unroll
-    for (int q = 0; q < 8; q++) {
-      uint32_t v = 0;
-#pragma unroll
-      for (int r = 0; r < 4; r++) v |= ((stage[4 * q + r][col] >> shift) & 0xFFu) << (8 * r);
-      out[q] = v;
-      const uint32_t below = __vcmpltu4(v, cap4);
-      if (below) {
-#pragma unroll
-        for (int r = 0; r < 4; r++)
-          if ((below >> (8 * r)) & 1) esum += degs[4 * q + r];
+      for (int r = 0; r < 4; r++)
+        if ((below >> (8 * r)) & 1) part += degs[4 * q + r];
+      part += __shfl_xor_sync(0xffffffffu, part, 1);
+      part += __shfl_xor_sync(0xffffffffu, part, 2);
+      part += __shfl_xor_sync(0xffffffffu, part, 4);
+      if (s < k) {
+        if (q == 0) esum[s] += part;
+        const uint32_t node = i0 + 4 * q;
+        uint8_t* dst = depth_out + (size_t)s * n + node;
+        if (aligned && node + 4 <= n) {
+          *reinterpret_cast<uint32_t*>(dst) = word;
+        } else {
+          for (uint32_t r = 0; r < 4 && node + r < n; r++) dst[r] = (uint8_t)(word >> (8 * r));
+        }
       }
     }
-    __syncwarp();
-    if (s < k) {
-      uint8_t* dst = depth_out + (size_t)s * n + i0;
-      if (aligned && i0 + 32 <= n) {
-        reinterpret_cast<uint4*>(dst)[0] = make_uint4(out[0], out[1], out[2], out[3]);
-        reinterpret_cast<uint4*>(dst)[1] = make_uint4(out[4], out[5], out[6], out[7]);
-      } else {
-        for (uint32_t q = 0; q < 32 && i0 + q < n; q++)
-          dst[q] = (uint8_t)(out[q >> 2] >> (8 * (q & 3)));
-      }
-    }
+    __syncthreads();
   }
-  if (s < k && esum) atomicAdd(edges + s, esum);
+  for (uint32_t x = threadIdx.x; x < k; x += blockDim.x)
+    if (esum[x]) atomicAdd(edges + x, esum[x]);
 }
 
 // One pass of up to 32·W sources.
@@ -470,10 +472,8 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
     note_launch(), msbfs_level_kernel<W><<<grid, 256, level_smem, st>>>(P);
   }
   ctx.phase_end();
-  // Depths: a warp per (word, 32 nodes); the grid's warp count is a
-  // multiple of W (8 warps a block, and an even block count for W = 16, a
-  // multiple of 4 for W = 32).
-  const uint32_t depth_grid = std::max<uint32_t>(4, max_blocks(4) & ~3u);
+  // Depths: persistent blocks of 32-node tiles.
+  const uint32_t depth_grid = max_blocks(4);
   ctx.phase_begin("depth");
   // Depths fit five bit planes up to level 31.
   if (levels + 1 <= 32)
