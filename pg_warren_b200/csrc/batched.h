@@ -7,7 +7,7 @@ namespace wc {
 
 struct BatchBuffers {
   DevBuf *V = nullptr, *F = nullptr, *bits = nullptr, *masks = nullptr, *counts = nullptr,
-         *nacc = nullptr;
+         *nacc = nullptr, *acc = nullptr, *touched = nullptr;
   wc_status reserve(Ctx& ctx, uint32_t words, uint32_t levels);
 };
 

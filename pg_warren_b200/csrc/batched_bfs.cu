@@ -47,7 +47,8 @@ template <int W>
 __global__ void msbfs_seed_kernel(const uint64_t* sources, const uint32_t* caps, uint32_t k,
                                   uint32_t levels, uint32_t n, uint32_t* V, uint32_t* F0,
                                   uint32_t* fbits0, uint32_t* wbits0, uint32_t* masks,
-                                  uint32_t* alive0, uint32_t* counts) {
+                                  uint32_t* alive0, uint32_t* counts, const uint32_t* foff,
+                                  unsigned long long* fedges0) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < k) {
     const uint32_t node = (uint32_t)sources[t];
@@ -55,7 +56,10 @@ __global__ void msbfs_seed_kernel(const uint64_t* sources, const uint32_t* caps,
     atomicOr(F0 + (size_t)node * W + (t >> 5), 1u << (t & 31));
     atomicOr(wbits0 + (node >> 5), 1u << (node & 31));
     atomicOr(alive0 + (t >> 5), 1u << (t & 31));
-    if (caps[t] > 0) atomicOr(fbits0 + (node >> 5), 1u << (node & 31));
+    if (caps[t] > 0) {
+      atomicOr(fbits0 + (node >> 5), 1u << (node & 31));
+      atomicAdd(fedges0, (unsigned long long)(foff[node + 1] - foff[node]));
+    }
   }
   // masks[L * W + w]: bit b set if source 32w+b exists and cap > L.
   for (uint32_t x = t; x < levels * W; x += gridDim.x * blockDim.x) {
@@ -97,7 +101,43 @@ struct MsLevel {
   uint32_t* alive;       // [level][W]: sources with a non-empty frontier
   uint32_t L;
   uint32_t* counts;
+  unsigned long long* fedges;  // [level]: out-edges of the rows expanding there
+  const uint32_t* foff;        // the forward CSR (push levels, out-degrees)
+  const uint32_t* ftgt;
+  const Unit* funits;
+  uint32_t funit_count;
+  uint64_t m;
+  uint32_t* acc;      // n × W push accumulators, all zero between levels
+  uint32_t* touched;  // rows with a push accumulator to settle, all zero between levels
 };
+
+// A level pushes (scatters the frontier rows over the forward CSR) while the
+// frontier's out-edges are below m / kPushDivisor, and pulls (gathers over
+// the reverse CSR) otherwise; every kernel of the level reads the same
+// counts, so they agree on the choice.
+constexpr uint64_t kPushDivisor = 32;
+__device__ inline bool level_pushes(const MsLevel& P) {
+  return P.fedges[P.L] * kPushDivisor < P.m;
+}
+
+// A warp's contribution to the next level's counts: rows admitted, their
+// out-edges, and the live sources.
+template <int W>
+__device__ inline void level_totals(const MsLevel& P, uint32_t admitted, unsigned long long fed,
+                                    uint32_t live) {
+  const unsigned lane = threadIdx.x & 31;
+  for (int o = 16; o > 0; o >>= 1) {
+    admitted += __shfl_down_sync(0xffffffffu, admitted, o);
+    fed += __shfl_down_sync(0xffffffffu, fed, o);
+  }
+  if (lane == 0 && admitted) {
+    atomicAdd(P.counts + P.L + 1, admitted);
+    atomicAdd(P.fedges + P.L + 1, fed);
+  }
+#pragma unroll
+  for (uint32_t o = W; o < 32; o <<= 1) live |= __shfl_xor_sync(0xffffffffu, live, o);
+  if (lane < W && live) atomicOr(P.alive + (P.L + 1) * W + lane, live);
+}
 
 template <int W> struct MsWarpSmem {
   uint32_t acc[32 * W];
@@ -109,6 +149,7 @@ template <int W> struct MsWarpSmem {
 template <int W>
 __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
   if (P.counts[P.L] == 0) return;  // nothing expands: F_{L+1} is not read
+  if (level_pushes(P)) return;     // msbfs_push_kernel and msbfs_settle_kernel run it
   constexpr uint32_t G = 32 / W;     // lane groups: rows or hits handled at once
   constexpr int Q = kTileEntries / 32;
   constexpr int U = 8;               // gathers in flight per lane
@@ -124,6 +165,7 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   uint32_t admitted = 0;
+  unsigned long long fed = 0;  // out-edges of the rows admitted
   uint32_t live = 0;  // this warp's fresh bits, for the next level's live set
 
   for (uint32_t u = warp; u < P.unit_count; u += warps) {
@@ -257,6 +299,7 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
         if (r < R && expands && w == 0) {
           atomicOr(P.fbits_next + ((r0 + r) >> 5), 1u << ((r0 + r) & 31));
           admitted++;
+          fed += __ldg(P.foff + r0 + r + 1) - __ldg(P.foff + r0 + r);
         }
       }
       __syncwarp();
@@ -296,16 +339,105 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
           if (expands) {
             atomicOr(P.fbits_next + (row >> 5), 1u << (row & 31));
             admitted++;
+            fed += __ldg(P.foff + row + 1) - __ldg(P.foff + row);
           }
         }
       }
     }
   }
-  for (int o = 16; o > 0; o >>= 1) admitted += __shfl_down_sync(0xffffffffu, admitted, o);
-  if (lane == 0 && admitted) atomicAdd(P.counts + P.L + 1, admitted);
-#pragma unroll
-  for (uint32_t o = W; o < 32; o <<= 1) live |= __shfl_xor_sync(0xffffffffu, live, o);
-  if (sub == 0 && live) atomicOr(P.alive + (P.L + 1) * W + w, live);
+  level_totals<W>(P, admitted, fed, live);
+}
+
+// Push, step 1: the frontier rows' words (masked to the live sources) are
+// OR-ed into the accumulators of their out-neighbours, walking the forward
+// CSR's schedule (a long row's pieces spread over warps); the neighbours
+// are marked touched.  Lane group g of a warp takes entries g, g+G, ... of a
+// row.
+template <int W>
+__global__ void __launch_bounds__(256) msbfs_push_kernel(MsLevel P) {
+  if (P.counts[P.L] == 0 || !level_pushes(P)) return;
+  constexpr uint32_t G = 32 / W;
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned sub = lane / W, w = lane % W;
+  const uint32_t a = P.masks[P.L * W + w] & P.alive[P.L * W + w];
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t u = warp; u < P.funit_count; u += warps) {
+    const Unit unit = P.funits[u];
+    const bool tile = (unit.c >> 31) == 0;
+    const uint32_t r0 = unit.a;
+    const uint32_t R = tile ? unit.b - unit.a : 1;
+    const bool in_frontier = lane < R && nbit(P.fbits, r0 + lane);
+    uint32_t rows = __ballot_sync(0xffffffffu, in_frontier);
+    while (rows) {
+      const uint32_t r = __ffs(rows) - 1;
+      rows &= rows - 1;
+      const uint32_t j = r0 + r;
+      const uint32_t val = P.Fcur[(size_t)j * W + w] & a;
+      if (!__ballot_sync(0xffffffffu, val != 0)) continue;
+      const uint32_t lo = tile ? __ldg(P.foff + j) : unit.b;
+      const uint32_t hi = tile ? __ldg(P.foff + j + 1) : unit.d;
+      for (uint32_t e = lo + sub; e < hi; e += G) {
+        const uint32_t i = __ldg(P.ftgt + e);
+        if (val) atomicOr(P.acc + (size_t)i * W + w, val);
+        if (w == 0 && !nbit(P.touched, i)) atomicOr(P.touched + (i >> 5), 1u << (i & 31));
+      }
+    }
+  }
+}
+
+// Push, step 2: each touched row settles its accumulator as a pulled row
+// does (fresh = acc & ~V), clears the accumulator and its touched bit.
+template <int W>
+__global__ void __launch_bounds__(256) msbfs_settle_kernel(MsLevel P) {
+  if (P.counts[P.L] == 0 || !level_pushes(P)) return;
+  constexpr uint32_t G = 32 / W;
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned sub = lane / W, w = lane % W;
+  const unsigned gmask = (W == 32) ? 0xffffffffu : (((1u << W) - 1) << (sub * W));
+  const uint32_t a_next = P.masks[(P.L + 1) * W + w];
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t words = (P.n + 31) / 32;
+  uint32_t admitted = 0;
+  unsigned long long fed = 0;
+  uint32_t live = 0;
+  for (uint32_t t = warp; t < words; t += warps) {
+    uint32_t bits = P.touched[t];
+    if (!bits) continue;
+    __syncwarp();
+    if (lane == 0) P.touched[t] = 0;
+    while (bits) {
+      // Group g takes the g-th lowest touched row left.
+      uint32_t mine = bits;
+      for (uint32_t q = 0; q < sub; q++) mine &= mine - 1;
+      for (uint32_t q = 0; q < G; q++) bits &= bits - 1;
+      uint32_t fresh = 0;
+      uint32_t i = 0;
+      if (mine) {
+        i = 32 * t + (__ffs(mine) - 1);
+        uint32_t* ap = P.acc + (size_t)i * W + w;
+        const uint32_t got = *ap;
+        if (got) *ap = 0;
+        const uint32_t v = P.V[(size_t)i * W + w];
+        fresh = got & ~v;
+        if (fresh) P.V[(size_t)i * W + w] = v | fresh;
+      }
+      const bool written = __ballot_sync(0xffffffffu, fresh != 0) & gmask;
+      if (mine && written) {
+        P.Fnext[(size_t)i * W + w] = fresh;
+        if (w == 0) atomicOr(P.wbits_next + (i >> 5), 1u << (i & 31));
+      }
+      live |= fresh;
+      const bool expands = __ballot_sync(0xffffffffu, (fresh & a_next) != 0) & gmask;
+      if (mine && expands && w == 0) {
+        atomicOr(P.fbits_next + (i >> 5), 1u << (i & 31));
+        admitted++;
+        fed += __ldg(P.foff + i + 1) - __ldg(P.foff + i);
+      }
+    }
+  }
+  level_totals<W>(P, admitted, fed, live);
 }
 
 // Depths from the kept frontiers, source-major, and each source's
@@ -442,7 +574,7 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
   const uint64_t bitmap_words = (n + 31) / 32;
   const uint64_t maps = (uint64_t)(levels + 2) * bitmap_words;
   WC_CUDA(cudaMemsetAsync(b.bits->ptr, 0, 2 * maps * 4, st), ctx.detail);
-  WC_CUDA(cudaMemsetAsync(b.counts->ptr, 0, (levels + 2) * 4, st), ctx.detail);
+  WC_CUDA(cudaMemsetAsync(b.counts->ptr, 0, (levels + 2) * 16, st), ctx.detail);
   uint32_t* V = b.V->as<uint32_t>();
   uint32_t* F = b.F->as<uint32_t>();
   uint32_t* fbits = b.bits->as<uint32_t>();
@@ -450,11 +582,14 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
   uint32_t* masks = b.masks->as<uint32_t>();
   uint32_t* alive = masks + (levels + 2) * W;
   uint32_t* counts = b.counts->as<uint32_t>();
+  unsigned long long* fedges =
+      reinterpret_cast<unsigned long long*>(b.counts->as<unsigned char>() + (levels + 2) * 8);
+  const uint32_t* foff = v->fwd.offsets.as<uint32_t>();
   WC_CUDA(cudaMemsetAsync(alive, 0, (uint64_t)(levels + 2) * W * 4, st), ctx.detail);
   note_launch(), msbfs_clear_kernel<W><<<(k + 255) / 256, 256, 0, st>>>(sources_dev, k, F);
   note_launch(), msbfs_seed_kernel<W><<<std::max<uint32_t>(1, (std::max(k, (levels + 1) * W) + 255) / 256), 256, 0,
                          st>>>(sources_dev, caps_dev, k, levels + 1, n, V, F, fbits, wbits, masks,
-                               alive, counts);
+                               alive, counts, foff, fedges);
   const DevCsr& csc = v->rev;
   const size_t level_smem = 8 * sizeof(MsWarpSmem<W>);
   if (level_smem > 48 * 1024)
@@ -462,13 +597,23 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
                                  (int)level_smem), ctx.detail);
   const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(
       max_blocks((int)blocks_per_sm), (csc.schedule.count + 7) / 8));
+  const DevCsr& fwd = v->fwd;
+  const uint32_t push_grid = std::max<uint32_t>(1, std::min<uint32_t>(
+      max_blocks(8), (fwd.schedule.count + 7) / 8));
+  const uint32_t settle_grid = std::max<uint32_t>(1, std::min<uint32_t>(
+      max_blocks(8), (uint32_t)((bitmap_words + 7) / 8)));
+  // Each level queues its push (scatter, settle) and its pull; the kernels
+  // that the level's frontier does not call for return at once.
   ctx.phase_begin("level");
   for (uint32_t L = 0; L < levels; L++) {
     MsLevel P{n, csc.offsets.as<uint32_t>(), csc.targets.as<uint32_t>(), csc.schedule.units.as<Unit>(),
               csc.schedule.count, csc.schedule.counters.as<uint32_t>(), b.nacc->as<uint32_t>(), V,
               F + L * fstride, F + (L + 1) * fstride, fbits + L * bitmap_words,
               fbits + (L + 1) * bitmap_words, wbits + (L + 1) * bitmap_words, masks, alive, L,
-              counts};
+              counts, fedges, foff, fwd.targets.as<uint32_t>(), fwd.schedule.units.as<Unit>(),
+              fwd.schedule.count, v->m, b.acc->as<uint32_t>(), b.touched->as<uint32_t>()};
+    note_launch(), msbfs_push_kernel<W><<<push_grid, 256, 0, st>>>(P);
+    note_launch(), msbfs_settle_kernel<W><<<settle_grid, 256, 0, st>>>(P);
     note_launch(), msbfs_level_kernel<W><<<grid, 256, level_smem, st>>>(P);
   }
   ctx.phase_end();
@@ -496,11 +641,23 @@ wc_status BatchBuffers::reserve(Ctx& ctx, uint32_t words, uint32_t levels) {
   WC_TRY(ctx.scratch(POOL_BATCH_2, ((n + 31) / 32) * 4 * (uint64_t)(levels + 2) * 2, &bits));
   // The level masks and the live sets, per level.
   WC_TRY(ctx.scratch(POOL_BATCH_3, (uint64_t)(levels + 2) * words * 4 * 2, &masks));
-  WC_TRY(ctx.scratch(POOL_BATCH_4, (uint64_t)(levels + 2) * 4, &counts));
+  // Per level: the admitted rows (u32) and their out-edges (u64).
+  WC_TRY(ctx.scratch(POOL_BATCH_4, (uint64_t)(levels + 2) * 16, &counts));
+  // The push accumulators and touched rows start zero and are left zero by
+  // each level.
+  {
+    const uint64_t acc_bytes = n * words * 4, touched_bytes = ((n + 31) / 32) * 4;
+    const bool fresh_acc = ctx.v->pool[POOL_MSBFS_ACC].bytes < acc_bytes;
+    WC_TRY(ctx.scratch(POOL_MSBFS_ACC, acc_bytes, &acc));
+    if (fresh_acc) WC_CUDA(cudaMemsetAsync(acc->ptr, 0, acc->bytes, ctx.stream), ctx.detail);
+    const bool fresh_t = ctx.v->pool[POOL_MSBFS_TOUCHED].bytes < touched_bytes;
+    WC_TRY(ctx.scratch(POOL_MSBFS_TOUCHED, touched_bytes, &touched));
+    if (fresh_t) WC_CUDA(cudaMemsetAsync(touched->ptr, 0, touched->bytes, ctx.stream), ctx.detail);
+  }
   // The long rows' accumulators start zero and are left zero by each level.
   const uint64_t nacc_bytes = (uint64_t)std::max<uint32_t>(ctx.v->rev.schedule.slots, 1) * words * 4;
-  const bool fresh = ctx.v->pool[POOL_BATCH_10].bytes < nacc_bytes;
-  WC_TRY(ctx.scratch(POOL_BATCH_10, nacc_bytes, &nacc));
+  const bool fresh = ctx.v->pool[POOL_MSBFS_NACC].bytes < nacc_bytes;
+  WC_TRY(ctx.scratch(POOL_MSBFS_NACC, nacc_bytes, &nacc));
   if (fresh) WC_CUDA(cudaMemsetAsync(nacc->ptr, 0, nacc->bytes, ctx.stream), ctx.detail);
   return WC_OK;
 }

@@ -265,6 +265,10 @@ enum PoolTag {
   POOL_EIG_7, POOL_EIG_8, POOL_EIG_9,
   POOL_ADJ_0 = 80, POOL_ADJ_1, POOL_ADJ_2, POOL_ADJ_3, POOL_ADJ_4, POOL_ADJ_5, POOL_ADJ_6,
   POOL_ADJ_7, POOL_ADJ_8, POOL_ADJ_9,
+  POOL_TOPK_0 = 100, POOL_TOPK_1,
+  // Buffers the batched BFS keeps all-zero between calls; no other role
+  // may share them.
+  POOL_MSBFS_NACC = 110, POOL_MSBFS_ACC, POOL_MSBFS_TOUCHED,
 };
 
 // A call's context: the stream, the caller's detail and cancellation.

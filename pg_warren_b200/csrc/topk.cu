@@ -46,7 +46,7 @@ static wc_status topk_typed(Ctx& ctx, const void* x, const uint64_t* tomb, uint6
   WC_TRY(ctx.scratch(POOL_BATCH_2, n, &live));
   WC_TRY(ctx.scratch(POOL_BATCH_3, (uint64_t)n * 8, &k2));
   WC_TRY(ctx.scratch(POOL_BATCH_4, (uint64_t)n * 4 * 2, &i2));
-  WC_TRY(ctx.scratch(POOL_BATCH_11, 16, &num));
+  WC_TRY(ctx.scratch(POOL_TOPK_0, 16, &num));
   note_launch(), topk_keys_kernel<E><<<max_blocks(4), 256, 0, ctx.stream>>>(
       static_cast<const E*>(x), tomb, n, desc, keys->as<uint64_t>(), ids->as<uint32_t>(),
       live->as<uint8_t>());
@@ -58,7 +58,7 @@ static wc_status topk_typed(Ctx& ctx, const void* x, const uint64_t* tomb, uint6
                                             ids->as<uint32_t>(), i2->as<uint32_t>(), (int)n, 0, 64,
                                             ctx.stream);
   t2 = std::max(t1, t3);
-  WC_TRY(ctx.scratch(POOL_BATCH_10, t2 + 256, &temp));
+  WC_TRY(ctx.scratch(POOL_TOPK_1, t2 + 256, &temp));
   cub::DeviceSelect::Flagged(temp->ptr, t1, keys->as<uint64_t>(), live->as<uint8_t>(),
                              k2->as<uint64_t>(), num->as<int>(), (int)n, ctx.stream);
   cub::DeviceSelect::Flagged(temp->ptr, t1, ids->as<uint32_t>(), live->as<uint8_t>(),

@@ -111,3 +111,37 @@ def test_autotuners_pick_valid_schedules():
     assert s.columns_per_pass in (4, 8, 16, 32)
     s = W.autotune(gv, "ppr", 100)
     assert s.columns_per_pass in (1, 2, 4, 8, 16, 32)
+
+
+@pytest.mark.parametrize("count", [1, 8, 600])
+def test_bfs_batched_push_and_pull_levels_agree(count):
+    # Few sources keep the early frontiers under the push threshold (the
+    # levels scatter over the forward CSR); many reach the pull levels.  A
+    # graph with hubs and a repeated call check the accumulators are left
+    # clear between levels and calls.
+    g, og, gv = graph(13, seed=4)
+    rng = np.random.default_rng(count)
+    src = rng.integers(0, g.id_space, count).astype(np.uint64)
+    caps = rng.integers(1, 17, count).astype(np.uint32)
+    do, eo = O.bfs_depths(og, src, caps)
+    for _ in range(2):
+        d, e = W.bfs_batched(gv, src, caps)
+        assert np.array_equal(d, do)
+        assert np.array_equal(e, eo)
+
+
+def test_bfs_batched_after_other_calls_on_the_version():
+    # Scratch that the batched search keeps zero between calls is not
+    # shared with other calls' scratch (top_k, the batched searches of
+    # other kinds).
+    g, og, gv = graph(12, seed=6)
+    rng = np.random.default_rng(8)
+    src = rng.integers(0, g.id_space, 200).astype(np.uint64)
+    caps = rng.integers(1, 17, 200).astype(np.uint32)
+    do, eo = O.bfs_depths(og, src, caps)
+    W.bfs_batched(gv, src, caps)
+    W.top_k(gv, rng.random(g.id_space), 50)
+    W.minplus_batched(gv, src[:40], caps[:40])
+    d, e = W.bfs_batched(gv, src, caps)
+    assert np.array_equal(d, do)
+    assert np.array_equal(e, eo)
