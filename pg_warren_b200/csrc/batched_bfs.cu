@@ -146,50 +146,115 @@ template <int W> struct MsWarpSmem {
   uint8_t rowof[kTileEntries];  // the tile row of each entry
 };
 
+// A lane's VEC consecutive words of a row, moved with one vector access.
+template <int N> struct Words {
+  uint32_t x[N];
+};
+template <int N> __device__ inline Words<N> load_words(const uint32_t* p) {
+  Words<N> r;
+  if constexpr (N == 4) {
+    const uint4 v = *reinterpret_cast<const uint4*>(p);
+    r.x[0] = v.x; r.x[1] = v.y; r.x[2] = v.z; r.x[3] = v.w;
+  } else if constexpr (N == 2) {
+    const uint2 v = *reinterpret_cast<const uint2*>(p);
+    r.x[0] = v.x; r.x[1] = v.y;
+  } else {
+    r.x[0] = *p;
+  }
+  return r;
+}
+template <int N> __device__ inline Words<N> ldg_words(const uint32_t* p) {
+  Words<N> r;
+  if constexpr (N == 4) {
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(p));
+    r.x[0] = v.x; r.x[1] = v.y; r.x[2] = v.z; r.x[3] = v.w;
+  } else if constexpr (N == 2) {
+    const uint2 v = __ldg(reinterpret_cast<const uint2*>(p));
+    r.x[0] = v.x; r.x[1] = v.y;
+  } else {
+    r.x[0] = __ldg(p);
+  }
+  return r;
+}
+template <int N> __device__ inline void store_words(uint32_t* p, const Words<N>& r) {
+  if constexpr (N == 4) *reinterpret_cast<uint4*>(p) = make_uint4(r.x[0], r.x[1], r.x[2], r.x[3]);
+  else if constexpr (N == 2) *reinterpret_cast<uint2*>(p) = make_uint2(r.x[0], r.x[1]);
+  else *p = r.x[0];
+}
+template <int N> __device__ inline bool any_words(const Words<N>& r) {
+  uint32_t o = 0;
+#pragma unroll
+  for (int i = 0; i < N; i++) o |= r.x[i];
+  return o != 0;
+}
+
+// The pull of one level.  A row's W words are spread over LPR = W/VEC
+// lanes holding VEC words each (one 16-byte access for W >= 4), so a warp
+// instruction covers G = 32/LPR rows or gathered frontier rows.
 template <int W>
 __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
   if (P.counts[P.L] == 0) return;  // nothing expands: F_{L+1} is not read
   if (level_pushes(P)) return;     // msbfs_push_kernel and msbfs_settle_kernel run it
-  constexpr uint32_t G = 32 / W;     // lane groups: rows or hits handled at once
+  constexpr uint32_t VEC = W >= 4 ? 4 : W;
+  constexpr uint32_t LPR = W / VEC;
+  constexpr uint32_t G = 32 / LPR;
+  constexpr uint32_t GM = LPR == 32 ? 0xffffffffu : (1u << LPR) - 1;
   constexpr int Q = kTileEntries / 32;
-  constexpr int U = 8;               // gathers in flight per lane
+  constexpr int U = 4;  // frontier rows in flight per lane
+  using V4 = Words<VEC>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   MsWarpSmem<W>& sm = reinterpret_cast<MsWarpSmem<W>*>(smem_raw)[threadIdx.x >> 5];
   const unsigned lane = threadIdx.x & 31;
-  const unsigned sub = lane / W, w = lane % W;
-  const unsigned gmask = (W == 32) ? 0xffffffffu : (((1u << W) - 1) << (sub * W));
+  const unsigned sub = lane / LPR, q = lane % LPR;
+  const uint32_t w0 = q * VEC;
+  const unsigned gmask = GM << (sub * LPR);
   // Sources still searching: cap above L and a non-empty frontier.  A row
   // all of whose such sources have reached it needs nothing this level.
-  const uint32_t a = P.masks[P.L * W + w] & P.alive[P.L * W + w];
-  const uint32_t a_next = P.masks[(P.L + 1) * W + w];
+  V4 a = load_words<VEC>(P.masks + P.L * W + w0);
+  {
+    const V4 alive = load_words<VEC>(P.alive + P.L * W + w0);
+#pragma unroll
+    for (int i = 0; i < (int)VEC; i++) a.x[i] &= alive.x[i];
+  }
+  const V4 a_next = load_words<VEC>(P.masks + (P.L + 1) * W + w0);
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   uint32_t admitted = 0;
   unsigned long long fed = 0;  // out-edges of the rows admitted
-  uint32_t live = 0;  // this warp's fresh bits, for the next level's live set
+  V4 live = {};                // this warp's fresh bits, for the next level's live set
 
   for (uint32_t u = warp; u < P.unit_count; u += warps) {
     const Unit unit = P.units[u];
     const bool tile = (unit.c >> 31) == 0;
     const uint32_t r0 = unit.a;
     const uint32_t R = tile ? unit.b - unit.a : 1;
-    // Which rows still lack an active source: the rows' V words are all
+    // Which rows still lack a searching source: the rows' V words are all
     // loaded first (kept for the write at the end), then tested.
-    constexpr uint32_t VR = kTileRows / G;
-    uint32_t vrow[VR];
+    constexpr uint32_t VR = kTileRows / G > 0 ? kTileRows / G : 1;
+    V4 vrow[VR];
 #pragma unroll
     for (uint32_t x = 0; x < VR; x++) {
       const uint32_t r = x * G + sub;
-      vrow[x] = r < R ? P.V[(size_t)(r0 + r) * W + w] : 0xffffffffu;
+      if (r < R) vrow[x] = load_words<VEC>(P.V + (size_t)(r0 + r) * W + w0);
+      else
+#pragma unroll
+        for (int i = 0; i < (int)VEC; i++) vrow[x].x[i] = 0xffffffffu;
     }
     uint32_t needy = 0;
 #pragma unroll
     for (uint32_t x = 0; x < VR; x++) {
       if (x * G >= R) break;
-      const uint32_t gb = __ballot_sync(0xffffffffu, (~vrow[x] & a) != 0);
+      bool nd = false;
 #pragma unroll
-      for (uint32_t g = 0; g < G; g++)
-        if ((gb >> (g * W)) & (W == 32 ? 0xffffffffu : ((1u << W) - 1))) needy |= 1u << (x * G + g);
+      for (int i = 0; i < (int)VEC; i++) nd |= (~vrow[x].x[i] & a.x[i]) != 0;
+      const uint32_t gb = __ballot_sync(0xffffffffu, nd);
+      if constexpr (LPR == 1) {
+        needy |= gb << (x * G);
+      } else {
+#pragma unroll
+        for (uint32_t g = 0; g < G; g++)
+          if ((gb >> (g * LPR)) & GM) needy |= 1u << (x * G + g);
+      }
     }
     needy &= R == 32 ? 0xffffffffu : ((1u << R) - 1);
     uint32_t base, count;
@@ -199,12 +264,12 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
         lo = __ldg(P.off + r0 + lane);
         hi = __ldg(P.off + r0 + lane + 1);
       }
-      base = __shfl_sync(0xffffffffu, lo, 0);
-      const uint32_t end = __shfl_sync(0xffffffffu, hi, R - 1);
-      count = end - base;
+      base = unit.d;
+      count = unit.c;
       if (needy)
         for (uint32_t k = lo - base; k < hi - base; k++) sm.rowof[k] = (uint8_t)lane;
-      for (uint32_t x = lane; x < R * W; x += 32) sm.acc[x] = 0;
+      for (uint32_t x = lane * 4; x < R * W; x += 128)
+        *reinterpret_cast<uint4*>(&sm.acc[x]) = make_uint4(0, 0, 0, 0);
     } else {
       base = unit.b;
       count = unit.d - unit.b;
@@ -215,22 +280,22 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
     if (needy) {
       uint32_t jv[Q];
 #pragma unroll
-      for (int q = 0; q < Q; q++) {
-        const uint32_t k = lane + 32 * q;
-        jv[q] = k < count ? __ldcs(P.tgt + base + k) : 0u;
+      for (int qq = 0; qq < Q; qq++) {
+        const uint32_t k = lane + 32 * qq;
+        jv[qq] = k < count ? __ldcs(P.tgt + base + k) : 0u;
       }
       bool fb[Q];
 #pragma unroll
-      for (int q = 0; q < Q; q++) fb[q] = (lane + 32 * q) < count && nbit(P.fbits, jv[q]);
+      for (int qq = 0; qq < Q; qq++) fb[qq] = (lane + 32 * qq) < count && nbit(P.fbits, jv[qq]);
 #pragma unroll
-      for (int q = 0; q < Q; q++) {
-        const uint32_t k = lane + 32 * q;
-        const uint32_t row = (tile && fb[q]) ? sm.rowof[k] : 0u;
-        const bool hit = fb[q] && ((needy >> row) & 1);
+      for (int qq = 0; qq < Q; qq++) {
+        const uint32_t k = lane + 32 * qq;
+        const uint32_t row = (tile && fb[qq]) ? sm.rowof[k] : 0u;
+        const bool hit = fb[qq] && ((needy >> row) & 1);
         const uint32_t m = __ballot_sync(0xffffffffu, hit);
         if (hit) {
           const uint32_t pos = H + __popc(m & ((1u << lane) - 1));
-          sm.hitj[pos] = jv[q];
+          sm.hitj[pos] = jv[qq];
           sm.hitr[pos] = (uint8_t)row;
         }
         H += __popc(m);
@@ -238,43 +303,53 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
     }
     __syncwarp();
     // Gather the hit rows.  Lane group g takes the contiguous run of hits
-    // [g·H/G, (g+1)·H/G) in order, U loads in flight; the hits of one row
-    // are consecutive, so they are OR-ed in a register and the row's word
-    // is added to its accumulator once, when the row changes (an atomicOr,
-    // as a row may straddle two groups' runs).  A piece is one row: its
-    // words gather in `racc`.
-    uint32_t racc = 0;
+    // [g·H/G, (g+1)·H/G) in order, U frontier rows in flight; the hits of
+    // one row are consecutive, so they are OR-ed in registers and the row's
+    // words are added to its accumulator once, when the row changes (atomic
+    // ORs, as a row may straddle two groups' runs).  A piece is one row:
+    // its words gather in `racc`.
+    V4 racc = {};
     if (H) {
       const uint32_t per = (H + G - 1) / G;
       const uint32_t h_lo = min(H, sub * per), h_hi = min(H, sub * per + per);
       uint32_t cur = h_lo < h_hi ? sm.hitr[h_lo] : 0u;
-      uint32_t run = 0;
+      V4 run = {};
       for (uint32_t h0 = h_lo; h0 < h_hi; h0 += U) {
-        uint32_t val[U], rr[U];
+        V4 val[U];
+        uint32_t rr[U];
 #pragma unroll
         for (int x = 0; x < U; x++) {
           const uint32_t h = h0 + x;
-          val[x] = 0;
           rr[x] = cur;
           if (h < h_hi) {
-            val[x] = __ldg(P.Fcur + (size_t)sm.hitj[h] * W + w);
+            val[x] = ldg_words<VEC>(P.Fcur + (size_t)sm.hitj[h] * W + w0);
             rr[x] = sm.hitr[h];
+          } else {
+#pragma unroll
+            for (int i = 0; i < (int)VEC; i++) val[x].x[i] = 0;
           }
         }
 #pragma unroll
         for (int x = 0; x < U; x++) {
           if (rr[x] != cur) {
-            if (run & a) atomicOr(&sm.acc[cur * W + w], run & a);
-            run = 0;
+#pragma unroll
+            for (int i = 0; i < (int)VEC; i++)
+              if (run.x[i] & a.x[i]) atomicOr(&sm.acc[cur * W + w0 + i], run.x[i] & a.x[i]);
+#pragma unroll
+            for (int i = 0; i < (int)VEC; i++) run.x[i] = 0;
             cur = rr[x];
           }
-          run |= val[x];
+#pragma unroll
+          for (int i = 0; i < (int)VEC; i++) run.x[i] |= val[x].x[i];
         }
       }
       if (tile) {
-        if (run & a) atomicOr(&sm.acc[cur * W + w], run & a);
+#pragma unroll
+        for (int i = 0; i < (int)VEC; i++)
+          if (run.x[i] & a.x[i]) atomicOr(&sm.acc[cur * W + w0 + i], run.x[i] & a.x[i]);
       } else {
-        racc = run & a;
+#pragma unroll
+        for (int i = 0; i < (int)VEC; i++) racc.x[i] = run.x[i] & a.x[i];
       }
     }
     __syncwarp();
@@ -283,20 +358,32 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
       for (uint32_t x = 0; x < VR; x++) {
         if (x * G >= R) break;
         const uint32_t r = x * G + sub;
-        uint32_t fresh = 0;
+        V4 fresh = {};
         if (r < R && ((needy >> r) & 1)) {
-          fresh = sm.acc[r * W + w] & ~vrow[x];
-          if (fresh) P.V[(size_t)(r0 + r) * W + w] = vrow[x] | fresh;
+          const V4 got = load_words<VEC>(&sm.acc[r * W + w0]);
+#pragma unroll
+          for (int i = 0; i < (int)VEC; i++) fresh.x[i] = got.x[i] & ~vrow[x].x[i];
+          if (any_words(fresh)) {
+            V4 nv;
+#pragma unroll
+            for (int i = 0; i < (int)VEC; i++) nv.x[i] = vrow[x].x[i] | fresh.x[i];
+            store_words<VEC>(P.V + (size_t)(r0 + r) * W + w0, nv);
+          }
         }
         // Only rows with fresh bits are written (and marked so).
-        const bool written = __ballot_sync(0xffffffffu, fresh != 0) & gmask;
+        const bool written = __ballot_sync(0xffffffffu, any_words(fresh)) & gmask;
         if (written) {
-          P.Fnext[(size_t)(r0 + r) * W + w] = fresh;
-          if (w == 0) atomicOr(P.wbits_next + ((r0 + r) >> 5), 1u << ((r0 + r) & 31));
+          store_words<VEC>(P.Fnext + (size_t)(r0 + r) * W + w0, fresh);
+          if (q == 0) atomicOr(P.wbits_next + ((r0 + r) >> 5), 1u << ((r0 + r) & 31));
         }
-        live |= fresh;
-        const bool expands = __ballot_sync(0xffffffffu, (fresh & a_next) != 0) & gmask;
-        if (r < R && expands && w == 0) {
+        bool ex = false;
+#pragma unroll
+        for (int i = 0; i < (int)VEC; i++) {
+          live.x[i] |= fresh.x[i];
+          ex |= (fresh.x[i] & a_next.x[i]) != 0;
+        }
+        const bool expands = __ballot_sync(0xffffffffu, ex) & gmask;
+        if (r < R && expands && q == 0) {
           atomicOr(P.fbits_next + ((r0 + r) >> 5), 1u << ((r0 + r) & 31));
           admitted++;
           fed += __ldg(P.foff + r0 + r + 1) - __ldg(P.foff + r0 + r);
@@ -306,13 +393,19 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
     } else {
       // OR the lane groups' words together, then into the row's accumulator.
 #pragma unroll
-      for (uint32_t o = W; o < 32; o <<= 1) racc |= __shfl_xor_sync(0xffffffffu, racc, o);
+      for (uint32_t o = LPR; o < 32; o <<= 1)
+#pragma unroll
+        for (int i = 0; i < (int)VEC; i++) racc.x[i] |= __shfl_xor_sync(0xffffffffu, racc.x[i], o);
       const uint32_t row = unit.a, slot = unit.c & 0x7fffffffu;
       const uint32_t row_lo = __ldg(P.off + row);
       const uint32_t deg = __ldg(P.off + row + 1) - row_lo;
       const uint32_t pieces = (deg + kPieceEntries - 1) / kPieceEntries;
       const uint32_t first = slot - (unit.b - row_lo) / kPieceEntries;
-      if (sub == 0 && racc) atomicOr(P.nacc + (size_t)first * W + w, racc);
+      uint32_t* nacc = P.nacc + (size_t)first * W + w0;
+      if (sub == 0)
+#pragma unroll
+        for (int i = 0; i < (int)VEC; i++)
+          if (racc.x[i]) atomicOr(nacc + i, racc.x[i]);
       __threadfence();
       __syncwarp();
       uint32_t arrived = 0;
@@ -320,20 +413,32 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
       arrived = __shfl_sync(0xffffffffu, arrived, 0);
       if (arrived == pieces - 1) {
         __threadfence();
-        uint32_t fresh = 0;
+        V4 fresh = {};
         if (sub == 0) {
-          const uint32_t tot = __ldcg(P.nacc + (size_t)first * W + w);
-          P.nacc[(size_t)first * W + w] = 0;
-          const uint32_t v = vrow[0];
-          fresh = tot & ~v & a;
-          if (fresh) P.V[(size_t)row * W + w] = v | fresh;
+#pragma unroll
+          for (int i = 0; i < (int)VEC; i++) {
+            const uint32_t tot = __ldcg(nacc + i);
+            fresh.x[i] = tot & ~vrow[0].x[i] & a.x[i];
+          }
+          store_words<VEC>(nacc, V4{});
+          if (any_words(fresh)) {
+            V4 nv;
+#pragma unroll
+            for (int i = 0; i < (int)VEC; i++) nv.x[i] = vrow[0].x[i] | fresh.x[i];
+            store_words<VEC>(P.V + (size_t)row * W + w0, nv);
+          }
         }
-        if (__ballot_sync(0xffffffffu, fresh != 0)) {
-          if (sub == 0) P.Fnext[(size_t)row * W + w] = fresh;
+        if (__ballot_sync(0xffffffffu, any_words(fresh))) {
+          if (sub == 0) store_words<VEC>(P.Fnext + (size_t)row * W + w0, fresh);
           if (lane == 0) atomicOr(P.wbits_next + (row >> 5), 1u << (row & 31));
         }
-        live |= fresh;
-        const bool expands = __ballot_sync(0xffffffffu, sub == 0 && (fresh & a_next) != 0) != 0;
+        bool ex = false;
+#pragma unroll
+        for (int i = 0; i < (int)VEC; i++) {
+          live.x[i] |= fresh.x[i];
+          ex |= (fresh.x[i] & a_next.x[i]) != 0;
+        }
+        const bool expands = __ballot_sync(0xffffffffu, sub == 0 && ex) != 0;
         if (lane == 0) {
           P.counters[first] = 0;
           if (expands) {
@@ -345,7 +450,22 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
       }
     }
   }
-  level_totals<W>(P, admitted, fed, live);
+  for (int o = 16; o > 0; o >>= 1) {
+    admitted += __shfl_down_sync(0xffffffffu, admitted, o);
+    fed += __shfl_down_sync(0xffffffffu, fed, o);
+  }
+  if (lane == 0 && admitted) {
+    atomicAdd(P.counts + P.L + 1, admitted);
+    atomicAdd(P.fedges + P.L + 1, fed);
+  }
+#pragma unroll
+  for (uint32_t o = LPR; o < 32; o <<= 1)
+#pragma unroll
+    for (int i = 0; i < (int)VEC; i++) live.x[i] |= __shfl_xor_sync(0xffffffffu, live.x[i], o);
+  if (sub == 0)
+#pragma unroll
+    for (int i = 0; i < (int)VEC; i++)
+      if (live.x[i]) atomicOr(P.alive + (P.L + 1) * W + w0 + i, live.x[i]);
 }
 
 // Push, step 1: the frontier rows' words (masked to the live sources) are
