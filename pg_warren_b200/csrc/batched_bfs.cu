@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
   constexpr uint32_t G = 32 / LPR;
   constexpr uint32_t GM = LPR == 32 ? 0xffffffffu : (1u << LPR) - 1;
   constexpr int Q = kTileEntries / 32;
-  constexpr int U = 4;  // frontier rows in flight per lane
+  constexpr int U = 8;  // frontier rows in flight per lane
   using V4 = Words<VEC>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   MsWarpSmem<W>& sm = reinterpret_cast<MsWarpSmem<W>*>(smem_raw)[threadIdx.x >> 5];
@@ -268,8 +268,13 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
       count = unit.c;
       if (needy)
         for (uint32_t k = lo - base; k < hi - base; k++) sm.rowof[k] = (uint8_t)lane;
-      for (uint32_t x = lane * 4; x < R * W; x += 128)
-        *reinterpret_cast<uint4*>(&sm.acc[x]) = make_uint4(0, 0, 0, 0);
+      // The accumulators start as the rows' visited words (the registers
+      // holding them are then free for the gathers).
+#pragma unroll
+      for (uint32_t x = 0; x < VR; x++) {
+        const uint32_t r = x * G + sub;
+        if (r < R) store_words<VEC>(&sm.acc[r * W + w0], vrow[x]);
+      }
     } else {
       base = unit.b;
       count = unit.d - unit.b;
@@ -360,15 +365,12 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
         const uint32_t r = x * G + sub;
         V4 fresh = {};
         if (r < R && ((needy >> r) & 1)) {
+          // acc = V | gathered: the new bits are those V lacks.
           const V4 got = load_words<VEC>(&sm.acc[r * W + w0]);
+          const V4 v = load_words<VEC>(P.V + (size_t)(r0 + r) * W + w0);
 #pragma unroll
-          for (int i = 0; i < (int)VEC; i++) fresh.x[i] = got.x[i] & ~vrow[x].x[i];
-          if (any_words(fresh)) {
-            V4 nv;
-#pragma unroll
-            for (int i = 0; i < (int)VEC; i++) nv.x[i] = vrow[x].x[i] | fresh.x[i];
-            store_words<VEC>(P.V + (size_t)(r0 + r) * W + w0, nv);
-          }
+          for (int i = 0; i < (int)VEC; i++) fresh.x[i] = got.x[i] & ~v.x[i];
+          if (any_words(fresh)) store_words<VEC>(P.V + (size_t)(r0 + r) * W + w0, got);
         }
         // Only rows with fresh bits are written (and marked so).
         const bool written = __ballot_sync(0xffffffffu, any_words(fresh)) & gmask;
@@ -415,16 +417,17 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
         __threadfence();
         V4 fresh = {};
         if (sub == 0) {
+          const V4 v = load_words<VEC>(P.V + (size_t)row * W + w0);
 #pragma unroll
           for (int i = 0; i < (int)VEC; i++) {
             const uint32_t tot = __ldcg(nacc + i);
-            fresh.x[i] = tot & ~vrow[0].x[i] & a.x[i];
+            fresh.x[i] = tot & ~v.x[i] & a.x[i];
           }
           store_words<VEC>(nacc, V4{});
           if (any_words(fresh)) {
             V4 nv;
 #pragma unroll
-            for (int i = 0; i < (int)VEC; i++) nv.x[i] = vrow[0].x[i] | fresh.x[i];
+            for (int i = 0; i < (int)VEC; i++) nv.x[i] = v.x[i] | fresh.x[i];
             store_words<VEC>(P.V + (size_t)row * W + w0, nv);
           }
         }
