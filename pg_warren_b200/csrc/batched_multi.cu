@@ -42,7 +42,8 @@ struct MpState {
   uint32_t* running;        // bit per column
   uint32_t* fell;           // bit per column, this iteration
   uint32_t* executed;       // iterations run by any column
-  uint32_t* iterations;     // P
+  uint32_t* iterations;     // the call's, indexed by cols[c]
+  const uint32_t* cols;     // P: the call's column of each pass column
   DeviceError* err;
 };
 
@@ -68,7 +69,7 @@ __global__ void mp_seed_kernel(MpState s, const uint64_t* sources) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     uint32_t run = 0;
     for (uint32_t c = 0; c < s.k; c++) {
-      s.iterations[c] = 0;
+      s.iterations[s.cols[c]] = 0;
       if (s.caps[c] > 0) run |= 1u << c;
     }
     *s.running = run;
@@ -104,18 +105,18 @@ __global__ void mp_control_kernel(MpState s, uint32_t it) {
   if (run) *s.executed = it + 1;
   for (uint32_t c = 0; c < s.k; c++) {
     if (!((run >> c) & 1)) continue;
-    s.iterations[c] = it + 1;
+    s.iterations[s.cols[c]] = it + 1;
     if (!((fell >> c) & 1) || it + 1 >= s.caps[c]) run &= ~(1u << c);
   }
   *s.running = run;
   *s.fell = 0;
 }
 
-// out[c * n + i] = x[i * P + c] from the buffer the last iteration wrote:
-// a 32-node tile through shared memory.
+// out[cols[c] * n + i] (cols NULL: c) = x[i * P + c] from the buffer the
+// last iteration wrote: a 32-node tile through shared memory.
 template <int P, class T>
 __global__ void columns_out_kernel(const T* x0, const T* x1, const uint32_t* executed, uint32_t n,
-                                   uint32_t k, T* out) {
+                                   uint32_t k, T* out, const uint32_t* cols) {
   __shared__ T tile[32][P + 1];
   const T* x = (*executed & 1) ? x1 : x0;
   const uint32_t tiles = (n + 31) / 32;
@@ -128,7 +129,7 @@ __global__ void columns_out_kernel(const T* x0, const T* x1, const uint32_t* exe
     __syncthreads();
     for (uint32_t q = threadIdx.x; q < 32 * k; q += blockDim.x) {
       const uint32_t c = q / 32, r = q % 32;
-      if (i0 + r < n) out[(size_t)c * n + i0 + r] = tile[r][c];
+      if (i0 + r < n) out[(size_t)(cols ? cols[c] : c) * n + i0 + r] = tile[r][c];
     }
     __syncthreads();
   }
@@ -139,8 +140,9 @@ struct MpPass {
 };
 
 template <int P>
-wc_status mp_pass(Ctx& ctx, const uint64_t* sources, const uint32_t* caps_dev, uint32_t k,
-                  uint32_t max_cap, int64_t* out, uint32_t* iterations_dev, uint32_t blocks_per_sm) {
+wc_status mp_pass(Ctx& ctx, const uint64_t* sources, const uint32_t* caps_dev, const uint32_t* cols,
+                  uint32_t k, uint32_t max_cap, int64_t* out, uint32_t* iterations_dev,
+                  uint32_t blocks_per_sm) {
   wc_version* v = ctx.v;
   const uint32_t n = (uint32_t)v->n;
   DevBuf *xb, *stb, *cb;
@@ -159,6 +161,7 @@ wc_status mp_pass(Ctx& ctx, const uint64_t* sources, const uint32_t* caps_dev, u
   s.fell = s.running + 1;
   s.executed = s.running + 2;
   s.iterations = iterations_dev;
+  s.cols = cols;
   s.err = v->error.as<DeviceError>();
   note_launch(), mp_seed_kernel<P><<<max_blocks(4), 256, 0, ctx.stream>>>(s, sources);
   note_launch(), mp_sources_kernel<P><<<1, 32, 0, ctx.stream>>>(s, sources);
@@ -178,8 +181,8 @@ wc_status mp_pass(Ctx& ctx, const uint64_t* sources, const uint32_t* caps_dev, u
                                                             carry);
     note_launch(), mp_control_kernel<<<1, 32, 0, ctx.stream>>>(s, it);
   }
-  note_launch(), columns_out_kernel<P, int64_t><<<max_blocks(4), 256, 0, ctx.stream>>>(s.x[0], s.x[1], s.executed,
-                                                                         n, k, out);
+  note_launch(), columns_out_kernel<P, int64_t><<<max_blocks(4), 256, 0, ctx.stream>>>(
+      s.x[0], s.x[1], s.executed, n, k, out, cols);
   return cuda_status(cudaGetLastError(), ctx.detail, "batched min-plus pass");
 }
 
@@ -195,8 +198,8 @@ static wc_status mp_reserve(Ctx& ctx, uint32_t P) {
                          sizeof(Partial<int64_t, WC_OP_MIN>), &b);
 }
 
-typedef wc_status (*MpFn)(Ctx&, const uint64_t*, const uint32_t*, uint32_t, uint32_t, int64_t*,
-                          uint32_t*, uint32_t);
+typedef wc_status (*MpFn)(Ctx&, const uint64_t*, const uint32_t*, const uint32_t*, uint32_t,
+                          uint32_t, int64_t*, uint32_t*, uint32_t);
 
 static MpFn mp_for(uint32_t p) {
   switch (p) {
@@ -386,8 +389,8 @@ wc_status ppr_pass(Ctx& ctx, const PageRankRun& base_run, const uint64_t* nodes,
       note_launch(), ppr_iter_kernel<P, void><<<grid, 256, 0, ctx.stream>>>(view_of<void>(v->rev, nullptr), s, it,
                                                              carry, max_iter);
   }
-  note_launch(), columns_out_kernel<P, double><<<max_blocks(4), 256, 0, ctx.stream>>>(s.x[0], s.x[1], s.executed,
-                                                                        n, k, out);
+  note_launch(), columns_out_kernel<P, double><<<max_blocks(4), 256, 0, ctx.stream>>>(
+      s.x[0], s.x[1], s.executed, n, k, out, nullptr);
   return cuda_status(cudaGetLastError(), ctx.detail, "batched pagerank pass");
 }
 
@@ -438,14 +441,18 @@ wc_status tune_minplus(Ctx& ctx, uint32_t width, wc_schedule* best) {
   const uint32_t sample = std::min<uint32_t>(width, 64);
   std::vector<uint64_t> src;
   sample_nodes((uint32_t)v->n, sample, src, 0x5eedu);
-  std::vector<uint32_t> caps(sample, 16);
-  DevBuf *S, *C, *D, *I;
+  std::vector<uint32_t> caps(sample, 16), cols(sample);
+  for (uint32_t c = 0; c < sample; c++) cols[c] = c;
+  DevBuf *S, *C, *D, *I, *ident;
   WC_TRY(ctx.scratch(POOL_BATCH_5, sample * 8, &S));
   WC_TRY(ctx.scratch(POOL_BATCH_6, sample * 4, &C));
   WC_TRY(ctx.scratch(POOL_BATCH_7, (uint64_t)sample * v->n * 8, &D));
   WC_TRY(ctx.scratch(POOL_BATCH_9, sample * 4, &I));
+  WC_TRY(ctx.scratch(POOL_BATCH_10, sample * 4, &ident));
   WC_CUDA(cudaMemcpyAsync(S->ptr, src.data(), sample * 8, cudaMemcpyHostToDevice, ctx.stream), ctx.detail);
   WC_CUDA(cudaMemcpyAsync(C->ptr, caps.data(), sample * 4, cudaMemcpyHostToDevice, ctx.stream), ctx.detail);
+  WC_CUDA(cudaMemcpyAsync(ident->ptr, cols.data(), sample * 4, cudaMemcpyHostToDevice, ctx.stream),
+          ctx.detail);
   cudaEvent_t a, b;
   WC_CUDA(cudaEventCreate(&a), ctx.detail);
   WC_CUDA(cudaEventCreate(&b), ctx.detail);
@@ -457,8 +464,8 @@ wc_status tune_minplus(Ctx& ctx, uint32_t width, wc_schedule* best) {
       float ms = 0;
       for (int rep = 0; rep < 2; rep++) {
         WC_CUDA(cudaEventRecord(a, ctx.stream), ctx.detail);
-        WC_TRY(mp_for(P)(ctx, S->as<uint64_t>(), C->as<uint32_t>(), k, 16, D->as<int64_t>(),
-                         I->as<uint32_t>(), bps));
+        WC_TRY(mp_for(P)(ctx, S->as<uint64_t>(), C->as<uint32_t>(), ident->as<uint32_t>(), k, 16,
+                         D->as<int64_t>(), I->as<uint32_t>(), bps));
         WC_CUDA(cudaEventRecord(b, ctx.stream), ctx.detail);
         WC_CUDA(cudaEventSynchronize(b), ctx.detail);
         WC_CUDA(cudaEventElapsedTime(&ms, a, b), ctx.detail);
@@ -546,9 +553,31 @@ wc_status wc_minplus_batched(wc_version* v, const wc_call* call, const uint64_t*
       return WC_NODE_OUTSIDE_ID_SPACE;
     }
   WC_TRY(ctx.begin());
-  Operand S(POOL_BATCH_5), C(POOL_BATCH_6), D(POOL_BATCH_7), I(POOL_BATCH_8);
-  WC_TRY(S.in(ctx, sources, width * 8));
-  WC_TRY(C.in(ctx, max_hops, width * 4));
+  // Passes take the searches in order of their caps, so that a pass's
+  // columns stop at about the same iteration; results go back to each
+  // search's own column.
+  std::vector<uint32_t> order(width);
+  for (uint32_t c = 0; c < width; c++) order[c] = c;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](uint32_t p, uint32_t q) { return caps[p] < caps[q]; });
+  std::vector<uint64_t> psrc(width);
+  std::vector<uint32_t> pcaps(width);
+  for (uint32_t c = 0; c < width; c++) {
+    psrc[c] = src[order[c]];
+    pcaps[c] = caps[order[c]];
+  }
+  DevBuf* pb;
+  WC_TRY(ctx.scratch(POOL_BATCH_10, (uint64_t)width * 16, &pb));
+  uint64_t* psrc_dev = pb->as<uint64_t>();
+  uint32_t* pcaps_dev = reinterpret_cast<uint32_t*>(psrc_dev + width);
+  uint32_t* pcols_dev = pcaps_dev + width;
+  WC_CUDA(cudaMemcpyAsync(psrc_dev, psrc.data(), width * 8, cudaMemcpyHostToDevice, ctx.stream),
+          ctx.detail);
+  WC_CUDA(cudaMemcpyAsync(pcaps_dev, pcaps.data(), width * 4, cudaMemcpyHostToDevice, ctx.stream),
+          ctx.detail);
+  WC_CUDA(cudaMemcpyAsync(pcols_dev, order.data(), width * 4, cudaMemcpyHostToDevice, ctx.stream),
+          ctx.detail);
+  Operand D(POOL_BATCH_7), I(POOL_BATCH_8);
   WC_TRY(D.output(ctx, dist_out, (uint64_t)width * v->n * 8));
   DevBuf* its;
   WC_TRY(ctx.scratch(POOL_BATCH_9, (uint64_t)width * 4, &its));
@@ -560,14 +589,12 @@ wc_status wc_minplus_batched(wc_version* v, const wc_call* call, const uint64_t*
   for (uint32_t c0 = 0; c0 < width; c0 += P) {
     const uint32_t k = std::min(P, width - c0);
     uint32_t max_cap = 0;
-    for (uint32_t c = c0; c < c0 + k; c++) max_cap = std::max(max_cap, caps[c]);
+    for (uint32_t c = c0; c < c0 + k; c++) max_cap = std::max(max_cap, pcaps[c]);
     const std::string gk = "minplus/" + std::to_string(P) + "/" + std::to_string(k) + "/" +
                            std::to_string(max_cap) + "/" + std::to_string(bps);
     WC_TRY(ctx.run_captured(gk, [&] {
-      return mp_for(P)(ctx, static_cast<const uint64_t*>(S.dev) + c0,
-                       static_cast<const uint32_t*>(C.dev) + c0, k, max_cap,
-                       static_cast<int64_t*>(D.dev) + (uint64_t)c0 * v->n,
-                       its->as<uint32_t>() + c0, bps);
+      return mp_for(P)(ctx, psrc_dev + c0, pcaps_dev + c0, pcols_dev + c0, k, max_cap,
+                       static_cast<int64_t*>(D.dev), its->as<uint32_t>(), bps);
     }));
   }
   WC_TRY(D.out(ctx));
