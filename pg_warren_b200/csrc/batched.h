@@ -16,4 +16,11 @@ wc_status bfs_batched_run(Ctx& ctx, const wc_schedule& sched, const uint64_t* so
                           const uint32_t* caps_dev, const uint32_t* caps_host, uint32_t width,
                           uint8_t* depth_dev, unsigned long long* edges_dev);
 
+// The 32-bit batched min-plus (batched_minplus32.cu): a pass of up to 64
+// columns, sources / caps / the call's column of each in device memory.
+typedef wc_status (*Mp32Fn)(Ctx&, const uint64_t*, const uint32_t*, const uint32_t*, uint32_t,
+                            uint32_t, int64_t*, uint32_t*, uint32_t);
+Mp32Fn mp32_for(uint32_t columns);
+wc_status mp32_reserve(Ctx& ctx, uint32_t columns);
+
 }  // namespace wc

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <string>
 
+#include "batched.h"
 #include "operand.h"
 #include "pagerank.h"
 #include "columns.cuh"
@@ -585,6 +586,29 @@ wc_status wc_minplus_batched(wc_version* v, const wc_call* call, const uint64_t*
   const wc_schedule sched = v->tuned.count(key) ? v->tuned[key] : wc_schedule{32, 1, 4, 0};
   const uint32_t P = std::max<uint32_t>(1, std::min<uint32_t>(32, sched.columns_per_pass));
   const uint32_t bps = sched.blocks_per_sm ? sched.blocks_per_sm : 4;
+  // 32-bit distances when no value can leave the 32-bit range.
+  const uint32_t cap_max = *std::max_element(caps.begin(), caps.end());
+  if (v->max_abs_iweight >= 0 && (uint64_t)cap_max * (uint64_t)v->max_abs_iweight < (1ull << 30)) {
+    const uint32_t P32 = width > 32 ? 64 : 32;
+    WC_TRY(mp32_reserve(ctx, P32));
+    for (uint32_t c0 = 0; c0 < width; c0 += P32) {
+      const uint32_t k = std::min(P32, width - c0);
+      uint32_t max_cap = 0;
+      for (uint32_t c = c0; c < c0 + k; c++) max_cap = std::max(max_cap, pcaps[c]);
+      const std::string gk = "minplus32/" + std::to_string(P32) + "/" + std::to_string(k) + "/" +
+                             std::to_string(max_cap);
+      WC_TRY(ctx.run_captured(gk, [&] {
+        return mp32_for(P32)(ctx, psrc_dev + c0, pcaps_dev + c0, pcols_dev + c0, k, max_cap,
+                             static_cast<int64_t*>(D.dev), its->as<uint32_t>(),
+                             P32 == 64 ? 2 : 3);
+      }));
+    }
+    WC_TRY(D.out(ctx));
+    if (iterations_out)
+      WC_CUDA(cudaMemcpyAsync(iterations_out, its->ptr, width * 4, cudaMemcpyDefault, ctx.stream),
+              ctx.detail);
+    return ctx.finish();
+  }
   WC_TRY(mp_reserve(ctx, P));
   for (uint32_t c0 = 0; c0 < width; c0 += P) {
     const uint32_t k = std::min(P, width - c0);

@@ -225,6 +225,7 @@ struct wc_version {
   int device = 0;
   bool weighted = false;
   bool integral = false;
+  int64_t max_abs_iweight = -1;  // max |w| when every weight is an i32 (1 unweighted), else -1
   bool symmetric = false;
   wc_budget* budget = nullptr;
   cudaStream_t stream = nullptr;
@@ -269,6 +270,8 @@ enum PoolTag {
   // Buffers the batched BFS keeps all-zero between calls; no other role
   // may share them.
   POOL_MSBFS_NACC = 110, POOL_MSBFS_ACC, POOL_MSBFS_TOUCHED,
+  // The 32-bit batched min-plus's long-row minima, kept at i32::MAX.
+  POOL_MINPLUS32_NACC = 120,
 };
 
 // A call's context: the stream, the caller's detail and cancellation.

@@ -2,6 +2,7 @@
 // of a built version's CSR and reverse CSR (graph/csr/mod.rs:38-237,
 // graph_csr.rs:15-55), with the row-split schedules the pull kernels walk.
 #include <algorithm>
+#include <cstdlib>
 #include <thread>
 
 #include "product.h"
@@ -186,12 +187,15 @@ wc_status wc_version_upload(uint64_t graph_id, uint64_t version, const wc_csr_ho
   v->budget = budget;
   v->weighted = csr->weights != nullptr;
   bool integral = v->weighted;
+  int64_t max_abs = v->weighted ? 0 : 1;
   if (v->weighted)
     for (uint64_t e = 0; e < m && integral; e++) {
-      double w = csr->weights[e];
-      integral = w == (double)(int32_t)w && w >= -2147483648.0 && w <= 2147483647.0;
+      const double w = csr->weights[e];
+      integral = w >= -2147483648.0 && w <= 2147483647.0 && w == (double)(int32_t)w;
+      if (integral) max_abs = std::max<int64_t>(max_abs, std::llabs((long long)w));
     }
   v->integral = integral;
+  v->max_abs_iweight = integral || !v->weighted ? max_abs : -1;
   // The reverse CSR: the caller's, or a counting transpose here.
   std::vector<uint64_t> roff;
   std::vector<uint32_t> rtgt;

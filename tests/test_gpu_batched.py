@@ -75,6 +75,29 @@ def test_minplus_batched_equals_the_sssp_loop_per_source(columns):
     assert np.array_equal(it, ito)
 
 
+@pytest.mark.parametrize("kind", ["wide", "negative", "fraction"])
+def test_minplus_batched_wide_negative_and_fractional_weights(kind):
+    # Weights of 2^28 with caps to 16 leave the 32-bit range (the i64 path);
+    # negative integer weights and non-integral weights (cast to i64 per
+    # edge, round half to even) take their own paths; all equal the loop.
+    g = W.rmat(12, seed=9)
+    rng = np.random.default_rng(3)
+    if kind == "wide":
+        w = rng.integers(1, 4, g.edges).astype(np.float64) * 2.0 ** 28
+    elif kind == "negative":
+        w = rng.integers(-3, 100, g.edges).astype(np.float64)
+    else:
+        w = rng.integers(0, 400, g.edges) / 4.0
+    og = O.Graph.from_csr(g.id_space, g.offsets, g.targets, w)
+    gv = W.GraphVersion(g.offsets, g.targets, w)
+    src = rng.integers(0, g.id_space, 50).astype(np.uint64)
+    hops = rng.integers(0, 17, 50).astype(np.uint32)
+    d, it = W.minplus_batched(gv, src, hops)
+    do, ito = O.sssp_i64(og, src, hops)
+    assert np.array_equal(d, do)
+    assert np.array_equal(it, ito)
+
+
 def test_minplus_batched_unweighted_and_capped():
     g = W.rmat(12, seed=4)
     og = O.Graph.from_csr(g.id_space, g.offsets, g.targets)
