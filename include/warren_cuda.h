@@ -335,6 +335,13 @@ wc_status wc_reachable(wc_version* version, const wc_call* call, wc_direction di
                        uint64_t start, uint64_t target, uint32_t max_depth, int32_t* reached,
                        wc_traversal_stats* stats);
 
+/* traversal/components.rs:21-58 (components): weakly connected components
+ * over the forward rows, each dense id labelled with the smallest dense id
+ * of its component (labels_out u64[id_space]); stats: every node visited,
+ * every forward edge traversed. */
+wc_status wc_components(wc_version* version, const wc_call* call, uint64_t* labels_out,
+                        wc_traversal_stats* stats);
+
 /* ------------------------------------------------- batched (no reference
  * counterpart: many searches as one semiring SpMM in a persistent kernel
  * under a captured CUDA graph) */

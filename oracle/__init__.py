@@ -102,6 +102,8 @@ def _declare(L):
     L.wo_bfs_depths.argtypes = [P, P, P, U32, P, P]
     L.wo_sssp_i64.restype = I32
     L.wo_sssp_i64.argtypes = [P, P, P, U32, P, P]
+    L.wo_components.restype = I32
+    L.wo_components.argtypes = [P, P, P, P]
     L.wo_topk_f64.restype = I32
     L.wo_topk_f64.argtypes = [P, U64, P, U64, I, P, P, P]
     if hasattr(L, "wo_eigen"):
@@ -278,6 +280,16 @@ def sssp_i64(g, sources, max_iter):
     _check(lib().wo_sssp_i64(g.handle, _ptr(sources), _ptr(max_iter), len(sources), _ptr(out),
                              _ptr(its)))
     return out, its
+
+
+def components(g):
+    """traversal/components.rs:21-58: (labels u64[n], nodes_visited,
+    edges_traversed)."""
+    labels = np.zeros(g.n, np.uint64)
+    nv = np.zeros(1, np.uint64)
+    et = np.zeros(1, np.uint64)
+    _check(lib().wo_components(g.handle, _ptr(labels), _ptr(nv), _ptr(et)))
+    return labels, int(nv[0]), int(et[0])
 
 
 def topk(x, k, descending=True, tombstones=None):

@@ -971,6 +971,40 @@ int32_t wo_sssp_i64(const wo_graph* gp, const uint64_t* sources, const uint32_t*
   });
 }
 
+// traversal/components.rs:21-58: weakly connected components by
+// union-find over the forward rows swept in ascending order, the larger
+// root hung under the smaller (path halving), then every node's label set
+// to its root's: the smallest dense id of its component.  Stats: every
+// node visited, every forward edge traversed.
+int32_t wo_components(const wo_graph* gp, uint64_t* labels, uint64_t* nodes_visited,
+                      uint64_t* edges_traversed) {
+  const Graph& g = *(const Graph*)gp;
+  const uint64_t n = g.fwd.n;
+  std::vector<uint64_t> parent(n);
+  for (uint64_t i = 0; i < n; i++) parent[i] = i;
+  auto root = [&](uint64_t x) {
+    while (parent[x] != x) {
+      const uint64_t gp2 = parent[parent[x]];
+      parent[x] = gp2;
+      x = gp2;
+    }
+    return x;
+  };
+  uint64_t edges = 0;
+  for (uint64_t u = 0; u < n; u++)
+    for (uint64_t e = g.fwd.off[u]; e < g.fwd.off[u + 1]; e++) {
+      edges++;
+      const uint64_t a = root(u), b = root(g.fwd.tgt[e]);
+      if (a < b) parent[b] = a;
+      else parent[a] = b;
+    }
+  for (uint64_t i = 0; i < n; i++) parent[i] = parent[parent[i]];
+  for (uint64_t i = 0; i < n; i++) labels[i] = parent[i];
+  *nodes_visited = n;
+  *edges_traversed = edges;
+  return WC_OK;
+}
+
 // compute/ranking.rs:15-80 (top_k) over f64 values.
 int32_t wo_topk_f64(const double* x, uint64_t n, const uint64_t* tomb, uint64_t k, int descending,
                     uint64_t* nodes, double* values, uint64_t* count) {

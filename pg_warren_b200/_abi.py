@@ -127,6 +127,7 @@ SIGNATURES = [
                                C.POINTER(TraversalStats)]),
     ("wc_reachable", I32, [P, C.POINTER(Call), I32, U64, U64, U32, C.POINTER(I32),
                            C.POINTER(TraversalStats)]),
+    ("wc_components", I32, [P, C.POINTER(Call), P, C.POINTER(TraversalStats)]),
     ("wc_autotune", I32, [P, C.POINTER(Call), I32, U32, C.POINTER(Schedule)]),
     ("wc_schedule_set", I32, [P, I32, U32, C.POINTER(Schedule)]),
     ("wc_bfs_batched", I32, [P, C.POINTER(Call), P, P, U32, P, P]),

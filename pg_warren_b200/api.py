@@ -587,6 +587,17 @@ def reachable_set(graph: GraphVersion, starts, max_depth=None, direction="out",
     return Traversed([int(v) for v in nodes[: count.value]], _stats(stats))
 
 
+def components(graph: GraphVersion, labels_out=None, interrupts=None):
+    """traversal/components.rs:21-58: each dense id's weakly connected
+    component, labelled by its smallest dense id: (labels u64[n], stats)."""
+    labels = labels_out if labels_out is not None else np.zeros(graph.id_space, np.uint64)
+    stats = A.TraversalStats()
+    call, detail = _call(interrupts)
+    _raise(A.load().wc_components(graph.handle, C.byref(call), _ptr(labels), C.byref(stats)),
+           detail)
+    return labels, _stats(stats)
+
+
 def reachable(graph: GraphVersion, start: int, target: int, max_depth=None,
               direction="out") -> Traversed:
     """traversal/reachable.rs:18-43."""

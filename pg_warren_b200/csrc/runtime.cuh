@@ -272,6 +272,7 @@ enum PoolTag {
   POOL_MSBFS_NACC = 110, POOL_MSBFS_ACC, POOL_MSBFS_TOUCHED,
   // The 32-bit batched min-plus's long-row minima, kept at i32::MAX.
   POOL_MINPLUS32_NACC = 120,
+  POOL_WCC_PARENT = 130, POOL_WCC_FLAG, POOL_WCC_LABELS,
 };
 
 // A call's context: the stream, the caller's detail and cancellation.

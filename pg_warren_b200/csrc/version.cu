@@ -290,7 +290,7 @@ int32_t wc_serves(const char* op, wc_dtype dtype) {
   std::string o(op);
   if (o == "spmv" || o == "spmm") return dtype >= WC_F32 && dtype <= WC_BOOL;
   if (o == "pagerank" || o == "eigen") return dtype == WC_F64;
-  if (o == "bfs" || o == "reachable_set" || o == "reachable") return 1;
+  if (o == "bfs" || o == "reachable_set" || o == "reachable" || o == "components") return 1;
   if (o == "vector_topk") return dtype == WC_F64;
   return 0;
 }

@@ -312,3 +312,27 @@ def test_reachable_set_rmat16_matches_including_pulled_levels():
         assert t.stats.edges_traversed == st["edges_traversed"]
         assert t.stats.nodes_visited == st["nodes_visited"]
         assert t.stats.pulled_levels == st["pulled_levels"]
+
+
+def test_components_match_the_oracle():
+    # traversal/components.rs: the reference's example, then R-MAT graphs
+    # (many components, directed) and a chain whose roots settle late.
+    g = O.Graph.from_edges(7, [(0, s, t, 1.0) for s, t in [(4, 2), (2, 0), (3, 1), (5, 1), (6, 6)]],
+                           weighted=False)
+    off, tgt, _, _, _, _ = g.csr()
+    labels, stats = W.components(W.GraphVersion(off, tgt))
+    assert list(labels) == [0, 1, 0, 1, 0, 1, 6]
+    assert (stats.nodes_visited, stats.edges_traversed) == (7, 5)
+    for scale, seed in ((10, 1), (14, 2), (16, 3)):
+        hg = W.rmat(scale, seed=seed)
+        og = O.Graph.from_csr(hg.id_space, hg.offsets, hg.targets, reverse=False)
+        want, nv, ne = O.components(og)
+        got, st = W.components(hg.upload())
+        assert np.array_equal(got, want)
+        assert (st.nodes_visited, st.edges_traversed) == (nv, ne)
+    n = 5000
+    chain = [(0, i + 1, i, 1.0) for i in range(n - 1)][::-1]
+    og = O.Graph.from_edges(n, chain, weighted=False)
+    off, tgt, _, _, _, _ = og.csr()
+    got, _ = W.components(W.GraphVersion(off, tgt))
+    assert np.all(got == 0)

@@ -485,3 +485,12 @@ def test_topk_sql_order_ties_to_smaller_id(oracle):
     assert list(nodes) == [4, 0]
     nodes, _ = O.topk(x, 10, descending=True, tombstones=O.tombstone_words(5, [2]))
     assert list(nodes) == [1, 3, 0, 4]
+
+
+def test_components_label_by_smallest_dense_id(oracle):
+    # traversal/components.rs:64-77: {0, 2, 4} via 4 → 2 → 0, {1, 3, 5} via
+    # 3 → 1 and 5 → 1, 6 alone; 7 nodes visited, 5 edges traversed.
+    g = directed(7, [(4, 2), (2, 0), (3, 1), (5, 1), (6, 6)])
+    labels, nodes, edges = O.components(g)
+    assert list(labels) == [0, 1, 0, 1, 0, 1, 6]
+    assert (nodes, edges) == (7, 5)
