@@ -107,6 +107,13 @@ static wc_status product(wc_version* v, const wc_call* call, const wc_product* p
   PullLaunch L;
   DevCsr& csr = p->transpose ? v->rev : v->fwd;
   WC_TRY(prepare_pull(ctx, csr, p->semiring, p->weighted, dtype, width, L));
+  if (width > 1) {
+    DevBuf* mc;
+    WC_TRY(ctx.scratch(POOL_SPMM_CARRY,
+                       (uint64_t)std::max<uint32_t>(csr.schedule.slots, 1) * kMultiCarryBytesPerSlot,
+                       &mc));
+    L.carry_multi = mc->ptr;
+  }
   if (p->mask) L.write = WriteArgs{M.dev, (int32_t)p->mask->dtype, p->mask->complement, p->replace,
                                    (int32_t)p->accumulate};
   else L.write = WriteArgs{nullptr, WC_F64, 0, p->replace, (int32_t)p->accumulate};

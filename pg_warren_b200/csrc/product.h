@@ -31,6 +31,7 @@ struct PullLaunch {
   uint32_t unit_count;
   uint32_t* counters;
   void* carry;
+  void* carry_multi;  // width > 1: 32 partials a long-row slot
   uint32_t n;
   uint32_t width;
   int32_t semiring;
@@ -49,5 +50,7 @@ wc_status launch_pull_bool(const PullLaunch& L, const void* x, void* y);
 // The bytes of carry space a long-row schedule needs per slot (the largest
 // partial accumulator: i64 plus keeps three 128-bit values).
 constexpr uint64_t kCarryBytesPerSlot = 64;
+// The SpMM's carry: a partial per column of a 32-column block, per slot.
+constexpr uint64_t kMultiCarryBytesPerSlot = 32 * kCarryBytesPerSlot;
 
 }  // namespace wc

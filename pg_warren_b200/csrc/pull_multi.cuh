@@ -18,12 +18,14 @@
 
 namespace wc {
 
-// Folds entries [e0, e1) of column `c` into `acc` in order.  All lanes of
-// the group run the same trip count (the group shares the row).
+// Folds entries [e0, e1) of column `c` into `acc` in order (X's rows are
+// `ld` elements apart; an inactive lane folds nothing).  All lanes of the
+// group run the same trip count (the group shares the row).
 template <class E, int S, class W, int P>
 __device__ inline void fold_run(const CsrView<W>& A, const E* __restrict__ X, uint32_t e0,
                                 uint32_t e1, uint32_t c, Partial<E, semiring_add(S)>& acc,
-                                DeviceError* err, uint32_t row) {
+                                DeviceError* err, uint32_t row, uint32_t ld = P,
+                                bool active = true) {
   constexpr int ADD = semiring_add(S);
   constexpr int U = 8;
   for (uint32_t e = e0; e < e1; e += U) {
@@ -39,10 +41,10 @@ __device__ inline void fold_run(const CsrView<W>& A, const E* __restrict__ X, ui
     E xv[U];
 #pragma unroll
     for (int q = 0; q < U; q++)
-      if (e + q < e1) xv[q] = X[(size_t)j[q] * P + c];
+      if (active && e + q < e1) xv[q] = X[(size_t)j[q] * ld + c];
 #pragma unroll
     for (int q = 0; q < U; q++) {
-      if (e + q < e1) {
+      if (active && e + q < e1) {
         E p;
         int32_t s = EntryOf<E, S, W>::product(wv[q], xv[q], &p);
         if (s) raise(err, s, row);
@@ -63,16 +65,19 @@ __device__ inline void fold_run(const CsrView<W>& A, const E* __restrict__ X, ui
 
 // Walks the schedule; `epi.cell(row, column, present, value)` is called
 // once per (row, column), always by a lane whose index is column mod P, so
-// an epilogue may keep per-column sums in registers.  `carry` holds P
+// an epilogue may keep per-column sums in registers.  X's rows are `ld`
+// elements apart; columns >= `columns` are folded by no lane.  `carry` holds P
 // partials per slot (the schedule's long-row pieces).
 template <class E, int S, class W, int P, class Epi>
 __device__ inline void pull_multi(const CsrView<W>& A, const E* __restrict__ X, Epi& epi,
-                                  DeviceError* err, Partial<E, semiring_add(S)>* carry) {
+                                  DeviceError* err, Partial<E, semiring_add(S)>* carry,
+                                  uint32_t ld = P, uint32_t columns = P) {
   static_assert(P >= 1 && P <= 32 && (P & (P - 1)) == 0, "P: a power of two up to 32");
   constexpr int ADD = semiring_add(S);
   constexpr uint32_t G = 32 / P;
   const unsigned lane = threadIdx.x & 31;
   const uint32_t c = lane % P, g = lane / P;
+  const bool active = c < columns;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t u = warp; u < A.unit_count; u += warps) {
@@ -81,7 +86,7 @@ __device__ inline void pull_multi(const CsrView<W>& A, const E* __restrict__ X, 
       for (uint32_t r = unit.a + g; r < unit.b; r += G) {
         const uint32_t lo = __ldg(A.off + r), hi = __ldg(A.off + r + 1);
         Partial<E, ADD> acc{Acc<E, ADD>::of(E{}), false};
-        fold_run<E, S, W, P>(A, X, lo, hi, c, acc, err, r);
+        fold_run<E, S, W, P>(A, X, lo, hi, c, acc, err, r, ld, active);
         E v{};
         if (acc.present) acc.acc.value(&v);
         epi.cell(r, c, acc.present, v);
@@ -92,7 +97,7 @@ __device__ inline void pull_multi(const CsrView<W>& A, const E* __restrict__ X, 
       const uint32_t run = (kPieceEntries + G - 1) / G;
       Partial<E, ADD> mine{Acc<E, ADD>::of(E{}), false};
       const uint32_t b0 = min(e1, e0 + g * run), b1 = min(e1, e0 + (g + 1) * run);
-      fold_run<E, S, W, P>(A, X, b0, b1, c, mine, err, row);
+      fold_run<E, S, W, P>(A, X, b0, b1, c, mine, err, row, ld, active);
       for (uint32_t o = P; o < 32; o <<= 1) {  // groups o/P apart: left to right
         Partial<E, ADD> other = shfl_partial(mine, o);
         if ((g & (2 * (o / P) - 1)) == 0) mine = join(mine, other);

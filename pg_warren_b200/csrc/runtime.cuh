@@ -273,6 +273,7 @@ enum PoolTag {
   // The 32-bit batched min-plus's long-row minima, kept at i32::MAX.
   POOL_MINPLUS32_NACC = 120,
   POOL_WCC_PARENT = 130, POOL_WCC_FLAG, POOL_WCC_LABELS,
+  POOL_SPMM_CARRY = 140,
 };
 
 // A call's context: the stream, the caller's detail and cancellation.

@@ -3,6 +3,7 @@
 #pragma once
 
 #include "pull.cuh"
+#include "pull_multi.cuh"
 #include "product.h"
 
 namespace wc {
@@ -15,53 +16,42 @@ __global__ void __launch_bounds__(kPullThreads, 3)
   pull_units<E, S, W>(A, x, epi, err, ring);
 }
 
-// SpMM, width > 1: a warp per row, each lane folding columns lane, lane+32,
-// ... over the row's entries in ascending order (the reference's `fold`,
-// compute/product/kernel.rs:184-198), the first entry setting each sum.
-template <class E, int S, class W>
-__global__ void __launch_bounds__(256)
-    spmm_rows_kernel(CsrView<W> A, uint32_t n, uint32_t width, const E* __restrict__ x, E* y,
-                     WriteArgs w, DeviceError* err) {
-  constexpr int ADD = semiring_add(S);
-  const unsigned lane = threadIdx.x & 31;
-  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  const E identity = Identity<E>::of(ADD);
-  for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += warps) {
-    const uint32_t lo = __ldg(A.off + row), hi = __ldg(A.off + row + 1);
-    const bool selected = mask_selects(w, row);
-    for (uint32_t k0 = 0; k0 < width; k0 += 32) {
-      const uint32_t k = k0 + lane;
-      if (k >= width) continue;
-      E* out = y + (size_t)row * width + k;
-      if (!selected) {
-        if (w.replace) *out = identity;
-        continue;
-      }
-      E sum{};
-      bool present = false;
-      for (uint32_t e = lo; e < hi; e++) {
-        const uint32_t j = __ldg(A.tgt + e);
-        E p;
-        int32_t s = EntryOf<E, S, W>::get(A, e, x[(size_t)j * width + k], &p);
-        if (s) raise(err, s, row);
-        if (present) {
-          s = Apply<E, ADD>::go(sum, p, &sum);
-          if (s) raise(err, s, row);
-        } else {
-          sum = p;
-          present = true;
-        }
-      }
-      if (w.accumulate < 0) {
-        *out = present ? sum : identity;
-      } else if (present) {
-        E r;
-        int32_t s = apply_rt<E>(w.accumulate, *out, sum, &r);
-        if (s) raise(err, s, row);
-        else *out = r;
-      }
+// SpMM, width > 1: the multi-column pull (pull_multi.cuh) over a block of
+// P columns at a time — the row-split schedule, each column folded over
+// the row's entries in ascending order (the reference's `fold`,
+// compute/product/kernel.rs:184-198), long rows split into pieces combined
+// in order — and the write (kernel.rs:200-240) per (row, column).
+template <class E, int S> struct SpmmEpi {
+  WriteArgs w;
+  E* y;
+  uint32_t width, c0;
+  DeviceError* err;
+  __device__ void cell(uint32_t row, uint32_t c, bool present, E t) {
+    const uint32_t col = c0 + c;
+    if (col >= width) return;
+    E* out = y + (size_t)row * width + col;
+    const E identity = Identity<E>::of(semiring_add(S));
+    if (!mask_selects(w, row)) {
+      if (w.replace) *out = identity;
+      return;
+    }
+    if (w.accumulate < 0) {
+      *out = present ? t : identity;
+    } else if (present) {
+      E r;
+      int32_t s = apply_rt<E>(w.accumulate, *out, t, &r);
+      if (s) raise(err, s, row);
+      else *out = r;
     }
   }
+};
+
+template <class E, int S, class W, int P>
+__global__ void __launch_bounds__(256)
+    spmm_multi_kernel(CsrView<W> A, const E* __restrict__ x, E* y, uint32_t width, uint32_t c0,
+                      WriteArgs w, DeviceError* err, Partial<E, semiring_add(S)>* carry) {
+  SpmmEpi<E, S> epi{w, y, width, c0, err};
+  pull_multi<E, S, W, P>(A, x + c0, epi, err, carry, width, min(P, width - c0));
 }
 
 template <class E, int S, class W>
@@ -79,10 +69,29 @@ wc_status launch_one(const PullLaunch& L, const void* x, void* y) {
     note_launch(), spmv_pull_kernel<E, S, W><<<blocks, kPullThreads, smem, L.stream>>>(
         A, static_cast<const E*>(x), epi, L.err);
   } else {
-    uint32_t blocks = (L.n + 7) / 8;
+    uint32_t blocks = (L.unit_count + 7) / 8;
     blocks = blocks < 1 ? 1 : (blocks > L.max_blocks ? L.max_blocks : blocks);
-    note_launch(), spmm_rows_kernel<E, S, W><<<blocks, 256, 0, L.stream>>>(
-        A, L.n, L.width, static_cast<const E*>(x), static_cast<E*>(y), L.write, L.err);
+    auto* carry = static_cast<Partial<E, semiring_add(S)>*>(L.carry_multi);
+    // Blocks of P columns: P the smallest power of two covering the width,
+    // at most 32.
+    for (uint32_t c0 = 0; c0 < L.width; c0 += 32) {
+      const uint32_t cols = L.width - c0;
+      if (cols >= 32)
+        note_launch(), spmm_multi_kernel<E, S, W, 32><<<blocks, 256, 0, L.stream>>>(
+            A, static_cast<const E*>(x), static_cast<E*>(y), L.width, c0, L.write, L.err, carry);
+      else if (cols > 8)
+        note_launch(), spmm_multi_kernel<E, S, W, 16><<<blocks, 256, 0, L.stream>>>(
+            A, static_cast<const E*>(x), static_cast<E*>(y), L.width, c0, L.write, L.err, carry);
+      else if (cols > 4)
+        note_launch(), spmm_multi_kernel<E, S, W, 8><<<blocks, 256, 0, L.stream>>>(
+            A, static_cast<const E*>(x), static_cast<E*>(y), L.width, c0, L.write, L.err, carry);
+      else if (cols > 2)
+        note_launch(), spmm_multi_kernel<E, S, W, 4><<<blocks, 256, 0, L.stream>>>(
+            A, static_cast<const E*>(x), static_cast<E*>(y), L.width, c0, L.write, L.err, carry);
+      else
+        note_launch(), spmm_multi_kernel<E, S, W, 2><<<blocks, 256, 0, L.stream>>>(
+            A, static_cast<const E*>(x), static_cast<E*>(y), L.width, c0, L.write, L.err, carry);
+    }
   }
   return cuda_status(cudaGetLastError(), L.detail, "product kernel launch");
 }

@@ -336,3 +336,29 @@ def test_components_match_the_oracle():
     off, tgt, _, _, _, _ = og.csr()
     got, _ = W.components(W.GraphVersion(off, tgt))
     assert np.all(got == 0)
+
+
+@pytest.mark.parametrize("width", [2, 3, 5, 16, 33])
+def test_spmm_hub_rows_every_width(width):
+    # Rows far over 256 entries (pieces combined in order) and widths that
+    # leave part of a column block idle; values are halves, so every sum is
+    # exact whatever the grouping.
+    rng = np.random.default_rng(width)
+    og, gv, *_ = hub_graph(rng, 6000, 4000)
+    n = gv.id_space
+    for semiring, dtype in (("plus_times", np.float64), ("min_plus", np.int64),
+                            ("max_times", np.float64), ("lor_land", np.uint8)):
+        x = values(rng, dtype, n, width=width)
+        y0 = values(rng, dtype, n, width=width)
+        for transpose in (False, True):
+            so, yo, sg, yg = run_both(og, gv, semiring, x, y0, transpose=transpose)
+            assert so == sg
+            if not so:
+                assert yg.tobytes() == yo.tobytes(), (semiring, transpose)
+    mask = (rng.random(n) < 0.5).astype(np.float64)
+    x = values(rng, np.float64, n, width=width)
+    y0 = values(rng, np.float64, n, width=width)
+    so, yo, sg, yg = run_both(og, gv, "plus_times", x, y0, mask=mask, complement=True,
+                              replace=True, accumulate="plus", transpose=True)
+    assert so == sg == 0
+    assert yg.tobytes() == yo.tobytes()
