@@ -536,7 +536,7 @@ def suite(args):
 
 
 # --------------------------------------------------------------- profiler cases
-# `python bench.py --case batched|spmv --scale S`: one small workload per
+# `python bench.py --case batched|spmv|ppr --scale S`: one small workload per
 # kernel family, for ncu captures (a few GB on the device at most).
 
 def profile_case(args):
@@ -560,6 +560,24 @@ def profile_case(args):
         torch.cuda.synchronize()
         print(json.dumps({"case": "batched", "nodes": n, "edges": g.edges,
                           "edges_traversed": int(e.sum())}))
+    elif args.case == "ppr":
+        # 32 personalised PageRank seed sets (sizes log-uniform 1..1000),
+        # one pass of 32 columns, tol 1e-10; two calls.
+        rng = np.random.default_rng(SEED)
+        sizes = np.exp(rng.uniform(0, np.log(1000), 32)).astype(np.int64)
+        sets = [rng.choice(n, int(s), replace=False) for s in sizes]
+        W.set_schedule(gv, "ppr", 32, columns_per_pass=32, blocks_per_sm=4)
+        r = torch.empty((32, n), dtype=torch.float64, device="cuda")
+        it = torch.empty(32, dtype=torch.int32, device="cuda")
+        for _ in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            W.ppr_batched(gv, sets, W.PageRank(0.85, 1e-10, 100), ranks_out=r,
+                          iterations_out=it)
+            torch.cuda.synchronize()
+            seconds = time.perf_counter() - t0
+        print(json.dumps({"case": "ppr", "nodes": n, "edges": g.edges, "seconds": seconds,
+                          "iterations_max": int(it.max()), "iterations_mean": float(it.float().mean())}))
     else:
         # SpMV plus_times (f64, unweighted) over the forward CSR three
         # times, then a PageRank of three iterations.
@@ -582,7 +600,7 @@ def main():
     ap.add_argument("--impl", default="warren")
     ap.add_argument("--suite", default=None,
                     help="comma-separated configurations to measure instead: c1,c2,c3,c4,c5")
-    ap.add_argument("--case", default=None, choices=["batched", "spmv"],
+    ap.add_argument("--case", default=None, choices=["batched", "spmv", "ppr"],
                     help="a small workload for profilers instead")
     ap.add_argument("--scale", type=int, default=20)
     args = ap.parse_args()

@@ -1,6 +1,8 @@
 // batched.h — buffers and entry points shared by the batched searches.
 #pragma once
 
+#include <vector>
+
 #include "runtime.cuh"
 
 namespace wc {
@@ -22,5 +24,8 @@ typedef wc_status (*Mp32Fn)(Ctx&, const uint64_t*, const uint32_t*, const uint32
                             uint32_t, int64_t*, uint32_t*, uint32_t);
 Mp32Fn mp32_for(uint32_t columns);
 wc_status mp32_reserve(Ctx& ctx, uint32_t columns);
+
+// `count` seeded node ids below n, for the tuners' sample columns.
+void sample_nodes(uint32_t n, uint32_t count, std::vector<uint64_t>& out, uint64_t salt);
 
 }  // namespace wc

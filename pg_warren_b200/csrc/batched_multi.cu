@@ -1,13 +1,11 @@
-// batched_multi.cu — wc_minplus_batched and wc_ppr_batched: many
-// min-plus searches, or many personalised PageRanks, run as one SpMM over
-// P columns at a time (pull_multi.cuh), with every column stopping at its
-// own iterate.  No reference counterpart; each column computes what the
-// reference computes for it alone:
-//  - min-plus: compute_sql/library/sssp_vector.sql:14-66 over i64 — next
-//    starts as a copy of x, spmv(x → next, min_plus, transpose, accumulate
-//    min), stop when no distance fell or after max_iter iterations;
-//  - PageRank: compute/pagerank/mod.rs:96-287 with a seed vector of 1 on
-//    the seed set (personalisation 1/|set| on its live nodes).
+// batched_multi.cu — wc_minplus_batched: many min-plus searches run as one
+// SpMM over P columns at a time (pull_multi.cuh), with every column
+// stopping at its own iterate.  No reference counterpart; each column
+// computes what compute_sql/library/sssp_vector.sql:14-66 computes over i64
+// for its source alone — next starts as a copy of x, spmv(x → next,
+// min_plus, transpose, accumulate min), stop when no distance fell or after
+// max_iter iterations.  Versions whose distances fit 32 bits take the
+// 32-bit path (batched_minplus32.cu).
 // Each pass's iterations are queued without a host round trip: a control
 // step after each iteration updates the columns still running on the
 // device, and iterations with no column left return at once.
@@ -22,16 +20,6 @@
 #include "sqlfloat.cuh"
 
 namespace wc {
-
-__device__ inline bool tomb_bit(const uint64_t* t, uint32_t i) {
-  return t && ((t[i >> 6] >> (i & 63)) & 1);
-}
-
-template <class W> CsrView<W> view_of(const DevCsr& csr, const void* weights) {
-  return CsrView<W>{csr.offsets.as<uint32_t>(), csr.targets.as<uint32_t>(),
-                    static_cast<const W*>(weights), csr.schedule.units.as<Unit>(),
-                    csr.schedule.count, csr.schedule.counters.as<uint32_t>(), nullptr};
-}
 
 // =================================================================== min-plus
 
@@ -213,220 +201,8 @@ static MpFn mp_for(uint32_t p) {
   }
 }
 
-// ================================================================= PageRank
-
-struct PprState {
-  uint32_t n;
-  double* x[2];    // n × P
-  double* msg[2];  // n × P
-  const double* out;
-  const uint32_t* member;  // n: bit c set if node i is in column c's seed set
-  const double* share;     // P: 1 / |live part of set c|
-  const uint64_t* tomb;
-  double start, damping, teleport, threshold;
-  bool has_tol;
-  uint32_t k;
-  uint32_t* running;     // bit per column
-  uint32_t* executed;    // iterations run by any column
-  double* dangling;      // P, this iteration's dangling rank per column
-  double* partials;      // blocks × P × 2
-  unsigned* counter;
-  uint32_t* iterations;  // P
-  DeviceError* err;
-};
-
-__device__ inline double ppr_spread(double x, double out, double* msg, DeviceError* err, uint32_t i) {
-  if (sql_cmp_f(out, 0.0) > 0) {
-    double m;
-    int32_t s = sql_float<F_DIV>(x, out, &m);
-    if (s) raise(err, s, i);
-    *msg = m;
-    return 0.0;
-  }
-  *msg = 0.0;
-  return x;
-}
-
-template <int P> struct PprEpi {
-  const PprState* s;
-  int cur;
-  uint32_t run_bits;
-  double dangling_in;   // this lane's column
-  double delta, dangling_out;
-  __device__ void cell(uint32_t i, uint32_t c, bool present, double y) {
-    const PprState& st = *s;
-    const size_t at = (size_t)i * P + c;
-    const double old = st.x[cur][at];
-    if (!((run_bits >> c) & 1)) {  // stopped: carried forward unchanged
-      st.x[cur ^ 1][at] = old;
-      st.msg[cur ^ 1][at] = st.msg[cur][at];
-      return;
-    }
-    if (!present) y = 0.0;
-    double next = 0.0;
-    if (!tomb_bit(st.tomb, i)) {
-      const double p = ((st.member[i] >> c) & 1) ? st.share[c] : 0.0;
-      double dp, flowed, a, b;
-      int32_t e = sql_float<F_MUL>(dangling_in, p, &dp);
-      if (!e) e = sql_float<F_ADD>(y, dp, &flowed);
-      if (!e) e = sql_float<F_MUL>(st.damping, flowed, &a);
-      if (!e) e = sql_float<F_MUL>(st.teleport, p, &b);
-      if (!e) e = sql_float<F_ADD>(a, b, &next);
-      if (e) raise(st.err, e, i);
-    }
-    delta += fabs(next - old);
-    st.x[cur ^ 1][at] = next;
-    dangling_out += ppr_spread(next, st.out[i], &st.msg[cur ^ 1][at], st.err, i);
-  }
-};
-
-template <int P>
-__global__ void ppr_init_kernel(PprState s) {
-  double none = 0.0, dangling = 0.0;
-  const unsigned c = threadIdx.x % P;
-  // Each lane walks nodes for its column c.
-  for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) / P; i < s.n;
-       i += gridDim.x * blockDim.x / P) {
-    const size_t at = (size_t)i * P + c;
-    const double x = tomb_bit(s.tomb, i) ? 0.0 : s.start;
-    s.x[0][at] = x;
-    dangling += ppr_spread(x, s.out[i], &s.msg[0][at], s.err, i);
-  }
-  if (reduce_columns<P>(none, dangling, s.partials, s.counter) && threadIdx.x < P) {
-    s.dangling[threadIdx.x] = dangling;
-    if (threadIdx.x == 0) {
-      uint32_t run = 0;
-      for (uint32_t q = 0; q < s.k; q++) run |= 1u << q;
-      *s.running = run;
-      *s.executed = 0;
-    }
-    if (threadIdx.x < s.k) s.iterations[threadIdx.x] = 0;
-  }
-}
-
-template <int P, class W>
-__global__ void __launch_bounds__(256) ppr_iter_kernel(CsrView<W> A, PprState s, uint32_t it,
-                                                       Partial<double, WC_OP_PLUS>* carry,
-                                                       uint32_t max_iter) {
-  const uint32_t run = *(volatile uint32_t*)s.running;
-  if (!run) return;
-  const unsigned c = threadIdx.x % P;
-  PprEpi<P> epi{&s, (int)(it & 1), run, s.dangling[c], 0.0, 0.0};
-  pull_multi<double, WC_PLUS_TIMES, W, P>(A, s.msg[it & 1], epi, s.err, carry);
-  double delta = epi.delta, dangling = epi.dangling_out;
-  if (reduce_columns<P>(delta, dangling, s.partials, s.counter)) {
-    // Threads c < P of the last block hold column c's totals.  The stop
-    // test per column (pagerank/mod.rs:144-148): delta < live × tol.
-    const uint32_t q = threadIdx.x;
-    if (q < P && ((run >> q) & 1)) {
-      s.dangling[q] = dangling;
-      s.iterations[q] = it + 1;
-      const bool stop = it + 1 >= max_iter || (s.has_tol && sql_cmp_f(delta, s.threshold) < 0);
-      if (stop) atomicAnd(s.running, ~(1u << q));
-    }
-    if (q == 0) *s.executed = it + 1;
-  }
-}
-
-__global__ void ppr_member_kernel(const uint64_t* nodes, const uint64_t* offsets, uint32_t k,
-                                  uint32_t base, uint32_t* member) {
-  const uint32_t c = blockIdx.x;
-  if (c >= k) return;
-  for (uint64_t q = offsets[base + c] + threadIdx.x; q < offsets[base + c + 1]; q += blockDim.x)
-    atomicOr(member + nodes[q], 1u << c);
-}
-
-template <int P>
-wc_status ppr_pass(Ctx& ctx, const PageRankRun& base_run, const uint64_t* nodes,
-                   const uint64_t* offsets, const double* shares, uint32_t c0,
-                   uint32_t k, double* out, uint32_t* iterations_dev, uint32_t blocks_per_sm) {
-  wc_version* v = ctx.v;
-  const uint32_t n = (uint32_t)v->n;
-  const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(
-      max_blocks((int)blocks_per_sm), (v->rev.schedule.count + 7) / 8));
-  DevBuf *xb, *mb, *memb, *sb, *cb;
-  WC_TRY(ctx.scratch(POOL_BATCH_0, (uint64_t)n * P * 8 * 2, &xb));
-  WC_TRY(ctx.scratch(POOL_BATCH_1, (uint64_t)n * P * 8 * 2, &mb));
-  WC_TRY(ctx.scratch(POOL_BATCH_2, (uint64_t)n * 4, &memb));
-  WC_TRY(ctx.scratch(POOL_BATCH_3, 4096 + (uint64_t)grid * P * 16 + 64 * P, &sb));
-  WC_TRY(ctx.scratch(POOL_BATCH_4,
-                     (uint64_t)std::max<uint32_t>(v->rev.schedule.slots, 1) * P *
-                         sizeof(Partial<double, WC_OP_PLUS>), &cb));
-  WC_CUDA(cudaMemsetAsync(memb->ptr, 0, (uint64_t)n * 4, ctx.stream), ctx.detail);
-  WC_CUDA(cudaMemsetAsync(sb->ptr, 0, sb->bytes, ctx.stream), ctx.detail);
-  note_launch(), ppr_member_kernel<<<k, 128, 0, ctx.stream>>>(nodes, offsets, k, c0, memb->as<uint32_t>());
-  unsigned char* sc = sb->as<unsigned char>();
-  PprState s{};
-  s.n = n;
-  s.x[0] = xb->as<double>();
-  s.x[1] = s.x[0] + (size_t)n * P;
-  s.msg[0] = mb->as<double>();
-  s.msg[1] = s.msg[0] + (size_t)n * P;
-  s.out = base_run.s.out;
-  s.member = memb->as<uint32_t>();
-  s.share = shares + c0;
-  s.tomb = base_run.s.tomb;
-  s.start = base_run.s.start;
-  s.damping = base_run.s.damping;
-  s.teleport = base_run.s.teleport;
-  s.threshold = base_run.s.threshold;
-  s.has_tol = base_run.s.has_tol;
-  s.k = k;
-  s.running = reinterpret_cast<uint32_t*>(sc + 8 * 32);
-  s.executed = reinterpret_cast<uint32_t*>(sc + 8 * 32 + 8);
-  s.counter = reinterpret_cast<unsigned*>(sc + 8 * 32 + 16);
-  s.dangling = reinterpret_cast<double*>(sc + 8 * 64);
-  s.iterations = iterations_dev;
-  s.partials = reinterpret_cast<double*>(sc + 4096);
-  s.err = v->error.as<DeviceError>();
-  note_launch(), ppr_init_kernel<P><<<grid, 256, 0, ctx.stream>>>(s);
-  auto* carry = cb->as<Partial<double, WC_OP_PLUS>>();
-  const uint32_t max_iter = base_run.opts.max_iter;
-  for (uint32_t it = 0; it < max_iter; it++) {
-    if (base_run.opts.weighted != 0 && v->weighted)
-      note_launch(), ppr_iter_kernel<P, double><<<grid, 256, 0, ctx.stream>>>(
-          view_of<double>(v->rev, v->rev.weights.ptr), s, it, carry, max_iter);
-    else
-      note_launch(), ppr_iter_kernel<P, void><<<grid, 256, 0, ctx.stream>>>(view_of<void>(v->rev, nullptr), s, it,
-                                                             carry, max_iter);
-  }
-  note_launch(), columns_out_kernel<P, double><<<max_blocks(4), 256, 0, ctx.stream>>>(
-      s.x[0], s.x[1], s.executed, n, k, out, nullptr);
-  return cuda_status(cudaGetLastError(), ctx.detail, "batched pagerank pass");
-}
-
-// The pass's scratch, acquired before a pass is captured.
-static wc_status ppr_reserve(Ctx& ctx, uint32_t P, uint32_t blocks_per_sm) {
-  wc_version* v = ctx.v;
-  const uint64_t n = v->n;
-  const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(
-      max_blocks((int)blocks_per_sm), (v->rev.schedule.count + 7) / 8));
-  DevBuf* b;
-  WC_TRY(ctx.scratch(POOL_BATCH_0, n * P * 8 * 2, &b));
-  WC_TRY(ctx.scratch(POOL_BATCH_1, n * P * 8 * 2, &b));
-  WC_TRY(ctx.scratch(POOL_BATCH_2, n * 4, &b));
-  WC_TRY(ctx.scratch(POOL_BATCH_3, 4096 + (uint64_t)grid * P * 16 + 64 * P, &b));
-  return ctx.scratch(POOL_BATCH_4,
-                     (uint64_t)std::max<uint32_t>(v->rev.schedule.slots, 1) * P *
-                         sizeof(Partial<double, WC_OP_PLUS>), &b);
-}
-
-typedef wc_status (*PprFn)(Ctx&, const PageRankRun&, const uint64_t*, const uint64_t*,
-                           const double*, uint32_t, uint32_t, double*, uint32_t*, uint32_t);
-
-static PprFn ppr_for(uint32_t p) {
-  switch (p) {
-    case 1: return ppr_pass<1>;
-    case 2: return ppr_pass<2>;
-    case 4: return ppr_pass<4>;
-    case 8: return ppr_pass<8>;
-    case 16: return ppr_pass<16>;
-    default: return ppr_pass<32>;
-  }
-}
-
 // Seeded sample columns for the tuners.
-static void sample_nodes(uint32_t n, uint32_t count, std::vector<uint64_t>& out, uint64_t salt) {
+void sample_nodes(uint32_t n, uint32_t count, std::vector<uint64_t>& out, uint64_t salt) {
   out.resize(count);
   uint64_t z = salt;
   for (uint32_t s = 0; s < count; s++) {
@@ -467,54 +243,6 @@ wc_status tune_minplus(Ctx& ctx, uint32_t width, wc_schedule* best) {
         WC_CUDA(cudaEventRecord(a, ctx.stream), ctx.detail);
         WC_TRY(mp_for(P)(ctx, S->as<uint64_t>(), C->as<uint32_t>(), ident->as<uint32_t>(), k, 16,
                          D->as<int64_t>(), I->as<uint32_t>(), bps));
-        WC_CUDA(cudaEventRecord(b, ctx.stream), ctx.detail);
-        WC_CUDA(cudaEventSynchronize(b), ctx.detail);
-        WC_CUDA(cudaEventElapsedTime(&ms, a, b), ctx.detail);
-      }
-      if (ms / k < best_per) {
-        best_per = ms / k;
-        *best = wc_schedule{P, 1, bps, 0};
-      }
-    }
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
-  return WC_OK;
-}
-
-wc_status tune_ppr(Ctx& ctx, uint32_t width, wc_schedule* best) {
-  wc_version* v = ctx.v;
-  const uint32_t sample = std::min<uint32_t>(width, 32);
-  std::vector<uint64_t> nodes;
-  sample_nodes((uint32_t)v->n, sample, nodes, 0x9e11u);
-  std::vector<uint64_t> offs(sample + 1);
-  for (uint32_t c = 0; c <= sample; c++) offs[c] = c;
-  std::vector<double> shares(sample, 1.0);
-  DevBuf *N, *F, *R, *I, *SH;
-  WC_TRY(ctx.scratch(POOL_BATCH_11, sample * 8, &SH));
-  WC_CUDA(cudaMemcpyAsync(SH->ptr, shares.data(), sample * 8, cudaMemcpyHostToDevice, ctx.stream),
-          ctx.detail);
-  WC_TRY(ctx.scratch(POOL_BATCH_5, sample * 8, &N));
-  WC_TRY(ctx.scratch(POOL_BATCH_6, (sample + 1) * 8, &F));
-  WC_TRY(ctx.scratch(POOL_BATCH_7, (uint64_t)sample * v->n * 8, &R));
-  WC_TRY(ctx.scratch(POOL_BATCH_9, sample * 4, &I));
-  WC_CUDA(cudaMemcpyAsync(N->ptr, nodes.data(), sample * 8, cudaMemcpyHostToDevice, ctx.stream), ctx.detail);
-  WC_CUDA(cudaMemcpyAsync(F->ptr, offs.data(), (sample + 1) * 8, cudaMemcpyHostToDevice, ctx.stream), ctx.detail);
-  wc_pagerank_opts o{0.85, 1e-10, 1, -1, 10, nullptr};
-  PageRankRun base;
-  WC_TRY(base.setup(ctx, &o, nullptr, nullptr));
-  cudaEvent_t a, b;
-  WC_CUDA(cudaEventCreate(&a), ctx.detail);
-  WC_CUDA(cudaEventCreate(&b), ctx.detail);
-  float best_per = 1e30f;
-  for (uint32_t P : {1u, 2u, 4u, 8u, 16u, 32u})
-    for (uint32_t bps : {4u, 8u}) {
-      if (P > sample && P != 1) continue;
-      const uint32_t k = std::min(P, sample);
-      float ms = 0;
-      for (int rep = 0; rep < 2; rep++) {
-        WC_CUDA(cudaEventRecord(a, ctx.stream), ctx.detail);
-        WC_TRY(ppr_for(P)(ctx, base, N->as<uint64_t>(), F->as<uint64_t>(), SH->as<double>(), 0, k,
-                          R->as<double>(), I->as<uint32_t>(), bps));
         WC_CUDA(cudaEventRecord(b, ctx.stream), ctx.detail);
         WC_CUDA(cudaEventSynchronize(b), ctx.detail);
         WC_CUDA(cudaEventElapsedTime(&ms, a, b), ctx.detail);
@@ -622,75 +350,6 @@ wc_status wc_minplus_batched(wc_version* v, const wc_call* call, const uint64_t*
     }));
   }
   WC_TRY(D.out(ctx));
-  if (iterations_out)
-    WC_CUDA(cudaMemcpyAsync(iterations_out, its->ptr, width * 4, cudaMemcpyDefault, ctx.stream),
-            ctx.detail);
-  return ctx.finish();
-}
-
-wc_status wc_ppr_batched(wc_version* v, const wc_call* call, const wc_pagerank_opts* o,
-                         const uint64_t* seed_nodes, const uint64_t* seed_offsets, uint32_t width,
-                         double* ranks_out, uint32_t* iterations_out) {
-  if (!v || !o || (width && (!seed_offsets || !ranks_out))) return WC_INVALID_ARGUMENT;
-  std::lock_guard<std::recursive_mutex> lock(v->mu);
-  WC_CUDA(cudaSetDevice(v->device), call ? call->detail : nullptr);
-  Ctx ctx(v, call);
-  if (ctx.cancelled()) return WC_CANCELLED;
-  if (width == 0) return WC_OK;
-  const uint64_t n = v->n;
-  std::vector<uint64_t> offs(width + 1);
-  WC_CUDA(cudaMemcpy(offs.data(), seed_offsets, (width + 1) * 8, cudaMemcpyDefault), ctx.detail);
-  std::vector<uint64_t> nodes(offs[width]);
-  if (!nodes.empty())
-    WC_CUDA(cudaMemcpy(nodes.data(), seed_nodes, nodes.size() * 8, cudaMemcpyDefault), ctx.detail);
-  WC_TRY(ctx.begin());
-  PageRankRun base;
-  WC_TRY(base.setup(ctx, o, nullptr, nullptr));
-  // Each set's personalisation (pagerank/mod.rs:155-199 with a seed of 1
-  // on the set): the set's live size summed in the reference's order is
-  // exact (integers), then 1 / size, then 1 × that share.
-  std::vector<double> shares(width);
-  std::vector<uint64_t> dedup;
-  for (uint32_t c = 0; c < width; c++) {
-    dedup.assign(nodes.begin() + offs[c], nodes.begin() + offs[c + 1]);
-    std::sort(dedup.begin(), dedup.end());
-    dedup.erase(std::unique(dedup.begin(), dedup.end()), dedup.end());
-    for (uint64_t q : dedup)
-      if (q >= n) {
-        if (ctx.detail) ctx.detail->node = q;
-        return WC_NODE_OUTSIDE_ID_SPACE;
-      }
-    double total;
-    WC_TRY((wc_status)sql_float<F_DIV>(1.0, (double)dedup.size(), &total));
-    shares[c] = total;
-  }
-  Operand N(POOL_BATCH_5), F(POOL_BATCH_6), R(POOL_BATCH_7);
-  WC_TRY(N.in(ctx, seed_nodes, std::max<uint64_t>(nodes.size(), 1) * 8));
-  WC_TRY(F.in(ctx, seed_offsets, (width + 1) * 8));
-  WC_TRY(R.output(ctx, ranks_out, (uint64_t)width * n * 8));
-  DevBuf* its;
-  WC_TRY(ctx.scratch(POOL_BATCH_9, (uint64_t)width * 4, &its));
-  const auto key = ((uint64_t)WC_BATCH_PPR << 32) | width;
-  const wc_schedule sched = v->tuned.count(key) ? v->tuned[key] : wc_schedule{4, 1, 4, 0};
-  const uint32_t P = std::max<uint32_t>(1, std::min<uint32_t>(32, sched.columns_per_pass));
-  const uint32_t bps = sched.blocks_per_sm ? sched.blocks_per_sm : 4;
-  DevBuf* sh;
-  WC_TRY(ctx.scratch(POOL_BATCH_11, (uint64_t)width * 8, &sh));
-  WC_CUDA(cudaMemcpyAsync(sh->ptr, shares.data(), (uint64_t)width * 8, cudaMemcpyHostToDevice,
-                          ctx.stream), ctx.detail);
-  WC_TRY(ppr_reserve(ctx, P, bps));
-  for (uint32_t c0 = 0; c0 < width; c0 += P) {
-    const uint32_t k = std::min(P, width - c0);
-    const std::string gk = "ppr/" + std::to_string(P) + "/" + std::to_string(k) + "/" +
-                           std::to_string(o->max_iter) + "/" + std::to_string(bps);
-    WC_TRY(ctx.run_captured(gk, [&] {
-      return ppr_for(P)(ctx, base, static_cast<const uint64_t*>(N.dev),
-                        static_cast<const uint64_t*>(F.dev), sh->as<double>(), c0, k,
-                        static_cast<double*>(R.dev) + (uint64_t)c0 * n, its->as<uint32_t>() + c0,
-                        bps);
-    }));
-  }
-  WC_TRY(R.out(ctx));
   if (iterations_out)
     WC_CUDA(cudaMemcpyAsync(iterations_out, its->ptr, width * 4, cudaMemcpyDefault, ctx.stream),
             ctx.detail);

@@ -18,6 +18,18 @@
 
 namespace wc {
 
+// Bit i of a tombstone bitmap (NULL: no tombstones).
+__device__ inline bool tomb_bit(const uint64_t* t, uint32_t i) {
+  return t && ((t[i >> 6] >> (i & 63)) & 1);
+}
+
+// The schedule view of one orientation with its weights (W = void: none).
+template <class W> CsrView<W> view_of(const DevCsr& csr, const void* weights) {
+  return CsrView<W>{csr.offsets.as<uint32_t>(), csr.targets.as<uint32_t>(),
+                    static_cast<const W*>(weights), csr.schedule.units.as<Unit>(),
+                    csr.schedule.count, csr.schedule.counters.as<uint32_t>(), nullptr};
+}
+
 // Folds entries [e0, e1) of column `c` into `acc` in order (X's rows are
 // `ld` elements apart; an inactive lane folds nothing).  All lanes of the
 // group run the same trip count (the group shares the row).
@@ -66,18 +78,21 @@ __device__ inline void fold_run(const CsrView<W>& A, const E* __restrict__ X, ui
 // Walks the schedule; `epi.cell(row, column, present, value)` is called
 // once per (row, column), always by a lane whose index is column mod P, so
 // an epilogue may keep per-column sums in registers.  X's rows are `ld`
-// elements apart; columns >= `columns` are folded by no lane.  `carry` holds P
-// partials per slot (the schedule's long-row pieces).
+// elements apart; columns >= `columns`, and columns whose bit in `mask` is
+// clear, are folded by no lane (their cells still come, with unspecified
+// values).  `carry` holds P partials per slot (the schedule's long-row
+// pieces).
 template <class E, int S, class W, int P, class Epi>
 __device__ inline void pull_multi(const CsrView<W>& A, const E* __restrict__ X, Epi& epi,
                                   DeviceError* err, Partial<E, semiring_add(S)>* carry,
-                                  uint32_t ld = P, uint32_t columns = P) {
+                                  uint32_t ld = P, uint32_t columns = P,
+                                  uint32_t mask = 0xffffffffu) {
   static_assert(P >= 1 && P <= 32 && (P & (P - 1)) == 0, "P: a power of two up to 32");
   constexpr int ADD = semiring_add(S);
   constexpr uint32_t G = 32 / P;
   const unsigned lane = threadIdx.x & 31;
   const uint32_t c = lane % P, g = lane / P;
-  const bool active = c < columns;
+  const bool active = c < columns && ((mask >> c) & 1);
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t u = warp; u < A.unit_count; u += warps) {

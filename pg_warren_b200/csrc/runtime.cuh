@@ -346,6 +346,15 @@ struct Ctx {
     if (!stream || cudaStreamIsCapturing(stream, &cs) != cudaSuccess ||
         cs != cudaStreamCaptureStatusNone)
       return enqueue();
+    cudaGraphExec_t exec = nullptr;
+    WC_TRY(capture(key, enqueue, &exec));
+    return cuda_status(cudaGraphLaunch(exec, stream), detail, "cudaGraphLaunch");
+  }
+
+  // Captures `enqueue`'s launch sequence from the stream (which no one may
+  // be capturing already) into the version's executable graph for `key`,
+  // updated in place or instantiated, and returns it without launching it.
+  template <class F> wc_status capture(const std::string& key, F&& enqueue, cudaGraphExec_t* out) {
     WC_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), detail);
     capturing = true;
     const wc_status st = enqueue();
@@ -375,7 +384,8 @@ struct Ctx {
       }
     }
     cudaGraphDestroy(graph);
-    return cuda_status(cudaGraphLaunch(exec, stream), detail, "cudaGraphLaunch");
+    *out = exec;
+    return WC_OK;
   }
 
   void collect_timings() {
