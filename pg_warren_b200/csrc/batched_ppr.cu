@@ -152,8 +152,59 @@ __global__ void ppr_init_kernel(PprStream s) {
   }
 }
 
-// One global iteration over the running slots; the last block runs each
-// slot's stop test and hands the next sets to the slots that stopped.
+// The last block's step after an iteration (threads q < P hold slot q's
+// delta and dangling mass): each running slot's stop test
+// (pagerank/mod.rs:144-148), then the next sets to the stopped slots in slot
+// order, and the progress report.
+template <int P>
+__device__ inline void ppr_control(const PprStream& s, uint32_t run, uint32_t g, double delta,
+                                   double dangling) {
+  PprCtl* ctl = s.ctl;
+  __shared__ uint32_t stopped;
+  if (threadIdx.x == 0) stopped = 0;
+  __syncthreads();
+  const uint32_t q = threadIdx.x;
+  if (q < P && ((run >> q) & 1)) {
+    const uint32_t its = ctl->slot_it[q] + 1;
+    ctl->slot_it[q] = its;
+    ctl->dangling[q] = dangling;
+    if (its >= s.max_iter || (s.has_tol && sql_cmp_f(delta, s.threshold) < 0)) {
+      s.iterations[ctl->slot_set[q]] = its;
+      atomicOr(&stopped, 1u << q);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t refilled = 0;
+    for (uint32_t b = stopped; b; b &= b - 1) {
+      const uint32_t slot = __ffs(b) - 1;
+      ctl->fin_set[slot] = ctl->slot_set[slot];
+      const uint32_t nx = ctl->next;
+      if (nx < s.width) {
+        ctl->next = nx + 1;
+        ctl->slot_set[slot] = nx;
+        ctl->share[slot] = s.shares[nx];
+        ctl->dangling[slot] = ctl->d0;
+        ctl->slot_it[slot] = 0;
+        refilled |= 1u << slot;
+      } else {
+        ctl->slot_set[slot] = kNoSet;
+      }
+    }
+    const uint32_t now = (run & ~stopped) | refilled;
+    ctl->running = now;
+    ctl->finished = stopped;
+    ctl->refilled = refilled;
+    ctl->g = g + 1;
+    if (s.pace) {
+      volatile uint32_t* pace = s.pace;
+      pace[1] = now == 0;
+      pace[0] = g + 1;
+    }
+  }
+}
+
+// One global iteration over the running slots (P = 8 or 16: pull_multi).
 template <int P, class W>
 __global__ void __launch_bounds__(256) ppr_iter_kernel(CsrView<W> A, PprStream s,
                                                        Partial<double, WC_OP_PLUS>* carry) {
@@ -172,51 +223,224 @@ __global__ void __launch_bounds__(256) ppr_iter_kernel(CsrView<W> A, PprStream s
   PprEpi<P> epi{&s, cur, run, ctl->dangling[c], ctl->share[c], 0.0, 0.0};
   pull_multi<double, WC_PLUS_TIMES, W, P>(A, s.msg[cur], epi, s.err, carry, P, P, run);
   double delta = epi.delta, dangling = epi.dangling_out;
-  if (reduce_columns<P>(delta, dangling, s.partials, &ctl->counter)) {
-    __shared__ uint32_t stopped;
-    if (threadIdx.x == 0) stopped = 0;
-    __syncthreads();
-    const uint32_t q = threadIdx.x;
-    if (q < P && ((run >> q) & 1)) {
-      const uint32_t its = ctl->slot_it[q] + 1;
-      ctl->slot_it[q] = its;
-      ctl->dangling[q] = dangling;
-      if (its >= s.max_iter || (s.has_tol && sql_cmp_f(delta, s.threshold) < 0)) {
-        s.iterations[ctl->slot_set[q]] = its;
-        atomicOr(&stopped, 1u << q);
+  if (reduce_columns<P>(delta, dangling, s.partials, &ctl->counter))
+    ppr_control<P>(s, run, g, delta, dangling);
+}
+
+// ------------------------------------------------------ the 32-slot pull
+// With 32 slots a row of the msg operand is 256 bytes and one lane owns one
+// column.  The iteration is bound by the latency of the row gathers, not by
+// bandwidth, so the warp keeps them in flight with asynchronous copies
+// (cp.async) into shared memory instead of registers: a unit's gathers go
+// out 16 entries at a time, two groups in flight, and the tile's old ranks
+// (the R rows of x, contiguous) arrive the same way while the targets,
+// row ends and per-row values load into lanes.  Entries are folded in
+// ascending order per row, as pull_multi folds them, so the ranks are the
+// same to the bit.
+
+constexpr uint32_t kPpr32Warps = 4;          // warps a block
+constexpr uint32_t kPpr32Chunk = 16;         // entries a gather group
+constexpr uint32_t kPpr32WarpDoubles = 2048;  // old ranks (32 × 32) + ring (2 × 16 × 32)
+
+__device__ inline void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src)
+               : "memory");
+}
+__device__ inline void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src)
+               : "memory");
+}
+__device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ inline void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// v[i] for a register array and a run-time i (selects, no local memory).
+template <class T> __device__ inline T pick8(const T (&v)[8], uint32_t i) {
+  T r = v[0];
+#pragma unroll
+  for (uint32_t q = 1; q < 8; q++)
+    if (i == q) r = v[q];
+  return r;
+}
+
+template <class W>
+__global__ void __launch_bounds__(kPpr32Warps * 32)
+    ppr_iter32_kernel(CsrView<W> A, PprStream s, Partial<double, WC_OP_PLUS>* carry) {
+  constexpr int ADD = WC_OP_PLUS;
+  typedef EntryOf<double, WC_PLUS_TIMES, W> Ent;
+  typedef Partial<double, ADD> Part;
+  PprCtl* ctl = s.ctl;
+  const uint32_t run = *(volatile uint32_t*)&ctl->running;
+  if (!run) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      ctl->finished = 0;
+      ctl->refilled = 0;
+    }
+    return;
+  }
+  extern __shared__ __align__(16) double ppr_smem[];
+  const uint32_t g = *(volatile uint32_t*)&ctl->g;
+  const int cur = g & 1;
+  const unsigned lane = threadIdx.x & 31;
+  double* xold = ppr_smem + (threadIdx.x >> 5) * kPpr32WarpDoubles;  // [row][column]
+  double* ring = xold + 32 * 32;                                      // [slot][column]
+  const bool active = (run >> lane) & 1;
+  const double dangling_in = ctl->dangling[lane], share = ctl->share[lane];
+  double delta = 0.0, dangling_out = 0.0;
+  const double* __restrict__ X = s.msg[cur];
+  const double* XO = s.x[cur];
+  double* XN = s.x[cur ^ 1];
+  double* MN = s.msg[cur ^ 1];
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+
+  // The rank update of row i for this lane's column (pagerank/mod.rs:201-282).
+  auto emit = [&](uint32_t i, const Part& acc, double old, uint32_t mem, double outw, bool dead) {
+    if (!active) return;
+    double y = 0.0;
+    if (acc.present) acc.acc.value(&y);
+    double next = 0.0;
+    if (!dead) {
+      const double p = ((mem >> lane) & 1) ? share : 0.0;
+      double dp, flowed, a, b;
+      int32_t e = sql_float<F_MUL>(dangling_in, p, &dp);
+      if (!e) e = sql_float<F_ADD>(y, dp, &flowed);
+      if (!e) e = sql_float<F_MUL>(s.damping, flowed, &a);
+      if (!e) e = sql_float<F_MUL>(s.teleport, p, &b);
+      if (!e) e = sql_float<F_ADD>(a, b, &next);
+      if (e) raise(s.err, e, i);
+    }
+    delta += fabs(next - old);
+    XN[(size_t)i * 32 + lane] = next;
+    dangling_out += ppr_spread(next, outw, &MN[(size_t)i * 32 + lane], s.err, i);
+  };
+  // Folds entry `e` (its gathered value in ring slot `slot`) into `acc`.
+  auto fold = [&](Part& acc, uint32_t slot, typename Ent::WT wv, uint32_t row) {
+    if (!active) return;
+    const double xv = ring[slot * 32 + lane];
+    double p;
+    int32_t st = Ent::product(wv, xv, &p);
+    if (st) raise(s.err, st, row);
+    if (acc.present) {
+      double sum;
+      acc.acc.value(&sum);
+      st = Apply<double, ADD>::go(sum, p, &sum);
+      if (st) raise(s.err, st, row);
+      acc.acc = Acc<double, ADD>::of(sum);
+    } else {
+      acc.acc = Acc<double, ADD>::of(p);
+      acc.present = true;
+    }
+  };
+
+  for (uint32_t u = warp; u < A.unit_count; u += warps) {
+    const Unit unit = A.units[u];
+    const bool tile = (unit.c >> 31) == 0;
+    const uint32_t a = unit.a;
+    const uint32_t R = tile ? unit.b - unit.a : 1;
+    const uint32_t base = tile ? unit.d : unit.b;
+    const uint32_t count = tile ? unit.c : unit.d - unit.b;
+    __syncwarp();  // every lane is done with the last unit's old ranks
+    if (tile) {
+      const double* src = XO + (size_t)a * 32;
+      for (uint32_t ch = lane; ch < R * 16; ch += 32) cp_async16(xold + ch * 2, src + ch * 2);
+    }
+    cp_async_commit();
+    // Targets and weights of the unit (≤ 256 entries): entry 32·q + lane in
+    // register q; per-row values of the tile: row `lane` in each lane.
+    uint32_t jr[8];
+    typename Ent::WT wr[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const uint32_t k = 32 * q + lane;
+      jr[q] = k < count ? __ldg(A.tgt + base + k) : 0u;
+      wr[q] = k < count ? Ent::load(A, base + k) : typename Ent::WT{};
+    }
+    uint32_t hi_l = count, mem_l = 0;
+    double out_l = 0.0;
+    bool dead_l = false;
+    if (tile && lane < R) {
+      hi_l = __ldg(A.off + a + lane + 1) - base;
+      mem_l = s.member[a + lane];
+      out_l = s.out[a + lane];
+      dead_l = tomb_bit(s.tomb, a + lane);
+    }
+    const uint32_t chunks = (count + kPpr32Chunk - 1) / kPpr32Chunk;
+    // Gather group q into ring half q & 1.
+    auto issue = [&](uint32_t q) {
+      const uint32_t jw = pick8(jr, q >> 1), off = (q & 1) * kPpr32Chunk;
+      double* dst = ring + off * 32 + lane;
+#pragma unroll
+      for (uint32_t t = 0; t < kPpr32Chunk; t++) {
+        const uint32_t j = __shfl_sync(0xffffffffu, jw, off + t);
+        if (active && q * kPpr32Chunk + t < count) cp_async8(dst + t * 32, X + (size_t)j * 32 + lane);
+      }
+      cp_async_commit();
+    };
+    if (chunks > 0) issue(0);
+    Part acc{Acc<double, ADD>::of(0.0), false};
+    uint32_t r = 0;
+    uint32_t hi_r = __shfl_sync(0xffffffffu, hi_l, 0);
+    for (uint32_t q = 0; q < chunks; q++) {
+      if (q + 1 < chunks) {
+        issue(q + 1);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncwarp();
+      const uint32_t n_q = min(kPpr32Chunk, count - q * kPpr32Chunk);
+      const typename Ent::WT ww = pick8(wr, q >> 1);
+      for (uint32_t t = 0; t < n_q; t++) {
+        const uint32_t k = q * kPpr32Chunk + t;
+        while (k >= hi_r) {  // rows ending before entry k (tiles only)
+          emit(a + r, acc, xold[r * 32 + lane], __shfl_sync(0xffffffffu, mem_l, r),
+               __shfl_sync(0xffffffffu, out_l, r), __shfl_sync(0xffffffffu, dead_l, r));
+          acc = Part{Acc<double, ADD>::of(0.0), false};
+          r++;
+          hi_r = __shfl_sync(0xffffffffu, hi_l, r);
+        }
+        const typename Ent::WT wv = (typename Ent::WT)__shfl_sync(0xffffffffu, ww, k & 31);
+        fold(acc, (q & 1) * kPpr32Chunk + t, wv, tile ? a + r : a);
       }
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      // New sets go to the stopped slots in slot order.
-      uint32_t refilled = 0;
-      for (uint32_t b = stopped; b; b &= b - 1) {
-        const uint32_t slot = __ffs(b) - 1;
-        ctl->fin_set[slot] = ctl->slot_set[slot];
-        const uint32_t nx = ctl->next;
-        if (nx < s.width) {
-          ctl->next = nx + 1;
-          ctl->slot_set[slot] = nx;
-          ctl->share[slot] = s.shares[nx];
-          ctl->dangling[slot] = ctl->d0;
-          ctl->slot_it[slot] = 0;
-          refilled |= 1u << slot;
-        } else {
-          ctl->slot_set[slot] = kNoSet;
-        }
+    if (chunks == 0) {
+      cp_async_wait<0>();
+      __syncwarp();
+    }
+    if (tile) {
+      for (; r < R; r++) {
+        emit(a + r, acc, xold[r * 32 + lane], __shfl_sync(0xffffffffu, mem_l, r),
+             __shfl_sync(0xffffffffu, out_l, r), __shfl_sync(0xffffffffu, dead_l, r));
+        acc = Part{Acc<double, ADD>::of(0.0), false};
       }
-      const uint32_t now = (run & ~stopped) | refilled;
-      ctl->running = now;
-      ctl->finished = stopped;
-      ctl->refilled = refilled;
-      ctl->g = g + 1;
-      if (s.pace) {
-        volatile uint32_t* pace = s.pace;
-        pace[1] = now == 0;
-        pace[0] = g + 1;
-      }
+      continue;
+    }
+    // A piece of a long row: its partial in the carry slot; the warp that
+    // brings the row's last piece combines the pieces in order and emits.
+    const uint32_t row = a, slot = unit.c & 0x7fffffffu;
+    const uint32_t row_lo = __ldg(A.off + row);
+    const uint32_t deg = __ldg(A.off + row + 1) - row_lo;
+    const uint32_t pieces = (deg + kPieceEntries - 1) / kPieceEntries;
+    const uint32_t first = slot - (base - row_lo) / kPieceEntries;
+    carry[(size_t)slot * 32 + lane] = acc;
+    __threadfence();
+    __syncwarp();
+    uint32_t arrived = 0;
+    if (lane == 0) arrived = atomicAdd(A.counters + first, 1u);
+    arrived = __shfl_sync(0xffffffffu, arrived, 0);
+    if (arrived == pieces - 1) {
+      __threadfence();
+      const Part total = combine_pieces<double, ADD, 32>(carry, first, pieces, lane, 0);
+      emit(row, total, XO[(size_t)row * 32 + lane], s.member[row], s.out[row],
+           tomb_bit(s.tomb, row));
+      __syncwarp();
+      if (lane == 0) A.counters[first] = 0;
     }
   }
+  if (reduce_columns<32>(delta, dangling_out, s.partials, &ctl->counter))
+    ppr_control<32>(s, run, g, delta, dangling_out);
 }
 
 // After an iteration: the stopped slots' ranks go out to their sets' rows,
@@ -270,16 +494,18 @@ __global__ void ppr_start_out_kernel(PprStream s) {
     s.iterations[q] = 0;
 }
 
-static uint32_t ppr_grid(const wc_version* v, uint32_t blocks_per_sm) {
+// Blocks of 8 warps (P = 8, 16) or kPpr32Warps (P = 32), at most one warp a unit.
+static uint32_t ppr_grid(const wc_version* v, uint32_t P, uint32_t blocks_per_sm) {
+  const uint32_t warps = P == 32 ? kPpr32Warps : 8;
   return std::max<uint32_t>(1, std::min<uint32_t>(max_blocks((int)blocks_per_sm),
-                                                  (v->rev.schedule.count + 7) / 8));
+                                                  (v->rev.schedule.count + warps - 1) / warps));
 }
 
 // The run's scratch, acquired before anything is queued or captured.
 static wc_status ppr_reserve(Ctx& ctx, uint32_t P, uint32_t blocks_per_sm) {
   wc_version* v = ctx.v;
   const uint64_t n = v->n;
-  const uint32_t grid = ppr_grid(v, blocks_per_sm);
+  const uint32_t grid = ppr_grid(v, P, blocks_per_sm);
   DevBuf* b;
   WC_TRY(ctx.scratch(POOL_BATCH_0, n * P * 8 * 2, &b));
   WC_TRY(ctx.scratch(POOL_BATCH_1, n * P * 8 * 2, &b));
@@ -294,12 +520,22 @@ template <int P>
 static void ppr_queue_iteration(Ctx& ctx, const PprStream& s, uint32_t grid, bool weighted,
                                 Partial<double, WC_OP_PLUS>* carry) {
   wc_version* v = ctx.v;
-  if (weighted)
-    note_launch(), ppr_iter_kernel<P, double><<<grid, 256, 0, ctx.stream>>>(
-        view_of<double>(v->rev, v->rev.weights.ptr), s, carry);
-  else
-    note_launch(), ppr_iter_kernel<P, void><<<grid, 256, 0, ctx.stream>>>(
-        view_of<void>(v->rev, nullptr), s, carry);
+  if constexpr (P == 32) {
+    constexpr size_t smem32 = kPpr32Warps * kPpr32WarpDoubles * sizeof(double);
+    if (weighted)
+      note_launch(), ppr_iter32_kernel<double><<<grid, kPpr32Warps * 32, smem32, ctx.stream>>>(
+          view_of<double>(v->rev, v->rev.weights.ptr), s, carry);
+    else
+      note_launch(), ppr_iter32_kernel<void><<<grid, kPpr32Warps * 32, smem32, ctx.stream>>>(
+          view_of<void>(v->rev, nullptr), s, carry);
+  } else {
+    if (weighted)
+      note_launch(), ppr_iter_kernel<P, double><<<grid, 256, 0, ctx.stream>>>(
+          view_of<double>(v->rev, v->rev.weights.ptr), s, carry);
+    else
+      note_launch(), ppr_iter_kernel<P, void><<<grid, 256, 0, ctx.stream>>>(
+          view_of<void>(v->rev, nullptr), s, carry);
+  }
   note_launch(), ppr_rows_kernel<P><<<max_blocks(4), 256, 0, ctx.stream>>>(s);
   note_launch(), ppr_members_kernel<<<P, 128, 0, ctx.stream>>>(s);
 }
@@ -313,7 +549,7 @@ wc_status ppr_stream(Ctx& ctx, const PageRankRun& base, const uint64_t* nodes,
                      uint32_t* iterations, uint32_t blocks_per_sm) {
   wc_version* v = ctx.v;
   const uint32_t n = (uint32_t)v->n;
-  const uint32_t grid = ppr_grid(v, blocks_per_sm);
+  const uint32_t grid = ppr_grid(v, P, blocks_per_sm);
   WC_TRY(ppr_reserve(ctx, P, blocks_per_sm));
   DevBuf *xb, *mb, *memb, *sb, *cb;
   WC_TRY(ctx.scratch(POOL_BATCH_0, (uint64_t)n * P * 8 * 2, &xb));
@@ -354,6 +590,13 @@ wc_status ppr_stream(Ctx& ctx, const PageRankRun& base, const uint64_t* nodes,
   }
   const bool weighted = base.opts.weighted != 0 && v->weighted;
   auto* carry = cb->as<Partial<double, WC_OP_PLUS>>();
+  if constexpr (P == 32) {
+    constexpr int smem32 = kPpr32Warps * kPpr32WarpDoubles * sizeof(double);
+    WC_CUDA(cudaFuncSetAttribute(ppr_iter32_kernel<double>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem32), ctx.detail);
+    WC_CUDA(cudaFuncSetAttribute(ppr_iter32_kernel<void>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem32), ctx.detail);
+  }
   // Greedy hand-out over P slots: no slot runs longer than the mean load
   // plus one set, so this many global iterations always finish every set.
   const uint64_t bound = ((uint64_t)width * s.max_iter + P - 1) / P + s.max_iter;
