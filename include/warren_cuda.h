@@ -396,6 +396,41 @@ wc_status wc_ppr_batched(wc_version* version, const wc_call* call, const wc_page
                          const uint64_t* seed_nodes, const uint64_t* seed_offsets, uint32_t width,
                          double* ranks_out, uint32_t* iterations_out);
 
+/* ------------------------------------------ multi-source centralities */
+
+/* compute/centrality/closeness.rs:36-56: closeness (NetworkX's, over the
+ * distances *to* each node, scaled by reached / other sources when
+ * wf_improved) or harmonic centrality, on the version's unweighted forward
+ * rows (for an undirected graph, upload it symmetrised), from `sources`. */
+typedef enum wc_centrality_measure { WC_CLOSENESS = 0, WC_HARMONIC = 1 } wc_centrality_measure;
+
+typedef struct wc_centrality_opts {
+    uint32_t measure;           /* wc_centrality_measure */
+    uint32_t wf_improved;       /* closeness: Wasserman and Faust's scaling */
+    uint32_t columns_per_pass;  /* sources a batched pass: 64 .. 1024 (0: 1024) */
+    uint32_t blocks_per_sm;     /* 0: 4 */
+} wc_centrality_opts;
+
+/* Chooses the sources as centrality/sources.rs:55-123 (Sources::choose):
+ * the live nodes the population mask selects (population[i] != 0, flipped
+ * by `complement`; NULL selects every node), then, if k >= 0 and fewer
+ * than them, the k with the smallest seeded keys; ascending.  sources_out
+ * holds up to id_space ids; count_out gets their number. */
+wc_status wc_sample_sources(uint64_t id_space, const uint64_t* tombstone_words,
+                            const uint8_t* population, int32_t complement, int64_t k,
+                            uint64_t seed, uint64_t* sources_out, uint64_t* count_out);
+
+/* Each node's centrality from `sources` (distinct live nodes, ascending, as
+ * wc_sample_sources gives them), as the reference's batched measures: the
+ * sources searched 64 at a time in ascending order, a node's totals added to
+ * batch by batch, then by distance (centrality/mod.rs:15-20, 158-190).  Exact
+ * when the sources are every live node, else the sampled estimate
+ * (closeness.rs:117-132, 229-241).  Tombstoned nodes get 0.  values_out
+ * f64[id_space].  A search deeper than 1,024 levels is WC_UNSUPPORTED. */
+wc_status wc_centrality(wc_version* version, const wc_call* call, const wc_centrality_opts* opts,
+                        const uint64_t* sources, uint64_t count, const uint64_t* tombstone_words,
+                        double* values_out);
+
 /* ------------------------------------------------------------- spectral */
 
 /* spectral/operator.rs:33-44 (Operator) and lanczos.rs:69-74 (Which). */

@@ -106,6 +106,10 @@ def _declare(L):
     L.wo_components.argtypes = [P, P, P, P]
     L.wo_topk_f64.restype = I32
     L.wo_topk_f64.argtypes = [P, U64, P, U64, I, P, P, P]
+    L.wo_sample_sources.restype = I32
+    L.wo_sample_sources.argtypes = [U64, P, P, I, C.c_int64, U64, P, P]
+    L.wo_centrality.restype = I32
+    L.wo_centrality.argtypes = [P, I, I, P, U64, P, P]
     if hasattr(L, "wo_eigen"):
         L.wo_eigen.restype = I32
         L.wo_eigen.argtypes = [P, I, I, I, I, D, U64, U64, P, P, P, P]
@@ -290,6 +294,28 @@ def components(g):
     et = np.zeros(1, np.uint64)
     _check(lib().wo_components(g.handle, _ptr(labels), _ptr(nv), _ptr(et)))
     return labels, int(nv[0]), int(et[0])
+
+
+def sample_sources(n, tombstones=None, population=None, complement=False, k=None, seed=0):
+    """centrality/sources.rs:55-123: the chosen sources, ascending."""
+    pop = None if population is None else np.ascontiguousarray(np.asarray(population) != 0,
+                                                                dtype=np.uint8)
+    out = np.zeros(max(n, 1), np.uint64)
+    count = np.zeros(1, np.uint64)
+    _check(lib().wo_sample_sources(n, _ptr(tombstones), _ptr(pop), int(complement),
+                                   -1 if k is None else int(k), seed & (2**64 - 1), _ptr(out),
+                                   _ptr(count)))
+    return out[:int(count[0])].copy()
+
+
+def centrality(g, measure, sources, tombstones=None, wf_improved=True):
+    """closeness.rs (measure "closeness" or "harmonic") from `sources`
+    (ascending), the batched measures' order: f64[n]."""
+    src = np.ascontiguousarray(sources, dtype=np.uint64)
+    out = np.zeros(g.n, np.float64)
+    _check(lib().wo_centrality(g.handle, 0 if measure == "closeness" else 1, int(wf_improved),
+                               _ptr(src), len(src), _ptr(tombstones), _ptr(out)))
+    return out
 
 
 def topk(x, k, descending=True, tombstones=None):

@@ -1005,6 +1005,103 @@ int32_t wo_components(const wo_graph* gp, uint64_t* labels, uint64_t* nodes_visi
   return WC_OK;
 }
 
+// compute/centrality/sources.rs:55-123 (Sources::choose): the live nodes
+// the population mask selects (nonzero, flipped by `complement`), then, if
+// k >= 0 is fewer, the k whose keys mix(mix(seed) ^ node·GOLDEN) are the
+// smallest (the keys are distinct), ascending by id.
+int32_t wo_sample_sources(uint64_t n, const uint64_t* tomb, const uint8_t* pop, int complement,
+                          int64_t k, uint64_t seed, uint64_t* out, uint64_t* count) {
+  std::vector<uint64_t> eligible;
+  for (uint64_t u = 0; u < n; u++)
+    if (!tombstoned(tomb, u) && (!pop || ((pop[u] != 0) != (complement != 0))))
+      eligible.push_back(u);
+  if (k >= 0 && (uint64_t)k < eligible.size()) {
+    std::vector<std::pair<uint64_t, uint64_t>> keyed;
+    for (uint64_t u : eligible) keyed.push_back({mix(mix(seed) ^ (u * GOLDEN)), u});
+    std::sort(keyed.begin(), keyed.end());
+    eligible.clear();
+    for (int64_t i = 0; i < k; i++) eligible.push_back(keyed[i].second);
+    std::sort(eligible.begin(), eligible.end());
+  }
+  std::copy(eligible.begin(), eligible.end(), out);
+  *count = eligible.size();
+  return WC_OK;
+}
+
+// compute/centrality/closeness.rs with the batched measures
+// (centrality/mod.rs:158-190, multi_source.rs:97-116): the sources in
+// batches of 64 in their order, each searched breadth-first over the
+// forward rows without a depth limit; per node, per batch, per distance d
+// ascending, the count c of the batch's sources first reaching it at d adds
+// c to reached, c·d to the distance sum and c / d to the harmonic sum.
+// Then closeness.rs:117-132 (closeness, r / total scaled by r / others
+// with wf_improved) or :229-241 (harmonic, scaled by (live - 1) / others
+// for a sample); tombstoned nodes 0.
+int32_t wo_centrality(const wo_graph* gp, int measure, int wf_improved, const uint64_t* sources,
+                      uint64_t count, const uint64_t* tomb, double* out) {
+  const Graph& g = *(const Graph*)gp;
+  const uint64_t n = g.fwd.n;
+  std::vector<uint64_t> reached(n, 0), dsum(n, 0);
+  std::vector<double> harm(n, 0.0);
+  std::vector<char> is_source(n, 0);
+  for (uint64_t i = 0; i < count; i++) is_source[sources[i]] = 1;
+  constexpr uint64_t kBatch = 64;
+  const uint64_t kFar = ~0ull;
+  std::vector<std::vector<uint64_t>> dist;
+  std::vector<uint64_t> queue, cnt;
+  for (uint64_t b0 = 0; b0 < count; b0 += kBatch) {
+    const uint64_t bk = std::min(kBatch, count - b0);
+    dist.assign(bk, std::vector<uint64_t>(n, kFar));
+    uint64_t deepest = 0;
+    for (uint64_t j = 0; j < bk; j++) {
+      std::vector<uint64_t>& d = dist[j];
+      queue.assign(1, sources[b0 + j]);
+      d[sources[b0 + j]] = 0;
+      for (uint64_t h = 0; h < queue.size(); h++) {
+        const uint64_t u = queue[h];
+        for (uint64_t e = g.fwd.off[u]; e < g.fwd.off[u + 1]; e++) {
+          const uint64_t t = g.fwd.tgt[e];
+          if (d[t] == kFar) {
+            d[t] = d[u] + 1;
+            deepest = std::max(deepest, d[t]);
+            queue.push_back(t);
+          }
+        }
+      }
+    }
+    cnt.assign(deepest + 1, 0);
+    for (uint64_t u = 0; u < n; u++) {
+      for (uint64_t j = 0; j < bk; j++)
+        if (dist[j][u] != kFar && dist[j][u] > 0) cnt[dist[j][u]]++;
+      for (uint64_t d = 1; d <= deepest; d++) {
+        if (!cnt[d]) continue;
+        reached[u] += cnt[d];
+        dsum[u] += cnt[d] * d;
+        harm[u] = harm[u] + (double)cnt[d] / (double)d;
+        cnt[d] = 0;
+      }
+    }
+  }
+  uint64_t live = 0;
+  for (uint64_t u = 0; u < n; u++) live += !tombstoned(tomb, u);
+  for (uint64_t u = 0; u < n; u++) {
+    double v = 0.0;
+    const uint64_t others = count - (uint64_t)is_source[u];
+    if (tombstoned(tomb, u)) {
+      v = 0.0;
+    } else if (measure == 0) {
+      const double r = (double)reached[u], total = (double)dsum[u];
+      if (total > 0.0 && live > 1) v = wf_improved ? r / total * (r / (double)others) : r / total;
+    } else if (count == live) {
+      v = harm[u];
+    } else if (others != 0) {
+      v = harm[u] * ((double)(live - 1) / (double)others);
+    }
+    out[u] = v;
+  }
+  return WC_OK;
+}
+
 // compute/ranking.rs:15-80 (top_k) over f64 values.
 int32_t wo_topk_f64(const double* x, uint64_t n, const uint64_t* tomb, uint64_t k, int descending,
                     uint64_t* nodes, double* values, uint64_t* count) {

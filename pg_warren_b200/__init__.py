@@ -11,11 +11,14 @@ from .api import *  # noqa: F401,F403
 from .api import (Budget, GraphVersion, Product, PageRank, Limits, EigenOptions, Interrupts,
                   spmv, spmm, pagerank, pagerank_noalloc, bfs, bfs_depths, reachable_set, reachable, components, bfs_batched,
                   minplus_batched, ppr_batched, autotune, set_schedule, eigen, pagerank_adjoint, top_k, rmat, gnm,
-                  edge_weights, node_set, HostGraph)
+                  edge_weights, node_set, HostGraph, Sampling, Centrality, sample_sources,
+                  closeness_centrality, harmonic_centrality)
 from ._abi import load, LIBRARY
 
 __all__ = ["Budget", "GraphVersion", "Product", "PageRank", "Limits", "EigenOptions",
            "Interrupts", "spmv", "spmm", "pagerank", "pagerank_noalloc", "bfs", "bfs_depths", "reachable_set",
            "reachable", "components", "bfs_batched", "minplus_batched", "ppr_batched", "autotune", "set_schedule", "eigen",
            "pagerank_adjoint", "top_k", "rmat", "gnm", "edge_weights", "node_set", "HostGraph",
+           "Sampling", "Centrality", "sample_sources", "closeness_centrality",
+           "harmonic_centrality",
            "load", "LIBRARY"]

@@ -85,6 +85,11 @@ class Schedule(C.Structure):
                 ("reserved", U32)]
 
 
+class CentralityOpts(C.Structure):
+    _fields_ = [("measure", U32), ("wf_improved", U32), ("columns_per_pass", U32),
+                ("blocks_per_sm", U32)]
+
+
 class EigenOpts(C.Structure):
     _fields_ = [("k", U32), ("which", I32), ("op", I32), ("symmetrize", I32), ("weighted", I32),
                 ("tol", D), ("max_iter", U64), ("seed", U64)]
@@ -133,6 +138,8 @@ SIGNATURES = [
     ("wc_bfs_batched", I32, [P, C.POINTER(Call), P, P, U32, P, P]),
     ("wc_minplus_batched", I32, [P, C.POINTER(Call), P, P, U32, P, P]),
     ("wc_ppr_batched", I32, [P, C.POINTER(Call), C.POINTER(PageRankOpts), P, P, U32, P, P]),
+    ("wc_sample_sources", I32, [U64, P, P, I32, C.c_int64, U64, P, C.POINTER(U64)]),
+    ("wc_centrality", I32, [P, C.POINTER(Call), C.POINTER(CentralityOpts), P, U64, P, P]),
     ("wc_eigen", I32, [P, C.POINTER(Call), C.POINTER(EigenOpts), P, P, P, C.POINTER(EigenStats)]),
     ("wc_pagerank_adjoint", I32, [P, C.POINTER(Call), C.POINTER(PageRankOpts), P, P, U32, D, P,
                                   P, P]),

@@ -598,6 +598,71 @@ def components(graph: GraphVersion, labels_out=None, interrupts=None):
     return labels, _stats(stats)
 
 
+# -------------------------------------------------------------- centrality
+
+
+@dataclass
+class Sampling:
+    """compute/centrality/sources.rs:22-33: `k` sources drawn with `seed`
+    from the live nodes `population` (a per-node mask, nonzero selects;
+    None: every node) selects; k None takes them all."""
+
+    k: Optional[int] = None
+    seed: int = 0
+    population: Optional[np.ndarray] = None
+    complement: bool = False
+
+
+@dataclass
+class Centrality:
+    """compute/centrality/mod.rs:67-73: the values and the number of sources."""
+
+    values: np.ndarray
+    sources: int
+
+
+def sample_sources(id_space: int, sampling: Sampling = Sampling(), tombstones=None) -> np.ndarray:
+    """The sources `sampling` chooses among the live nodes, ascending
+    (Sources::choose, sources.rs:55-95)."""
+    pop = None
+    if sampling.population is not None:
+        pop = np.ascontiguousarray(np.asarray(sampling.population) != 0, dtype=np.uint8)
+        if len(pop) != id_space:
+            raise IdSpaceMismatch(f"population over {len(pop)} nodes, id space {id_space}")
+    out = np.zeros(max(id_space, 1), np.uint64)
+    count = C.c_uint64(0)
+    k = -1 if sampling.k is None else int(sampling.k)
+    _raise(A.load().wc_sample_sources(id_space, _ptr(tombstones), _ptr(pop),
+                                      int(sampling.complement), k, sampling.seed & (2**64 - 1),
+                                      _ptr(out), C.byref(count)), A.ErrorDetail())
+    return out[:count.value].copy()
+
+
+def _centrality(graph: GraphVersion, measure: int, sampling: Sampling, tombstones,
+                wf_improved: bool, columns_per_pass: int, interrupts) -> Centrality:
+    sources = sample_sources(graph.id_space, sampling, tombstones)
+    values = np.zeros(graph.id_space, np.float64)
+    o = A.CentralityOpts(measure, int(wf_improved), columns_per_pass, 0)
+    call, detail = _call(interrupts)
+    _raise(A.load().wc_centrality(graph.handle, C.byref(call), C.byref(o), _ptr(sources),
+                                  len(sources), _ptr(tombstones), _ptr(values)), detail)
+    return Centrality(values, len(sources))
+
+
+def closeness_centrality(graph: GraphVersion, sampling: Sampling = Sampling(),
+                         wf_improved: bool = True, tombstones=None, columns_per_pass: int = 0,
+                         interrupts=None) -> Centrality:
+    """compute/centrality/closeness.rs:36-45 on the version's unweighted
+    forward rows (an undirected graph: upload it symmetrised)."""
+    return _centrality(graph, 0, sampling, tombstones, wf_improved, columns_per_pass, interrupts)
+
+
+def harmonic_centrality(graph: GraphVersion, sampling: Sampling = Sampling(), tombstones=None,
+                        columns_per_pass: int = 0, interrupts=None) -> Centrality:
+    """compute/centrality/closeness.rs:49-56, as closeness_centrality."""
+    return _centrality(graph, 1, sampling, tombstones, False, columns_per_pass, interrupts)
+
+
 def reachable(graph: GraphVersion, start: int, target: int, max_depth=None,
               direction="out") -> Traversed:
     """traversal/reachable.rs:18-43."""

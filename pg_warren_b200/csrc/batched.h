@@ -13,7 +13,21 @@ struct BatchBuffers {
   wc_status reserve(Ctx& ctx, uint32_t words, uint32_t levels);
 };
 
+// A centrality pass's per-node totals (kept across passes) and its flag
+// for a frontier left after the last level.
+struct CentArgs {
+  unsigned long long* reached;  // sources (other than the node) that reach it
+  unsigned long long* dsum;     // their summed distances
+  double* harm;                 // Σ 1 / distance, batch by batch
+  int* cut;
+};
+
 wc_schedule default_bfs_schedule(uint32_t width);
+// One batched BFS pass of up to `columns` (64 .. 1024) sources, every cap
+// `levels`, whose per-node counts go to `cent` instead of depths.
+wc_status bfs_centrality_pass(Ctx& ctx, BatchBuffers& b, uint32_t columns,
+                              const uint64_t* sources_dev, const uint32_t* caps_dev, uint32_t k,
+                              uint32_t levels, uint32_t blocks_per_sm, const CentArgs& cent);
 wc_status bfs_batched_run(Ctx& ctx, const wc_schedule& sched, const uint64_t* sources_dev,
                           const uint32_t* caps_dev, const uint32_t* caps_host, uint32_t width,
                           uint8_t* depth_dev, unsigned long long* edges_dev);

@@ -681,11 +681,69 @@ __global__ void __launch_bounds__(256)
     if (esum[x]) atomicAdd(edges + x, esum[x]);
 }
 
+// Centrality passes (wc_centrality): no depths; after the levels, a flag
+// if the last level reached any node (the pass must be run deeper), and
+// otherwise each node's counts added to its totals.
+__global__ void msbfs_cut_kernel(const uint32_t* wbits_last, uint32_t words, int* cut) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += gridDim.x * blockDim.x)
+    if (wbits_last[i]) *cut = 1;
+}
+
+// For each node u, the sources of the pass that first reach it at level L
+// are the bits of its row of F_L (rows marked written; level 0 is the
+// sources themselves).  They are counted per 64-source batch and the
+// totals taken in the order of compute/centrality/closeness.rs's batched
+// measures (mod.rs:15-20): batch by batch, then by distance — reached and
+// the distance sum as integers, the harmonic sum as count / distance added
+// one at a time.
+template <int W>
+__global__ void __launch_bounds__(256) msbfs_centrality_kernel(uint32_t n, uint32_t levels,
+                                                               const uint32_t* F, uint64_t fstride,
+                                                               const uint32_t* wbits,
+                                                               uint32_t bitmap_words, CentArgs c) {
+  static_assert(W % 2 == 0, "whole 64-source batches");
+  if (*(volatile const int*)c.cut) return;
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+    const uint32_t word = u >> 5, bit = u & 31;
+    unsigned long long reached = 0, dsum = 0;
+    double h = 0.0;
+    bool loaded = false;
+    for (uint32_t b = 0; b < W / 2; b++) {
+      for (uint32_t L0 = 1; L0 <= levels; L0 += 32) {
+        uint32_t lm = 0;  // written levels L0 .. L0 + 31
+        for (uint32_t j = 0; j < 32 && L0 + j <= levels; j++)
+          lm |= ((wbits[(size_t)(L0 + j) * bitmap_words + word] >> bit) & 1u) << j;
+        while (lm) {
+          const uint32_t L = L0 + __ffs(lm) - 1;
+          lm &= lm - 1;
+          const uint2 w2 = __ldg(reinterpret_cast<const uint2*>(F + (size_t)L * fstride +
+                                                                (size_t)u * W) + b);
+          const uint32_t cnt = __popc(w2.x) + __popc(w2.y);
+          if (cnt) {
+            if (!loaded) {
+              h = c.harm[u];
+              loaded = true;
+            }
+            reached += cnt;
+            dsum += (unsigned long long)cnt * L;
+            h = h + (double)cnt / (double)L;
+          }
+        }
+      }
+    }
+    if (loaded) {
+      c.reached[u] += reached;
+      c.dsum[u] += dsum;
+      c.harm[u] = h;
+    }
+  }
+}
+
 // One pass of up to 32·W sources.
 template <int W>
 wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const uint32_t* caps_dev,
                    uint32_t k, uint32_t levels, uint8_t* depth_dev, unsigned long long* edges_dev,
-                   uint32_t blocks_per_sm) {
+                   uint32_t blocks_per_sm, const CentArgs* cent) {
   wc_version* v = ctx.v;
   const uint32_t n = (uint32_t)v->n;
   const uint64_t row_words = (uint64_t)n * W;
@@ -740,6 +798,19 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
     note_launch(), msbfs_level_kernel<W><<<grid, 256, level_smem, st>>>(P);
   }
   ctx.phase_end();
+  if (cent) {
+    if constexpr (W % 2 == 0) {
+      // Rows first reached at the last level (F_levels's written rows) may
+      // have neighbours deeper still.
+      note_launch(), msbfs_cut_kernel<<<max_blocks(2), 256, 0, st>>>(
+          wbits + (uint64_t)levels * bitmap_words, (uint32_t)bitmap_words, cent->cut);
+      note_launch(), msbfs_centrality_kernel<W><<<max_blocks(4), 256, 0, st>>>(
+          n, levels, F, fstride, wbits, (uint32_t)bitmap_words, *cent);
+      return cuda_status(cudaGetLastError(), ctx.detail, "centrality pass");
+    } else {
+      return WC_INVALID_ARGUMENT;
+    }
+  }
   // Depths: persistent blocks of 32-node tiles.
   const uint32_t depth_grid = max_blocks(4);
   ctx.phase_begin("depth");
@@ -786,7 +857,7 @@ wc_status BatchBuffers::reserve(Ctx& ctx, uint32_t words, uint32_t levels) {
 }
 
 typedef wc_status (*PassFn)(Ctx&, BatchBuffers&, const uint64_t*, const uint32_t*, uint32_t,
-                            uint32_t, uint8_t*, unsigned long long*, uint32_t);
+                            uint32_t, uint8_t*, unsigned long long*, uint32_t, const CentArgs*);
 
 static PassFn pass_for(uint32_t columns) {
   switch (columns) {
@@ -830,10 +901,21 @@ wc_status bfs_batched_run(Ctx& ctx, const wc_schedule& sched, const uint64_t* so
                             std::to_string(levels) + "/" + std::to_string(bps);
     WC_TRY(ctx.run_captured(key, [&] {
       return pass_for(columns)(ctx, b, sources_dev + s0, caps_dev + s0, k, levels,
-                               depth_dev + (uint64_t)s0 * ctx.v->n, edges_dev + s0, bps);
+                               depth_dev + (uint64_t)s0 * ctx.v->n, edges_dev + s0, bps, nullptr);
     }));
   }
   return WC_OK;
+}
+
+wc_status bfs_centrality_pass(Ctx& ctx, BatchBuffers& b, uint32_t columns,
+                              const uint64_t* sources_dev, const uint32_t* caps_dev, uint32_t k,
+                              uint32_t levels, uint32_t blocks_per_sm, const CentArgs& cent) {
+  const std::string key = "cent/" + std::to_string(columns) + "/" + std::to_string(k) + "/" +
+                          std::to_string(levels) + "/" + std::to_string(blocks_per_sm);
+  return ctx.run_captured(key, [&] {
+    return pass_for(columns)(ctx, b, sources_dev, caps_dev, k, levels, nullptr, nullptr,
+                             blocks_per_sm, &cent);
+  });
 }
 
 wc_status tune_minplus(Ctx& ctx, uint32_t width, wc_schedule* best);

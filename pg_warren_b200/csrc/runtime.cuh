@@ -274,6 +274,8 @@ enum PoolTag {
   POOL_MINPLUS32_NACC = 120,
   POOL_WCC_PARENT = 130, POOL_WCC_FLAG, POOL_WCC_LABELS,
   POOL_SPMM_CARRY = 140,
+  POOL_CENT_TOTALS = 150, POOL_CENT_FLAG, POOL_CENT_SOURCES, POOL_CENT_CAPS, POOL_CENT_LIST,
+  POOL_CENT_TOMB, POOL_CENT_VALUES,
 };
 
 // A call's context: the stream, the caller's detail and cancellation.

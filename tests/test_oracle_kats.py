@@ -494,3 +494,56 @@ def test_components_label_by_smallest_dense_id(oracle):
     labels, nodes, edges = O.components(g)
     assert list(labels) == [0, 1, 0, 1, 0, 1, 6]
     assert (nodes, edges) == (7, 5)
+
+
+def centrality_example():
+    # compute/centrality/tests.rs:117-124, with its self-loop.
+    return directed(5, [(0, 1), (1, 2), (2, 3), (0, 2), (3, 0), (1, 3), (4, 1), (2, 2)])
+
+
+def test_closeness_and_harmonic_use_incoming_distances(oracle):
+    # compute/centrality/tests.rs:117-143 (NetworkX's values).
+    g = centrality_example()
+    every = O.sample_sources(5)
+    for wf in (True, False):
+        assert np.allclose(O.centrality(g, "closeness", every, wf_improved=wf),
+                           [0.5, 4 / 7, 2 / 3, 2 / 3, 0.0], rtol=1e-15, atol=0)
+    assert np.allclose(O.centrality(g, "harmonic", every), [7 / 3, 17 / 6, 3, 3, 0],
+                       rtol=1e-15, atol=0)
+    two = O.sample_sources(5, population=np.array([1, 0, 1, 0, 0]))
+    assert list(two) == [0, 2]
+    assert np.allclose(O.centrality(g, "harmonic", two),
+                       [0.5 * 4, 4 / 3 * 2, 1 * 4, 1.5 * 2, 0], rtol=1e-15, atol=0)
+
+
+def test_source_sampling_known_answers(oracle):
+    # compute/centrality/sources.rs:150-190.
+    import pg_warren_b200 as W
+    tomb = W.node_set(5, [2])
+    assert list(O.sample_sources(5, tombstones=tomb)) == [0, 1, 3, 4]
+    sel = np.array([1, 0, 1, 1, 0])
+    assert list(O.sample_sources(5, tombstones=W.node_set(5, [3]), population=sel)) == [0, 2]
+    assert list(O.sample_sources(4, k=9, seed=3)) == [0, 1, 2, 3]
+    a, b = O.sample_sources(1000, k=10, seed=7), O.sample_sources(1000, k=10, seed=8)
+    assert list(a) == list(O.sample_sources(1000, k=10, seed=7)) and list(a) != list(b)
+    counts = np.zeros(20, int)
+    for seed in range(2000):
+        counts[O.sample_sources(20, k=5, seed=seed)] += 1
+    assert ((400 <= counts) & (counts < 600)).all()
+
+
+def test_library_sampler_is_the_oracles(oracle):
+    # wc_sample_sources is host code: it runs without a device.
+    import pg_warren_b200 as W
+    rng = np.random.default_rng(3)
+    for _ in range(40):
+        n = int(rng.integers(1, 300))
+        tomb = W.node_set(n, rng.integers(0, n, int(rng.integers(0, 10))))
+        pop = rng.integers(0, 2, n) if rng.random() < 0.5 else None
+        comp = bool(rng.random() < 0.3)
+        k = None if rng.random() < 0.2 else int(rng.integers(0, n + 5))
+        seed = int(rng.integers(0, 2**63))
+        s = W.Sampling(k=k, seed=seed, population=pop, complement=comp)
+        got = W.sample_sources(n, s, tomb)
+        want = O.sample_sources(n, tombstones=tomb, population=pop, complement=comp, k=k, seed=seed)
+        assert np.array_equal(got, want)
