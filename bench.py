@@ -516,6 +516,50 @@ def leg_c5(W, O, torch, dev, stream, peak):
             "adjoint_iterations": int(its[1]), "fd_checks": checks}
 
 
+def leg_cent(W, O, torch, dev, stream, peak):
+    """Closeness and harmonic centrality on the batched BFS (no reference
+    configuration names them; R-MAT 22 and 16 as C1-C3): a seeded sample of
+    1,024 sources on R-MAT 22, every node of R-MAT 16, and a 64-source
+    sample checked bit for bit against the oracle, which also times it."""
+    out = {}
+    g = W.rmat(22)
+    gv = g.upload()
+    t0 = time.perf_counter()
+    src = W.sample_sources(g.id_space, W.Sampling(k=1024, seed=7))
+    sample_s = time.perf_counter() - t0
+    W.closeness_centrality(gv, sources=src)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    c = W.closeness_centrality(gv, sources=src)
+    t1 = time.perf_counter()
+    W.harmonic_centrality(gv, sources=src)
+    t2 = time.perf_counter()
+    out["rmat22_sample1024"] = {"sources": c.sources, "sample_s": sample_s,
+                                "closeness_s": t1 - t0, "harmonic_s": t2 - t1,
+                                "source_edges_per_s": c.sources * g.edges / (t1 - t0)}
+    del gv
+    g16 = W.rmat(16)
+    gv16 = g16.upload()
+    every = W.sample_sources(g16.id_space)
+    W.closeness_centrality(gv16, sources=every)
+    t0 = time.perf_counter()
+    c16 = W.closeness_centrality(gv16, sources=every)
+    every_s = time.perf_counter() - t0
+    og16 = O.Graph.from_csr(g16.id_space, g16.offsets, g16.targets)
+    small = W.Sampling(k=64, seed=3)
+    src = W.sample_sources(g16.id_space, small)
+    t0 = time.perf_counter()
+    want = O.centrality(og16, "harmonic", src)
+    cpu_s = time.perf_counter() - t0
+    got = W.harmonic_centrality(gv16, small).values
+    out["rmat16_every_node"] = {"sources": c16.sources, "seconds": every_s,
+                                "per_source_us": every_s / c16.sources * 1e6}
+    out["rmat16_sample64"] = {"bit_exact_vs_oracle": bool(got.tobytes() == want.tobytes()),
+                              "cpu_oracle_s": cpu_s, "cpu_threads": 1,
+                              "cpu_per_source_ms": cpu_s / 64 * 1e3}
+    return out
+
+
 def suite(args):
     import torch
     import pg_warren_b200 as W
@@ -525,7 +569,8 @@ def suite(args):
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(dev)
     peak, kind = measured_peaks()
-    legs = {"c1": leg_c1, "c2": leg_c2, "c3": leg_c3, "c4": leg_c4, "c5": leg_c5}
+    legs = {"c1": leg_c1, "c2": leg_c2, "c3": leg_c3, "c4": leg_c4, "c5": leg_c5,
+            "cent": leg_cent}
     out = {"peak_gbs": peak, "peak_kind": kind}
     for name in args.suite.split(","):
         t0 = time.time()
@@ -599,7 +644,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="warren")
     ap.add_argument("--suite", default=None,
-                    help="comma-separated configurations to measure instead: c1,c2,c3,c4,c5")
+                    help="comma-separated configurations to measure instead: c1,c2,c3,c4,c5,cent")
     ap.add_argument("--case", default=None, choices=["batched", "spmv", "ppr"],
                     help="a small workload for profilers instead")
     ap.add_argument("--scale", type=int, default=20)

@@ -639,8 +639,10 @@ def sample_sources(id_space: int, sampling: Sampling = Sampling(), tombstones=No
 
 
 def _centrality(graph: GraphVersion, measure: int, sampling: Sampling, tombstones,
-                wf_improved: bool, columns_per_pass: int, interrupts) -> Centrality:
-    sources = sample_sources(graph.id_space, sampling, tombstones)
+                wf_improved: bool, columns_per_pass: int, interrupts, sources) -> Centrality:
+    if sources is None:
+        sources = sample_sources(graph.id_space, sampling, tombstones)
+    sources = np.ascontiguousarray(sources, dtype=np.uint64)
     values = np.zeros(graph.id_space, np.float64)
     o = A.CentralityOpts(measure, int(wf_improved), columns_per_pass, 0)
     call, detail = _call(interrupts)
@@ -651,16 +653,19 @@ def _centrality(graph: GraphVersion, measure: int, sampling: Sampling, tombstone
 
 def closeness_centrality(graph: GraphVersion, sampling: Sampling = Sampling(),
                          wf_improved: bool = True, tombstones=None, columns_per_pass: int = 0,
-                         interrupts=None) -> Centrality:
+                         interrupts=None, sources=None) -> Centrality:
     """compute/centrality/closeness.rs:36-45 on the version's unweighted
-    forward rows (an undirected graph: upload it symmetrised)."""
-    return _centrality(graph, 0, sampling, tombstones, wf_improved, columns_per_pass, interrupts)
+    forward rows (an undirected graph: upload it symmetrised).  `sources`
+    (ascending, as sample_sources gives them) replaces the sampling."""
+    return _centrality(graph, 0, sampling, tombstones, wf_improved, columns_per_pass, interrupts,
+                       sources)
 
 
 def harmonic_centrality(graph: GraphVersion, sampling: Sampling = Sampling(), tombstones=None,
-                        columns_per_pass: int = 0, interrupts=None) -> Centrality:
+                        columns_per_pass: int = 0, interrupts=None, sources=None) -> Centrality:
     """compute/centrality/closeness.rs:49-56, as closeness_centrality."""
-    return _centrality(graph, 1, sampling, tombstones, False, columns_per_pass, interrupts)
+    return _centrality(graph, 1, sampling, tombstones, False, columns_per_pass, interrupts,
+                       sources)
 
 
 def reachable(graph: GraphVersion, start: int, target: int, max_depth=None,

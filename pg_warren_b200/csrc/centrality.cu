@@ -88,8 +88,12 @@ wc_status wc_sample_sources(uint64_t id_space, const uint64_t* tombstone_words,
     // The k smallest keys (sources.rs:97-118), then ascending ids.
     std::priority_queue<std::pair<uint64_t, uint64_t>> largest;
     for (uint64_t u : pop) {
-      largest.push({sample_key(seed, u), u});
-      if (largest.size() > (uint64_t)k) largest.pop();
+      const uint64_t key = sample_key(seed, u);
+      if (largest.size() == (uint64_t)k) {
+        if (k == 0 || key >= largest.top().first) continue;  // keys are distinct
+        largest.pop();
+      }
+      largest.push({key, u});
     }
     pop.clear();
     for (; !largest.empty(); largest.pop()) pop.push_back(largest.top().second);
