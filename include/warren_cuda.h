@@ -482,6 +482,32 @@ wc_status wc_pagerank_adjoint(wc_version* version, const wc_call* call,
                               const uint64_t* loss_offsets, uint32_t losses, double adjoint_tol,
                               double* grad_out, double* ranks_out, uint32_t* iterations_out);
 
+/* ------------------------------------------------------- vector reduce */
+
+/* compute/reduce.rs:23-38 (Reduction) and :74-82 (Norm), in order. */
+typedef enum wc_reduction {
+    WC_REDUCE_SUM = 0, WC_REDUCE_MAX = 1, WC_REDUCE_MIN = 2, WC_REDUCE_L1 = 3, WC_REDUCE_L2 = 4,
+    WC_REDUCE_NNZ = 5
+} wc_reduction;
+typedef enum wc_norm { WC_NORM_L1 = 0, WC_NORM_L2 = 1, WC_NORM_LINF = 2 } wc_norm;
+
+/* compute/reduce.rs:118-153 (reduce / reduce_live): `reduction` over the
+ * id_space × width elements of x (row-major, read as f64, bool as 0 / 1),
+ * skipping the rows tombstone_words marks (NULL: none), to the bit: chunks
+ * of 65,536 elements summed in order from +0, then the chunks in order.
+ * *is_null (may be NULL) is set for the max or min of no elements. */
+wc_status wc_vector_reduce(wc_version* version, const wc_call* call, wc_dtype dtype,
+                           const void* x, uint32_t width, const uint64_t* tombstone_words,
+                           wc_reduction reduction, double* result, int32_t* is_null);
+
+/* compute/reduce.rs:175-206 (norm_diff): norm(a − b), rows aligned by dense
+ * id and a row past the shorter vector's end counting as zero; 0 for no
+ * elements.  The vectors may be over other id spaces than the version's. */
+wc_status wc_vector_norm_diff(wc_version* version, const wc_call* call, wc_dtype dtype_a,
+                              const void* a, uint64_t id_space_a, wc_dtype dtype_b,
+                              const void* b, uint64_t id_space_b, uint32_t width, wc_norm norm,
+                              double* result);
+
 /* ------------------------------------------------------------- ranking */
 
 /* compute/ranking.rs:52 (top_k): the k live rows with the largest

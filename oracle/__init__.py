@@ -106,6 +106,10 @@ def _declare(L):
     L.wo_components.argtypes = [P, P, P, P]
     L.wo_topk_f64.restype = I32
     L.wo_topk_f64.argtypes = [P, U64, P, U64, I, P, P, P]
+    L.wo_reduce.restype = I32
+    L.wo_reduce.argtypes = [I, P, U64, U64, P, I, P, P]
+    L.wo_norm_diff.restype = I32
+    L.wo_norm_diff.argtypes = [I, P, U64, I, P, U64, U64, I, P]
     L.wo_sample_sources.restype = I32
     L.wo_sample_sources.argtypes = [U64, P, P, I, C.c_int64, U64, P, P]
     L.wo_centrality.restype = I32
@@ -294,6 +298,32 @@ def components(g):
     et = np.zeros(1, np.uint64)
     _check(lib().wo_components(g.handle, _ptr(labels), _ptr(nv), _ptr(et)))
     return labels, int(nv[0]), int(et[0])
+
+
+REDUCTIONS = ["sum", "max", "min", "l1", "l2", "nnz"]
+NORMS = ["l1", "l2", "linf"]
+_DT = {np.dtype(np.float32): 0, np.dtype(np.float64): 1, np.dtype(np.int64): 2,
+       np.dtype(np.bool_): 3, np.dtype(np.uint8): 3}
+
+
+def reduce(x, reduction, width=1, tombstones=None):
+    """compute/reduce.rs:118-153: the reduction of x's elements (rows of
+    `width`), skipping tombstoned rows; None for the max / min of none."""
+    x = np.ascontiguousarray(x)
+    out = np.zeros(1, np.float64)
+    null = np.zeros(1, np.int32)
+    _check(lib().wo_reduce(_DT[x.dtype], _ptr(x), x.size // width, width, _ptr(tombstones),
+                           REDUCTIONS.index(reduction), _ptr(out), _ptr(null)))
+    return None if null[0] else float(out[0])
+
+
+def norm_diff(a, b, norm, width=1):
+    """compute/reduce.rs:175-206."""
+    a, b = np.ascontiguousarray(a), np.ascontiguousarray(b)
+    out = np.zeros(1, np.float64)
+    _check(lib().wo_norm_diff(_DT[a.dtype], _ptr(a), a.size // width, _DT[b.dtype], _ptr(b),
+                              b.size // width, width, NORMS.index(norm), _ptr(out)))
+    return float(out[0])
 
 
 def sample_sources(n, tombstones=None, population=None, complement=False, k=None, seed=0):

@@ -1102,6 +1102,87 @@ int32_t wo_centrality(const wo_graph* gp, int measure, int wf_improved, const ui
   return WC_OK;
 }
 
+// compute/reduce.rs: elements read as f64 (bool 0 / 1), reduced in chunks
+// of 65,536 (reduce.rs:20) — sums in element order from +0, max / min
+// keeping the first of equal elements in SQL order — then the chunks'
+// results combined in chunk order (reduce.rs:250-268).
+static double elem_f64(int dtype, const void* p, uint64_t i, uint64_t len) {
+  if (i >= len) return 0.0;
+  switch (dtype) {
+    case 0: return (double)((const float*)p)[i];
+    case 1: return ((const double*)p)[i];
+    case 2: return (double)((const int64_t*)p)[i];
+    default: return ((const uint8_t*)p)[i] ? 1.0 : 0.0;
+  }
+}
+
+// reduction: 0 sum, 1 max, 2 min, 3 l1, 4 l2, 5 nnz; values(i) yields the
+// i-th element or nothing (skipped).
+static bool reduce_chunks(uint64_t len, int reduction,
+                          const std::function<bool(uint64_t, double*)>& values, double* result) {
+  const uint64_t kChunk = 1ull << 16;
+  const bool extreme = reduction == 1 || reduction == 2;
+  auto pick = [&](double a, double b) {  // greatest / least: the first on a tie
+    const int c = float_cmp(b, a);
+    return (reduction == 1 ? c > 0 : c < 0) ? b : a;
+  };
+  std::vector<std::pair<bool, double>> partials;
+  for (uint64_t c0 = 0; c0 < len; c0 += kChunk) {
+    bool any = false;
+    double acc = 0.0;
+    for (uint64_t i = c0; i < std::min(len, c0 + kChunk); i++) {
+      double v;
+      if (!values(i, &v)) continue;
+      if (extreme) {
+        acc = any ? pick(acc, v) : v;
+      } else {
+        const double term = reduction == 3 ? std::fabs(v) : reduction == 4 ? v * v
+                          : reduction == 5 ? (v != 0.0 ? 1.0 : 0.0) : v;
+        acc = acc + term;
+      }
+      any = true;
+    }
+    partials.push_back({extreme ? any : true, acc});
+  }
+  bool any = false;
+  double out = 0.0;
+  for (auto& p : partials) {
+    if (!p.first) continue;
+    out = extreme ? (any ? pick(out, p.second) : p.second) : out + p.second;
+    any = true;
+  }
+  if (reduction == 4) out = std::sqrt(out);
+  *result = out;
+  return extreme ? any : true;
+}
+
+int32_t wo_reduce(int dtype, const void* x, uint64_t n, uint64_t width, const uint64_t* tomb,
+                  int reduction, double* result, int32_t* is_null) {
+  const uint64_t len = n * width;
+  const bool found = reduce_chunks(len, reduction, [&](uint64_t i, double* v) {
+    if (tombstoned(tomb, i / width)) return false;
+    *v = elem_f64(dtype, x, i, len);
+    return true;
+  }, result);
+  *is_null = !found;
+  return WC_OK;
+}
+
+// reduce.rs:175-206 (norm_diff): 0 l1, 1 l2, 2 linf of a − b, a row past
+// the shorter vector's end read as zero; 0 for no elements.
+int32_t wo_norm_diff(int dtype_a, const void* a, uint64_t na, int dtype_b, const void* b,
+                     uint64_t nb, uint64_t width, int norm, double* result) {
+  const uint64_t la = na * width, lb = nb * width, len = std::max(la, lb);
+  const int reduction = norm == 0 ? 3 : norm == 1 ? 4 : 1;
+  const bool found = reduce_chunks(len, reduction, [&](uint64_t i, double* v) {
+    const double d = elem_f64(dtype_a, a, i, la) - elem_f64(dtype_b, b, i, lb);
+    *v = norm == 2 ? std::fabs(d) : d;
+    return true;
+  }, result);
+  if (!found) *result = 0.0;
+  return WC_OK;
+}
+
 // compute/ranking.rs:15-80 (top_k) over f64 values.
 int32_t wo_topk_f64(const double* x, uint64_t n, const uint64_t* tomb, uint64_t k, int descending,
                     uint64_t* nodes, double* values, uint64_t* count) {

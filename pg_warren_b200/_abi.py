@@ -143,6 +143,10 @@ SIGNATURES = [
     ("wc_eigen", I32, [P, C.POINTER(Call), C.POINTER(EigenOpts), P, P, P, C.POINTER(EigenStats)]),
     ("wc_pagerank_adjoint", I32, [P, C.POINTER(Call), C.POINTER(PageRankOpts), P, P, U32, D, P,
                                   P, P]),
+    ("wc_vector_reduce", I32, [P, C.POINTER(Call), I32, P, U32, P, I32, C.POINTER(D),
+                               C.POINTER(I32)]),
+    ("wc_vector_norm_diff", I32, [P, C.POINTER(Call), I32, P, U64, I32, P, U64, U32, I32,
+                                  C.POINTER(D)]),
     ("wc_topk", I32, [P, C.POINTER(Call), I32, P, P, U64, I32, P, P, C.POINTER(U64)]),
     ("wc_graph_rmat", I32, [U32, U32, D, D, D, U64, I32, C.POINTER(HostCsr)]),
     ("wc_graph_gnm", I32, [U64, U64, U64, I32, C.POINTER(HostCsr)]),

@@ -598,6 +598,49 @@ def components(graph: GraphVersion, labels_out=None, interrupts=None):
     return labels, _stats(stats)
 
 
+# ------------------------------------------------------------ vector reduce
+
+REDUCTIONS = ["sum", "max", "min", "l1", "l2", "nnz"]  # compute/reduce.rs:23-38
+NORMS = ["l1", "l2", "linf"]                            # compute/reduce.rs:74-82
+
+
+def _reduction(name: str, names) -> int:
+    if name not in names:
+        raise InvalidArgument(40)  # reduce.rs:64-72: an unknown reduction or norm
+    return names.index(name)
+
+
+def vector_reduce(graph: GraphVersion, x, reduction: str, tombstones=None, interrupts=None):
+    """compute/reduce.rs:118-153 (reduce, or reduce_live with tombstones):
+    `reduction` over x's id_space × width elements; None for the max or
+    min of no elements."""
+    width = 1 if getattr(x, "ndim", 1) == 1 else int(x.shape[1])
+    if _len(x) != graph.id_space:
+        raise IdSpaceMismatch(4)
+    out = C.c_double(0.0)
+    null = C.c_int32(0)
+    call, detail = _call(interrupts)
+    _raise(A.load().wc_vector_reduce(graph.handle, C.byref(call), _dtype(x), _ptr(x), width,
+                                     _ptr(tombstones), _reduction(reduction, REDUCTIONS),
+                                     C.byref(out), C.byref(null)), detail)
+    return None if null.value else out.value
+
+
+def vector_norm_diff(graph: GraphVersion, a, b, norm: str, interrupts=None) -> float:
+    """compute/reduce.rs:175-206 (norm_diff): norm(a - b), a row past the
+    shorter vector's end counting as zero."""
+    wa = 1 if getattr(a, "ndim", 1) == 1 else int(a.shape[1])
+    wb = 1 if getattr(b, "ndim", 1) == 1 else int(b.shape[1])
+    if wa != wb:
+        raise WidthMismatch(5)
+    out = C.c_double(0.0)
+    call, detail = _call(interrupts)
+    _raise(A.load().wc_vector_norm_diff(graph.handle, C.byref(call), _dtype(a), _ptr(a), _len(a),
+                                        _dtype(b), _ptr(b), _len(b), wa,
+                                        _reduction(norm, NORMS), C.byref(out)), detail)
+    return out.value
+
+
 # -------------------------------------------------------------- centrality
 
 
@@ -628,7 +671,7 @@ def sample_sources(id_space: int, sampling: Sampling = Sampling(), tombstones=No
     if sampling.population is not None:
         pop = np.ascontiguousarray(np.asarray(sampling.population) != 0, dtype=np.uint8)
         if len(pop) != id_space:
-            raise IdSpaceMismatch(f"population over {len(pop)} nodes, id space {id_space}")
+            raise IdSpaceMismatch(4)
     out = np.zeros(max(id_space, 1), np.uint64)
     count = C.c_uint64(0)
     k = -1 if sampling.k is None else int(sampling.k)

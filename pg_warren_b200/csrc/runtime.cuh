@@ -276,6 +276,7 @@ enum PoolTag {
   POOL_SPMM_CARRY = 140,
   POOL_CENT_TOTALS = 150, POOL_CENT_FLAG, POOL_CENT_SOURCES, POOL_CENT_CAPS, POOL_CENT_LIST,
   POOL_CENT_TOMB, POOL_CENT_VALUES,
+  POOL_VEC_PARTIAL = 160, POOL_VEC_RESULT,
 };
 
 // A call's context: the stream, the caller's detail and cancellation.

@@ -547,3 +547,53 @@ def test_library_sampler_is_the_oracles(oracle):
         got = W.sample_sources(n, s, tomb)
         want = O.sample_sources(n, tombstones=tomb, population=pop, complement=comp, k=k, seed=seed)
         assert np.array_equal(got, want)
+
+
+def test_reductions_known_answers(oracle):
+    # compute/reduce.rs:326-383.
+    x = np.array([3.0, -4.0, 0.0, 1.0])
+    found = [O.reduce(x, r, width=2) for r in ("sum", "max", "min", "l1", "l2", "nnz")]
+    assert found == [0.0, 3.0, -4.0, 8.0, 26 ** 0.5, 3.0]
+    assert O.reduce(np.array([2, -5, 7], np.int64), "sum") == 4.0
+    assert O.reduce(np.array([True, False, True]), "sum") == 2.0
+    assert O.reduce(np.array([True, False, True]), "nnz") == 2.0
+    assert O.reduce(np.array([1.5, -0.5], np.float32), "min") == -0.5
+    nan = np.array([1.0, np.nan, -2.0])
+    assert np.isnan(O.reduce(nan, "max")) and O.reduce(nan, "min") == -2.0
+    assert O.reduce(nan, "nnz") == 3.0 and np.isnan(O.reduce(nan, "sum"))
+    empty = np.zeros(0)
+    assert O.reduce(empty, "max") is None and O.reduce(empty, "min") is None
+    assert (O.reduce(empty, "sum"), O.reduce(empty, "l2"), O.reduce(empty, "nnz")) == (0.0, 0.0, 0.0)
+    import pg_warren_b200 as W
+    x = np.array([3.0, -4.0, 0.0, -9.0, 1.0, 5.0])
+    tomb = W.node_set(3, [1])
+    found = [O.reduce(x, r, width=2, tombstones=tomb) for r in ("sum", "max", "min", "l1", "l2", "nnz")]
+    assert found == [5.0, 5.0, -4.0, 13.0, 51 ** 0.5, 4.0]
+    assert O.reduce(x, "min", width=2, tombstones=W.node_set(3, [0, 1, 2])) is None
+
+
+def test_norm_diff_known_answers(oracle):
+    # compute/reduce.rs:385-395.
+    old, new = np.array([1.0, 2.0]), np.array([1.0, 5.0, -4.0])
+    assert O.norm_diff(new, old, "l1") == 7.0
+    assert O.norm_diff(old, new, "l2") == 5.0
+    assert O.norm_diff(old, new, "linf") == 4.0
+    assert O.norm_diff(np.array([1, 2], np.int64), old, "l1") == 0.0
+    assert O.norm_diff(np.zeros(0), np.zeros(0), "linf") == 0.0
+
+
+def test_chunked_sums_follow_the_chunk_order(oracle):
+    # Over several 65,536-element chunks the result is the chunk partials
+    # summed in order, each an in-order sum from +0 (reduce.rs:195-268).
+    rng = np.random.default_rng(4)
+    x = rng.standard_normal(200_003) * 10.0 ** rng.integers(-8, 9, 200_003)
+    parts = []
+    for c0 in range(0, len(x), 1 << 16):
+        s = 0.0
+        for v in x[c0:c0 + (1 << 16)]:
+            s = s + float(v)
+        parts.append(s)
+    total = 0.0
+    for p in parts:
+        total = total + p
+    assert O.reduce(x, "sum") == total
