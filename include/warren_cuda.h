@@ -70,6 +70,24 @@ typedef enum wc_status {
     WC_EIGENPAIR_COUNT = 32,        /* EigenpairCount {k, dimension} */
     WC_WORKING_SET = 33,            /* WorkingSet {bytes, in_use, limit} */
     WC_NOT_FINITE = 34,             /* NotFinite */
+    /* GraphError (graph/error.rs), from wc_version_load_segments */
+    WC_SEGMENT_TRUNCATED = 50,          /* SegmentTruncated */
+    WC_SEGMENT_MAGIC = 51,              /* SegmentMagic */
+    WC_SEGMENT_FORMAT = 52,             /* SegmentFormat {found} */
+    WC_SEGMENT_KIND = 53,               /* SegmentKind {expected, found} */
+    WC_SEGMENT_RESERVED = 54,           /* SegmentReserved {found} */
+    WC_SEGMENT_WIDTH = 55,              /* SegmentWidth {expected, found} */
+    WC_SEGMENT_LENGTH = 56,             /* SegmentLength {expected, found} */
+    WC_OFFSETS_LENGTH = 57,             /* OffsetsLength {expected, found} */
+    WC_FIRST_OFFSET_NOT_ZERO = 58,      /* FirstOffsetNotZero */
+    WC_STORED_ROWS_NOT_ASCENDING = 59,  /* StoredRowsNotAscending {index: node} */
+    WC_STORED_ROW_OUTSIDE_ID_SPACE = 60, /* StoredRowOutsideIdSpace {row: node} */
+    WC_STORED_ROW_EMPTY = 61,           /* StoredRowEmpty {row: node} */
+    WC_OFFSETS_NOT_MONOTONE = 62,       /* OffsetsNotMonotone {row: node} */
+    WC_FINAL_OFFSET = 63,               /* FinalOffset {expected, found} */
+    WC_TARGET_OUTSIDE_ID_SPACE = 64,    /* TargetOutsideIdSpace {row: node, target: found} */
+    WC_ROW_NOT_SORTED = 65,             /* RowNotSorted {row: node} */
+    WC_WEIGHTS_LENGTH = 66,             /* WeightsLength {expected, found} */
     /* the backend's own */
     WC_INVALID_ARGUMENT = 40,       /* a null pointer, a bad enum value, ... */
     WC_UNSUPPORTED = 41,            /* not served here: the adapter keeps the native kernel */
@@ -172,7 +190,28 @@ typedef struct wc_csr_host {
     const uint64_t* reverse_offsets;  /* NULL: built on the device */
     const uint32_t* reverse_targets;
     const double* reverse_weights;
+    /* With reverse_offsets NULL: nonzero when the version has a reverse CSR
+     * (RelationCsr.reverse), built here on the device from the forward one;
+     * zero when it has none (the device still builds one for the pull, but
+     * traversals In / Both report WC_REVERSE_CSR_MISSING). */
+    int32_t reverse_on_device;
 } wc_csr_host;
+
+/* graph/segment/csr.rs:83-122 (AnyCsr::decode) straight into a device copy:
+ * a version's CSR segments as stored (a 16-byte header, then the
+ * little-endian payload; rows_segment only with sparse offsets, weights
+ * NULL when unweighted), checked as Csr::from_segments checks them
+ * (graph/csr/mod.rs:78-137, the first violation reported in the order the
+ * reference checks) and uploaded without a host-side decode; the reverse
+ * CSR is built on the device.  has_reverse: the version has a reverse CSR
+ * (as wc_csr_host.reverse_on_device). */
+wc_status wc_version_load_segments(uint64_t graph_id, uint64_t version, uint64_t id_space,
+                                   const uint8_t* rows_segment, uint64_t rows_len,
+                                   const uint8_t* offsets_segment, uint64_t offsets_len,
+                                   const uint8_t* targets_segment, uint64_t targets_len,
+                                   const uint8_t* weights_segment, uint64_t weights_len,
+                                   int32_t has_reverse, wc_budget* budget, const wc_call* call,
+                                   wc_version** out);
 
 typedef struct wc_version_info {
     uint64_t id_space;

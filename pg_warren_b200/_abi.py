@@ -49,7 +49,7 @@ class Call(C.Structure):
 class CsrHost(C.Structure):
     _fields_ = [("id_space", U64), ("edges", U64), ("offsets", P), ("targets", P),
                 ("weights", P), ("reverse_offsets", P), ("reverse_targets", P),
-                ("reverse_weights", P)]
+                ("reverse_weights", P), ("reverse_on_device", I32)]
 
 
 class VersionInfo(C.Structure):
@@ -112,6 +112,8 @@ SIGNATURES = [
     ("wc_budget_in_use", U64, [P]),
     ("wc_budget_peak", U64, [P]),
     ("wc_version_upload", I32, [U64, U64, C.POINTER(CsrHost), P, C.POINTER(Call), C.POINTER(P)]),
+    ("wc_version_load_segments", I32, [U64, U64, U64, P, U64, P, U64, P, U64, P, U64, I32, P,
+                                       C.POINTER(Call), C.POINTER(P)]),
     ("wc_version_release", I32, [P]),
     ("wc_version_info_get", I32, [P, C.POINTER(VersionInfo)]),
     ("wc_version_sync", I32, [P, C.POINTER(Call)]),

@@ -142,6 +142,78 @@ class NotFinite(SpectralError):
     pass
 
 
+class GraphError(WarrenError):
+    """graph/error.rs: a stored segment or CSR that does not decode."""
+
+
+class SegmentTruncated(GraphError):
+    pass
+
+
+class SegmentMagic(GraphError):
+    pass
+
+
+class SegmentFormat(GraphError):
+    pass
+
+
+class SegmentKind(GraphError):
+    pass
+
+
+class SegmentReserved(GraphError):
+    pass
+
+
+class SegmentWidth(GraphError):
+    pass
+
+
+class SegmentLength(GraphError):
+    pass
+
+
+class OffsetsLength(GraphError):
+    pass
+
+
+class FirstOffsetNotZero(GraphError):
+    pass
+
+
+class StoredRowsNotAscending(GraphError):
+    pass
+
+
+class StoredRowOutsideIdSpace(GraphError):
+    pass
+
+
+class StoredRowEmpty(GraphError):
+    pass
+
+
+class OffsetsNotMonotone(GraphError):
+    pass
+
+
+class FinalOffset(GraphError):
+    pass
+
+
+class TargetOutsideIdSpace(GraphError):
+    pass
+
+
+class RowNotSorted(GraphError):
+    pass
+
+
+class WeightsLength(GraphError):
+    pass
+
+
 class BackendError(WarrenError):
     pass
 
@@ -173,6 +245,11 @@ _ERRORS = {
     21: NodeFilterIdSpace, 22: ReverseCsrMissing, 30: NotSymmetric, 31: NonPositiveDegree,
     32: EigenpairCount, 33: WorkingSet, 34: NotFinite, 40: InvalidArgument, 41: Unsupported,
     42: CudaError, 43: DeviceTimeout, 44: NoDevice,
+    50: SegmentTruncated, 51: SegmentMagic, 52: SegmentFormat, 53: SegmentKind,
+    54: SegmentReserved, 55: SegmentWidth, 56: SegmentLength, 57: OffsetsLength,
+    58: FirstOffsetNotZero, 59: StoredRowsNotAscending, 60: StoredRowOutsideIdSpace,
+    61: StoredRowEmpty, 62: OffsetsNotMonotone, 63: FinalOffset, 64: TargetOutsideIdSpace,
+    65: RowNotSorted, 66: WeightsLength,
 }
 
 
@@ -289,22 +366,16 @@ class GraphVersion:
         targets = np.ascontiguousarray(targets, dtype=np.uint32)
         n = len(offsets) - 1
         m = len(targets)
-        csr = A.CsrHost(n, m, offsets.ctypes.data, targets.ctypes.data, None, None, None, None)
+        csr = A.CsrHost(n, m, offsets.ctypes.data, targets.ctypes.data, None, None, None, None,
+                        0)
         self._keep = [offsets, targets]
         if weights is not None:
             weights = np.ascontiguousarray(weights, dtype=np.float64)
             csr.weights = weights.ctypes.data
             self._keep.append(weights)
         if reverse is True:
-            roff = np.zeros(n + 1, np.uint64)
-            rtgt = np.zeros(max(m, 1), np.uint32)
-            rw = np.zeros(max(m, 1), np.float64) if weights is not None else None
-            _raise(A.load().wc_host_transpose(n, m, offsets.ctypes.data, targets.ctypes.data,
-                                              _ptr(weights), roff.ctypes.data, rtgt.ctypes.data,
-                                              _ptr(rw)), A.ErrorDetail())
-            csr.reverse_offsets, csr.reverse_targets = roff.ctypes.data, rtgt.ctypes.data
-            csr.reverse_weights = _ptr(rw)
-            self._keep += [roff, rtgt, rw]
+            # The version has a reverse CSR: the library transposes on the device.
+            csr.reverse_on_device = 1
         elif reverse:
             roff, rtgt, rw = reverse
             roff = np.ascontiguousarray(roff, dtype=np.uint64)
@@ -323,6 +394,30 @@ class GraphVersion:
         self.id_space = n
         self.edges = m
         self.weighted = weights is not None
+
+    @classmethod
+    def from_segments(cls, id_space: int, offsets: bytes, targets: bytes, weights=None,
+                      rows=None, reverse: bool = True, budget: Budget = None,
+                      graph_id: int = 0, version: int = 0) -> "GraphVersion":
+        """A version loaded straight from its stored CSR segments
+        (graph/segment/csr.rs:83-122), checked on the device as the
+        reference's decode checks them."""
+        self = cls.__new__(cls)
+        self.budget = budget or Budget()
+        bufs = [None if b is None else np.frombuffer(bytes(b), np.uint8)
+                for b in (rows, offsets, targets, weights)]
+        # An empty segment is passed as a non-null pointer to no bytes.
+        ptr = [None if b is None else (b.ctypes.data if len(b) else 1) for b in bufs]
+        ln = [0 if b is None else len(b) for b in bufs]
+        call, detail = _call()
+        h = A.P()
+        _raise(A.load().wc_version_load_segments(
+            graph_id, version, id_space, ptr[0], ln[0], ptr[1], ln[1], ptr[2], ln[2], ptr[3],
+            ln[3], int(bool(reverse)), self.budget.handle, C.byref(call), C.byref(h)), detail)
+        self.handle = h
+        info = self.info()
+        self.id_space, self.edges, self.weighted = info.id_space, info.edges, bool(info.weighted)
+        return self
 
     def info(self) -> A.VersionInfo:
         info = A.VersionInfo()
@@ -351,6 +446,50 @@ class GraphVersion:
         n = C.c_uint32(0)
         ms = A.load().wc_version_timing(self.handle, phase.encode(), C.byref(n))
         return ms, n.value
+
+
+def host_reverse(offsets, targets, weights=None):
+    """The reverse CSR by the host's counting transpose
+    (graph/csr/transpose.rs:14-44): (offsets, targets, weights or None), to
+    give GraphVersion(reverse=...) instead of the device transpose."""
+    offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+    targets = np.ascontiguousarray(targets, dtype=np.uint32)
+    n, m = len(offsets) - 1, len(targets)
+    roff = np.zeros(n + 1, np.uint64)
+    rtgt = np.zeros(max(m, 1), np.uint32)
+    rw = None
+    if weights is not None:
+        weights = np.ascontiguousarray(weights, dtype=np.float64)
+        rw = np.zeros(max(m, 1), np.float64)
+    _raise(A.load().wc_host_transpose(n, m, offsets.ctypes.data, targets.ctypes.data,
+                                      _ptr(weights), roff.ctypes.data, rtgt.ctypes.data,
+                                      _ptr(rw)), A.ErrorDetail())
+    return roff, rtgt[:m], None if rw is None else rw[:m]
+
+
+def encode_segment(kind: int, elements: np.ndarray) -> bytes:
+    """One stored segment as the reference writes it (graph/segment/mod.rs:
+    1-16, 190-272): the 16-byte header (magic, format 2 for a CSR's
+    segments, kind, element width, reserved 0, count) and the little-endian
+    elements.  Kinds: offsets 1, targets 2, weights 3, rows 11."""
+    elements = np.ascontiguousarray(elements)
+    header = b"WRSG" + bytes([2, kind, elements.dtype.itemsize, 0])
+    return header + int(len(elements)).to_bytes(8, "little") + elements.astype(
+        elements.dtype.newbyteorder("<"), copy=False).tobytes()
+
+
+def csr_segments(offsets, targets, weights=None, sparse: bool = False):
+    """A CSR's segments (segment/csr.rs:124-131): (rows or None, offsets,
+    targets, weights or None); with `sparse`, only the non-empty rows are
+    stored, with one offset each plus the end."""
+    offsets = np.asarray(offsets, np.uint64)
+    rows = None
+    if sparse:
+        keep = np.nonzero(np.diff(offsets))[0]
+        rows = encode_segment(11, keep.astype(np.uint32))
+        offsets = np.append(offsets[keep], offsets[-1]).astype(np.uint64)
+    return (rows, encode_segment(1, offsets), encode_segment(2, np.asarray(targets, np.uint32)),
+            None if weights is None else encode_segment(3, np.asarray(weights, np.float64)))
 
 
 # ----------------------------------------------------------------- products

@@ -1,0 +1,24 @@
+// upload.h — the steps that build a version's device copy, shared by
+// wc_version_upload (host arrays) and wc_version_load_segments (stored
+// segments).
+#pragma once
+
+#include "runtime.cuh"
+
+namespace wc {
+
+// No usable sm_100 device: WC_NO_DEVICE with the reason in the detail.
+wc_status wc_device_check(wc_error_detail* detail);
+// The reverse CSR from the forward one, on the device (v->rev, and its
+// offsets on the host).
+wc_status device_reverse(wc_version* v, wc_error_detail* detail);
+// Whether every weight is an i32 integer (then i32 copies of both
+// orientations' weights) and the largest magnitude.
+wc_status device_weight_facts(wc_version* v, wc_error_detail* detail);
+// Whether the forward and reverse CSR are equal, weights included.
+wc_status device_symmetric(wc_version* v, wc_error_detail* detail);
+// With both orientations on the device: the weights' facts, the symmetry
+// test, the row-split schedules, the error word and the mapped words.
+wc_status finish_version(wc_version* v, wc_error_detail* detail);
+
+}  // namespace wc

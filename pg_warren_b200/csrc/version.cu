@@ -3,10 +3,12 @@
 // graph_csr.rs:15-55), with the row-split schedules the pull kernels walk.
 #include <algorithm>
 #include <cstdlib>
+#include <memory>
 #include <thread>
 
 #include "product.h"
 #include "runtime.cuh"
+#include "upload.h"
 
 namespace wc {
 
@@ -62,8 +64,9 @@ static void build_units(uint64_t n, const uint64_t* off, std::vector<Unit>& unit
   }
 }
 
-static wc_status upload_csr(wc_version* v, DevCsr& d, const uint64_t* off, const uint32_t* tgt,
-                            const double* w, bool integral, wc_error_detail* detail) {
+// One orientation's arrays, copied from the host (u32 offsets).
+static wc_status put_csr(wc_version* v, DevCsr& d, const uint64_t* off, const uint32_t* tgt,
+                         const double* w, wc_error_detail* detail) {
   const uint64_t n = v->n, m = v->m;
   std::vector<uint32_t> off32(n + 1);
   for (uint64_t i = 0; i <= n; i++) off32[i] = (uint32_t)off[i];
@@ -71,29 +74,69 @@ static wc_status upload_csr(wc_version* v, DevCsr& d, const uint64_t* off, const
   // their spans to 16-byte boundaries.
   WC_TRY(d.offsets.alloc(v->budget, (n + 1) * 4 + kBulkPad, detail));
   WC_TRY(d.targets.alloc(v->budget, m * 4 + kBulkPad, detail));
-  WC_CUDA(cudaMemcpy(d.offsets.ptr, off32.data(), (n + 1) * 4, cudaMemcpyHostToDevice), detail);
-  WC_CUDA(cudaMemcpy(d.targets.ptr, tgt, m * 4, cudaMemcpyHostToDevice), detail);
+  WC_CUDA(cudaMemcpyAsync(d.offsets.ptr, off32.data(), (n + 1) * 4, cudaMemcpyHostToDevice,
+                          v->stream), detail);
+  if (m)
+    WC_CUDA(cudaMemcpyAsync(d.targets.ptr, tgt, m * 4, cudaMemcpyHostToDevice, v->stream), detail);
   if (w) {
     WC_TRY(d.weights.alloc(v->budget, m * 8 + kBulkPad, detail));
-    WC_CUDA(cudaMemcpy(d.weights.ptr, w, m * 8, cudaMemcpyHostToDevice), detail);
-    if (integral) {
-      std::vector<int32_t> wi(m);
-      for (uint64_t e = 0; e < m; e++) wi[e] = (int32_t)w[e];
-      WC_TRY(d.iweights.alloc(v->budget, m * 4 + kBulkPad, detail));
-      WC_CUDA(cudaMemcpy(d.iweights.ptr, wi.data(), m * 4, cudaMemcpyHostToDevice), detail);
-    }
+    if (m)
+      WC_CUDA(cudaMemcpyAsync(d.weights.ptr, w, m * 8, cudaMemcpyHostToDevice, v->stream), detail);
   }
+  // The copies read the host staging of the offsets: wait for them.
+  return cuda_status(cudaStreamSynchronize(v->stream), detail, "version upload");
+}
+
+// The schedule of one orientation from its host offsets.
+static wc_status put_schedule(wc_version* v, DevCsr& d, const std::vector<uint64_t>& off,
+                              wc_error_detail* detail) {
   std::vector<Unit> units;
   Schedule& s = d.schedule;
-  build_units(n, off, units, s.slots, s.long_rows, s.tiles, d.max_degree);
+  build_units(v->n, off.data(), units, s.slots, s.long_rows, s.tiles, d.max_degree);
   s.count = (uint32_t)units.size();
-  WC_TRY(s.units.alloc(v->budget, units.size() * sizeof(Unit), detail));
-  WC_CUDA(cudaMemcpy(s.units.ptr, units.data(), units.size() * sizeof(Unit),
-                     cudaMemcpyHostToDevice), detail);
+  WC_TRY(s.units.alloc(v->budget, std::max<size_t>(units.size(), 1) * sizeof(Unit), detail));
+  if (!units.empty())
+    WC_CUDA(cudaMemcpy(s.units.ptr, units.data(), units.size() * sizeof(Unit),
+                       cudaMemcpyHostToDevice), detail);
   WC_TRY(s.counters.alloc(v->budget, (uint64_t)std::max<uint32_t>(s.slots, 1) * 4, detail));
   WC_CUDA(cudaMemset(s.counters.ptr, 0, (uint64_t)std::max<uint32_t>(s.slots, 1) * 4), detail);
   WC_TRY(s.carry.alloc(v->budget, (uint64_t)std::max<uint32_t>(s.slots, 1) * kCarryBytesPerSlot,
                        detail));
+  return WC_OK;
+}
+
+wc_status wc_device_check(wc_error_detail* detail) {
+  int device = 0, count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    set_message(detail, "no CUDA device");
+    return WC_NO_DEVICE;
+  }
+  WC_CUDA(cudaGetDevice(&device), detail);
+  cudaDeviceProp prop;
+  WC_CUDA(cudaGetDeviceProperties(&prop, device), detail);
+  if (prop.major < 10) {
+    set_message(detail, "device %d is sm_%d%d; this library is built for sm_100a", device,
+                prop.major, prop.minor);
+    return WC_NO_DEVICE;
+  }
+  return WC_OK;
+}
+
+wc_status finish_version(wc_version* v, wc_error_detail* detail) {
+  WC_TRY(device_weight_facts(v, detail));
+  WC_TRY(device_symmetric(v, detail));
+  WC_TRY(put_schedule(v, v->fwd, v->host_offsets, detail));
+  WC_TRY(put_schedule(v, v->rev, v->host_rev_offsets, detail));
+  WC_TRY(v->error.alloc(v->budget, sizeof(DeviceError), detail));
+  WC_CUDA(cudaMemset(v->error.ptr, 0, sizeof(DeviceError)), detail);
+  // Four mapped words: the cancel word, then the pacing words (iterations
+  // completed, done) that iterative kernels report to the host.
+  WC_CUDA(cudaHostAlloc((void**)&v->cancel_host, 4 * sizeof(int32_t), cudaHostAllocMapped), detail);
+  for (int q = 0; q < 4; q++) v->cancel_host[q] = 0;
+  WC_CUDA(cudaHostGetDevicePointer((void**)&v->cancel_dev, v->cancel_host, 0), detail);
+  v->pace_host = reinterpret_cast<volatile uint32_t*>(v->cancel_host + 1);
+  v->pace_dev = reinterpret_cast<uint32_t*>(v->cancel_dev + 1);
   return WC_OK;
 }
 
@@ -123,6 +166,23 @@ const char* wc_status_name(wc_status s) {
     case WC_NODE_FILTER_ID_SPACE: return "node filter over another id space";
     case WC_REVERSE_CSR_MISSING: return "the reverse CSR is missing";
     case WC_NOT_SYMMETRIC: return "the matrix is not symmetric";
+    case WC_SEGMENT_TRUNCATED: return "segment truncated";
+    case WC_SEGMENT_MAGIC: return "not a pg_warren segment";
+    case WC_SEGMENT_FORMAT: return "unsupported segment format";
+    case WC_SEGMENT_KIND: return "segment kind mismatch";
+    case WC_SEGMENT_RESERVED: return "segment reserved byte is not 0";
+    case WC_SEGMENT_WIDTH: return "segment element width mismatch";
+    case WC_SEGMENT_LENGTH: return "segment payload length mismatch";
+    case WC_OFFSETS_LENGTH: return "CSR offsets length mismatch";
+    case WC_FIRST_OFFSET_NOT_ZERO: return "CSR offsets do not start at 0";
+    case WC_STORED_ROWS_NOT_ASCENDING: return "CSR stored rows not ascending";
+    case WC_STORED_ROW_OUTSIDE_ID_SPACE: return "CSR stores a row outside the id space";
+    case WC_STORED_ROW_EMPTY: return "CSR stores a row without targets";
+    case WC_OFFSETS_NOT_MONOTONE: return "CSR offsets decrease";
+    case WC_FINAL_OFFSET: return "CSR final offset mismatch";
+    case WC_TARGET_OUTSIDE_ID_SPACE: return "CSR target outside the id space";
+    case WC_ROW_NOT_SORTED: return "CSR row not strictly ascending";
+    case WC_WEIGHTS_LENGTH: return "CSR weights length mismatch";
     case WC_NON_POSITIVE_DEGREE: return "a node with an edge has a non-positive degree";
     case WC_EIGENPAIR_COUNT: return "eigenpair count out of range";
     case WC_WORKING_SET: return "the eigenproblem's working set does not fit the compute memory";
@@ -157,20 +217,7 @@ wc_status wc_version_upload(uint64_t graph_id, uint64_t version, const wc_csr_ho
     set_message(detail, "id spaces and edge counts of 2^32 or more are not served");
     return WC_UNSUPPORTED;
   }
-  int device = 0, count = 0;
-  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
-    cudaGetLastError();
-    set_message(detail, "no CUDA device");
-    return WC_NO_DEVICE;
-  }
-  WC_CUDA(cudaGetDevice(&device), detail);
-  cudaDeviceProp prop;
-  WC_CUDA(cudaGetDeviceProperties(&prop, device), detail);
-  if (prop.major < 10) {
-    set_message(detail, "device %d is sm_%d%d; this library is built for sm_100a", device,
-                prop.major, prop.minor);
-    return WC_NO_DEVICE;
-  }
+  WC_TRY(wc_device_check(detail));
   const uint64_t n = csr->id_space, m = csr->edges;
   if (csr->offsets[0] != 0 || csr->offsets[n] != m) return WC_INVALID_ARGUMENT;
   for (uint64_t e = 0; e < m; e++)
@@ -178,61 +225,30 @@ wc_status wc_version_upload(uint64_t graph_id, uint64_t version, const wc_csr_ho
       if (detail) detail->node = csr->targets[e];
       return WC_NODE_OUTSIDE_ID_SPACE;
     }
+  if (csr->reverse_offsets && (!csr->reverse_targets || (csr->weights && !csr->reverse_weights)))
+    return WC_INVALID_ARGUMENT;
   std::unique_ptr<wc_version> v(new wc_version);
   v->graph_id = graph_id;
   v->version = version;
   v->n = n;
   v->m = m;
-  v->device = device;
   v->budget = budget;
   v->weighted = csr->weights != nullptr;
-  bool integral = v->weighted;
-  int64_t max_abs = v->weighted ? 0 : 1;
-  if (v->weighted)
-    for (uint64_t e = 0; e < m && integral; e++) {
-      const double w = csr->weights[e];
-      integral = w >= -2147483648.0 && w <= 2147483647.0 && w == (double)(int32_t)w;
-      if (integral) max_abs = std::max<int64_t>(max_abs, std::llabs((long long)w));
-    }
-  v->integral = integral;
-  v->max_abs_iweight = integral || !v->weighted ? max_abs : -1;
-  // The reverse CSR: the caller's, or a counting transpose here.
-  std::vector<uint64_t> roff;
-  std::vector<uint32_t> rtgt;
-  std::vector<double> rw;
-  const uint64_t* ro = csr->reverse_offsets;
-  const uint32_t* rt = csr->reverse_targets;
-  const double* rwp = csr->reverse_weights;
-  if (!ro) {
-    roff.resize(n + 1);
-    rtgt.resize(m);
-    if (v->weighted) rw.resize(m);
-    host_transpose(n, m, csr->offsets, csr->targets, csr->weights, roff.data(), rtgt.data(),
-                   v->weighted ? rw.data() : nullptr);
-    ro = roff.data();
-    rt = rtgt.data();
-    rwp = v->weighted ? rw.data() : nullptr;
-  } else if (v->weighted && !rwp) {
-    return WC_INVALID_ARGUMENT;
-  }
-  v->symmetric = std::equal(csr->offsets, csr->offsets + n + 1, ro) &&
-                 std::equal(csr->targets, csr->targets + m, rt) &&
-                 (!v->weighted || std::equal(csr->weights, csr->weights + m, rwp));
+  WC_CUDA(cudaGetDevice(&v->device), detail);
   WC_CUDA(cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking), detail);
-  WC_TRY(upload_csr(v.get(), v->fwd, csr->offsets, csr->targets, csr->weights, integral, detail));
-  WC_TRY(upload_csr(v.get(), v->rev, ro, rt, rwp, integral, detail));
+  WC_TRY(put_csr(v.get(), v->fwd, csr->offsets, csr->targets, csr->weights, detail));
   v->host_offsets.assign(csr->offsets, csr->offsets + n + 1);
-  v->host_rev_offsets.assign(ro, ro + n + 1);
-  v->reverse_given = csr->reverse_offsets != nullptr;
-  WC_TRY(v->error.alloc(v->budget, sizeof(DeviceError), detail));
-  WC_CUDA(cudaMemset(v->error.ptr, 0, sizeof(DeviceError)), detail);
-  // Four mapped words: the cancel word, then the pacing words (iterations
-  // completed, done) that iterative kernels report to the host.
-  WC_CUDA(cudaHostAlloc((void**)&v->cancel_host, 4 * sizeof(int32_t), cudaHostAllocMapped), detail);
-  for (int q = 0; q < 4; q++) v->cancel_host[q] = 0;
-  WC_CUDA(cudaHostGetDevicePointer((void**)&v->cancel_dev, v->cancel_host, 0), detail);
-  v->pace_host = reinterpret_cast<volatile uint32_t*>(v->cancel_host + 1);
-  v->pace_dev = reinterpret_cast<uint32_t*>(v->cancel_dev + 1);
+  // The reverse CSR: the caller's, or a transpose on the device.
+  if (csr->reverse_offsets) {
+    WC_TRY(put_csr(v.get(), v->rev, csr->reverse_offsets, csr->reverse_targets,
+                   v->weighted ? csr->reverse_weights : nullptr, detail));
+    v->host_rev_offsets.assign(csr->reverse_offsets, csr->reverse_offsets + n + 1);
+    v->reverse_given = true;
+  } else {
+    WC_TRY(device_reverse(v.get(), detail));
+    v->reverse_given = csr->reverse_on_device != 0;
+  }
+  WC_TRY(finish_version(v.get(), detail));
   *out = v.release();
   return WC_OK;
 }
