@@ -560,6 +560,39 @@ def leg_cent(W, O, torch, dev, stream, peak):
     return out
 
 
+def leg_load(W, O, torch, dev, stream, peak):
+    """A version's device copy at R-MAT 22 (weighted, f64): from host arrays
+    with the reverse CSR transposed on the device, with the reverse given
+    (the host's counting transpose, timed apart), and from the stored CSR
+    segments (dense and sparse offsets), checked on the device."""
+    from pg_warren_b200 import api
+    g = W.rmat(22)
+    w = W.edge_weights(g, "uniform")
+    out = {"nodes": g.id_space, "edges": g.edges}
+
+    def timed(make):
+        gv = make()
+        del gv
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        gv = make()
+        seconds = time.perf_counter() - t0
+        del gv
+        return seconds
+
+    out["arrays_device_reverse_s"] = timed(lambda: W.GraphVersion(g.offsets, g.targets, w))
+    t0 = time.perf_counter()
+    rev = api.host_reverse(g.offsets, g.targets, w)
+    out["host_transpose_s"] = time.perf_counter() - t0
+    out["arrays_given_reverse_s"] = timed(lambda: W.GraphVersion(g.offsets, g.targets, w,
+                                                                 reverse=rev))
+    for sparse in (False, True):
+        rows, off, tgt, ws = api.csr_segments(g.offsets, g.targets, w, sparse=sparse)
+        key = "segments_sparse_s" if sparse else "segments_dense_s"
+        out[key] = timed(lambda: W.GraphVersion.from_segments(g.id_space, off, tgt, ws, rows))
+    return out
+
+
 def suite(args):
     import torch
     import pg_warren_b200 as W
@@ -570,7 +603,7 @@ def suite(args):
     stream = torch.cuda.Stream(dev)
     peak, kind = measured_peaks()
     legs = {"c1": leg_c1, "c2": leg_c2, "c3": leg_c3, "c4": leg_c4, "c5": leg_c5,
-            "cent": leg_cent}
+            "cent": leg_cent, "load": leg_load}
     out = {"peak_gbs": peak, "peak_kind": kind}
     for name in args.suite.split(","):
         t0 = time.time()
@@ -644,7 +677,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="warren")
     ap.add_argument("--suite", default=None,
-                    help="comma-separated configurations to measure instead: c1,c2,c3,c4,c5,cent")
+                    help="comma-separated configurations to measure instead: c1,c2,c3,c4,c5,cent,load")
     ap.add_argument("--case", default=None, choices=["batched", "spmv", "ppr"],
                     help="a small workload for profilers instead")
     ap.add_argument("--scale", type=int, default=20)
