@@ -60,6 +60,11 @@ typedef enum wc_status {
     WC_FLOAT_OVERFLOW = 11,       /* FloatOverflow */
     WC_FLOAT_UNDERFLOW = 12,      /* FloatUnderflow */
     WC_DIVISION_BY_ZERO = 13,     /* DivisionByZero */
+    WC_SQRT_OF_NEGATIVE = 14,     /* SqrtOfNegative */
+    WC_LOG_OF_ZERO = 15,          /* LogOfZero */
+    WC_LOG_OF_NEGATIVE = 16,      /* LogOfNegative */
+    WC_ZERO_TO_NEGATIVE_POWER = 17, /* ZeroToNegativePower */
+    WC_COMPLEX_POWER = 18,        /* ComplexPower */
     /* TraversalError (traversal/error.rs) */
     WC_NODE_OUTSIDE_ID_SPACE = 20,  /* NodeOutsideIdSpace {node} */
     WC_NODE_FILTER_ID_SPACE = 21,   /* NodeFilterIdSpace {expected, found} */
@@ -88,6 +93,10 @@ typedef enum wc_status {
     WC_TARGET_OUTSIDE_ID_SPACE = 64,    /* TargetOutsideIdSpace {row: node, target: found} */
     WC_ROW_NOT_SORTED = 65,             /* RowNotSorted {row: node} */
     WC_WEIGHTS_LENGTH = 66,             /* WeightsLength {expected, found} */
+    /* ComputeError, from wc_vector_map */
+    WC_UNKNOWN_OPERAND = 70,            /* UnknownOperand {index: node, operands: expected} */
+    WC_OPERAND_TYPE = 71,               /* OperandType {index: node, expected, found} (wc_dtype) */
+    WC_NULL_RESULT = 72,                /* NullResult {dtype: expected} */
     /* the backend's own */
     WC_INVALID_ARGUMENT = 40,       /* a null pointer, a bad enum value, ... */
     WC_UNSUPPORTED = 41,            /* not served here: the adapter keeps the native kernel */
@@ -520,6 +529,66 @@ wc_status wc_pagerank_adjoint(wc_version* version, const wc_call* call,
                               const wc_pagerank_opts* opts, const uint64_t* loss_targets,
                               const uint64_t* loss_offsets, uint32_t losses, double adjoint_tol,
                               double* grad_out, double* ranks_out, uint32_t* iterations_out);
+
+/* ---------------------------------------------------------- vector map */
+
+/* compute/map/expr.rs (the vector_map IR), one node per expression node.
+ * A node's children are children[first .. first + count), in the IR's
+ * order: CASE lists (condition, value) pairs, then the ELSE if has_else;
+ * COMPARE and the binary operations their two operands; CAST its operand. */
+typedef enum wc_map_kind {
+    WC_MAP_LITERAL = 0,   /* value in i (bool, bigint) or f (real, double); is_null: a typed NULL */
+    WC_MAP_VECTOR = 1,    /* operand i at the current element */
+    WC_MAP_CAST = 2,      /* the child, cast to `type` as SQL casts (compute/cast.rs) */
+    WC_MAP_CASE = 3,
+    WC_MAP_NULLIF = 4,
+    WC_MAP_COALESCE = 5,
+    WC_MAP_LEAST = 6,
+    WC_MAP_GREATEST = 7,
+    WC_MAP_NEGATE = 8,    /* bigint, real, double */
+    WC_MAP_ARITHMETIC = 9, /* op: 0 +, 1 -, 2 *, 3 / */
+    WC_MAP_MODULO = 10,   /* bigint */
+    WC_MAP_ABS = 11,      /* bigint, real */
+    WC_MAP_CALL = 12,     /* double; op: 0 abs, 1 sqrt, 2 exp, 3 ln, 4 log, 5 floor, 6 ceil,
+                             7 round, 8 sign (expr.rs:176-197) */
+    WC_MAP_POWER = 13,    /* double */
+    WC_MAP_COMPARE = 14,  /* boolean; op: 0 =, 1 <>, 2 <, 3 <=, 4 >, 5 >= over the children's type */
+    WC_MAP_NOT = 15,
+    WC_MAP_AND = 16,
+    WC_MAP_OR = 17
+} wc_map_kind;
+
+typedef struct wc_map_node {
+    int32_t kind;      /* wc_map_kind */
+    int32_t type;      /* the node's wc_dtype */
+    int32_t op;        /* by kind, above */
+    int32_t has_else;  /* CASE */
+    uint32_t first;    /* children */
+    uint32_t count;
+    int32_t is_null;   /* LITERAL */
+    int32_t reserved;
+    int64_t i;         /* LITERAL (bool, bigint) or VECTOR (operand index) */
+    double f;          /* LITERAL (real, double) */
+} wc_map_node;
+
+/* compute/map/mod.rs:49-78 (map): `root`'s value at every element of the
+ * version's id space, row-major over rows of the widest operand's width
+ * (operands of width 1 and literals repeat across a row), written to out
+ * (id_space × width elements of the root's type; *out_width gets the width).
+ * SQL semantics as the reference's: CASE, COALESCE, AND and OR evaluate an
+ * argument only where SQL would; NULL stores NaN in real and double results
+ * and is WC_NULL_RESULT in bigint and boolean ones; the error reported is
+ * the first failing element's in row-major order.  Operand checks as the
+ * reference: id space and width, then every operand reference, evaluated or
+ * not.  All results are the reference's to the bit except exp, ln, log and
+ * power, which use the device's functions (within 2 units in the last
+ * place).  Expressions whose evaluation needs more than 32 stack values or
+ * more than 16 operands are WC_UNSUPPORTED. */
+wc_status wc_vector_map(wc_version* version, const wc_call* call, const wc_map_node* nodes,
+                        uint32_t node_count, const uint32_t* children, uint32_t child_count,
+                        uint32_t root, const void* const* operands, const wc_dtype* operand_dtypes,
+                        const uint64_t* operand_id_spaces, const uint32_t* operand_widths,
+                        uint32_t operand_count, void* out, uint32_t* out_width);
 
 /* ------------------------------------------------------- vector reduce */
 

@@ -12,7 +12,8 @@ from .api import (Budget, GraphVersion, Product, PageRank, Limits, EigenOptions,
                   spmv, spmm, pagerank, pagerank_noalloc, bfs, bfs_depths, reachable_set, reachable, components, bfs_batched,
                   minplus_batched, ppr_batched, autotune, set_schedule, eigen, pagerank_adjoint, top_k, rmat, gnm,
                   edge_weights, node_set, HostGraph, Sampling, Centrality, sample_sources,
-                  closeness_centrality, harmonic_centrality, vector_reduce, vector_norm_diff)
+                  closeness_centrality, harmonic_centrality, vector_reduce, vector_norm_diff,
+                  vector_map)
 from ._abi import load, LIBRARY
 
 __all__ = ["Budget", "GraphVersion", "Product", "PageRank", "Limits", "EigenOptions",
@@ -20,5 +21,5 @@ __all__ = ["Budget", "GraphVersion", "Product", "PageRank", "Limits", "EigenOpti
            "reachable", "components", "bfs_batched", "minplus_batched", "ppr_batched", "autotune", "set_schedule", "eigen",
            "pagerank_adjoint", "top_k", "rmat", "gnm", "edge_weights", "node_set", "HostGraph",
            "Sampling", "Centrality", "sample_sources", "closeness_centrality",
-           "harmonic_centrality", "vector_reduce", "vector_norm_diff",
+           "harmonic_centrality", "vector_reduce", "vector_norm_diff", "vector_map",
            "load", "LIBRARY"]

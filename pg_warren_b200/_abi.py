@@ -145,6 +145,8 @@ SIGNATURES = [
     ("wc_eigen", I32, [P, C.POINTER(Call), C.POINTER(EigenOpts), P, P, P, C.POINTER(EigenStats)]),
     ("wc_pagerank_adjoint", I32, [P, C.POINTER(Call), C.POINTER(PageRankOpts), P, P, U32, D, P,
                                   P, P]),
+    ("wc_vector_map", I32, [P, C.POINTER(Call), P, U32, P, U32, U32, P, P, P, P, U32, P,
+                            C.POINTER(U32)]),
     ("wc_vector_reduce", I32, [P, C.POINTER(Call), I32, P, U32, P, I32, C.POINTER(D),
                                C.POINTER(I32)]),
     ("wc_vector_norm_diff", I32, [P, C.POINTER(Call), I32, P, U64, I32, P, U64, U32, I32,

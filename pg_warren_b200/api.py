@@ -737,6 +737,74 @@ def components(graph: GraphVersion, labels_out=None, interrupts=None):
     return labels, _stats(stats)
 
 
+# --------------------------------------------------------------- vector map
+
+_MAP_NP = {"f32": np.float32, "f64": np.float64, "i64": np.int64, "bool": np.bool_}
+
+
+class UnknownOperand(ComputeError):
+    pass
+
+
+class OperandType(ComputeError):
+    pass
+
+
+class NullResult(ComputeError):
+    pass
+
+
+class SqrtOfNegative(ArithmeticError_):
+    pass
+
+
+class LogOfZero(ArithmeticError_):
+    pass
+
+
+class LogOfNegative(ArithmeticError_):
+    pass
+
+
+class ZeroToNegativePower(ArithmeticError_):
+    pass
+
+
+class ComplexPower(ArithmeticError_):
+    pass
+
+
+_ERRORS.update({14: SqrtOfNegative, 15: LogOfZero, 16: LogOfNegative, 17: ZeroToNegativePower,
+                18: ComplexPower, 70: UnknownOperand, 71: OperandType, 72: NullResult})
+
+
+def vector_map(graph: GraphVersion, expr, operands=(), out=None, interrupts=None):
+    """compute/map/mod.rs:49-78 (map): `expr` (a pg_warren_b200.expr tree)
+    at every element of the version's id space, over `operands` (numpy
+    arrays or CUDA tensors, id_space rows, width 1 or the widest width);
+    returns the result, id_space × width of the expression's type."""
+    from . import expr as X
+    nodes, children, root = X.serialize(expr)
+    ops = [np.ascontiguousarray(o) if isinstance(o, np.ndarray) else o for o in operands]
+    count = len(ops)
+    ptrs = (C.c_void_p * max(count, 1))(*[_ptr(o) for o in ops])
+    dtypes = (C.c_int32 * max(count, 1))(*[_dtype(o) for o in ops])
+    spaces = (C.c_uint64 * max(count, 1))(*[_len(o) for o in ops])
+    widths = (C.c_uint32 * max(count, 1))(*[1 if len(o.shape) == 1 else int(o.shape[1])
+                                            for o in ops])
+    width = max([1] + list(widths[:count]))
+    if out is None:
+        shape = (graph.id_space,) if width == 1 else (graph.id_space, width)
+        out = np.zeros(shape, _MAP_NP[expr.type])
+    got = C.c_uint32(0)
+    call, detail = _call(interrupts)
+    _raise(A.load().wc_vector_map(graph.handle, C.byref(call), nodes.ctypes.data, len(nodes),
+                                  children.ctypes.data if len(children) else None, len(children),
+                                  root, ptrs, dtypes, spaces, widths, count, _ptr(out),
+                                  C.byref(got)), detail)
+    return out
+
+
 # ------------------------------------------------------------ vector reduce
 
 REDUCTIONS = ["sum", "max", "min", "l1", "l2", "nnz"]  # compute/reduce.rs:23-38

@@ -277,6 +277,8 @@ enum PoolTag {
   POOL_CENT_TOTALS = 150, POOL_CENT_FLAG, POOL_CENT_SOURCES, POOL_CENT_CAPS, POOL_CENT_LIST,
   POOL_CENT_TOMB, POOL_CENT_VALUES,
   POOL_VEC_PARTIAL = 160, POOL_VEC_RESULT,
+  POOL_MAP_PROGRAM = 170, POOL_MAP_ERROR, POOL_MAP_OUT,
+  POOL_MAP_OPERAND_0 = 180,  // .. 195: one per operand
 };
 
 // A call's context: the stream, the caller's detail and cancellation.
