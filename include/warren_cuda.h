@@ -479,6 +479,26 @@ wc_status wc_centrality(wc_version* version, const wc_call* call, const wc_centr
                         const uint64_t* sources, uint64_t count, const uint64_t* tombstone_words,
                         double* values_out);
 
+/* compute/centrality/betweenness.rs:18-37 (BetweennessScale and the
+ * graph's direction, which the rescale reads). */
+typedef struct wc_betweenness_opts {
+    int32_t normalized;      /* divide by the pairs a path could join */
+    int32_t endpoints;       /* count a path's ends as on it */
+    int32_t directed;        /* the version's rows are directed (else uploaded symmetrised) */
+    uint32_t blocks_per_sm;  /* 0: 4 */
+} wc_betweenness_opts;
+
+/* compute/centrality/betweenness.rs:27-38: each node's betweenness over the
+ * fewest-edge shortest paths of the version's forward rows (weights are not
+ * read), by Brandes' algorithm from `sources` (distinct live nodes,
+ * ascending, as wc_sample_sources gives them), rescaled as NetworkX 3.7
+ * (betweenness.rs:113-141); tombstoned nodes 0.  Path counts are f64 as in
+ * the reference, and the values are the reference's to the bit while they
+ * stay below 2^53.  A search deeper than 1,024 levels is WC_UNSUPPORTED. */
+wc_status wc_betweenness(wc_version* version, const wc_call* call, const wc_betweenness_opts* opts,
+                         const uint64_t* sources, uint64_t count, const uint64_t* tombstone_words,
+                         double* values_out);
+
 /* ------------------------------------------------------------- spectral */
 
 /* spectral/operator.rs:33-44 (Operator) and lanczos.rs:69-74 (Which). */

@@ -110,6 +110,8 @@ def _declare(L):
     L.wo_reduce.argtypes = [I, P, U64, U64, P, I, P, P]
     L.wo_norm_diff.restype = I32
     L.wo_norm_diff.argtypes = [I, P, U64, I, P, U64, U64, I, P]
+    L.wo_betweenness.restype = I32
+    L.wo_betweenness.argtypes = [P, P, U64, P, I, I, I, P]
     L.wo_sample_sources.restype = I32
     L.wo_sample_sources.argtypes = [U64, P, P, I, C.c_int64, U64, P, P]
     L.wo_centrality.restype = I32
@@ -336,6 +338,15 @@ def sample_sources(n, tombstones=None, population=None, complement=False, k=None
                                    -1 if k is None else int(k), seed & (2**64 - 1), _ptr(out),
                                    _ptr(count)))
     return out[:int(count[0])].copy()
+
+
+def betweenness(g, sources, tombstones=None, normalized=True, endpoints=False, directed=True):
+    """betweenness.rs with paths.rs (unweighted), sources in order: f64[n]."""
+    src = np.ascontiguousarray(sources, dtype=np.uint64)
+    out = np.zeros(g.n, np.float64)
+    _check(lib().wo_betweenness(g.handle, _ptr(src), len(src), _ptr(tombstones), int(normalized),
+                                int(endpoints), int(directed), _ptr(out)))
+    return out
 
 
 def centrality(g, measure, sources, tombstones=None, wf_improved=True):

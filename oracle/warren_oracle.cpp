@@ -1183,6 +1183,75 @@ int32_t wo_norm_diff(int dtype_a, const void* a, uint64_t na, int dtype_b, const
   return WC_OK;
 }
 
+// compute/centrality/betweenness.rs with paths.rs:148-260 (unweighted):
+// per source in the given order, a breadth-first search over the forward
+// rows counting shortest paths (f64), then the dependencies in reverse
+// search order, each row's out-neighbours in ascending order; every node's
+// total gains each source's dependency in source order (the source none,
+// or with endpoints the other nodes it reaches, every reached node one
+// more); then betweenness.rs:113-141's rescale; tombstoned nodes 0.
+int32_t wo_betweenness(const wo_graph* gp, const uint64_t* sources, uint64_t count,
+                       const uint64_t* tomb, int normalized, int endpoints, int directed,
+                       double* out) {
+  const Graph& g = *(const Graph*)gp;
+  const uint64_t n = g.fwd.n;
+  std::vector<double> total(n, 0.0), dist(n, INFINITY), sigma(n, 0.0), dep(n, 0.0);
+  std::vector<uint64_t> order;
+  for (uint64_t q = 0; q < count; q++) {
+    const uint64_t s = sources[q];
+    for (uint64_t v : order) dist[v] = INFINITY, sigma[v] = 0.0, dep[v] = 0.0;
+    order.assign(1, s);
+    dist[s] = 0.0;
+    sigma[s] = 1.0;
+    for (size_t h = 0; h < order.size(); h++) {
+      const uint64_t u = order[h];
+      const double through = dist[u] + 1.0;
+      for (uint64_t e = g.fwd.off[u]; e < g.fwd.off[u + 1]; e++) {
+        const uint64_t t = g.fwd.tgt[e];
+        if (dist[t] == INFINITY) {
+          dist[t] = through;
+          order.push_back(t);
+        }
+        if (dist[t] == through) sigma[t] += sigma[u];
+      }
+    }
+    for (size_t h = order.size(); h-- > 0;) {
+      const uint64_t v = order[h];
+      double gained = 0.0;
+      for (uint64_t e = g.fwd.off[v]; e < g.fwd.off[v + 1]; e++) {
+        const uint64_t w = g.fwd.tgt[e];
+        if (w != v && dist[v] + 1.0 == dist[w]) gained += sigma[v] / sigma[w] * (1.0 + dep[w]);
+      }
+      dep[v] = gained;
+    }
+    dep[s] = 0.0;
+    if (endpoints) {
+      for (size_t h = 1; h < order.size(); h++) dep[order[h]] += 1.0;
+      dep[s] = (double)(order.size() - 1);
+    }
+    for (uint64_t v = 0; v < n; v++) total[v] += dep[v];
+  }
+  uint64_t live = 0;
+  for (uint64_t v = 0; v < n; v++) live += !tombstoned(tomb, v);
+  const bool every = count == live;
+  const __int128 pairs = (__int128)live - (endpoints ? 0 : 1);
+  double fs = 1.0, fo = 1.0;
+  if (pairs >= 2) {
+    const __int128 corr = directed ? 1 : 2, ks = every ? pairs : (__int128)count;
+    auto factor = [&](__int128 k) {
+      return normalized ? 1.0 / (double)(k * (pairs - 1)) : (double)pairs / (double)(k * corr);
+    };
+    fo = factor(ks);
+    fs = (every || endpoints) ? fo : (ks > 1 ? factor(ks - 1) : NAN);
+  }
+  std::vector<char> is_source(n, 0);
+  if (!every)
+    for (uint64_t q = 0; q < count; q++) is_source[sources[q]] = 1;
+  for (uint64_t v = 0; v < n; v++)
+    out[v] = tombstoned(tomb, v) ? 0.0 : total[v] * (is_source[v] ? fs : fo);
+  return WC_OK;
+}
+
 // compute/ranking.rs:15-80 (top_k) over f64 values.
 int32_t wo_topk_f64(const double* x, uint64_t n, const uint64_t* tomb, uint64_t k, int descending,
                     uint64_t* nodes, double* values, uint64_t* count) {

@@ -13,7 +13,7 @@ from .api import (Budget, GraphVersion, Product, PageRank, Limits, EigenOptions,
                   minplus_batched, ppr_batched, autotune, set_schedule, eigen, pagerank_adjoint, top_k, rmat, gnm,
                   edge_weights, node_set, HostGraph, Sampling, Centrality, sample_sources,
                   closeness_centrality, harmonic_centrality, vector_reduce, vector_norm_diff,
-                  vector_map)
+                  vector_map, betweenness_centrality)
 from ._abi import load, LIBRARY
 
 __all__ = ["Budget", "GraphVersion", "Product", "PageRank", "Limits", "EigenOptions",
@@ -22,4 +22,5 @@ __all__ = ["Budget", "GraphVersion", "Product", "PageRank", "Limits", "EigenOpti
            "pagerank_adjoint", "top_k", "rmat", "gnm", "edge_weights", "node_set", "HostGraph",
            "Sampling", "Centrality", "sample_sources", "closeness_centrality",
            "harmonic_centrality", "vector_reduce", "vector_norm_diff", "vector_map",
+           "betweenness_centrality",
            "load", "LIBRARY"]

@@ -85,6 +85,11 @@ class Schedule(C.Structure):
                 ("reserved", U32)]
 
 
+class BetweennessOpts(C.Structure):
+    _fields_ = [("normalized", I32), ("endpoints", I32), ("directed", I32),
+                ("blocks_per_sm", U32)]
+
+
 class CentralityOpts(C.Structure):
     _fields_ = [("measure", U32), ("wf_improved", U32), ("columns_per_pass", U32),
                 ("blocks_per_sm", U32)]
@@ -141,6 +146,7 @@ SIGNATURES = [
     ("wc_minplus_batched", I32, [P, C.POINTER(Call), P, P, U32, P, P]),
     ("wc_ppr_batched", I32, [P, C.POINTER(Call), C.POINTER(PageRankOpts), P, P, U32, P, P]),
     ("wc_sample_sources", I32, [U64, P, P, I32, C.c_int64, U64, P, C.POINTER(U64)]),
+    ("wc_betweenness", I32, [P, C.POINTER(Call), C.POINTER(BetweennessOpts), P, U64, P, P]),
     ("wc_centrality", I32, [P, C.POINTER(Call), C.POINTER(CentralityOpts), P, U64, P, P]),
     ("wc_eigen", I32, [P, C.POINTER(Call), C.POINTER(EigenOpts), P, P, P, C.POINTER(EigenStats)]),
     ("wc_pagerank_adjoint", I32, [P, C.POINTER(Call), C.POINTER(PageRankOpts), P, P, U32, D, P,

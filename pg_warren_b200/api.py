@@ -918,6 +918,24 @@ def harmonic_centrality(graph: GraphVersion, sampling: Sampling = Sampling(), to
                        sources)
 
 
+def betweenness_centrality(graph: GraphVersion, sampling: Sampling = Sampling(),
+                           normalized: bool = True, endpoints: bool = False,
+                           directed: bool = True, tombstones=None, interrupts=None,
+                           sources=None) -> Centrality:
+    """compute/centrality/betweenness.rs:27-38 on the version's unweighted
+    forward rows (an undirected graph: upload it symmetrised and pass
+    directed=False, which the rescale reads)."""
+    if sources is None:
+        sources = sample_sources(graph.id_space, sampling, tombstones)
+    sources = np.ascontiguousarray(sources, dtype=np.uint64)
+    values = np.zeros(graph.id_space, np.float64)
+    o = A.BetweennessOpts(int(normalized), int(endpoints), int(directed), 0)
+    call, detail = _call(interrupts)
+    _raise(A.load().wc_betweenness(graph.handle, C.byref(call), C.byref(o), _ptr(sources),
+                                   len(sources), _ptr(tombstones), _ptr(values)), detail)
+    return Centrality(values, len(sources))
+
+
 def reachable(graph: GraphVersion, start: int, target: int, max_depth=None,
               direction="out") -> Traversed:
     """traversal/reachable.rs:18-43."""

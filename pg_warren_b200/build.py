@@ -22,8 +22,10 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# -fmad=false: a product and a sum stay two roundings, as on the host, so
+# floating-point results follow the reference's operation order bit for bit.
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", f"-I{INCLUDE}",
-         "--expt-relaxed-constexpr", "--extended-lambda"]
+         "--expt-relaxed-constexpr", "--extended-lambda", "-fmad=false"]
 
 
 def sources():

@@ -20,6 +20,7 @@ struct CentArgs {
   unsigned long long* dsum;     // their summed distances
   double* harm;                 // Σ 1 / distance, batch by batch
   int* cut;
+  bool keep_only = false;       // keep the snapshots for the caller's kernels, count nothing
 };
 
 wc_schedule default_bfs_schedule(uint32_t width);

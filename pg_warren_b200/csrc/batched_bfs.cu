@@ -804,8 +804,9 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
       // have neighbours deeper still.
       note_launch(), msbfs_cut_kernel<<<max_blocks(2), 256, 0, st>>>(
           wbits + (uint64_t)levels * bitmap_words, (uint32_t)bitmap_words, cent->cut);
-      note_launch(), msbfs_centrality_kernel<W><<<max_blocks(4), 256, 0, st>>>(
-          n, levels, F, fstride, wbits, (uint32_t)bitmap_words, *cent);
+      if (!cent->keep_only)
+        note_launch(), msbfs_centrality_kernel<W><<<max_blocks(4), 256, 0, st>>>(
+            n, levels, F, fstride, wbits, (uint32_t)bitmap_words, *cent);
       return cuda_status(cudaGetLastError(), ctx.detail, "centrality pass");
     } else {
       return WC_INVALID_ARGUMENT;
@@ -911,7 +912,8 @@ wc_status bfs_centrality_pass(Ctx& ctx, BatchBuffers& b, uint32_t columns,
                               const uint64_t* sources_dev, const uint32_t* caps_dev, uint32_t k,
                               uint32_t levels, uint32_t blocks_per_sm, const CentArgs& cent) {
   const std::string key = "cent/" + std::to_string(columns) + "/" + std::to_string(k) + "/" +
-                          std::to_string(levels) + "/" + std::to_string(blocks_per_sm);
+                          std::to_string(levels) + "/" + std::to_string(blocks_per_sm) +
+                          (cent.keep_only ? "/keep" : "");
   return ctx.run_captured(key, [&] {
     return pass_for(columns)(ctx, b, sources_dev, caps_dev, k, levels, nullptr, nullptr,
                              blocks_per_sm, &cent);

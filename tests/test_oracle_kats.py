@@ -597,3 +597,27 @@ def test_chunked_sums_follow_the_chunk_order(oracle):
     for p in parts:
         total = total + p
     assert O.reduce(x, "sum") == total
+
+
+BETWEENNESS_KATS = [  # compute/centrality/tests.rs:86-113 (NetworkX's values)
+    (True, True, [0.45, 0.325, 0.325, 0.45, 0.0], [0.625, 0.3125, 0.5625, 0.5, 0.0]),
+    (True, False, [0.25, 1 / 24, 1 / 24, 0.25, 0.0], [1 / 3, 1 / 12, 1 / 6, 1 / 3, 0.0]),
+    (False, True, [9.0, 6.5, 6.5, 9.0, 0.0], [12.5, 6.25, 11.25, 10.0, 0.0]),
+    (False, False, [3.0, 0.5, 0.5, 3.0, 0.0], [4.0, 1.0, 2.0, 4.0, 0.0]),
+]
+
+
+def betweenness_example():
+    # compute/centrality/tests.rs:79-85: 0 → 1 → 2 → 3 → 0, 0 → 2, 1 → 3, node 4 alone.
+    return directed(5, [(0, 1), (1, 2), (2, 3), (0, 2), (3, 0), (1, 3)])
+
+
+def test_betweenness_known_answers(oracle):
+    g = betweenness_example()
+    every = O.sample_sources(5)
+    two = O.sample_sources(5, population=np.array([1, 0, 1, 0, 0]))
+    for normalized, endpoints, exact, from_two in BETWEENNESS_KATS:
+        got = O.betweenness(g, every, normalized=normalized, endpoints=endpoints)
+        assert np.allclose(got, exact, rtol=1e-12, atol=0), (normalized, endpoints)
+        got = O.betweenness(g, two, normalized=normalized, endpoints=endpoints)
+        assert np.allclose(got, from_two, rtol=1e-12, atol=0), (normalized, endpoints)
