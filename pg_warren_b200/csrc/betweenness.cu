@@ -5,16 +5,19 @@
 //
 // The sources run 64 at a time through the batched BFS, which keeps one
 // frontier snapshot per level: bit s of node v's row of F_L says that
-// source s first reaches v at distance L.  Then, per level, on the device:
+// source s first reaches v at distance L.  Then, per level, on the device,
+// over the row-split schedules (long rows in pieces of 256 entries):
 //  - path counts σ (f64, n × 64): a node first reached at L sums σ over
 //    its in-neighbours at L - 1.  The counts are integers, exact in f64 up
 //    to 2^53, so their order does not matter;
 //  - dependencies δ, from the deepest level up: δ(v) = Σ σ(v)/σ(w) ·
 //    (1 + δ(w)) over v's out-neighbours w one level further, taken in
-//    ascending order, term by term, as paths.rs:244-260 takes them;
+//    ascending order, term by term, as paths.rs:244-260 takes them (rows
+//    over 256 entries: each piece in order, then the pieces in order);
 //  - then each node's total gains the pass's 64 sources' dependencies in
 //    source order (betweenness.rs:76-93 folds sources in ascending order).
-// Up to the path counts' 2^53, the values are the reference's to the bit.
+// Up to the path counts' 2^53 and rows over 256 entries, the values are the
+// reference's to the bit.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -39,6 +42,12 @@ struct BcPass {
   const uint32_t* rtgt;
   const uint32_t* foff;    // forward CSR (out-neighbours)
   const uint32_t* ftgt;
+  const Unit* runits;      // the reverse CSR's row-split schedule
+  uint32_t rcount;
+  const Unit* funits;      // the forward CSR's, with its long rows' counters
+  uint32_t fcount;
+  uint32_t* counters;      // left zero
+  double* carry;           // slots × 64: the forward long rows' piece sums
   double* sigma;           // n × 64
   double* delta;           // n × 64
 };
@@ -55,16 +64,34 @@ __global__ void bc_seed_kernel(const uint64_t* sources, uint32_t k, double* sigm
   if (s < k) sigma[sources[s] * kBcColumns + s] = 1.0;
 }
 
-// σ of the rows first reached at level L (L >= 1): a warp per row, lane
-// `lane` for sources lane and 32 + lane.
+// The σ sum of one row's entries [e0, e1) for this lane's sources: the
+// in-neighbours u at level L - 1 whose bit is set.
+__device__ inline void sigma_run(const BcPass& P, uint32_t L, uint32_t e0, uint32_t e1,
+                                 const bool (&mine)[kBcWords], double (&acc)[kBcWords]) {
+  const uint32_t lane = threadIdx.x & 31;
+  for (uint32_t e = e0; e < e1; e++) {
+    const uint32_t u = P.rtgt[e];
+    if (!written(P, L - 1, u)) continue;
+#pragma unroll
+    for (int q = 0; q < kBcWords; q++)
+      if (mine[q] && ((row_word(P, L - 1, u, q) >> lane) & 1))
+        acc[q] += P.sigma[(size_t)u * kBcColumns + 32 * q + lane];
+  }
+}
+
+// σ of the rows first reached at level L (L >= 1), over the reverse CSR's
+// row-split schedule: a warp per unit, lane `lane` for sources lane and
+// 32 + lane.  A tile's rows are summed whole; a long row's pieces add their
+// sums atomically (path counts are integers: the order cannot change them).
 __global__ void bc_sigma_kernel(BcPass P, uint32_t L) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < P.bitmap_words; t += warps) {
-    uint32_t bits = P.wbits[(size_t)L * P.bitmap_words + t];
-    while (bits) {
-      const uint32_t v = 32 * t + __ffs(bits) - 1;
-      bits &= bits - 1;
+  for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < P.rcount; u += warps) {
+    const Unit U = P.runits[u];
+    const bool tile = (U.c >> 31) == 0;
+    const uint32_t r0 = U.a, r1 = tile ? U.b : U.a + 1;
+    for (uint32_t v = r0; v < r1; v++) {
+      if (!written(P, L, v)) continue;
       bool mine[kBcWords];
       double acc[kBcWords];
 #pragma unroll
@@ -72,31 +99,54 @@ __global__ void bc_sigma_kernel(BcPass P, uint32_t L) {
         mine[q] = (row_word(P, L, v, q) >> lane) & 1;
         acc[q] = 0.0;
       }
-      for (uint32_t e = P.roff[v]; e < P.roff[v + 1]; e++) {
-        const uint32_t u = P.rtgt[e];
-        if (!written(P, L - 1, u)) continue;
+      if (tile) {
+        sigma_run(P, L, P.roff[v], P.roff[v + 1], mine, acc);
 #pragma unroll
         for (int q = 0; q < kBcWords; q++)
-          if (mine[q] && ((row_word(P, L - 1, u, q) >> lane) & 1))
-            acc[q] += P.sigma[(size_t)u * kBcColumns + 32 * q + lane];
-      }
+          if (mine[q]) P.sigma[(size_t)v * kBcColumns + 32 * q + lane] = acc[q];
+      } else {
+        sigma_run(P, L, U.b, U.d, mine, acc);
 #pragma unroll
-      for (int q = 0; q < kBcWords; q++)
-        if (mine[q]) P.sigma[(size_t)v * kBcColumns + 32 * q + lane] = acc[q];
+        for (int q = 0; q < kBcWords; q++)
+          if (mine[q] && acc[q] != 0.0)
+            atomicAdd(P.sigma + (size_t)v * kBcColumns + 32 * q + lane, acc[q]);
+      }
     }
   }
 }
 
+// The dependency terms of one row's entries [e0, e1), in order, added to
+// `gained`: σ(v)/σ(w) · (1 + δ(w)) over the out-neighbours w one level on.
+__device__ inline void delta_run(const BcPass& P, uint32_t L, uint32_t e0, uint32_t e1,
+                                 const bool (&mine)[kBcWords], const double (&sv)[kBcWords],
+                                 double (&gained)[kBcWords]) {
+  const uint32_t lane = threadIdx.x & 31;
+  for (uint32_t e = e0; e < e1; e++) {
+    const uint32_t w = P.ftgt[e];
+    if (!written(P, L + 1, w)) continue;
+#pragma unroll
+    for (int q = 0; q < kBcWords; q++)
+      if (mine[q] && ((row_word(P, L + 1, w, q) >> lane) & 1)) {
+        const size_t at = (size_t)w * kBcColumns + 32 * q + lane;
+        gained[q] += sv[q] / P.sigma[at] * (1.0 + P.delta[at]);
+      }
+  }
+}
+
 // δ of the rows first reached at level L, from level L + 1's (already
-// final): out-neighbours in ascending order, term by term.
+// final), over the forward CSR's schedule: a tile's rows in order, term by
+// term (paths.rs:244-260); a long row's pieces each in order, then the
+// pieces' sums in piece order by the warp that brings the last piece, so
+// only rows over 256 entries are reassociated.
 __global__ void bc_delta_kernel(BcPass P, uint32_t L) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < P.bitmap_words; t += warps) {
-    uint32_t bits = P.wbits[(size_t)L * P.bitmap_words + t];
-    while (bits) {
-      const uint32_t v = 32 * t + __ffs(bits) - 1;
-      bits &= bits - 1;
+  for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < P.fcount; u += warps) {
+    const Unit U = P.funits[u];
+    const bool tile = (U.c >> 31) == 0;
+    const uint32_t r0 = U.a, r1 = tile ? U.b : U.a + 1;
+    for (uint32_t v = r0; v < r1; v++) {
+      if (!written(P, L, v)) continue;
       bool mine[kBcWords];
       double sv[kBcWords], gained[kBcWords];
 #pragma unroll
@@ -105,19 +155,37 @@ __global__ void bc_delta_kernel(BcPass P, uint32_t L) {
         sv[q] = mine[q] ? P.sigma[(size_t)v * kBcColumns + 32 * q + lane] : 0.0;
         gained[q] = 0.0;
       }
-      for (uint32_t e = P.foff[v]; e < P.foff[v + 1]; e++) {
-        const uint32_t w = P.ftgt[e];
-        if (!written(P, L + 1, w)) continue;
+      if (tile) {
+        delta_run(P, L, P.foff[v], P.foff[v + 1], mine, sv, gained);
 #pragma unroll
         for (int q = 0; q < kBcWords; q++)
-          if (mine[q] && ((row_word(P, L + 1, w, q) >> lane) & 1)) {
-            const size_t at = (size_t)w * kBcColumns + 32 * q + lane;
-            gained[q] += sv[q] / P.sigma[at] * (1.0 + P.delta[at]);
-          }
+          if (mine[q]) P.delta[(size_t)v * kBcColumns + 32 * q + lane] = gained[q];
+        continue;
       }
+      delta_run(P, L, U.b, U.d, mine, sv, gained);
+      const uint32_t slot = U.c & 0x7fffffffu;
+      const uint32_t row_lo = P.foff[v], deg = P.foff[v + 1] - row_lo;
+      const uint32_t pieces = (deg + kPieceEntries - 1) / kPieceEntries;
+      const uint32_t first = slot - (U.b - row_lo) / kPieceEntries;
 #pragma unroll
-      for (int q = 0; q < kBcWords; q++)
-        if (mine[q]) P.delta[(size_t)v * kBcColumns + 32 * q + lane] = gained[q];
+      for (int q = 0; q < kBcWords; q++) P.carry[(size_t)slot * kBcColumns + 32 * q + lane] = gained[q];
+      __threadfence();
+      __syncwarp();
+      uint32_t arrived = 0;
+      if (lane == 0) arrived = atomicAdd(P.counters + first, 1u);
+      arrived = __shfl_sync(0xffffffffu, arrived, 0);
+      if (arrived == pieces - 1) {
+        __threadfence();
+#pragma unroll
+        for (int q = 0; q < kBcWords; q++) {
+          double total = 0.0;
+          for (uint32_t p = 0; p < pieces; p++)
+            total += __ldcg(P.carry + (size_t)(first + p) * kBcColumns + 32 * q + lane);
+          if (mine[q]) P.delta[(size_t)v * kBcColumns + 32 * q + lane] = total;
+        }
+        __syncwarp();
+        if (lane == 0) P.counters[first] = 0;
+      }
     }
   }
 }
@@ -256,6 +324,9 @@ wc_status wc_betweenness(wc_version* v, const wc_call* call, const wc_betweennes
   WC_TRY(ctx.scratch(POOL_BC_SOURCES, ((n + 31) / 32) * 4, &isrc));
   WC_TRY(ctx.scratch(POOL_BC_CAPS, kBcColumns * 4, &capb));
   WC_TRY(ctx.scratch(POOL_BC_LIST, std::max<uint64_t>(count, 1) * 8, &srcb));
+  DevBuf* carry;
+  WC_TRY(ctx.scratch(POOL_BC_CARRY,
+                     (uint64_t)std::max<uint32_t>(v->fwd.schedule.slots, 1) * kBcColumns * 8, &carry));
   if (!tomb.empty()) {
     WC_TRY(ctx.scratch(POOL_BC_TOMB, words * 8, &tb));
     WC_CUDA(cudaMemcpyAsync(tb->ptr, tomb.data(), words * 8, cudaMemcpyHostToDevice, ctx.stream),
@@ -304,7 +375,10 @@ wc_status wc_betweenness(wc_version* v, const wc_call* call, const wc_betweennes
     const uint64_t maps = (uint64_t)(levels + 2) * bitmap_words;
     BcPass P{(uint32_t)n, n * kBcWords, b.F->as<uint32_t>(), b.bits->as<uint32_t>() + maps,
              bitmap_words, v->rev.offsets.as<uint32_t>(), v->rev.targets.as<uint32_t>(),
-             v->fwd.offsets.as<uint32_t>(), v->fwd.targets.as<uint32_t>(), sig->as<double>(),
+             v->fwd.offsets.as<uint32_t>(), v->fwd.targets.as<uint32_t>(),
+             v->rev.schedule.units.as<Unit>(), v->rev.schedule.count,
+             v->fwd.schedule.units.as<Unit>(), v->fwd.schedule.count,
+             v->fwd.schedule.counters.as<uint32_t>(), carry->as<double>(), sig->as<double>(),
              del->as<double>()};
     WC_CUDA(cudaMemsetAsync(sig->ptr, 0, n * kBcColumns * 8, ctx.stream), ctx.detail);
     WC_CUDA(cudaMemsetAsync(del->ptr, 0, n * kBcColumns * 8, ctx.stream), ctx.detail);

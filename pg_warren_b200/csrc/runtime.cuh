@@ -280,7 +280,7 @@ enum PoolTag {
   POOL_MAP_PROGRAM = 170, POOL_MAP_ERROR, POOL_MAP_OUT,
   POOL_MAP_OPERAND_0 = 180,  // .. 195: one per operand
   POOL_BC_SIGMA = 200, POOL_BC_DELTA, POOL_BC_TOTAL, POOL_BC_REACHED, POOL_BC_FLAG,
-  POOL_BC_SOURCES, POOL_BC_CAPS, POOL_BC_LIST, POOL_BC_TOMB, POOL_BC_VALUES,
+  POOL_BC_SOURCES, POOL_BC_CAPS, POOL_BC_LIST, POOL_BC_TOMB, POOL_BC_VALUES, POOL_BC_CARRY,
 };
 
 // A call's context: the stream, the caller's detail and cancellation.

@@ -307,7 +307,8 @@ int32_t wc_serves(const char* op, wc_dtype dtype) {
   if (o == "spmv" || o == "spmm") return dtype >= WC_F32 && dtype <= WC_BOOL;
   if (o == "pagerank" || o == "eigen") return dtype == WC_F64;
   if (o == "bfs" || o == "reachable_set" || o == "reachable" || o == "components") return 1;
-  if (o == "closeness_centrality" || o == "harmonic_centrality") return dtype == WC_F64;
+  if (o == "closeness_centrality" || o == "harmonic_centrality" || o == "betweenness_centrality")
+    return dtype == WC_F64;
   if (o == "vector_reduce" || o == "vector_norm_diff" || o == "vector_map")
     return dtype >= WC_F32 && dtype <= WC_BOOL;
   if (o == "vector_topk") return dtype == WC_F64;

@@ -1,7 +1,8 @@
 """Betweenness centrality on the batched BFS (wc_betweenness) against the
 oracle's restatement of the reference's one-source-at-a-time Brandes: the
-reference's known answers, and R-MAT graphs bit for bit (path counts stay
-far below 2^53 here)."""
+reference's known answers, and R-MAT graphs bit for bit while no row has
+over 256 entries (path counts stay far below 2^53 here), within 1e-13
+relative where a long row's pieces are summed in order.""" 
 
 import numpy as np
 import pytest
@@ -41,7 +42,10 @@ def test_rmat_matches_the_oracle_bit_for_bit(scale, k, endpoints):
         got = W.betweenness_centrality(gv, normalized=normalized, endpoints=endpoints,
                                        tombstones=tomb, sources=src)
         want = O.betweenness(og, src, tombstones=tomb, normalized=normalized, endpoints=endpoints)
-        assert got.values.tobytes() == want.tobytes(), normalized
+        if np.diff(g.offsets.astype(np.int64)).max() <= 256:
+            assert got.values.tobytes() == want.tobytes(), normalized
+        else:  # rows over 256 entries sum their pieces in order: reassociated
+            assert np.allclose(got.values, want, rtol=1e-13, atol=0), normalized
 
 
 def test_undirected_deep_graph():
