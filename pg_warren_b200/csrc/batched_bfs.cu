@@ -567,17 +567,60 @@ __global__ void __launch_bounds__(256) msbfs_settle_kernel(MsLevel P) {
 // edges_traversed: Σ out-degree over the nodes it reached at a depth below
 // its cap.  A block takes 32 nodes at a time, all sources of the pass.
 // Phase 1: a thread per (node, word) — the lanes of a warp cover whole node
-// rows, so each level's row is read coalesced (only rows marked written) —
-// folds the node's frontier words into NB bit planes of the depth (plane b:
-// the sources that reached it at a level with bit b set) and the reached
-// set, turns them into 32 depth bytes with a multiply that spreads four bits
-// to four bytes, and scatters them into a shared [source][node] tile (rows
-// of each 32-source block shifted by one word, which keeps the scatter free
-// of bank conflicts).  Phase 2: eight threads a source row store its 32
-// bytes, four each, and add the out-degrees of the nodes whose depth is
-// below the source's cap (four bytes compared at once) to the source's
-// shared sum; the sums go to the global counts once per block.
-__device__ inline uint32_t spread4(uint32_t nibble) { return (nibble * 0x00204081u) & 0x01010101u; }
+// rows, so each level's row is read coalesced (only rows marked written,
+// four levels' loads in flight).  A ballot over the tile's written-row
+// words, a level per lane, gives the node its written levels; a node no
+// source reached stores 255s at once.  Otherwise the node's frontier words
+// fold into NB bit planes of the depth (plane b: the sources that reached
+// it at a level with bit b set) and the unreached set, and an 8×8
+// bit-matrix transpose turns 8 planes × 8 sources into 8 depth bytes
+// (unreached sources have every plane set: 255).  The 32 bytes go to a
+// node-major shared tile as two 16-byte stores, the 16-byte groups of row j
+// XOR-swizzled by j/4.
+// Phase 2: a thread per (four sources, four nodes) reads four words of the
+// tile, transposes their bytes so each word is one source's four nodes, and
+// stores it; eight threads cover a source's 32 nodes in one 32-byte sector.
+// The out-degrees of the nodes whose depth is below the source's cap
+// (bytes compared four at a time, weighted by dp4a) are summed over the
+// eight threads by shuffles into the source's shared sum; the sums go to
+// the global counts once per block.
+
+// Rows a0..a3 of a 4×4 byte matrix become its columns: afterwards a_t
+// holds [a0.t, a1.t, a2.t, a3.t] of the inputs.
+__device__ inline void byte_transpose4(uint32_t& a0, uint32_t& a1, uint32_t& a2, uint32_t& a3) {
+  const uint32_t p = __byte_perm(a0, a1, 0x5140), q = __byte_perm(a2, a3, 0x5140);
+  const uint32_t r = __byte_perm(a0, a1, 0x7362), s = __byte_perm(a2, a3, 0x7362);
+  a0 = __byte_perm(p, q, 0x5410);
+  a1 = __byte_perm(p, q, 0x7632);
+  a2 = __byte_perm(r, s, 0x5410);
+  a3 = __byte_perm(r, s, 0x7632);
+}
+
+// The 8×8 bit matrix held as eight bytes (lo: bytes 0-3, hi: bytes 4-7;
+// element (r, c) is bit c of byte r) transposed: three rounds of swapping
+// the off-diagonal 1×1, 2×2 and 4×4 blocks.
+__device__ inline void bit_transpose8(uint32_t& lo, uint32_t& hi) {
+  uint32_t t;
+  t = (lo ^ (lo >> 7)) & 0x00AA00AAu;
+  lo ^= t ^ (t << 7);
+  t = (hi ^ (hi >> 7)) & 0x00AA00AAu;
+  hi ^= t ^ (t << 7);
+  t = (lo ^ (lo >> 14)) & 0x0000CCCCu;
+  lo ^= t ^ (t << 14);
+  t = (hi ^ (hi >> 14)) & 0x0000CCCCu;
+  hi ^= t ^ (t << 14);
+  t = (lo ^ (hi << 4)) & 0xF0F0F0F0u;
+  lo ^= t;
+  hi ^= t >> 4;
+}
+
+// Per byte, 1 where a < b (unsigned), else 0.  The low seven bits are
+// compared by a subtraction that cannot borrow across bytes; the top bits
+// decide where they differ.
+__device__ inline uint32_t bytes_below(uint32_t a, uint32_t b) {
+  const uint32_t x = (a | 0x80808080u) - (b & 0x7F7F7F7Fu);
+  return (((~a & b) | (~(a ^ b) & ~x)) & 0x80808080u) >> 7;
+}
 
 template <int W, int NB>
 __global__ void __launch_bounds__(256)
@@ -585,12 +628,16 @@ __global__ void __launch_bounds__(256)
                        const uint32_t* wbits, uint32_t bitmap_words, const uint32_t* caps,
                        const uint32_t* off, const uint32_t* counts, uint8_t* depth_out,
                        unsigned long long* edges) {
-  constexpr uint32_t S = 32 * W;  // sources in the pass (k <= S)
-  __shared__ __align__(16) uint32_t tile[S * 8 + W];
+  constexpr uint32_t S = 32 * W;            // sources in the pass (k <= S)
+  constexpr uint32_t Q = 8 * W;             // four-source words in a node row of the tile
+  constexpr uint32_t G = 2 * W;             // 16-byte groups in a node row
+  constexpr uint32_t NPW = 32 / W;          // nodes a warp's lanes cover at once
+  constexpr uint32_t LC = NB == 5 ? 1 : 8;  // 32-level chunks of the written levels
+  __shared__ __align__(16) uint32_t tile[32 * Q];
+  __shared__ __align__(16) uint32_t cap4s[S];
   __shared__ unsigned long long esum[S];
-  __shared__ uint32_t cap4s[S];
-  __shared__ uint32_t degs[32];
-  uint8_t* tbytes = reinterpret_cast<uint8_t*>(tile);
+  __shared__ __align__(16) uint32_t degs[32];
+  const uint32_t lane = threadIdx.x & 31;
   // The snapshots written: F_L exists for L < used (F_L is written only if
   // level L-1 had a frontier to expand).
   uint32_t used = 1;
@@ -598,80 +645,157 @@ __global__ void __launch_bounds__(256)
   for (uint32_t x = threadIdx.x; x < S; x += blockDim.x) {
     esum[x] = 0;
     // Depth bytes below the cap count as expanded; 255 marks "not reached".
-    cap4s[x] = (x < k ? min(caps[x], 255u) : 0u) * 0x01010101u;
+    // With five planes depths are at most 31, so a cap above 127 compares
+    // as 127 (the one-subtraction compare of phase 2 needs caps <= 127).
+    cap4s[x] = (x < k ? min(caps[x], NB == 5 ? 127u : 255u) : 0u) * 0x01010101u;
   }
   const bool aligned = (n & 3u) == 0;
   const uint32_t tiles = (n + 31) / 32;
   for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
     const uint32_t i0 = t * 32;
+    // Lane L holds level 32c + L's written-row word of the tile.
+    uint32_t wl[LC];
+#pragma unroll
+    for (uint32_t c = 0; c < LC; c++) {
+      const uint32_t L = 32 * c + lane;
+      wl[c] = L < used ? wbits[(size_t)L * bitmap_words + t] : 0u;
+    }
+    if (threadIdx.x < 32) {
+      const uint32_t i = i0 + threadIdx.x;
+      degs[threadIdx.x] = i < n ? __ldg(off + i + 1) - __ldg(off + i) : 0u;
+    }
     for (uint32_t x = threadIdx.x; x < 32 * W; x += blockDim.x) {
-      const uint32_t j = x / W, w = x % W, i = i0 + j;
-      uint32_t plane[NB];
+      const uint32_t j = x / W, w = x % W;
+      const uint32_t jbase = (x - lane) / W;  // the warp's first node
+      uint32_t lm[LC];
+      uint32_t any = 0;
 #pragma unroll
-      for (int b = 0; b < NB; b++) plane[b] = 0;
+      for (uint32_t c = 0; c < LC; c++) {
+        lm[c] = 0;
+#pragma unroll
+        for (uint32_t jj = 0; jj < NPW; jj++) {
+          const uint32_t bal = __ballot_sync(0xffffffffu, (wl[c] >> (jbase + jj)) & 1u);
+          if (lane / W == jj) lm[c] = bal;
+        }
+        if (i0 + j >= n) lm[c] = 0;
+        any |= lm[c];
+      }
+      uint32_t* trow = tile + j * Q;
+      const uint32_t sw = (j >> 2) & (G - 1);
+      uint4* grp0 = reinterpret_cast<uint4*>(trow + (((2 * w) ^ sw) << 2));
+      uint4* grp1 = reinterpret_cast<uint4*>(trow + (((2 * w + 1) ^ sw) << 2));
+      if (any == 0) {
+        *grp0 = make_uint4(~0u, ~0u, ~0u, ~0u);
+        *grp1 = make_uint4(~0u, ~0u, ~0u, ~0u);
+        continue;
+      }
+      const uint32_t* row = F + (size_t)(i0 + j) * W + w;
+      uint32_t P[NB];
+#pragma unroll
+      for (int b = 0; b < NB; b++) P[b] = 0;
       uint32_t reached = 0;
-      if (i < n) {
-        // Eight levels' words requested at once; within a chunk the low
-        // three bits of the level are the position in the chunk.
-        for (uint32_t L0 = 0; L0 < used; L0 += 8) {
-          uint32_t f[8];
 #pragma unroll
-          for (int q = 0; q < 8; q++) {
-            const uint32_t L = L0 + q;
-            f[q] = L < used && ((wbits[L * bitmap_words + (i >> 5)] >> (i & 31)) & 1)
-                       ? F[L * fstride + (size_t)i * W + w]
-                       : 0u;
+      for (uint32_t c = 0; c < LC; c++) {
+        uint32_t m = lm[c];
+        while (m) {
+          uint32_t Ls[4], f[4];
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            Ls[u] = 0;
+            f[u] = 0;
+            if (m) {
+              Ls[u] = 32 * c + __ffs(m) - 1;
+              m &= m - 1;
+              f[u] = __ldg(row + (size_t)Ls[u] * fstride);
+            }
           }
-          uint32_t chunk = 0;
 #pragma unroll
-          for (int q = 0; q < 8; q++) {
-            chunk |= f[q];
+          for (int u = 0; u < 4; u++) {
+            reached |= f[u];
 #pragma unroll
-            for (int b = 0; b < 3 && b < NB; b++)
-              if ((q >> b) & 1) plane[b] |= f[q];
+            for (int b = 0; b < NB; b++)
+              if ((Ls[u] >> b) & 1u) P[b] |= f[u];
           }
-          reached |= chunk;
-#pragma unroll
-          for (int b = 3; b < NB; b++)
-            if ((L0 >> b) & 1) plane[b] |= chunk;
         }
       }
-      if (w == 0) degs[j] = i < n ? __ldg(off + i + 1) - __ldg(off + i) : 0u;
-      // Source 32w + b's byte for node j: row 32w + b of the tile, which
-      // starts at word (32w + b)·8 + w.
-      uint8_t* col = tbytes + ((size_t)(32 * w) * 8 + w) * 4 + j;
+      const uint32_t U = ~reached;
 #pragma unroll
-      for (int g = 0; g < 8; g++) {
-        uint32_t word = 0xFFFFFFFFu;
-        if (reached) {
-          word = spread4((~reached >> (4 * g)) & 0xFu) * 0xFFu;
+      for (int b = 0; b < NB; b++) P[b] |= U;
+      // lo[g], hi[g]: byte b is plane b's byte g (planes NB..7 are U).
+      uint32_t lo[4] = {P[0], P[1], P[2], P[3]}, hi[4];
+      byte_transpose4(lo[0], lo[1], lo[2], lo[3]);
+      if constexpr (NB == 5) {
 #pragma unroll
-          for (int b = 0; b < NB; b++) word |= spread4((plane[b] >> (4 * g)) & 0xFu) << b;
-        }
-#pragma unroll
-        for (int r = 0; r < 4; r++) col[(4 * g + r) * 32] = (uint8_t)(word >> (8 * r));
+        for (uint32_t g = 0; g < 4; g++)
+          hi[g] = __byte_perm(P[4], U, g | (4 + g) << 4 | (4 + g) << 8 | (4 + g) << 12);
+      } else {
+        hi[0] = P[4];
+        hi[1] = P[5];
+        hi[2] = P[6];
+        hi[3] = P[7];
+        byte_transpose4(hi[0], hi[1], hi[2], hi[3]);
       }
+#pragma unroll
+      for (int g = 0; g < 4; g++) bit_transpose8(lo[g], hi[g]);
+      // Sources 32w + 8g .. +3 are lo[g], +4 .. +7 hi[g]: the word's 16-byte
+      // groups are 2w and 2w + 1.
+      *grp0 = make_uint4(lo[0], hi[0], lo[1], hi[1]);
+      *grp1 = make_uint4(lo[2], hi[2], lo[3], hi[3]);
     }
     __syncthreads();
-    for (uint32_t x = threadIdx.x; x < S * 8; x += blockDim.x) {
-      const uint32_t s = x >> 3, q = x & 7;
-      const uint32_t word = tile[s * 8 + (s >> 5) + q];
-      const uint32_t below = __vcmpltu4(word, cap4s[s]);
-      uint32_t part = 0;
+    for (uint32_t y = threadIdx.x; y < Q * 8; y += blockDim.x) {
+      const uint32_t g = y >> 3, q = y & 7;  // source quad, node quad
+      const uint32_t col = (((g >> 2) ^ (q & (G - 1))) << 2) | (g & 3);
+      uint32_t o[4];
 #pragma unroll
-      for (int r = 0; r < 4; r++)
-        if ((below >> (8 * r)) & 1) part += degs[4 * q + r];
-      part += __shfl_xor_sync(0xffffffffu, part, 1);
-      part += __shfl_xor_sync(0xffffffffu, part, 2);
-      part += __shfl_xor_sync(0xffffffffu, part, 4);
-      if (s < k) {
-        if (q == 0) esum[s] += part;
-        const uint32_t node = i0 + 4 * q;
-        uint8_t* dst = depth_out + (size_t)s * n + node;
-        if (aligned && node + 4 <= n) {
-          *reinterpret_cast<uint32_t*>(dst) = word;
+      for (uint32_t r = 0; r < 4; r++) o[r] = tile[(4 * q + r) * Q + col];
+      byte_transpose4(o[0], o[1], o[2], o[3]);  // o[t]: source 4g + t at nodes 4q .. 4q + 3
+      const uint4 d = *reinterpret_cast<const uint4*>(degs + 4 * q);
+      const uint4 c4 = *reinterpret_cast<const uint4*>(cap4s + 4 * g);
+      const uint32_t cap[4] = {c4.x, c4.y, c4.z, c4.w};
+      // The degrees' low two bytes as byte planes; a node of degree 2^16 or
+      // more takes the plain sum.
+      const bool wide = ((d.x | d.y | d.z | d.w) >> 16) != 0;
+      const uint32_t b0 = __byte_perm(__byte_perm(d.x, d.y, 0x0040), __byte_perm(d.z, d.w, 0x0040), 0x5410);
+      const uint32_t b1 = __byte_perm(__byte_perm(d.x, d.y, 0x0051), __byte_perm(d.z, d.w, 0x0051), 0x5410);
+      uint32_t part[4];
+#pragma unroll
+      for (int s = 0; s < 4; s++) {
+        uint32_t lt;
+        if constexpr (NB == 5) {
+          // Depths are at most 31 or 255 and caps at most 127: (0x80 | depth)
+          // - cap cannot borrow, and its bit 7 is set where depth >= cap.
+          lt = (~((o[s] | 0x80808080u) - cap[s]) & 0x80808080u) >> 7;
         } else {
-          for (uint32_t r = 0; r < 4 && node + r < n; r++) dst[r] = (uint8_t)(word >> (8 * r));
+          lt = bytes_below(o[s], cap[s]);
+        }
+        if (!wide)
+          part[s] = __dp4a(lt, b0, 0u) + (__dp4a(lt, b1, 0u) << 8);
+        else
+          part[s] = (lt & 1u ? d.x : 0u) + ((lt >> 8) & 1u ? d.y : 0u) +
+                    ((lt >> 16) & 1u ? d.z : 0u) + ((lt >> 24) & 1u ? d.w : 0u);
+      }
+      // Sum over the eight lanes of the source quad: after the exchanges a
+      // lane holds source 4g + 2·(lane bit 0) + (lane bit 1).
+      const bool b0l = lane & 1u, b1l = lane & 2u;
+      uint32_t v0 = b0l ? part[2] : part[0], v1 = b0l ? part[3] : part[1];
+      v0 += __shfl_xor_sync(0xffffffffu, b0l ? part[0] : part[2], 1);
+      v1 += __shfl_xor_sync(0xffffffffu, b0l ? part[1] : part[3], 1);
+      uint32_t sum = b1l ? v1 : v0;
+      sum += __shfl_xor_sync(0xffffffffu, b1l ? v0 : v1, 2);
+      sum += __shfl_xor_sync(0xffffffffu, sum, 4);
+      const uint32_t mine = 4 * g + 2 * (lane & 1u) + ((lane >> 1) & 1u);
+      if ((lane & 4u) == 0 && mine < k) esum[mine] += sum;
+      const uint32_t node = i0 + 4 * q;
+      const bool whole = aligned && node + 4 <= n;
+      uint8_t* dst = depth_out + (size_t)(4 * g) * n + node;
+#pragma unroll
+      for (uint32_t s = 0; s < 4; s++, dst += n) {
+        if (4 * g + s >= k) break;
+        if (whole) {
+          *reinterpret_cast<uint32_t*>(dst) = o[s];
+        } else {
+          for (uint32_t r = 0; r < 4 && node + r < n; r++) dst[r] = (uint8_t)(o[s] >> (8 * r));
         }
       }
     }
