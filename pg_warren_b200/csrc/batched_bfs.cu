@@ -188,9 +188,28 @@ template <int N> __device__ inline bool any_words(const Words<N>& r) {
   return o != 0;
 }
 
+// Requests into L2 the lines a unit reads first — its rows' visited words,
+// its targets and (a tile) its row offsets — so that when the warp reaches
+// the unit those loads hit L2 rather than DRAM.  Every address is inside
+// the unit's own ranges.
+__device__ inline void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+template <int W>
+__device__ inline void prefetch_unit(const MsLevel& P, const Unit& d, unsigned lane) {
+  const bool tile = (d.c >> 31) == 0;
+  const uint32_t r0 = d.a, R = tile ? d.b - d.a : 1;
+  const uint32_t e0 = tile ? d.d : d.b, cnt = tile ? d.c : d.d - d.b;
+  if (lane < R) prefetch_l2(P.V + (size_t)(r0 + lane) * W);
+  if (32 * lane < cnt) prefetch_l2(P.tgt + e0 + 32 * lane);
+  if (tile && lane == 31) prefetch_l2(P.off + r0);
+}
+
 // The pull of one level.  A row's W words are spread over LPR = W/VEC
 // lanes holding VEC words each (one 16-byte access for W >= 4), so a warp
-// instruction covers G = 32/LPR rows or gathered frontier rows.
+// instruction covers G = 32/LPR rows or gathered frontier rows.  While a
+// unit runs, the warp's next unit is prefetched into L2 (its descriptor
+// was loaded one unit earlier, so the prefetch does not wait on it).
 template <int W>
 __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
   if (P.counts[P.L] == 0) return;  // nothing expands: F_{L+1} is not read
@@ -223,8 +242,14 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
   unsigned long long fed = 0;  // out-edges of the rows admitted
   V4 live = {};                // this warp's fresh bits, for the next level's live set
 
+  Unit nxt{};
+  if (warp + warps < P.unit_count) nxt = P.units[warp + warps];
   for (uint32_t u = warp; u < P.unit_count; u += warps) {
-    const Unit unit = P.units[u];
+    const Unit unit = P.units[u];  // loaded a unit earlier as `nxt`: a cache hit
+    if (u + warps < P.unit_count) {
+      prefetch_unit<W>(P, nxt, lane);
+      if (u + 2 * warps < P.unit_count) nxt = P.units[u + 2 * warps];
+    }
     const bool tile = (unit.c >> 31) == 0;
     const uint32_t r0 = unit.a;
     const uint32_t R = tile ? unit.b - unit.a : 1;
@@ -622,6 +647,22 @@ __device__ inline uint32_t bytes_below(uint32_t a, uint32_t b) {
   return (((~a & b) | (~(a ^ b) & ~x)) & 0x80808080u) >> 7;
 }
 
+// Item x's node's written levels: bit L set where level L's word of the
+// tile (held by lane L as `word`) has the node's bit.  One ballot per node
+// the warp covers (32 / W of them); every lane of the warp must call it.
+template <int W>
+__device__ inline uint32_t written_levels(uint32_t word, uint32_t x, uint32_t lane, bool valid) {
+  constexpr uint32_t NPW = 32 / W;
+  const uint32_t jbase = (x - lane) / W;  // the warp's first node
+  uint32_t lm = 0;
+#pragma unroll
+  for (uint32_t jj = 0; jj < NPW; jj++) {
+    const uint32_t bal = __ballot_sync(0xffffffffu, (word >> (jbase + jj)) & 1u);
+    if (lane / W == jj) lm = bal;
+  }
+  return valid ? lm : 0u;
+}
+
 template <int W, int NB>
 __global__ void __launch_bounds__(256)
     msbfs_depth_kernel(uint32_t n, uint32_t k, uint32_t levels, const uint32_t* F, uint64_t fstride,
@@ -631,7 +672,7 @@ __global__ void __launch_bounds__(256)
   constexpr uint32_t S = 32 * W;            // sources in the pass (k <= S)
   constexpr uint32_t Q = 8 * W;             // four-source words in a node row of the tile
   constexpr uint32_t G = 2 * W;             // 16-byte groups in a node row
-  constexpr uint32_t NPW = 32 / W;          // nodes a warp's lanes cover at once
+  constexpr uint32_t IT = (32 * W + 255) / 256;  // phase-1 items a thread takes (blocks of 256)
   constexpr uint32_t LC = NB == 5 ? 1 : 8;  // 32-level chunks of the written levels
   __shared__ __align__(16) uint32_t tile[32 * Q];
   __shared__ __align__(16) uint32_t cap4s[S];
@@ -664,20 +705,40 @@ __global__ void __launch_bounds__(256)
       const uint32_t i = i0 + threadIdx.x;
       degs[threadIdx.x] = i < n ? __ldg(off + i + 1) - __ldg(off + i) : 0u;
     }
-    for (uint32_t x = threadIdx.x; x < 32 * W; x += blockDim.x) {
+    // Phase 1a: every item's written levels 0..31 and the loads of its
+    // first four, all in flight before any item is folded.
+    uint32_t lm0[IT], fv[IT][4];
+#pragma unroll
+    for (uint32_t it = 0; it < IT; it++) {
+      const uint32_t x = threadIdx.x + 256 * it;
+      lm0[it] = 0;
+#pragma unroll
+      for (int u = 0; u < 4; u++) fv[it][u] = 0;
+      if (x < 32 * W) {
+        const uint32_t j = x / W, w = x % W;
+        lm0[it] = written_levels<W>(wl[0], x, lane, i0 + j < n);
+        const uint32_t* row = F + (size_t)(i0 + j) * W + w;
+        uint32_t m = lm0[it];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          if (m) {
+            fv[it][u] = __ldg(row + (size_t)(__ffs(m) - 1) * fstride);
+            m &= m - 1;
+          }
+      }
+    }
+    // Phase 1b: fold each item's levels into planes and bytes.
+#pragma unroll
+    for (uint32_t it = 0; it < IT; it++) {
+      const uint32_t x = threadIdx.x + 256 * it;
+      if (x >= 32 * W) break;
       const uint32_t j = x / W, w = x % W;
-      const uint32_t jbase = (x - lane) / W;  // the warp's first node
       uint32_t lm[LC];
-      uint32_t any = 0;
+      lm[0] = lm0[it];
+      uint32_t any = lm[0];
 #pragma unroll
-      for (uint32_t c = 0; c < LC; c++) {
-        lm[c] = 0;
-#pragma unroll
-        for (uint32_t jj = 0; jj < NPW; jj++) {
-          const uint32_t bal = __ballot_sync(0xffffffffu, (wl[c] >> (jbase + jj)) & 1u);
-          if (lane / W == jj) lm[c] = bal;
-        }
-        if (i0 + j >= n) lm[c] = 0;
+      for (uint32_t c = 1; c < LC; c++) {
+        lm[c] = written_levels<W>(wl[c], x, lane, i0 + j < n);
         any |= lm[c];
       }
       uint32_t* trow = tile + j * Q;
@@ -694,6 +755,21 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
       for (int b = 0; b < NB; b++) P[b] = 0;
       uint32_t reached = 0;
+      {
+        // The four levels loaded in phase 1a (a word is 0 past the last).
+        uint32_t m = lm[0];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const uint32_t L = m ? __ffs(m) - 1 : 0u;
+          m &= m - 1;
+          const uint32_t f = fv[it][u];
+          reached |= f;
+#pragma unroll
+          for (int b = 0; b < NB; b++)
+            if ((L >> b) & 1u) P[b] |= f;
+        }
+        lm[0] = m;
+      }
 #pragma unroll
       for (uint32_t c = 0; c < LC; c++) {
         uint32_t m = lm[c];
