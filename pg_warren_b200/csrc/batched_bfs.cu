@@ -590,24 +590,28 @@ __global__ void __launch_bounds__(256) msbfs_settle_kernel(MsLevel P) {
 
 // Depths from the kept frontiers, source-major, and each source's
 // edges_traversed: Σ out-degree over the nodes it reached at a depth below
-// its cap.  A block takes 32 nodes at a time, all sources of the pass.
+// its cap.  A block of 512 threads takes 64 nodes at a time, all sources of
+// the pass, so that each source's bytes of the tile are one 64-byte run:
+// 32-byte runs spread over a thousand rows 2^22 bytes apart reached a third
+// of the write bandwidth that 64-byte runs do.
 // Phase 1: a thread per (node, word) — the lanes of a warp cover whole node
 // rows, so each level's row is read coalesced (only rows marked written,
-// four levels' loads in flight).  A ballot over the tile's written-row
-// words, a level per lane, gives the node its written levels; a node no
-// source reached stores 255s at once.  Otherwise the node's frontier words
-// fold into NB bit planes of the depth (plane b: the sources that reached
-// it at a level with bit b set) and the unreached set, and an 8×8
-// bit-matrix transpose turns 8 planes × 8 sources into 8 depth bytes
-// (unreached sources have every plane set: 255).  The 32 bytes go to a
-// node-major shared tile as two 16-byte stores, the 16-byte groups of row j
-// XOR-swizzled by j/4.
+// every node's first four levels in flight before any is folded).  A
+// ballot over the tile's written-row words, a level per lane, gives the
+// node its written levels; a node no source reached stores 255s at once.
+// Otherwise the node's frontier words fold into NB bit planes of the depth
+// (plane b: the sources that reached it at a level with bit b set) and the
+// unreached set, and an 8×8 bit-matrix transpose turns 8 planes × 8 sources
+// into 8 depth bytes (unreached sources have every plane set: 255).  The 32
+// bytes go to a node-major shared tile as two 16-byte stores; word g of
+// node row j sits at g ^ (2·(j/4)), which keeps phase 2's reads free of
+// bank conflicts.
 // Phase 2: a thread per (four sources, four nodes) reads four words of the
 // tile, transposes their bytes so each word is one source's four nodes, and
-// stores it; eight threads cover a source's 32 nodes in one 32-byte sector.
+// stores it; sixteen lanes cover a source's 64 nodes in one 64-byte run.
 // The out-degrees of the nodes whose depth is below the source's cap
 // (bytes compared four at a time, weighted by dp4a) are summed over the
-// eight threads by shuffles into the source's shared sum; the sums go to
+// sixteen lanes by shuffles into the source's shared sum; the sums go to
 // the global counts once per block.
 
 // Rows a0..a3 of a 4×4 byte matrix become its columns: afterwards a_t
@@ -647,37 +651,64 @@ __device__ inline uint32_t bytes_below(uint32_t a, uint32_t b) {
   return (((~a & b) | (~(a ^ b) & ~x)) & 0x80808080u) >> 7;
 }
 
-// Item x's node's written levels: bit L set where level L's word of the
-// tile (held by lane L as `word`) has the node's bit.  One ballot per node
-// the warp covers (32 / W of them); every lane of the warp must call it.
+// Item x's node's written levels: bit L set where level L's words of the
+// tile (lane L holds the words of the tile's 64 nodes) have the node's bit.
+// One ballot per node the warp covers (32 / W of them); every lane of the
+// warp must call it.
 template <int W>
-__device__ inline uint32_t written_levels(uint32_t word, uint32_t x, uint32_t lane, bool valid) {
+__device__ inline uint32_t written_levels(const uint32_t (&wl)[2], uint32_t x, uint32_t lane,
+                                          bool valid) {
   constexpr uint32_t NPW = 32 / W;
   const uint32_t jbase = (x - lane) / W;  // the warp's first node
   uint32_t lm = 0;
 #pragma unroll
   for (uint32_t jj = 0; jj < NPW; jj++) {
-    const uint32_t bal = __ballot_sync(0xffffffffu, (word >> (jbase + jj)) & 1u);
+    const uint32_t node = jbase + jj;
+    const uint32_t word = node < 32 ? wl[0] : wl[1];
+    const uint32_t bal = __ballot_sync(0xffffffffu, (word >> (node & 31)) & 1u);
     if (lane / W == jj) lm = bal;
   }
   return valid ? lm : 0u;
 }
 
+// Out word p of a 16-byte group takes in word p ^ e (e < 4).
+__device__ inline uint4 permute_words(uint32_t v0, uint32_t v1, uint32_t v2, uint32_t v3, uint32_t e) {
+  if (e & 1u) {
+    const uint32_t t0 = v0, t2 = v2;
+    v0 = v1; v1 = t0; v2 = v3; v3 = t2;
+  }
+  if (e & 2u) {
+    const uint32_t t0 = v0, t1 = v1;
+    v0 = v2; v1 = v3; v2 = t0; v3 = t1;
+  }
+  return make_uint4(v0, v1, v2, v3);
+}
+
+constexpr uint32_t kDepthThreads = 512;
+constexpr uint32_t kDepthNodes = 64;
+
+// The depth kernel's dynamic shared memory: the tile, the caps, the sums
+// and the tile's degrees.
+template <int W> constexpr size_t depth_smem_bytes() {
+  return (size_t)kDepthNodes * 8 * W * 4 + 32 * W * 4 + 32 * W * 8 + kDepthNodes * 4;
+}
+
 template <int W, int NB>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kDepthThreads, 2)
     msbfs_depth_kernel(uint32_t n, uint32_t k, uint32_t levels, const uint32_t* F, uint64_t fstride,
                        const uint32_t* wbits, uint32_t bitmap_words, const uint32_t* caps,
                        const uint32_t* off, const uint32_t* counts, uint8_t* depth_out,
                        unsigned long long* edges) {
   constexpr uint32_t S = 32 * W;            // sources in the pass (k <= S)
+  constexpr uint32_t TN = kDepthNodes;      // nodes of a tile
   constexpr uint32_t Q = 8 * W;             // four-source words in a node row of the tile
-  constexpr uint32_t G = 2 * W;             // 16-byte groups in a node row
-  constexpr uint32_t IT = (32 * W + 255) / 256;  // phase-1 items a thread takes (blocks of 256)
+  constexpr uint32_t IT = (TN * W + kDepthThreads - 1) / kDepthThreads;  // phase-1 items a thread takes
   constexpr uint32_t LC = NB == 5 ? 1 : 8;  // 32-level chunks of the written levels
-  __shared__ __align__(16) uint32_t tile[32 * Q];
-  __shared__ __align__(16) uint32_t cap4s[S];
-  __shared__ unsigned long long esum[S];
-  __shared__ __align__(16) uint32_t degs[32];
+  extern __shared__ __align__(16) unsigned char depth_smem[];
+  uint32_t* tile = reinterpret_cast<uint32_t*>(depth_smem);                    // [TN][Q]
+  uint32_t* cap4s = tile + TN * Q;                                              // [S]
+  unsigned long long* esum = reinterpret_cast<unsigned long long*>(cap4s + S);  // [S]
+  uint32_t* degs = reinterpret_cast<uint32_t*>(esum + S);                       // [TN]
   const uint32_t lane = threadIdx.x & 31;
   // The snapshots written: F_L exists for L < used (F_L is written only if
   // level L-1 had a frontier to expand).
@@ -691,17 +722,21 @@ __global__ void __launch_bounds__(256)
     cap4s[x] = (x < k ? min(caps[x], NB == 5 ? 127u : 255u) : 0u) * 0x01010101u;
   }
   const bool aligned = (n & 3u) == 0;
-  const uint32_t tiles = (n + 31) / 32;
+  const uint32_t tiles = (n + TN - 1) / TN;
   for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-    const uint32_t i0 = t * 32;
-    // Lane L holds level 32c + L's written-row word of the tile.
-    uint32_t wl[LC];
+    const uint32_t i0 = t * TN;
+    // Lane L holds level 32c + L's written-row words of the tile's nodes.
+    uint32_t wl[LC][2];
 #pragma unroll
     for (uint32_t c = 0; c < LC; c++) {
       const uint32_t L = 32 * c + lane;
-      wl[c] = L < used ? wbits[(size_t)L * bitmap_words + t] : 0u;
+#pragma unroll
+      for (uint32_t b = 0; b < 2; b++) {
+        const uint32_t wi = 2 * t + b;
+        wl[c][b] = L < used && wi < bitmap_words ? wbits[(size_t)L * bitmap_words + wi] : 0u;
+      }
     }
-    if (threadIdx.x < 32) {
+    if (threadIdx.x < TN) {
       const uint32_t i = i0 + threadIdx.x;
       degs[threadIdx.x] = i < n ? __ldg(off + i + 1) - __ldg(off + i) : 0u;
     }
@@ -710,11 +745,11 @@ __global__ void __launch_bounds__(256)
     uint32_t lm0[IT], fv[IT][4];
 #pragma unroll
     for (uint32_t it = 0; it < IT; it++) {
-      const uint32_t x = threadIdx.x + 256 * it;
+      const uint32_t x = threadIdx.x + kDepthThreads * it;
       lm0[it] = 0;
 #pragma unroll
       for (int u = 0; u < 4; u++) fv[it][u] = 0;
-      if (x < 32 * W) {
+      if (x < TN * W) {
         const uint32_t j = x / W, w = x % W;
         lm0[it] = written_levels<W>(wl[0], x, lane, i0 + j < n);
         const uint32_t* row = F + (size_t)(i0 + j) * W + w;
@@ -730,8 +765,8 @@ __global__ void __launch_bounds__(256)
     // Phase 1b: fold each item's levels into planes and bytes.
 #pragma unroll
     for (uint32_t it = 0; it < IT; it++) {
-      const uint32_t x = threadIdx.x + 256 * it;
-      if (x >= 32 * W) break;
+      const uint32_t x = threadIdx.x + kDepthThreads * it;
+      if (x >= TN * W) break;
       const uint32_t j = x / W, w = x % W;
       uint32_t lm[LC];
       lm[0] = lm0[it];
@@ -741,10 +776,12 @@ __global__ void __launch_bounds__(256)
         lm[c] = written_levels<W>(wl[c], x, lane, i0 + j < n);
         any |= lm[c];
       }
+      // Word g of the row sits at g ^ sw: 16-byte group h at h ^ (sw / 4),
+      // its words permuted by sw % 4.
+      const uint32_t sw = (2 * (j >> 2)) & (Q - 1);
       uint32_t* trow = tile + j * Q;
-      const uint32_t sw = (j >> 2) & (G - 1);
-      uint4* grp0 = reinterpret_cast<uint4*>(trow + (((2 * w) ^ sw) << 2));
-      uint4* grp1 = reinterpret_cast<uint4*>(trow + (((2 * w + 1) ^ sw) << 2));
+      uint4* grp0 = reinterpret_cast<uint4*>(trow + (((2 * w) ^ (sw >> 2)) << 2));
+      uint4* grp1 = reinterpret_cast<uint4*>(trow + (((2 * w + 1) ^ (sw >> 2)) << 2));
       if (any == 0) {
         *grp0 = make_uint4(~0u, ~0u, ~0u, ~0u);
         *grp1 = make_uint4(~0u, ~0u, ~0u, ~0u);
@@ -815,13 +852,15 @@ __global__ void __launch_bounds__(256)
       for (int g = 0; g < 4; g++) bit_transpose8(lo[g], hi[g]);
       // Sources 32w + 8g .. +3 are lo[g], +4 .. +7 hi[g]: the word's 16-byte
       // groups are 2w and 2w + 1.
-      *grp0 = make_uint4(lo[0], hi[0], lo[1], hi[1]);
-      *grp1 = make_uint4(lo[2], hi[2], lo[3], hi[3]);
+      *grp0 = permute_words(lo[0], hi[0], lo[1], hi[1], sw & 3u);
+      *grp1 = permute_words(lo[2], hi[2], lo[3], hi[3], sw & 3u);
     }
     __syncthreads();
-    for (uint32_t y = threadIdx.x; y < Q * 8; y += blockDim.x) {
-      const uint32_t g = y >> 3, q = y & 7;  // source quad, node quad
-      const uint32_t col = (((g >> 2) ^ (q & (G - 1))) << 2) | (g & 3);
+    // Phase 2: lanes 16h .. 16h + 15 of a warp take source quad g, lane q
+    // of them nodes 4q .. 4q + 3.
+    for (uint32_t y = threadIdx.x; y < Q * 16; y += blockDim.x) {
+      const uint32_t g = y >> 4, q = y & 15;
+      const uint32_t col = g ^ ((2 * q) & (Q - 1));
       uint32_t o[4];
 #pragma unroll
       for (uint32_t r = 0; r < 4; r++) o[r] = tile[(4 * q + r) * Q + col];
@@ -836,23 +875,23 @@ __global__ void __launch_bounds__(256)
       const uint32_t b1 = __byte_perm(__byte_perm(d.x, d.y, 0x0051), __byte_perm(d.z, d.w, 0x0051), 0x5410);
       uint32_t part[4];
 #pragma unroll
-      for (int s = 0; s < 4; s++) {
+      for (int t4 = 0; t4 < 4; t4++) {
         uint32_t lt;
         if constexpr (NB == 5) {
           // Depths are at most 31 or 255 and caps at most 127: (0x80 | depth)
           // - cap cannot borrow, and its bit 7 is set where depth >= cap.
-          lt = (~((o[s] | 0x80808080u) - cap[s]) & 0x80808080u) >> 7;
+          lt = (~((o[t4] | 0x80808080u) - cap[t4]) & 0x80808080u) >> 7;
         } else {
-          lt = bytes_below(o[s], cap[s]);
+          lt = bytes_below(o[t4], cap[t4]);
         }
         if (!wide)
-          part[s] = __dp4a(lt, b0, 0u) + (__dp4a(lt, b1, 0u) << 8);
+          part[t4] = __dp4a(lt, b0, 0u) + (__dp4a(lt, b1, 0u) << 8);
         else
-          part[s] = (lt & 1u ? d.x : 0u) + ((lt >> 8) & 1u ? d.y : 0u) +
-                    ((lt >> 16) & 1u ? d.z : 0u) + ((lt >> 24) & 1u ? d.w : 0u);
+          part[t4] = (lt & 1u ? d.x : 0u) + ((lt >> 8) & 1u ? d.y : 0u) +
+                     ((lt >> 16) & 1u ? d.z : 0u) + ((lt >> 24) & 1u ? d.w : 0u);
       }
-      // Sum over the eight lanes of the source quad: after the exchanges a
-      // lane holds source 4g + 2·(lane bit 0) + (lane bit 1).
+      // Sum over the sixteen lanes of the source quad: after the first two
+      // exchanges a lane holds source 4g + 2·(lane bit 0) + (lane bit 1).
       const bool b0l = lane & 1u, b1l = lane & 2u;
       uint32_t v0 = b0l ? part[2] : part[0], v1 = b0l ? part[3] : part[1];
       v0 += __shfl_xor_sync(0xffffffffu, b0l ? part[0] : part[2], 1);
@@ -860,18 +899,19 @@ __global__ void __launch_bounds__(256)
       uint32_t sum = b1l ? v1 : v0;
       sum += __shfl_xor_sync(0xffffffffu, b1l ? v0 : v1, 2);
       sum += __shfl_xor_sync(0xffffffffu, sum, 4);
+      sum += __shfl_xor_sync(0xffffffffu, sum, 8);
       const uint32_t mine = 4 * g + 2 * (lane & 1u) + ((lane >> 1) & 1u);
-      if ((lane & 4u) == 0 && mine < k) esum[mine] += sum;
+      if ((lane & 12u) == 0 && mine < k) esum[mine] += sum;
       const uint32_t node = i0 + 4 * q;
       const bool whole = aligned && node + 4 <= n;
       uint8_t* dst = depth_out + (size_t)(4 * g) * n + node;
 #pragma unroll
-      for (uint32_t s = 0; s < 4; s++, dst += n) {
-        if (4 * g + s >= k) break;
+      for (uint32_t t4 = 0; t4 < 4; t4++, dst += n) {
+        if (4 * g + t4 >= k) break;
         if (whole) {
-          *reinterpret_cast<uint32_t*>(dst) = o[s];
+          *reinterpret_cast<uint32_t*>(dst) = o[t4];
         } else {
-          for (uint32_t r = 0; r < 4 && node + r < n; r++) dst[r] = (uint8_t)(o[s] >> (8 * r));
+          for (uint32_t r = 0; r < 4 && node + r < n; r++) dst[r] = (uint8_t)(o[t4] >> (8 * r));
         }
       }
     }
@@ -1012,18 +1052,24 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
       return WC_INVALID_ARGUMENT;
     }
   }
-  // Depths: persistent blocks of 32-node tiles.
-  const uint32_t depth_grid = max_blocks(4);
+  // Depths: persistent blocks of 64-node tiles, two blocks an SM.
+  const uint32_t depth_grid = max_blocks(2);
+  constexpr size_t depth_smem = depth_smem_bytes<W>();
   ctx.phase_begin("depth");
   // Depths fit five bit planes up to level 31.
-  if (levels + 1 <= 32)
-    note_launch(), msbfs_depth_kernel<W, 5><<<depth_grid, 256, 0, st>>>(
+  if (levels + 1 <= 32) {
+    WC_CUDA(cudaFuncSetAttribute(msbfs_depth_kernel<W, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)depth_smem), ctx.detail);
+    note_launch(), msbfs_depth_kernel<W, 5><<<depth_grid, kDepthThreads, depth_smem, st>>>(
         n, k, levels + 1, F, fstride, wbits, (uint32_t)bitmap_words, caps_dev,
         v->fwd.offsets.as<uint32_t>(), counts, depth_dev, edges_dev);
-  else
-    note_launch(), msbfs_depth_kernel<W, 8><<<depth_grid, 256, 0, st>>>(
+  } else {
+    WC_CUDA(cudaFuncSetAttribute(msbfs_depth_kernel<W, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)depth_smem), ctx.detail);
+    note_launch(), msbfs_depth_kernel<W, 8><<<depth_grid, kDepthThreads, depth_smem, st>>>(
         n, k, levels + 1, F, fstride, wbits, (uint32_t)bitmap_words, caps_dev,
         v->fwd.offsets.as<uint32_t>(), counts, depth_dev, edges_dev);
+  }
   ctx.phase_end();
   return cuda_status(cudaGetLastError(), ctx.detail, "batched bfs pass");
 }
