@@ -606,13 +606,13 @@ __global__ void __launch_bounds__(256) msbfs_settle_kernel(MsLevel P) {
 // bytes go to a node-major shared tile as two 16-byte stores; word g of
 // node row j sits at g ^ (2·(j/4)), which keeps phase 2's reads free of
 // bank conflicts.
-// Phase 2: a thread per (four sources, eight nodes) reads eight words of the
-// tile, transposes the bytes of each four so a word is one source's four
-// nodes, and stores each source's eight bytes; eight lanes cover a source's
-// 64 nodes in one 64-byte run.  The out-degrees of the nodes whose depth is
-// below the source's cap (bytes compared four at a time, weighted by dp4a)
-// are summed over the eight lanes by shuffles into the source's shared sum;
-// the sums go to the global counts once per block.
+// Phase 2: a thread per (four sources, sixteen nodes) reads sixteen words of
+// the tile, transposes the bytes of each four so a word is one source's
+// four nodes, and stores each source's sixteen bytes; four lanes cover a
+// source's 64 nodes in one 64-byte run.  The out-degrees of the nodes whose
+// depth is below the source's cap (bytes compared four at a time, weighted
+// by dp4a) are summed over the four lanes by shuffles into the source's
+// shared sum; the sums go to the global counts once per block.
 
 // Rows a0..a3 of a 4×4 byte matrix become its columns: afterwards a_t
 // holds [a0.t, a1.t, a2.t, a3.t] of the inputs.
@@ -856,17 +856,17 @@ __global__ void __launch_bounds__(kDepthThreads, 2)
       *grp1 = permute_words(lo[2], hi[2], lo[3], hi[3], sw & 3u);
     }
     __syncthreads();
-    // Phase 2: lanes 8h .. 8h + 7 of a warp take source quad g, lane p of
-    // them nodes 8p .. 8p + 7 (node quads 2p and 2p + 1).
-    for (uint32_t y = threadIdx.x; y < Q * 8; y += blockDim.x) {
-      const uint32_t g = y >> 3, p = y & 7;
+    // Phase 2: lanes 4h .. 4h + 3 of a warp take source quad g, lane p of
+    // them nodes 16p .. 16p + 15 (node quads 4p .. 4p + 3).
+    for (uint32_t y = threadIdx.x; y < Q * 4; y += blockDim.x) {
+      const uint32_t g = y >> 2, p = y & 3;
       const uint4 c4 = *reinterpret_cast<const uint4*>(cap4s + 4 * g);
       const uint32_t cap[4] = {c4.x, c4.y, c4.z, c4.w};
-      uint32_t o[2][4];  // [node quad][source]
+      uint32_t o[4][4];  // [node quad][source]
       uint32_t part[4] = {0, 0, 0, 0};
 #pragma unroll
-      for (uint32_t h = 0; h < 2; h++) {
-        const uint32_t q = 2 * p + h;
+      for (uint32_t h = 0; h < 4; h++) {
+        const uint32_t q = 4 * p + h;
         const uint32_t col = g ^ ((2 * q) & (Q - 1));
 #pragma unroll
         for (uint32_t r = 0; r < 4; r++) o[h][r] = tile[(4 * q + r) * Q + col];
@@ -896,27 +896,26 @@ __global__ void __launch_bounds__(kDepthThreads, 2)
                         ((lt >> 16) & 1u ? d.z : 0u) + ((lt >> 24) & 1u ? d.w : 0u);
         }
       }
-      // Sum over the eight lanes of the source quad: after the first two
-      // exchanges a lane holds source 4g + 2·(lane bit 0) + (lane bit 1).
+      // Sum over the four lanes of the source quad: afterwards a lane holds
+      // source 4g + 2·(lane bit 0) + (lane bit 1).
       const bool b0l = lane & 1u, b1l = lane & 2u;
       uint32_t v0 = b0l ? part[2] : part[0], v1 = b0l ? part[3] : part[1];
       v0 += __shfl_xor_sync(0xffffffffu, b0l ? part[0] : part[2], 1);
       v1 += __shfl_xor_sync(0xffffffffu, b0l ? part[1] : part[3], 1);
       uint32_t sum = b1l ? v1 : v0;
       sum += __shfl_xor_sync(0xffffffffu, b1l ? v0 : v1, 2);
-      sum += __shfl_xor_sync(0xffffffffu, sum, 4);
       const uint32_t mine = 4 * g + 2 * (lane & 1u) + ((lane >> 1) & 1u);
-      if ((lane & 4u) == 0 && mine < k) esum[mine] += sum;
-      const uint32_t node = i0 + 8 * p;
-      const bool whole = (n & 7u) == 0 && node + 8 <= n;
+      if (mine < k) esum[mine] += sum;
+      const uint32_t node = i0 + 16 * p;
+      const bool whole = (n & 15u) == 0 && node + 16 <= n;
       uint8_t* dst = depth_out + (size_t)(4 * g) * n + node;
 #pragma unroll
       for (uint32_t t4 = 0; t4 < 4; t4++, dst += n) {
         if (4 * g + t4 >= k) break;
         if (whole) {
-          *reinterpret_cast<uint2*>(dst) = make_uint2(o[0][t4], o[1][t4]);
+          *reinterpret_cast<uint4*>(dst) = make_uint4(o[0][t4], o[1][t4], o[2][t4], o[3][t4]);
         } else {
-          for (uint32_t h = 0; h < 2; h++) {
+          for (uint32_t h = 0; h < 4; h++) {
             const uint32_t nq = node + 4 * h;
             if (aligned && nq + 4 <= n)
               *reinterpret_cast<uint32_t*>(dst + 4 * h) = o[h][t4];
