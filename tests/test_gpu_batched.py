@@ -29,6 +29,45 @@ def test_bfs_batched_equals_per_source_bfs(width):
     assert np.array_equal(e, eo)
 
 
+def ragged_graph(n, seed):
+    """n nodes (not a multiple of 4): a path 1 -> 2 -> ... -> 70 -> 0 that
+    nothing else enters (depths past 31), a hub 0 with an edge to every node
+    from 71 on (out-degree above 2^16) and 0 to 3 random edges from each of
+    those nodes to the others or the hub; targets sorted and distinct per
+    row."""
+    rng = np.random.default_rng(seed)
+    rows = [np.arange(71, n)]
+    rows += [np.array([u + 1]) for u in range(1, 70)]
+    rows.append(np.array([0]))
+    for u in range(71, n):
+        t = rng.integers(70, n, rng.integers(0, 4))
+        t[t == 70] = 0
+        rows.append(np.unique(t[t != u]))
+    offsets = np.zeros(n + 1, np.uint32)
+    offsets[1:] = np.cumsum([len(r) for r in rows])
+    targets = np.concatenate(rows).astype(np.uint32)
+    og = O.Graph.from_csr(n, offsets, targets, reverse=False)
+    return og, W.GraphVersion(offsets, targets)
+
+
+@pytest.mark.parametrize("width,cap_hi", [(37, 17), (37, 201), (1030, 201)])
+def test_bfs_batched_ragged_sizes_deep_caps_and_a_wide_hub(width, cap_hi):
+    # Node count not a multiple of 4 (partial tiles, byte stores), source
+    # counts not a multiple of 4, caps above 31 (eight depth bit planes) and
+    # a node of out-degree above 2^16 (the plain degree sum).
+    n = 70_003
+    og, gv = ragged_graph(n, seed=width + cap_hi)
+    rng = np.random.default_rng(cap_hi)
+    src = rng.integers(0, n, width).astype(np.uint64)
+    src[:3] = [0, 1, 5]
+    caps = rng.integers(0, cap_hi, width).astype(np.uint32)
+    caps[:3] = cap_hi - 1
+    d, e = W.bfs_batched(gv, src, caps)
+    do, eo = O.bfs_depths(og, src, caps)
+    assert np.array_equal(d, do)
+    assert np.array_equal(e, eo)
+
+
 def test_bfs_batched_autotuned_schedules_agree():
     g, og, gv = graph(15)
     rng = np.random.default_rng(3)
