@@ -211,7 +211,7 @@ __device__ inline void prefetch_unit(const MsLevel& P, const Unit& d, unsigned l
 // unit runs, the warp's next unit is prefetched into L2 (its descriptor
 // was loaded one unit earlier, so the prefetch does not wait on it).
 template <int W>
-__global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
+__global__ void __launch_bounds__(256, 4) msbfs_level_kernel(MsLevel P) {
   if (P.counts[P.L] == 0) return;  // nothing expands: F_{L+1} is not read
   if (level_pushes(P)) return;     // msbfs_push_kernel and msbfs_settle_kernel run it
   constexpr uint32_t VEC = W >= 4 ? 4 : W;
@@ -235,7 +235,9 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
 #pragma unroll
     for (int i = 0; i < (int)VEC; i++) a.x[i] &= alive.x[i];
   }
-  const V4 a_next = load_words<VEC>(P.masks + (P.L + 1) * W + w0);
+  // The next level's searching sources are read where a row is written
+  // (an L1 hit), not kept in registers across the gathers.
+  const uint32_t* a_next_p = P.masks + (P.L + 1) * W + w0;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   uint32_t admitted = 0;
@@ -346,14 +348,11 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
       V4 run = {};
       for (uint32_t h0 = h_lo; h0 < h_hi; h0 += U) {
         V4 val[U];
-        uint32_t rr[U];
 #pragma unroll
         for (int x = 0; x < U; x++) {
           const uint32_t h = h0 + x;
-          rr[x] = cur;
           if (h < h_hi) {
             val[x] = ldg_words<VEC>(P.Fcur + (size_t)sm.hitj[h] * W + w0);
-            rr[x] = sm.hitr[h];
           } else {
 #pragma unroll
             for (int i = 0; i < (int)VEC; i++) val[x].x[i] = 0;
@@ -361,13 +360,15 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
         }
 #pragma unroll
         for (int x = 0; x < U; x++) {
-          if (rr[x] != cur) {
+          // The hit's row, read again here rather than held through the loads.
+          const uint32_t rrx = h0 + x < h_hi ? sm.hitr[h0 + x] : cur;
+          if (rrx != cur) {
 #pragma unroll
             for (int i = 0; i < (int)VEC; i++)
               if (run.x[i] & a.x[i]) atomicOr(&sm.acc[cur * W + w0 + i], run.x[i] & a.x[i]);
 #pragma unroll
             for (int i = 0; i < (int)VEC; i++) run.x[i] = 0;
-            cur = rr[x];
+            cur = rrx;
           }
 #pragma unroll
           for (int i = 0; i < (int)VEC; i++) run.x[i] |= val[x].x[i];
@@ -404,6 +405,7 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
           if (q == 0) atomicOr(P.wbits_next + ((r0 + r) >> 5), 1u << ((r0 + r) & 31));
         }
         bool ex = false;
+        const V4 a_next = load_words<VEC>(a_next_p);
 #pragma unroll
         for (int i = 0; i < (int)VEC; i++) {
           live.x[i] |= fresh.x[i];
@@ -461,6 +463,7 @@ __global__ void __launch_bounds__(256, 3) msbfs_level_kernel(MsLevel P) {
           if (lane == 0) atomicOr(P.wbits_next + (row >> 5), 1u << (row & 31));
         }
         bool ex = false;
+        const V4 a_next = load_words<VEC>(a_next_p);
 #pragma unroll
         for (int i = 0; i < (int)VEC; i++) {
           live.x[i] |= fresh.x[i];
