@@ -194,8 +194,11 @@ struct PrEpi {
   }
 };
 
+// Unweighted, four blocks an SM (64 registers) keep more gathers in flight;
+// with weights the extra registers would spill, so three.
 template <class W>
-__global__ void __launch_bounds__(kPullThreads, 3) pr_iter_kernel(CsrView<W> A, PrState s, uint32_t it) {
+__global__ void __launch_bounds__(kPullThreads, WSize<W>::v == 0 ? 4 : 3)
+    pr_iter_kernel(CsrView<W> A, PrState s, uint32_t it) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (*(volatile int32_t*)s.done) return;
   const int cur = it & 1;
