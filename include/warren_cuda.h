@@ -3,8 +3,8 @@
  * whole-graph compute path.
  *
  * pg_warren names a kernel seam between its SQL adapters and whatever runs a
- * kernel (the `Kernels` trait of the reference's DESIGN.md:1208-1243, today
- * the free functions of warren-core).  Every entry point below replaces one
+ * kernel (the `Kernels` trait that the reference's top-level design document
+ * proposes, its lines 1208-1243; today the free functions of warren-core).  Every entry point below replaces one
  * of those functions for one dense-id graph version; the comment on each
  * names the reference function (path within the reference project, file:line)
  * whose arguments, results and errors it keeps.
@@ -160,8 +160,9 @@ uint64_t wc_budget_peak(const wc_budget* budget);
  * units done.  `total` is UINT64_MAX when unknown. */
 typedef void (*wc_progress_fn)(void* context, const char* phase, uint64_t done, uint64_t total);
 
-/* What a call is given besides its operands: the seam's `Call`
- * (DESIGN.md:1213-1220) plus the stream the work goes on. */
+/* What a call is given besides its operands: the seam's `Call` (the
+ * reference's design document, lines 1213-1220) plus the stream the work
+ * goes on. */
 typedef struct wc_call {
     wc_budget* memory;             /* scratch is charged here; NULL: the version's budget */
     volatile const int32_t* cancel; /* non-zero: stop (WC_CANCELLED); may be NULL */
@@ -233,7 +234,8 @@ typedef struct wc_version_info {
 } wc_version_info;
 
 /* Uploads `csr` for (graph_id, version) to the current device: the derived
- * device copy the seam keys by version (DESIGN.md:1240).  Charged to
+ * device copy the seam keys by version (the reference's design document,
+ * line 1240).  Charged to
  * `budget` (which must outlive the handle). */
 wc_status wc_version_upload(uint64_t graph_id, uint64_t version, const wc_csr_host* csr,
                             wc_budget* budget, const wc_call* call, wc_version** out);
@@ -252,7 +254,7 @@ double wc_version_timing(const wc_version* version, const char* phase, uint32_t*
 uint64_t wc_kernel_launches(void);
 
 /* Whether this backend serves `operation` over `dtype` (the seam's
- * `Kernels::serves`, DESIGN.md:1224).  Operations: "spmv", "spmm", "pagerank",
+ * `Kernels::serves`, the reference's design document, line 1224).  Operations: "spmv", "spmm", "pagerank",
  * "bfs", "reachable_set", "eigen", "vector_topk". */
 int32_t wc_serves(const char* operation, wc_dtype dtype);
 
