@@ -606,9 +606,9 @@ __global__ void __launch_bounds__(256) msbfs_settle_kernel(MsLevel P) {
 // (plane b: the sources that reached it at a level with bit b set) and the
 // unreached set, and an 8×8 bit-matrix transpose turns 8 planes × 8 sources
 // into 8 depth bytes (unreached sources have every plane set: 255).  The 32
-// bytes go to a node-major shared tile as two 16-byte stores; word g of
-// node row j sits at g ^ (2·(j/4)), which keeps phase 2's reads free of
-// bank conflicts.
+// bytes go to a node-major shared tile as two 16-byte stores; 16-byte group
+// h of node row j sits at h ^ (2·(j/16)), which keeps phase 2's reads free
+// of bank conflicts.
 // Phase 2: a thread per (four sources, sixteen nodes) reads sixteen words of
 // the tile, transposes the bytes of each four so a word is one source's
 // four nodes, and stores each source's sixteen bytes; four lanes cover a
@@ -672,19 +672,6 @@ __device__ inline uint32_t written_levels(const uint32_t (&wl)[2], uint32_t x, u
     if (lane / W == jj) lm = bal;
   }
   return valid ? lm : 0u;
-}
-
-// Out word p of a 16-byte group takes in word p ^ e (e < 4).
-__device__ inline uint4 permute_words(uint32_t v0, uint32_t v1, uint32_t v2, uint32_t v3, uint32_t e) {
-  if (e & 1u) {
-    const uint32_t t0 = v0, t2 = v2;
-    v0 = v1; v1 = t0; v2 = v3; v3 = t2;
-  }
-  if (e & 2u) {
-    const uint32_t t0 = v0, t1 = v1;
-    v0 = v2; v1 = v3; v2 = t0; v3 = t1;
-  }
-  return make_uint4(v0, v1, v2, v3);
 }
 
 constexpr uint32_t kDepthThreads = 512;
@@ -779,12 +766,11 @@ __global__ void __launch_bounds__(kDepthThreads, 2)
         lm[c] = written_levels<W>(wl[c], x, lane, i0 + j < n);
         any |= lm[c];
       }
-      // Word g of the row sits at g ^ sw: 16-byte group h at h ^ (sw / 4),
-      // its words permuted by sw % 4.
-      const uint32_t sw = (2 * (j >> 2)) & (Q - 1);
+      // The row's 16-byte group h sits at h ^ sw.
+      const uint32_t sw = (2 * (j >> 4)) & (2 * W - 1);
       uint32_t* trow = tile + j * Q;
-      uint4* grp0 = reinterpret_cast<uint4*>(trow + (((2 * w) ^ (sw >> 2)) << 2));
-      uint4* grp1 = reinterpret_cast<uint4*>(trow + (((2 * w + 1) ^ (sw >> 2)) << 2));
+      uint4* grp0 = reinterpret_cast<uint4*>(trow + (((2 * w) ^ sw) << 2));
+      uint4* grp1 = reinterpret_cast<uint4*>(trow + (((2 * w + 1) ^ sw) << 2));
       if (any == 0) {
         *grp0 = make_uint4(~0u, ~0u, ~0u, ~0u);
         *grp1 = make_uint4(~0u, ~0u, ~0u, ~0u);
@@ -796,11 +782,12 @@ __global__ void __launch_bounds__(kDepthThreads, 2)
       for (int b = 0; b < NB; b++) P[b] = 0;
       uint32_t reached = 0;
       {
-        // The four levels loaded in phase 1a (a word is 0 past the last).
+        // The levels loaded in phase 1a (at most four).
         uint32_t m = lm[0];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-          const uint32_t L = m ? __ffs(m) - 1 : 0u;
+          if (!m) break;
+          const uint32_t L = __ffs(m) - 1;
           m &= m - 1;
           const uint32_t f = fv[it][u];
           reached |= f;
@@ -855,8 +842,8 @@ __global__ void __launch_bounds__(kDepthThreads, 2)
       for (int g = 0; g < 4; g++) bit_transpose8(lo[g], hi[g]);
       // Sources 32w + 8g .. +3 are lo[g], +4 .. +7 hi[g]: the word's 16-byte
       // groups are 2w and 2w + 1.
-      *grp0 = permute_words(lo[0], hi[0], lo[1], hi[1], sw & 3u);
-      *grp1 = permute_words(lo[2], hi[2], lo[3], hi[3], sw & 3u);
+      *grp0 = make_uint4(lo[0], hi[0], lo[1], hi[1]);
+      *grp1 = make_uint4(lo[2], hi[2], lo[3], hi[3]);
     }
     __syncthreads();
     // Phase 2: lanes 4h .. 4h + 3 of a warp take source quad g, lane p of
@@ -870,7 +857,7 @@ __global__ void __launch_bounds__(kDepthThreads, 2)
 #pragma unroll
       for (uint32_t h = 0; h < 4; h++) {
         const uint32_t q = 4 * p + h;
-        const uint32_t col = g ^ ((2 * q) & (Q - 1));
+        const uint32_t col = (((g >> 2) ^ ((2 * p) & (2 * W - 1))) << 2) | (g & 3);
 #pragma unroll
         for (uint32_t r = 0; r < 4; r++) o[h][r] = tile[(4 * q + r) * Q + col];
         // o[h][t]: source 4g + t at nodes 4q .. 4q + 3.
