@@ -636,8 +636,9 @@ def suite(args):
 
 
 # --------------------------------------------------------------- profiler cases
-# `python bench.py --case batched|spmv|ppr --scale S`: one small workload per
-# kernel family, for ncu captures (a few GB on the device at most).
+# `python bench.py --case batched|spmv|ppr|minplus|eigen|adjoint --scale S`: one
+# small workload per kernel family, for ncu captures (a few GB on the device
+# at most).
 
 def profile_case(args):
     import torch
@@ -678,6 +679,66 @@ def profile_case(args):
             seconds = time.perf_counter() - t0
         print(json.dumps({"case": "ppr", "nodes": n, "edges": g.edges, "seconds": seconds,
                           "iterations_max": int(it.max()), "iterations_mean": float(it.float().mean())}))
+    elif args.case == "minplus":
+        # Batched min-plus: 1,024 sources, int32 weights 1..100, caps
+        # U{1..16}, as the suite's C3 leg at a smaller scale; two calls.
+        rng = np.random.default_rng(SEED)
+        wi = rng.integers(1, 101, g.edges).astype(np.float64)
+        gw = W.GraphVersion(g.offsets, g.targets, wi)
+        src = rng.integers(0, n, 1024).astype(np.uint64)
+        caps = rng.integers(1, 17, 1024).astype(np.uint32)
+        d = torch.empty((1024, n), dtype=torch.int64, device="cuda")
+        it = torch.empty(1024, dtype=torch.int32, device="cuda")
+        for _ in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            W.minplus_batched(gw, src, caps, dist_out=d, iterations_out=it)
+            torch.cuda.synchronize()
+            seconds = time.perf_counter() - t0
+        print(json.dumps({"case": "minplus", "nodes": n, "edges": g.edges, "seconds": seconds,
+                          "column_iterations": int(it.sum())}))
+    elif args.case == "eigen":
+        # Lanczos on the largest connected component of the symmetrised
+        # R-MAT: normalised Laplacian, 16 smallest, as the suite's C4
+        # variant at a smaller scale; two calls.
+        from scipy.sparse import csr_matrix
+        from scipy.sparse.csgraph import connected_components
+        gs = W.rmat(args.scale, undirected=True)
+        ns, ms = gs.id_space, gs.edges
+        rows = np.repeat(np.arange(ns), np.diff(gs.offsets).astype(np.int64))
+        a = csr_matrix((np.ones(ms), (rows, gs.targets)), shape=(ns, ns))
+        _, labels = connected_components(a, directed=False)
+        keep = np.where(labels == np.bincount(labels).argmax())[0]
+        sub = a[keep][:, keep].tocsr()
+        sub.sort_indices()
+        gl = W.GraphVersion(sub.indptr.astype(np.uint64), sub.indices.astype(np.uint32))
+        opts = W.EigenOptions(16, which="smallest", operator="normalized_laplacian", tol=1e-10,
+                              max_iter=4000, seed=7)
+        for _ in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            e = W.eigen(gl, opts)
+            torch.cuda.synchronize()
+            seconds = time.perf_counter() - t0
+        print(json.dumps({"case": "eigen", "nodes": int(len(keep)), "entries": int(sub.nnz),
+                          "seconds": seconds, "steps": int(e.iterations)}))
+    elif args.case == "adjoint":
+        # PageRank adjoint: lognormal(0,1) row-normalised weights, 64
+        # losses of 1,000 random targets, as the suite's C5 leg at a smaller
+        # scale; two calls.
+        rng = np.random.default_rng(SEED)
+        gw = W.GraphVersion(g.offsets, g.targets, W.edge_weights(g, "lognormal"))
+        losses = [rng.choice(n, 1000, replace=False) for _ in range(64)]
+        grad = torch.empty((64, g.edges), dtype=torch.float64, device="cuda")
+        for _ in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            _, _, its = W.pagerank_adjoint(gw, losses, W.PageRank(0.85, None, 100),
+                                           adjoint_tol=1e-14, grad_out=grad)
+            torch.cuda.synchronize()
+            seconds = time.perf_counter() - t0
+        print(json.dumps({"case": "adjoint", "nodes": n, "edges": g.edges, "seconds": seconds,
+                          "iterations": [int(i) for i in its]}))
     else:
         # SpMV plus_times (f64, unweighted) over the forward CSR three
         # times, then a PageRank of three iterations.
@@ -700,7 +761,7 @@ def main():
     ap.add_argument("--impl", default="warren")
     ap.add_argument("--suite", default=None,
                     help="comma-separated configurations to measure instead: c1,c2,c3,c4,c5,cent,load")
-    ap.add_argument("--case", default=None, choices=["batched", "spmv", "ppr"],
+    ap.add_argument("--case", default=None, choices=["batched", "spmv", "ppr", "minplus", "eigen", "adjoint"],
                     help="a small workload for profilers instead")
     ap.add_argument("--scale", type=int, default=20)
     args = ap.parse_args()
