@@ -595,8 +595,8 @@ __global__ void __launch_bounds__(256) msbfs_settle_kernel(MsLevel P) {
 // edges_traversed: Σ out-degree over the nodes it reached at a depth below
 // its cap.  A block of 512 threads takes 64 nodes at a time, all sources of
 // the pass, so that each source's bytes of the tile are one 64-byte run:
-// 32-byte runs spread over a thousand rows 2^22 bytes apart reached a third
-// of the write bandwidth that 64-byte runs do.
+// 32-byte runs spread over a thousand rows 2^22 bytes apart reached under
+// half the write bandwidth that 64-byte runs do.
 // Phase 1: a thread per (node, word) — the lanes of a warp cover whole node
 // rows, so each level's row is read coalesced (only rows marked written,
 // every node's first four levels in flight before any is folded).  A
