@@ -711,7 +711,11 @@ __global__ void __launch_bounds__(kDepthThreads, 2)
     // as 127 (the one-subtraction compare of phase 2 needs caps <= 127).
     cap4s[x] = (x < k ? min(caps[x], NB == 5 ? 127u : 255u) : 0u) * 0x01010101u;
   }
-  const bool aligned = (n & 3u) == 0;
+  // Word and 16-byte stores need the rows (and the caller's buffer) to
+  // start on such boundaries; otherwise bytes are stored one at a time.
+  const uintptr_t base = reinterpret_cast<uintptr_t>(depth_out);
+  const bool aligned = (n & 3u) == 0 && (base & 3u) == 0;
+  const bool aligned16 = (n & 15u) == 0 && (base & 15u) == 0;
   const uint32_t tiles = (n + TN - 1) / TN;
   for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
     const uint32_t i0 = t * TN;
@@ -897,7 +901,7 @@ __global__ void __launch_bounds__(kDepthThreads, 2)
       const uint32_t mine = 4 * g + 2 * (lane & 1u) + ((lane >> 1) & 1u);
       if (mine < k) esum[mine] += sum;
       const uint32_t node = i0 + 16 * p;
-      const bool whole = (n & 15u) == 0 && node + 16 <= n;
+      const bool whole = aligned16 && node + 16 <= n;
       uint8_t* dst = depth_out + (size_t)(4 * g) * n + node;
 #pragma unroll
       for (uint32_t t4 = 0; t4 < 4; t4++, dst += n) {
