@@ -146,24 +146,32 @@ def config(n, m, **extra):
     return c
 
 
-def cpu_bfs(offsets, targets, sources, caps, budget_s):
-    """The oracle's per-source push BFS (warren-core's LevelSearch restated)
-    on all host threads, over as many of the sources as fit the budget:
-    (GTEPS, sources run, threads, seconds)."""
+def cpu_bfs(offsets, targets, sources, caps, budget_s, check=None, batched=True):
+    """The oracle (warren-core's traversal restated in C++) on all host
+    threads, over as many of the sources as fit the budget: (GTEPS, sources
+    run, threads, seconds).  `batched`: the reference's own batched shape
+    (compute/centrality/multi_source.rs: 64 sources a word, parallel over
+    the frontier); otherwise one LevelSearch per source, the searches in
+    parallel.  `check(slice, depths, edges)`, if given, is called outside
+    the timed region with each batch's results, to compare them with the
+    GPU's."""
     import oracle as O
     O.build()
     og = O.Graph.from_csr(len(offsets) - 1, offsets, targets, reverse=False)
     threads = int(O.lib().wo_threads())
-    O.bfs_depths(og, sources[:1], caps[:1])  # warm
-    batch = max(1, threads)
+    search = O.bfs_depths_batched64 if batched else O.bfs_depths
+    search(og, sources[:1], caps[:1])  # warm
+    batch = 64 if batched else max(1, threads)
     done, edges, secs = 0, 0, 0.0
     while done < len(sources) and secs < budget_s:
         sl = slice(done, min(len(sources), done + batch))
         t0 = time.perf_counter()
-        _, e = O.bfs_depths(og, sources[sl], caps[sl])
+        d, e = search(og, sources[sl], caps[sl])
         secs += time.perf_counter() - t0
         edges += int(e.sum())
         done = sl.stop
+        if check is not None:
+            check(sl, d, e)
     return edges / secs / 1e9, done, threads, secs
 
 
@@ -175,14 +183,18 @@ def reference_arm(args):
     same 1,024 searches.  Rank 0 only."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    g = make_graph()
-    src, caps = sources_and_caps(g.id_space)
-    per_step = max(2.0, 60.0 / max(1, args.steps + args.warmup))
     import oracle as O
     O.build()
+    # The graph from the oracle's own copy of the generator: this arm maps
+    # no library of the GPU path.
+    g = O.rmat(SCALE, 16, 0.57, 0.19, 0.19, SEED)
+    src, caps = sources_and_caps(g.id_space)
+    per_step = max(2.0, 60.0 / max(1, args.steps + args.warmup))
     og = O.Graph.from_csr(g.id_space, g.offsets, g.targets, reverse=False)
     threads = int(O.lib().wo_threads())
-    batch = max(1, threads)
+    # The reference's own batched shape (multi_source.rs: 64 sources a word,
+    # the frontier's nodes in parallel tasks), the faster of its CPU paths.
+    batch = 64
     pos = 0
 
     def step():
@@ -192,7 +204,7 @@ def reference_arm(args):
             idx = [(pos + q) % WIDTH for q in range(batch)]
             pos = (pos + batch) % WIDTH
             t0 = time.perf_counter()
-            _, e = O.bfs_depths(og, src[idx], caps[idx])
+            _, e = O.bfs_depths_batched64(og, src[idx], caps[idx])
             secs += time.perf_counter() - t0
             edges += int(e.sum())
         return edges, secs
@@ -205,7 +217,8 @@ def reference_arm(args):
         tot_e += e
         tot_s += s
     gteps = tot_e / tot_s / 1e9
-    sample = f"searches from the {WIDTH} sources, {batch} at a time, ≈{per_step:.0f} s per step"
+    sample = (f"searches from the {WIDTH} sources, {batch} at a time (one 64-source word), "
+              f"≈{per_step:.0f} s per step")
     print(json.dumps({
         "metric": METRIC, "impl": "reference", "value": gteps, "unit": "GTEPS",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -911,13 +924,33 @@ def main():
     e2e_value = edges_all * args.steps / e2e_total / 1e9
     assert int(edges_h.sum()) == edges_step, "host and device runs disagree"
 
-    # ---- CPU baseline (rank 0, one GPU only)
-    cpu = None
+    # ---- CPU baseline (rank 0, one GPU only), which also checks parity:
+    # each sampled search's depths and edge count from the oracle against
+    # the same source's row of the device-resident run and of the run with
+    # host buffers, byte for byte.
+    cpu, parity = None, None
     if rank == 0 and world == 1:
-        gt, done, threads, secs = cpu_bfs(g.offsets, g.targets, src, caps, CPU_BUDGET_S)
+        mismatches = []
+
+        def check(sl, d, e):
+            dev_rows = depth_d[sl].cpu().numpy()
+            if not (np.array_equal(d, dev_rows) and np.array_equal(d, depth_h[sl].numpy())
+                    and np.array_equal(e.astype(np.int64), edges_d[sl].cpu().numpy())
+                    and np.array_equal(e.astype(np.int64), edges_h[sl].numpy())):
+                mismatches.append(sl.start)
+
+        gt, done, threads, secs = cpu_bfs(g.offsets, g.targets, src, caps, CPU_BUDGET_S, check)
         cpu = {"value": gt, "unit": "GTEPS", "cores": threads, "kind": "port",
-               "sample": f"{done} of the {WIDTH} searches (push BFS per source, "
-                         f"{threads} threads, {secs:.1f} s)"}
+               "sample": f"{done} of the {WIDTH} searches, 64 a word (the reference's batched "
+                         f"multi_source shape, {threads} threads, {secs:.1f} s)"}
+        pgt, pdone, _, psecs = cpu_bfs(g.offsets, g.targets, src, caps, CPU_BUDGET_S / 2, None,
+                                       batched=False)
+        cpu["per_source"] = {"value": pgt, "unit": "GTEPS", "cores": threads,
+                             "sample": f"{pdone} of the searches, one LevelSearch each, "
+                                       f"{threads} at a time ({psecs:.1f} s)"}
+        parity = {"checked_sources": done, "of": WIDTH, "bit_exact": not mismatches,
+                  "compared": "depth bytes and edges_traversed of each sampled source, "
+                              "device-resident and host-buffer runs, against the oracle"}
 
     line = {
         "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world,
@@ -935,6 +968,7 @@ def main():
                      "level_ms_per_step": level_ms / args.steps,
                      "depth_ms_per_step": depth_ms / args.steps},
         "cpu_baseline": cpu,
+        "parity": parity,
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
         "edges_traversed_per_step": edges_step,

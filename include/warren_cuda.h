@@ -164,7 +164,10 @@ typedef void (*wc_progress_fn)(void* context, const char* phase, uint64_t done, 
  * reference's design document, lines 1213-1220) plus the stream the work
  * goes on. */
 typedef struct wc_call {
-    wc_budget* memory;             /* scratch is charged here; NULL: the version's budget */
+    wc_budget* memory;             /* the call's budget: the working memory it uses is charged
+                                      here for the call's duration (WC_MEMORY_LIMIT past it);
+                                      the device memory itself stays in the version's pool,
+                                      charged to the version's budget.  NULL: none */
     volatile const int32_t* cancel; /* non-zero: stop (WC_CANCELLED); may be NULL */
     wc_progress_fn progress;       /* may be NULL */
     void* progress_context;
@@ -231,6 +234,7 @@ typedef struct wc_version_info {
     int32_t integral_weights;  /* every weight is an integer in int32 range: an int32 copy is kept */
     int32_t device;            /* CUDA ordinal */
     int32_t symmetric;         /* the CSR equals its transpose (values included) */
+    uint64_t scratch_bytes;    /* calls' working memory kept between calls (also charged) */
 } wc_version_info;
 
 /* Uploads `csr` for (graph_id, version) to the current device: the derived
@@ -252,6 +256,21 @@ double wc_version_timing(const wc_version* version, const char* phase, uint32_t*
 /* The number of kernels this library has launched since it was loaded
  * (a diagnostic: the count a benchmark reports for its timed region). */
 uint64_t wc_kernel_launches(void);
+
+/* compute/random.rs:11-25 (uniform) on the device, the generator wc_eigen
+ * draws its start vectors from: out[i] = uniform(seed, stream, i) over the
+ * version's id space, in [-1, 1) (a diagnostic, so that the device values
+ * can be compared with the reference's bit for bit). */
+wc_status wc_random_uniform(wc_version* version, const wc_call* call, uint64_t seed,
+                            uint64_t stream, double* out);
+
+/* Runs, on the current device, one kernel that waits on a shared-memory
+ * barrier nothing completes, through the same bounded wait the kernels'
+ * bulk-copy rings use, with a limit of `limit_us` microseconds (at most
+ * 2 s).  The wait gives up, the kernel records WC_DEVICE_TIMEOUT and
+ * returns, and so does this call: a self-test that a device wait which
+ * runs out ends with a status and leaves the device usable. */
+wc_status wc_selftest_bounded_wait(const wc_call* call, uint32_t limit_us);
 
 /* Whether this backend serves `operation` over `dtype` (the seam's
  * `Kernels::serves`, the reference's design document, line 1224).  Operations: "spmv", "spmm", "pagerank",
@@ -317,8 +336,10 @@ wc_status wc_pagerank(wc_version* version, const wc_call* call, const wc_pageran
  * memory held by another allocator; no cudaMalloc/cudaFree on a latency
  * budget).  Results equal wc_pagerank's.  Seeded (personalised) solves and
  * WC_CALL_TIMING are not offered.  The array is shared by every call on a
- * device: calls are serialised per device and return after their kernels
- * finish, and any other use overlapping one on that device would race.  The
+ * device: calls are serialised per device and return (errors included)
+ * after their kernels finish, and any other use overlapping one on that
+ * device would race.  The progress hook is called before and after the
+ * solve with no lock held, so it may itself call this entry point.  The
  * first call on each device looks the array's address up with that device
  * current; make it before any stream capture on that device. */
 wc_status wc_pagerank_noalloc(wc_version* version, const wc_call* call,
@@ -422,7 +443,11 @@ wc_status wc_schedule_set(wc_version* version, wc_batch_kind kind, uint32_t widt
  * source-major: depth_out[s * id_space + i] = depth of i from sources[s]
  * (255 if not reached within the cap).  Identical to `width` calls of
  * wc_bfs (node, depth).  edges_traversed_out[s] (may be NULL) gets the edges
- * a push-only bfs from that source would scan. */
+ * a push-only bfs from that source would scan.  A byte holds depths up to
+ * 254: caps above 254 are served while every search ends within 254 levels;
+ * a search that still has nodes to expand at depth 254 with a deeper cap
+ * makes the call return WC_UNSUPPORTED (the outputs are then unspecified),
+ * never a short answer. */
 wc_status wc_bfs_batched(wc_version* version, const wc_call* call, const uint64_t* sources,
                          const uint32_t* max_depths, uint32_t width, uint8_t* depth_out,
                          uint64_t* edges_traversed_out);

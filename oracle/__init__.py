@@ -18,6 +18,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SOURCE = os.path.join(HERE, "warren_oracle.cpp")
+# The benchmark graphs' generator (workload synthesis, not the compute path)
+# is compiled into the oracle from the same source as into the CUDA library,
+# so the CPU baseline builds its graph without mapping that library.
+GRAPHGEN = os.path.join(HERE, "..", "pg_warren_b200", "csrc", "graphgen.cpp")
 LIBRARY = os.path.join(HERE, "liboracle.so")
 
 # Status codes shared with include/warren_cuda.h.
@@ -28,7 +32,7 @@ _lib = None
 
 def build(force: bool = False) -> str:
     """Compiles the oracle (g++, -O3, threads) into oracle/liboracle.so."""
-    deps = [SOURCE, os.path.join(HERE, "warren_lanczos.cpp"),
+    deps = [SOURCE, os.path.join(HERE, "warren_lanczos.cpp"), GRAPHGEN,
             os.path.join(HERE, "..", "include", "warren_cuda.h")]
     deps = [d for d in deps if os.path.exists(d)]
     if not force and os.path.exists(LIBRARY):
@@ -100,6 +104,8 @@ def _declare(L):
     L.wo_reachable_set.argtypes = [P, I, P, U64, U32, P, U64, P, P]
     L.wo_bfs_depths.restype = I32
     L.wo_bfs_depths.argtypes = [P, P, P, U32, P, P]
+    L.wo_bfs_depths_batched64.restype = I32
+    L.wo_bfs_depths_batched64.argtypes = [P, P, P, U32, P, P]
     L.wo_sssp_i64.restype = I32
     L.wo_sssp_i64.argtypes = [P, P, P, U32, P, P]
     L.wo_components.restype = I32
@@ -121,6 +127,51 @@ def _declare(L):
         L.wo_eigen.argtypes = [P, I, I, I, I, D, U64, U64, P, P, P, P]
     L.wo_pagerank_adjoint.restype = I32
     L.wo_pagerank_adjoint.argtypes = [P, D, I, D, U32, P, P, U32, D, P, P, P]
+    L.wc_graph_rmat.restype = I32
+    L.wc_graph_rmat.argtypes = [U32, U32, D, D, D, U64, I32, C.POINTER(HostCsr)]
+    L.wc_graph_gnm.restype = I32
+    L.wc_graph_gnm.argtypes = [U64, U64, U64, I32, C.POINTER(HostCsr)]
+    L.wc_host_csr_free.argtypes = [C.POINTER(HostCsr)]
+
+
+class HostCsr(C.Structure):
+    """wc_host_csr (include/warren_cuda.h): a generated graph's CSR."""
+
+    _fields_ = [("id_space", U64), ("edges", U64), ("offsets", C.POINTER(U64)),
+                ("targets", C.POINTER(U32)), ("external_ids", C.POINTER(C.c_int64))]
+
+
+class SyntheticGraph:
+    """A generated graph's CSR arrays (offsets u64, targets u32)."""
+
+    def __init__(self, offsets, targets):
+        self.offsets = offsets
+        self.targets = targets
+        self.id_space = len(offsets) - 1
+        self.edges = len(targets)
+
+
+def _take(csr):
+    n, m = csr.id_space, csr.edges
+    off = np.ctypeslib.as_array(csr.offsets, shape=(n + 1,)).copy()
+    tgt = np.ctypeslib.as_array(csr.targets, shape=(max(m, 1),))[:m].copy()
+    lib().wc_host_csr_free(C.byref(csr))
+    return SyntheticGraph(off, tgt)
+
+
+def rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1, undirected=False):
+    """The benchmark's seeded R-MAT graph (the generator the CUDA library
+    also exports, compiled here from the same source)."""
+    csr = HostCsr()
+    _check(lib().wc_graph_rmat(scale, edge_factor, a, b, c, seed, int(undirected), C.byref(csr)))
+    return _take(csr)
+
+
+def gnm(n, m, seed=1, undirected=False):
+    """The benchmark's seeded G(n, m) graph, as rmat."""
+    csr = HostCsr()
+    _check(lib().wc_graph_gnm(n, m, seed, int(undirected), C.byref(csr)))
+    return _take(csr)
 
 
 def _ptr(a):
@@ -278,6 +329,18 @@ def bfs_depths(g, sources, caps):
     edges = np.zeros(len(sources), np.uint64)
     _check(lib().wo_bfs_depths(g.handle, _ptr(sources), _ptr(caps), len(sources), _ptr(out),
                                _ptr(edges)))
+    return out, edges
+
+
+def bfs_depths_batched64(g, sources, caps):
+    """bfs_depths by the reference's own batched shape (multi_source.rs:
+    64 sources a word, atomic-OR push, per-level settle): same results."""
+    sources = np.ascontiguousarray(sources, dtype=np.uint64)
+    caps = np.ascontiguousarray(caps, dtype=np.uint32)
+    out = np.zeros((len(sources), g.n), np.uint8)
+    edges = np.zeros(len(sources), np.uint64)
+    _check(lib().wo_bfs_depths_batched64(g.handle, _ptr(sources), _ptr(caps), len(sources),
+                                         _ptr(out), _ptr(edges)))
     return out, edges
 
 

@@ -22,6 +22,7 @@
 #include <limits>
 #include <numeric>
 #include <queue>
+#include <array>
 #include <thread>
 #include <vector>
 
@@ -920,6 +921,109 @@ int32_t wo_bfs_depths(const wo_graph* gp, const uint64_t* sources, const uint32_
     if (edges_out) edges_out[s] = st.edges_traversed;
     return WC_OK;
   });
+}
+
+// The reference's own batched shape, compute/centrality/multi_source.rs:33-160
+// (SourceBatch, after Then et al., "The More the Merrier"): up to 64
+// sources searched together, one bit each in a u64 word per node.  A step
+// pushes each frontier node's word along its row into its neighbours' next
+// words (an atomic OR less the sources that have already reached them,
+// :126-150), listing a neighbour when its next word first turns non-zero;
+// then each listed node takes next into seen and its frontier (:155-175).
+// Frontier nodes are taken in tasks of 4,096 (centrality/mod.rs:79), in
+// parallel.  With each source's depth cap applied as LevelSearch applies
+// max_depth (a node at depth d is expanded for the sources whose cap is
+// above d, traversal/level.rs:119-123), the depths and edges_traversed
+// equal wo_bfs_depths's for every source.  Batches of 64 run in order.
+int32_t wo_bfs_depths_batched64(const wo_graph* gp, const uint64_t* sources, const uint32_t* caps,
+                                uint32_t width, uint8_t* depth_out, uint64_t* edges_out) {
+  const Graph& g = *(const Graph*)gp;
+  const uint64_t n = g.fwd.n;
+  constexpr size_t kTask = 4096;
+  std::vector<std::atomic<uint64_t>> seen(n), next(n);
+  std::vector<uint64_t> frontier(n, 0);
+  std::vector<uint64_t> current, listed(n);
+  for (uint64_t i = 0; i < n; i++) {
+    seen[i].store(0, std::memory_order_relaxed);
+    next[i].store(0, std::memory_order_relaxed);
+  }
+  for (uint32_t s = 0; s < width; s++)
+    if (sources[s] >= n) return WC_NODE_OUTSIDE_ID_SPACE;
+  std::fill(depth_out, depth_out + (uint64_t)width * n, 255);
+  for (uint32_t b0 = 0; b0 < width; b0 += 64) {
+    const uint32_t bk = std::min<uint32_t>(64, width - b0);
+    uint64_t edges[64] = {0};
+    current.clear();
+    for (uint32_t bit = 0; bit < bk; bit++) {
+      const uint64_t node = sources[b0 + bit];
+      if (!seen[node].load(std::memory_order_relaxed) && !frontier[node]) current.push_back(node);
+      seen[node].fetch_or(1ull << bit, std::memory_order_relaxed);
+      frontier[node] |= 1ull << bit;
+      depth_out[(uint64_t)(b0 + bit) * n + node] = 0;
+    }
+    for (uint32_t d = 1; !current.empty(); d++) {
+      // Sources whose cap lets them expand depth d - 1.
+      uint64_t expands = 0;
+      for (uint32_t bit = 0; bit < bk; bit++)
+        if (caps[b0 + bit] > d - 1) expands |= 1ull << bit;
+      std::atomic<size_t> count{0};
+      const size_t tasks = (current.size() + kTask - 1) / kTask;
+      std::vector<std::array<uint64_t, 64>> task_edges(tasks);
+      parallel_tasks(tasks, [&](size_t t) -> Status {
+        std::array<uint64_t, 64>& te = task_edges[t];
+        te.fill(0);
+        std::vector<uint64_t> mine;
+        const size_t lo = t * kTask, hi = std::min(current.size(), lo + kTask);
+        for (size_t q = lo; q < hi; q++) {
+          const uint64_t node = current[q];
+          const uint64_t word = frontier[node] & expands;
+          frontier[node] = 0;
+          if (!word) continue;
+          const uint64_t r0 = g.fwd.off[node], r1 = g.fwd.off[node + 1];
+          for (uint64_t w = word; w; w &= w - 1) te[__builtin_ctzll(w)] += r1 - r0;
+          for (uint64_t e = r0; e < r1; e++) {
+            const uint64_t t2 = g.fwd.tgt[e];
+            const uint64_t fresh = word & ~seen[t2].load(std::memory_order_relaxed);
+            if (fresh & ~next[t2].load(std::memory_order_relaxed)) {
+              if (next[t2].fetch_or(fresh, std::memory_order_relaxed) == 0) mine.push_back(t2);
+            }
+          }
+        }
+        const size_t at = count.fetch_add(mine.size());
+        std::copy(mine.begin(), mine.end(), listed.begin() + at);
+        return WC_OK;
+      });
+      for (const auto& te : task_edges)
+        for (uint32_t bit = 0; bit < 64; bit++) edges[bit] += te[bit];
+      // Settle: each listed node takes its next word (less what it has
+      // seen) into seen and its frontier, and records the depth.
+      const size_t found = count.load();
+      const size_t stasks = (found + kTask - 1) / kTask;
+      parallel_tasks(stasks, [&](size_t t) -> Status {
+        const size_t lo = t * kTask, hi = std::min(found, lo + kTask);
+        for (size_t q = lo; q < hi; q++) {
+          const uint64_t node = listed[q];
+          const uint64_t got = next[node].exchange(0, std::memory_order_relaxed) &
+                               ~seen[node].load(std::memory_order_relaxed);
+          seen[node].fetch_or(got, std::memory_order_relaxed);
+          frontier[node] = got;
+          for (uint64_t w = got; w; w &= w - 1)
+            depth_out[(uint64_t)(b0 + __builtin_ctzll(w)) * n + node] = (uint8_t)std::min(d, 255u);
+        }
+        return WC_OK;
+      });
+      current.assign(listed.begin(), listed.begin() + found);
+    }
+    // Clear seen for the next batch (the reference clears after each search).
+    parallel_tasks((n + kTask * 16 - 1) / (kTask * 16), [&](size_t t) -> Status {
+      const uint64_t lo = t * kTask * 16, hi = std::min<uint64_t>(n, lo + kTask * 16);
+      for (uint64_t i = lo; i < hi; i++) seen[i].store(0, std::memory_order_relaxed);
+      return WC_OK;
+    });
+    if (edges_out)
+      for (uint32_t bit = 0; bit < bk; bit++) edges_out[b0 + bit] = edges[bit];
+  }
+  return WC_OK;
 }
 
 // compute_sql/library/sssp_vector.sql:14-66 over the i64 dtype: x = {source:

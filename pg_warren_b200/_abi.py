@@ -54,7 +54,8 @@ class CsrHost(C.Structure):
 
 class VersionInfo(C.Structure):
     _fields_ = [("id_space", U64), ("edges", U64), ("device_bytes", U64), ("weighted", I32),
-                ("integral_weights", I32), ("device", I32), ("symmetric", I32)]
+                ("integral_weights", I32), ("device", I32), ("symmetric", I32),
+                ("scratch_bytes", U64)]
 
 
 class Mask(C.Structure):
@@ -125,6 +126,8 @@ SIGNATURES = [
     ("wc_serves", I32, [C.c_char_p, I32]),
     ("wc_kernel_launches", U64, []),
     ("wc_version_timing", D, [P, C.c_char_p, C.POINTER(U32)]),
+    ("wc_random_uniform", I32, [P, C.POINTER(Call), U64, U64, P]),
+    ("wc_selftest_bounded_wait", I32, [C.POINTER(Call), U32]),
     ("wc_spmv", I32, [P, C.POINTER(Call), C.POINTER(ProductC), I32, P, P]),
     ("wc_spmm", I32, [P, C.POINTER(Call), C.POINTER(ProductC), I32, U32, P, P]),
     ("wc_pagerank", I32, [P, C.POINTER(Call), C.POINTER(PageRankOpts), P, P, C.POINTER(U32)]),

@@ -542,20 +542,22 @@ def _check_operands(graph: GraphVersion, x, y, width: Optional[int]):
 
 
 def spmv(graph: GraphVersion, product: Product, x, y, interrupts=None, stream=None,
-         asynchronous=False):
-    """y = A ⊗ x (or Aᵀ ⊗ x), y updated in place (product/mod.rs:77-92)."""
+         asynchronous=False, memory: Optional[Budget] = None):
+    """y = A ⊗ x (or Aᵀ ⊗ x), y updated in place (product/mod.rs:77-92).
+    `memory`: the call's own budget (ComputeMemory) for its working memory."""
     _check_operands(graph, x, y, 1)
     pc, mask = _product_c(product)
-    call, detail = _call(interrupts, stream, 1 if asynchronous else 0)
+    call, detail = _call(interrupts, stream, 1 if asynchronous else 0, memory)
     _raise(A.load().wc_spmv(graph.handle, C.byref(call), C.byref(pc), _dtype(y), _ptr(x), _ptr(y)),
            detail)
 
 
-def spmm(graph: GraphVersion, product: Product, x, y, interrupts=None, stream=None):
+def spmm(graph: GraphVersion, product: Product, x, y, interrupts=None, stream=None,
+         memory: Optional[Budget] = None):
     """Y = A ⊗ X over row-major id_space × width matrices (product/mod.rs:97-110)."""
     width = _check_operands(graph, x, y, None)
     pc, mask = _product_c(product)
-    call, detail = _call(interrupts, stream)
+    call, detail = _call(interrupts, stream, 0, memory)
     _raise(A.load().wc_spmm(graph.handle, C.byref(call), C.byref(pc), _dtype(y), width, _ptr(x),
                             _ptr(y)), detail)
 
@@ -593,12 +595,17 @@ def _pr_opts(p: PageRank):
 
 
 def pagerank(graph: GraphVersion, tombstones=None, pagerank: PageRank = PageRank(), out=None,
-             interrupts=None, stream=None, timing=False) -> Ranks:
-    """compute/pagerank/mod.rs:96-151; `tombstones` are NodeSet words."""
+             interrupts=None, stream=None, timing=False, memory: Optional[Budget] = None,
+             timeout_ms: int = 0) -> Ranks:
+    """compute/pagerank/mod.rs:96-151; `tombstones` are NodeSet words.
+    `memory`: the call's own budget; `timeout_ms`: a bound on the wait for
+    the device (0: the library's default), past which the call stops its
+    kernels and raises DeviceTimeout."""
     o, seed = _pr_opts(pagerank)
     ranks = out if out is not None else np.zeros(graph.id_space, np.float64)
     it = C.c_uint32(0)
-    call, detail = _call(interrupts, stream, CALL_TIMING if timing else 0)
+    call, detail = _call(interrupts, stream, CALL_TIMING if timing else 0, memory)
+    call.timeout_ms = timeout_ms
     _raise(A.load().wc_pagerank(graph.handle, C.byref(call), C.byref(o), _ptr(tombstones),
                                 _ptr(ranks), C.byref(it)), detail)
     return Ranks(ranks, it.value)
@@ -615,6 +622,22 @@ def pagerank_noalloc(graph: GraphVersion, tombstones=None, pagerank: PageRank = 
     _raise(A.load().wc_pagerank_noalloc(graph.handle, C.byref(call), C.byref(o),
                                         _ptr(tombstones), _ptr(ranks), C.byref(it)), detail)
     return Ranks(ranks, it.value)
+
+
+def random_uniform(graph: GraphVersion, seed: int, stream: int = 0, out=None):
+    """compute/random.rs:11-25 evaluated on the device over the version's id
+    space (the start vectors wc_eigen draws)."""
+    x = out if out is not None else np.zeros(graph.id_space, np.float64)
+    call, detail = _call()
+    _raise(A.load().wc_random_uniform(graph.handle, C.byref(call), seed, stream, _ptr(x)), detail)
+    return x
+
+
+def selftest_bounded_wait(limit_us: int, stream=None):
+    """A device wait that nothing completes, bounded to `limit_us`: raises
+    DeviceTimeout once it gives up (wc_selftest_bounded_wait)."""
+    call, detail = _call(None, stream)
+    _raise(A.load().wc_selftest_bounded_wait(C.byref(call), limit_us), detail)
 
 
 def last_margin(graph: GraphVersion) -> float:
@@ -952,7 +975,8 @@ def reachable(graph: GraphVersion, start: int, target: int, max_depth=None,
 
 
 def bfs_batched(graph: GraphVersion, sources, max_depths, depth_out=None, edges_out=None,
-                stream=None, timing=False):
+                stream=None, timing=False, interrupts=None, memory: Optional[Budget] = None,
+                timeout_ms: int = 0):
     """`len(sources)` BFS searches as one bit-packed boolean SpMM: depths
     u8[k, n] (255: not reached within the source's cap).  Sources, caps and
     outputs may be host arrays or device tensors."""
@@ -963,7 +987,8 @@ def bfs_batched(graph: GraphVersion, sources, max_depths, depth_out=None, edges_
     k = len(src)
     d = depth_out if depth_out is not None else np.zeros((k, graph.id_space), np.uint8)
     e = edges_out if edges_out is not None else np.zeros(k, np.uint64)
-    call, detail = _call(None, stream, CALL_TIMING if timing else 0)
+    call, detail = _call(interrupts, stream, CALL_TIMING if timing else 0, memory)
+    call.timeout_ms = timeout_ms
     _raise(A.load().wc_bfs_batched(graph.handle, C.byref(call), _ptr(src), _ptr(caps), k, _ptr(d),
                                    _ptr(e)), detail)
     return d, e

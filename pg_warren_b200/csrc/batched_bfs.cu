@@ -109,7 +109,15 @@ struct MsLevel {
   uint64_t m;
   uint32_t* acc;      // n × W push accumulators, all zero between levels
   uint32_t* touched;  // rows with a push accumulator to settle, all zero between levels
+  const int32_t* cancel;  // the call's cancel word (host-mapped): a raised word ends the pass
 };
+
+// Whether level P.L runs at all: it has a frontier and the call is not
+// cancelled.  A level that does not run leaves the next level's count zero,
+// so every later level returns at once too.
+__device__ inline bool level_runs(const MsLevel& P) {
+  return P.counts[P.L] != 0 && !*(volatile const int32_t*)P.cancel;
+}
 
 // A level pushes (scatters the frontier rows over the forward CSR) while the
 // frontier's out-edges are below m / kPushDivisor, and pulls (gathers over
@@ -212,8 +220,8 @@ __device__ inline void prefetch_unit(const MsLevel& P, const Unit& d, unsigned l
 // was loaded one unit earlier, so the prefetch does not wait on it).
 template <int W>
 __global__ void __launch_bounds__(256, 4) msbfs_level_kernel(MsLevel P) {
-  if (P.counts[P.L] == 0) return;  // nothing expands: F_{L+1} is not read
-  if (level_pushes(P)) return;     // msbfs_push_kernel and msbfs_settle_kernel run it
+  if (!level_runs(P)) return;  // nothing expands (or cancelled): F_{L+1} is not read
+  if (level_pushes(P)) return;  // msbfs_push_kernel and msbfs_settle_kernel run it
   constexpr uint32_t VEC = W >= 4 ? 4 : W;
   constexpr uint32_t LPR = W / VEC;
   constexpr uint32_t G = 32 / LPR;
@@ -506,7 +514,7 @@ __global__ void __launch_bounds__(256, 4) msbfs_level_kernel(MsLevel P) {
 // row.
 template <int W>
 __global__ void __launch_bounds__(256) msbfs_push_kernel(MsLevel P) {
-  if (P.counts[P.L] == 0 || !level_pushes(P)) return;
+  if (!level_runs(P) || !level_pushes(P)) return;
   constexpr uint32_t G = 32 / W;
   const unsigned lane = threadIdx.x & 31;
   const unsigned sub = lane / W, w = lane % W;
@@ -541,6 +549,8 @@ __global__ void __launch_bounds__(256) msbfs_push_kernel(MsLevel P) {
 // does (fresh = acc & ~V), clears the accumulator and its touched bit.
 template <int W>
 __global__ void __launch_bounds__(256) msbfs_settle_kernel(MsLevel P) {
+  // No cancel check here: a push that ran must be settled, which also
+  // leaves the accumulators and touched bits zero for the next call.
   if (P.counts[P.L] == 0 || !level_pushes(P)) return;
   constexpr uint32_t G = 32 / W;
   const unsigned lane = threadIdx.x & 31;
@@ -925,6 +935,20 @@ __global__ void __launch_bounds__(kDepthThreads, 2)
     if (esum[x]) atomicAdd(edges + x, esum[x]);
 }
 
+// Depths are bytes with 255 for "not reached", so a pass runs at most
+// kMaxLevels levels.  When a source's cap is deeper than that, the pass is
+// cut short; if some source still had nodes to expand at the cut (rows
+// admitted to the frontier of level kMaxLevels for a source whose cap is
+// above it), the result would differ from wc_bfs, and the call is refused
+// with WC_UNSUPPORTED (the adapter keeps the native search) instead of
+// answering short.  Searches that end within kMaxLevels levels are served
+// whatever their caps.
+constexpr uint32_t kMaxLevels = 254;
+
+__global__ void msbfs_truncated_kernel(const uint32_t* counts_at_cut, DeviceError* err) {
+  if (threadIdx.x == 0 && *counts_at_cut != 0) raise(err, WC_UNSUPPORTED, kMaxLevels);
+}
+
 // Centrality passes (wc_centrality): no depths; after the levels, a flag
 // if the last level reached any node (the pass must be run deeper), and
 // otherwise each node's counts added to its totals.
@@ -986,8 +1010,8 @@ __global__ void __launch_bounds__(256) msbfs_centrality_kernel(uint32_t n, uint3
 // One pass of up to 32·W sources.
 template <int W>
 wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const uint32_t* caps_dev,
-                   uint32_t k, uint32_t levels, uint8_t* depth_dev, unsigned long long* edges_dev,
-                   uint32_t blocks_per_sm, const CentArgs* cent) {
+                   uint32_t k, uint32_t levels, bool clipped, uint8_t* depth_dev,
+                   unsigned long long* edges_dev, uint32_t blocks_per_sm, const CentArgs* cent) {
   wc_version* v = ctx.v;
   const uint32_t n = (uint32_t)v->n;
   const uint64_t row_words = (uint64_t)n * W;
@@ -1036,12 +1060,15 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
               F + L * fstride, F + (L + 1) * fstride, fbits + L * bitmap_words,
               fbits + (L + 1) * bitmap_words, wbits + (L + 1) * bitmap_words, masks, alive, L,
               counts, fedges, foff, fwd.targets.as<uint32_t>(), fwd.schedule.units.as<Unit>(),
-              fwd.schedule.count, v->m, b.acc->as<uint32_t>(), b.touched->as<uint32_t>()};
+              fwd.schedule.count, v->m, b.acc->as<uint32_t>(), b.touched->as<uint32_t>(),
+              v->cancel_dev};
     note_launch(), msbfs_push_kernel<W><<<push_grid, 256, 0, st>>>(P);
     note_launch(), msbfs_settle_kernel<W><<<settle_grid, 256, 0, st>>>(P);
     note_launch(), msbfs_level_kernel<W><<<grid, 256, level_smem, st>>>(P);
   }
   ctx.phase_end();
+  if (clipped)
+    note_launch(), msbfs_truncated_kernel<<<1, 32, 0, st>>>(counts + levels, v->error.as<DeviceError>());
   if (cent) {
     if constexpr (W % 2 == 0) {
       // Rows first reached at the last level (F_levels's written rows) may
@@ -1108,7 +1135,8 @@ wc_status BatchBuffers::reserve(Ctx& ctx, uint32_t words, uint32_t levels) {
 }
 
 typedef wc_status (*PassFn)(Ctx&, BatchBuffers&, const uint64_t*, const uint32_t*, uint32_t,
-                            uint32_t, uint8_t*, unsigned long long*, uint32_t, const CentArgs*);
+                            uint32_t, bool, uint8_t*, unsigned long long*, uint32_t,
+                            const CentArgs*);
 
 static PassFn pass_for(uint32_t columns) {
   switch (columns) {
@@ -1139,19 +1167,21 @@ wc_status bfs_batched_run(Ctx& ctx, const wc_schedule& sched, const uint64_t* so
   BatchBuffers b;
   uint32_t max_levels = 0;
   for (uint32_t s = 0; s < width; s++) max_levels = std::max(max_levels, caps_host[s]);
-  max_levels = std::min<uint32_t>(max_levels, 254);
+  max_levels = std::min<uint32_t>(max_levels, kMaxLevels);
   WC_TRY(b.reserve(ctx, columns / 32, max_levels));
   WC_CUDA(cudaMemsetAsync(edges_dev, 0, width * 8, ctx.stream), ctx.detail);
   for (uint32_t s0 = 0; s0 < width; s0 += columns) {
     const uint32_t k = std::min(columns, width - s0);
     uint32_t levels = 0;
     for (uint32_t s = s0; s < s0 + k; s++) levels = std::max(levels, caps_host[s]);
-    levels = std::min<uint32_t>(levels, 254);
+    const bool clipped = levels > kMaxLevels;
+    levels = std::min<uint32_t>(levels, kMaxLevels);
     const uint32_t bps = sched.blocks_per_sm ? sched.blocks_per_sm : 4;
     const std::string key = "bfs/" + std::to_string(columns) + "/" + std::to_string(k) + "/" +
-                            std::to_string(levels) + "/" + std::to_string(bps);
+                            std::to_string(levels) + "/" + std::to_string(bps) +
+                            (clipped ? "/clipped" : "");
     WC_TRY(ctx.run_captured(key, [&] {
-      return pass_for(columns)(ctx, b, sources_dev + s0, caps_dev + s0, k, levels,
+      return pass_for(columns)(ctx, b, sources_dev + s0, caps_dev + s0, k, levels, clipped,
                                depth_dev + (uint64_t)s0 * ctx.v->n, edges_dev + s0, bps, nullptr);
     }));
   }
@@ -1165,7 +1195,7 @@ wc_status bfs_centrality_pass(Ctx& ctx, BatchBuffers& b, uint32_t columns,
                           std::to_string(levels) + "/" + std::to_string(blocks_per_sm) +
                           (cent.keep_only ? "/keep" : "");
   return ctx.run_captured(key, [&] {
-    return pass_for(columns)(ctx, b, sources_dev, caps_dev, k, levels, nullptr, nullptr,
+    return pass_for(columns)(ctx, b, sources_dev, caps_dev, k, levels, false, nullptr, nullptr,
                              blocks_per_sm, &cent);
   });
 }
@@ -1292,7 +1322,11 @@ wc_status wc_bfs_batched(wc_version* v, const wc_call* call, const uint64_t* sou
   if (edges_traversed_out)
     WC_CUDA(cudaMemcpyAsync(edges_traversed_out, edges->ptr, width * 8, cudaMemcpyDefault,
                             ctx.stream), ctx.detail);
-  return ctx.finish();
+  const wc_status st = ctx.finish();
+  if (st == WC_UNSUPPORTED)
+    set_message(ctx.detail, "a search still expands at depth %u with a deeper cap; depths past %u "
+                            "do not fit the byte output", kMaxLevels, kMaxLevels);
+  return st;
 }
 
 }  // extern "C"

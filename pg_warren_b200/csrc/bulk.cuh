@@ -32,6 +32,23 @@ __device__ inline void mbar_arrive_expect(uint64_t* bar, uint32_t bytes) {
                : "memory");
 }
 
+// An L2 policy under which the lines a load brings in are the first to be
+// evicted: for data streamed once per pass (a CSR's arrays), so that it does
+// not push out the vectors that the gathers re-read.
+__device__ inline uint64_t l2_evict_first_policy() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+// An L2 policy under which the lines are kept longest: for the vector the
+// gathers of a pull re-read (its values are read once per entry).
+__device__ inline uint64_t l2_evict_last_policy() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
 // Global → shared bulk copy of `bytes` (a multiple of 16, both addresses
 // 16-byte aligned), completing its bytes on `bar`.
 __device__ inline void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
@@ -39,6 +56,16 @@ __device__ inline void bulk_load(void* dst, const void* src, uint32_t bytes, uin
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
           "r"(smem_addr(dst)),
       "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// bulk_load under an L2 policy (l2_evict_first_policy for a stream).
+__device__ inline void bulk_load_hint(void* dst, const void* src, uint32_t bytes, uint64_t* bar,
+                                      uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1], %2, [%3], %4;" ::"r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
       : "memory");
 }
 

@@ -1150,4 +1150,23 @@ wc_status wc_eigen(wc_version* v, const wc_call* call, const wc_eigen_opts* opts
   return ctx.finish();
 }
 
+wc_status wc_random_uniform(wc_version* v, const wc_call* call, uint64_t seed, uint64_t stream,
+                            double* out) {
+  if (!v || !out) return WC_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lock(v->mu);
+  WC_CUDA(cudaSetDevice(v->device), call ? call->detail : nullptr);
+  Ctx ctx(v, call);
+  if (ctx.cancelled()) return WC_CANCELLED;
+  WC_TRY(ctx.begin());
+  Operand X(POOL_EIG_0);
+  WC_TRY(X.output(ctx, out, v->n * 8));
+  const uint32_t n = (uint32_t)v->n;
+  const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>((n + 255) / 256, max_blocks(4)));
+  note_launch(), random_kernel<<<grid, 256, 0, ctx.stream>>>(static_cast<double*>(X.dev), nullptr,
+                                                             n, seed, stream, 1);
+  WC_CUDA(cudaGetLastError(), ctx.detail);
+  WC_TRY(X.out(ctx));
+  return ctx.finish();
+}
+
 }  // extern "C"

@@ -16,6 +16,7 @@
 #include "pagerank.h"
 #include "pull.cuh"
 #include "sqlfloat.cuh"
+#include "upload.h"
 
 namespace wc {
 
@@ -39,10 +40,11 @@ static std::mutex g_scratch_mu[kMaxDevices];
 static uint64_t align256(uint64_t b) { return (b + 255) & ~255ull; }
 
 // The bytes a solve of n nodes and max_iter iterations needs, in the order
-// they are laid out: x[2], msg[2], out, tombstones (if any), scalars.
+// they are laid out: x[2], msg[2], out, tombstones (if any: the caller's
+// words and their renumbering into the locality order), scalars.
 static uint64_t static_bytes(uint64_t n, uint32_t max_iter, uint32_t blocks, bool tomb) {
   uint64_t b = align256(2 * n * 8) * 2 + align256(n * 8);
-  if (tomb) b += align256(((n + 63) / 64) * 8);
+  if (tomb) b += align256(2 * ((n + 63) / 64) * 8);
   b += align256((2 * (uint64_t)max_iter + 8) * 8 + 2 * (uint64_t)blocks * 8 + 64);
   return b;
 }
@@ -86,8 +88,8 @@ static wc_status static_setup(Ctx& ctx, PageRankRun& run, const wc_pagerank_opts
   WC_TRY((wc_status)sql_float<F_SUB>(1.0, o->damping, &teleport));
   if (o->has_tol && o->max_iter > 0)
     WC_TRY((wc_status)sql_float<F_MUL>(run.nodes, o->tol, &threshold));
-  const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>(
-      (v->rev.schedule.count + kPullWarps - 1) / kPullWarps, max_blocks(8)));
+  run.local = true;  // wc_pagerank's own numbering, so the results are its
+  const uint32_t blocks = pagerank_grid(run.csc(v));
   run.grid = blocks;
 
   unsigned char* p = base;
@@ -101,9 +103,11 @@ static wc_status static_setup(Ctx& ctx, PageRankRun& run, const wc_pagerank_opts
   double* out = reinterpret_cast<double*>(take(n * 8));
   uint64_t* tomb = nullptr;
   if (tomb_in) {
-    tomb = reinterpret_cast<uint64_t*>(take(((n + 63) / 64) * 8));
-    WC_CUDA(cudaMemcpyAsync(tomb, tomb_in, ((n + 63) / 64) * 8, cudaMemcpyDefault, ctx.stream),
-            ctx.detail);
+    const uint64_t words = (n + 63) / 64;
+    uint64_t* ids = reinterpret_cast<uint64_t*>(take(2 * words * 8));
+    WC_CUDA(cudaMemcpyAsync(ids, tomb_in, words * 8, cudaMemcpyDefault, ctx.stream), ctx.detail);
+    tomb = ids + words;
+    WC_TRY(bits_to_locality(v, ctx.stream, ids, tomb));
   }
   const uint64_t scalar_bytes = (2 * (uint64_t)o->max_iter + 8) * 8 + 2 * (uint64_t)blocks * 8 + 64;
   double* sc = reinterpret_cast<double*>(take(scalar_bytes));
@@ -133,11 +137,68 @@ static wc_status static_setup(Ctx& ctx, PageRankRun& run, const wc_pagerank_opts
   s.cancel = v->cancel_dev;
   s.pace = v->pace_dev;
   s.err = v->error.as<DeviceError>();
-  // out = plus_first over the forward CSR: each row's out-weight.
+  // out = plus_first over the forward CSR: each row's out-weight, into the
+  // second message buffer, then renumbered.
   PullLaunch L;
   WC_TRY(prepare_pull(ctx, v->fwd, WC_PLUS_FIRST, o->weighted, WC_F64, 1, L));
-  WC_TRY(launch_pull(L, WC_F64, x, out));
+  WC_TRY(launch_pull(L, WC_F64, x, s.msg[1]));
+  WC_TRY(to_locality(v, ctx.stream, s.msg[1], out));
   return cuda_status(cudaGetLastError(), ctx.detail, "pagerank setup");
+}
+
+// On an early return after work was queued on the call's stream, waits for
+// that work before the locks are released, so that no kernel of this call
+// still uses the shared array when the next caller takes it.
+struct DrainOnExit {
+  cudaStream_t stream = nullptr;
+  bool armed = false;
+  ~DrainOnExit() {
+    if (armed) cudaStreamSynchronize(stream);
+  }
+};
+
+// The solve under the device's and the version's locks.  No callback of the
+// caller runs here: a progress hook that called back into this entry point
+// on the same device would otherwise wait on its own lock.
+static wc_status noalloc_solve(wc_version* v, const wc_call* call, const wc_pagerank_opts* o,
+                               const uint64_t* tombstones, double* ranks, uint32_t* iterations,
+                               wc_error_detail* detail) {
+  std::lock_guard<std::mutex> device_lock(g_scratch_mu[v->device]);
+  std::lock_guard<std::recursive_mutex> lock(v->mu);
+  WC_CUDA(cudaSetDevice(v->device), detail);
+  if (!g_scratch_addr[v->device]) {
+    void* addr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&addr, g_pagerank_scratch);
+    if (e != cudaSuccess) return cuda_status(e, detail, "cudaGetSymbolAddress");
+    if (!addr) {
+      set_message(detail, "cudaGetSymbolAddress gave no address for the fixed scratch");
+      return WC_CUDA_ERROR;
+    }
+    g_scratch_addr[v->device] = addr;
+  }
+  // No events, and no progress hook inside the locks.
+  wc_call plain{};
+  if (call) {
+    plain = *call;
+    plain.flags &= ~WC_CALL_TIMING;
+    plain.progress = nullptr;
+  }
+  Ctx ctx(v, call ? &plain : nullptr);
+  if (ctx.cancelled()) return WC_CANCELLED;
+  DrainOnExit drain;  // declared after the locks: runs before they are released
+  drain.stream = ctx.stream;
+  drain.armed = true;
+  WC_TRY(ctx.begin());
+  PageRankRun run;
+  WC_TRY(static_setup(ctx, run, o, tombstones,
+                      static_cast<unsigned char*>(g_scratch_addr[v->device])));
+  WC_TRY(run.run(ctx));
+  WC_TRY(ctx.finish());
+  double margin = 0.0;
+  WC_TRY(run.result(ctx, ranks, iterations, &margin));
+  drain.armed = false;
+  v->last_margin = margin;
+  return WC_OK;
 }
 
 }  // namespace wc
@@ -158,8 +219,7 @@ wc_status wc_pagerank_noalloc(wc_version* v, const wc_call* call, const wc_pager
     set_message(detail, "a personalised PageRank needs per-call memory; use wc_pagerank");
     return WC_UNSUPPORTED;
   }
-  const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>(
-      (v->rev.schedule.count + kPullWarps - 1) / kPullWarps, max_blocks(8)));
+  const uint32_t blocks = pagerank_grid(v->loc.csc);
   const uint64_t need = static_bytes(v->n, o->max_iter, blocks, tombstones != nullptr);
   if (need > kStaticScratchBytes) {
     if (detail) {
@@ -171,39 +231,13 @@ wc_status wc_pagerank_noalloc(wc_version* v, const wc_call* call, const wc_pager
                 (unsigned long long)kStaticScratchBytes);
     return WC_WORKING_SET;
   }
-  std::lock_guard<std::mutex> device_lock(g_scratch_mu[v->device]);
-  std::lock_guard<std::recursive_mutex> lock(v->mu);
-  WC_CUDA(cudaSetDevice(v->device), detail);
-  if (!g_scratch_addr[v->device]) {
-    void* addr = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&addr, g_pagerank_scratch);
-    if (e != cudaSuccess) return cuda_status(e, detail, "cudaGetSymbolAddress");
-    if (!addr) {
-      set_message(detail, "cudaGetSymbolAddress gave no address for the fixed scratch");
-      return WC_CUDA_ERROR;
-    }
-    g_scratch_addr[v->device] = addr;
-  }
-  // No events: WC_CALL_TIMING is not honoured here.
-  wc_call plain{};
-  if (call) {
-    plain = *call;
-    plain.flags &= ~WC_CALL_TIMING;
-  }
-  Ctx ctx(v, call ? &plain : nullptr);
-  if (ctx.cancelled()) return WC_CANCELLED;
-  WC_TRY(ctx.begin());
-  PageRankRun run;
-  WC_TRY(static_setup(ctx, run, o, tombstones,
-                      static_cast<unsigned char*>(g_scratch_addr[v->device])));
-  ctx.progress("iterating", 0, o->max_iter);
-  WC_TRY(run.run(ctx));
-  WC_TRY(ctx.finish());
-  double margin = 0.0;
-  WC_TRY(run.result(ctx, ranks, iterations, &margin));
-  v->last_margin = margin;
-  ctx.progress("iterating", iterations ? *iterations : 0, o->max_iter);
-  return WC_OK;
+  // The progress hook runs outside the locks, before and after the solve.
+  const bool hook = call && call->progress;
+  if (hook) call->progress(call->progress_context, "iterating", 0, o->max_iter);
+  const wc_status st = noalloc_solve(v, call, o, tombstones, ranks, iterations, detail);
+  if (st == WC_OK && hook)
+    call->progress(call->progress_context, "iterating", iterations ? *iterations : 0, o->max_iter);
+  return st;
 }
 
 }  // extern "C"

@@ -22,10 +22,16 @@
 #include "pagerank.h"
 #include "pull.cuh"
 #include "sqlfloat.cuh"
+#include "upload.h"
 
 namespace wc {
 
 constexpr uint64_t kChunk = 1 << 16;  // compute/reduce.rs:20
+
+// Over the locality-ordered CSC, the messages of the nodes numbered below
+// this (the most gathered) are kept in L1: 64 KB of them, what the SM's L1
+// holds beside four blocks' staging rings.
+constexpr uint32_t kHotNodes = 8192;
 
 __device__ inline bool tomb_at(const uint64_t* t, uint32_t i) {
   return t && ((t[i >> 6] >> (i & 63)) & 1);
@@ -196,7 +202,7 @@ struct PrEpi {
 
 // Unweighted, four blocks an SM (64 registers) keep more gathers in flight;
 // with weights the extra registers would spill, so three.
-template <class W>
+template <class W, bool SPLIT>
 __global__ void __launch_bounds__(kPullThreads, WSize<W>::v == 0 ? 4 : 3)
     pr_iter_kernel(CsrView<W> A, PrState s, uint32_t it) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -204,7 +210,7 @@ __global__ void __launch_bounds__(kPullThreads, WSize<W>::v == 0 ? 4 : 3)
   const int cur = it & 1;
   PrEpi epi{&s, cur, s.dangling[it], 0.0, 0.0};
   PullRing<double, W>* ring = reinterpret_cast<PullRing<double, W>*>(smem) + (threadIdx.x >> 5);
-  pull_units<double, WC_PLUS_TIMES, W>(A, s.msg[cur], epi, s.err, ring);
+  pull_units<double, WC_PLUS_TIMES, W, PrEpi, SPLIT>(A, s.msg[cur], epi, s.err, ring);
   double delta = epi.delta, dangling = epi.dangling_out;
   if (reduce_two(delta, dangling, s.partials, s.counter)) {
     s.delta[it] = delta;
@@ -229,12 +235,18 @@ __global__ void __launch_bounds__(kPullThreads, WSize<W>::v == 0 ? 4 : 3)
 template <class W>
 wc_status launch_iter(const PullLaunch& L, const PrState& s, uint32_t it, uint32_t blocks) {
   CsrView<W> A{L.off, L.tgt, static_cast<const W*>(L.weights), L.units, L.unit_count, L.counters,
-               L.carry};
+               L.carry, L.hot};
   constexpr size_t smem = pull_smem_bytes<double, W>();
   static const cudaError_t attr = cudaFuncSetAttribute(
-      pr_iter_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      pr_iter_kernel<W, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  static const cudaError_t attr_split = cudaFuncSetAttribute(
+      pr_iter_kernel<W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (attr != cudaSuccess) return cuda_status(attr, L.detail, "pagerank kernel attributes");
-  note_launch(), pr_iter_kernel<W><<<blocks, kPullThreads, smem, L.stream>>>(A, s, it);
+  if (attr_split != cudaSuccess) return cuda_status(attr_split, L.detail, "pagerank kernel attributes");
+  if (L.hot)
+    note_launch(), pr_iter_kernel<W, true><<<blocks, kPullThreads, smem, L.stream>>>(A, s, it);
+  else
+    note_launch(), pr_iter_kernel<W, false><<<blocks, kPullThreads, smem, L.stream>>>(A, s, it);
   return WC_OK;
 }
 
@@ -253,19 +265,26 @@ uint64_t live_count(const uint64_t* tomb, uint64_t n) {
   return n - dead;
 }
 
+uint32_t pagerank_grid(const DevCsr& csc) {
+  return std::max<uint32_t>(1, std::min<uint32_t>((csc.schedule.count + kPullWarps - 1) / kPullWarps,
+                                                  max_blocks(8)));
+}
+
 wc_status PageRankRun::setup(Ctx& ctx, const wc_pagerank_opts* o, const uint64_t* tomb_host,
-                             const double* seed) {
+                             const double* seed, bool in_locality_order) {
   wc_version* v = ctx.v;
   const uint64_t n = v->n;
+  const uint64_t words = (n + 63) / 64;
   opts = *o;
+  local = in_locality_order;
   // Tombstones: the caller's words, on the device.
-  std::vector<uint64_t> words;
+  std::vector<uint64_t> host_words;
   const uint64_t* th = tomb_host;
   if (tomb_host && is_device_pointer(tomb_host)) {
-    words.resize((n + 63) / 64);
-    WC_CUDA(cudaMemcpy(words.data(), tomb_host, words.size() * 8, cudaMemcpyDeviceToHost),
+    host_words.resize(words);
+    WC_CUDA(cudaMemcpy(host_words.data(), tomb_host, words * 8, cudaMemcpyDeviceToHost),
             ctx.detail);
-    th = words.data();
+    th = host_words.data();
   }
   live = live_count(th, n);
   nodes = (double)live;
@@ -275,18 +294,24 @@ wc_status PageRankRun::setup(Ctx& ctx, const wc_pagerank_opts* o, const uint64_t
   WC_TRY((wc_status)sql_float<F_SUB>(1.0, o->damping, &teleport));
   double threshold = 0.0;
   if (o->has_tol && o->max_iter > 0) WC_TRY((wc_status)sql_float<F_MUL>(nodes, o->tol, &threshold));
-  const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>(
-      (v->rev.schedule.count + kPullWarps - 1) / kPullWarps, max_blocks(8)));
+  const uint32_t blocks = pagerank_grid(csc(v));
   grid = blocks;
   WC_TRY(ctx.scratch(POOL_PR_X, 2 * n * 8, &x));
   WC_TRY(ctx.scratch(POOL_PR_MSG, 2 * n * 8, &msg));
   WC_TRY(ctx.scratch(POOL_PR_OUT, n * 8, &out));
   const uint64_t scalar_bytes = (2 * (uint64_t)o->max_iter + 8) * 8 + 2 * blocks * 8 + 64;
   WC_TRY(ctx.scratch(POOL_PR_SCALARS, scalar_bytes, &scalars));
+  uint64_t* tomb_dev = nullptr;
   if (th) {
-    WC_TRY(ctx.scratch(POOL_PR_TOMB, ((n + 63) / 64) * 8, &tomb));
-    WC_CUDA(cudaMemcpyAsync(tomb->ptr, th, ((n + 63) / 64) * 8, cudaMemcpyHostToDevice,
-                            ctx.stream), ctx.detail);
+    // In locality order the words are renumbered into the buffer's second half.
+    WC_TRY(ctx.scratch(POOL_PR_TOMB, words * 8 * (local ? 2 : 1), &tomb));
+    WC_CUDA(cudaMemcpyAsync(tomb->ptr, th, words * 8, cudaMemcpyHostToDevice, ctx.stream),
+            ctx.detail);
+    tomb_dev = tomb->as<uint64_t>();
+    if (local) {
+      WC_TRY(bits_to_locality(v, ctx.stream, tomb_dev, tomb_dev + words));
+      tomb_dev += words;
+    }
   }
   WC_CUDA(cudaMemsetAsync(scalars->ptr, 0, scalar_bytes, ctx.stream), ctx.detail);
   double* sc = scalars->as<double>();
@@ -297,7 +322,7 @@ wc_status PageRankRun::setup(Ctx& ctx, const wc_pagerank_opts* o, const uint64_t
   s.msg[0] = msg->as<double>();
   s.msg[1] = msg->as<double>() + n;
   s.out = out->as<double>();
-  s.tomb = th ? tomb->as<uint64_t>() : nullptr;
+  s.tomb = tomb_dev;
   s.start = start;
   s.damping = o->damping;
   s.teleport = teleport;
@@ -313,22 +338,29 @@ wc_status PageRankRun::setup(Ctx& ctx, const wc_pagerank_opts* o, const uint64_t
   s.cancel = v->cancel_dev;
   s.pace = v->pace_dev;
   s.err = v->error.as<DeviceError>();
-  // out = plus_first over the forward CSR: each row's out-weight.
+  // out = plus_first over the forward CSR: each row's out-weight (in
+  // locality order: into the second message buffer, then renumbered).
   PullLaunch L;
   WC_TRY(prepare_pull(ctx, v->fwd, WC_PLUS_FIRST, o->weighted, WC_F64, 1, L));
-  WC_TRY(launch_pull(L, WC_F64, s.x[0], out->ptr));
-  // The personalisation.
+  WC_TRY(launch_pull(L, WC_F64, s.x[0], local ? s.msg[1] : out->ptr));
+  if (local) WC_TRY(to_locality(v, ctx.stream, s.msg[1], out->as<double>()));
+  // The personalisation, summed in dense-id order (the reference's chunks).
   if (seed) {
     Operand S(POOL_SEED);
     WC_TRY(S.in(ctx, seed, n * 8));
     const double* sd = static_cast<const double*>(S.dev);
     const uint32_t chunks = (uint32_t)((n + kChunk - 1) / kChunk);
-    WC_TRY(ctx.scratch(POOL_PR_SHARES, n * 8 + (uint64_t)chunks * 8, &shares));
-    double* partial = shares->as<double>() + n;
-    note_launch(), seed_chunks_kernel<<<(chunks + 127) / 128, 128, 0, ctx.stream>>>(sd, s.tomb, n, partial);
-    note_launch(), seed_shares_kernel<<<max_blocks(4), 256, 0, ctx.stream>>>(sd, s.tomb, (uint32_t)n, partial,
+    WC_TRY(ctx.scratch(POOL_PR_SHARES, n * 8 * (local ? 2 : 1) + (uint64_t)chunks * 8, &shares));
+    double* partial = shares->as<double>() + n * (local ? 2 : 1);
+    const uint64_t* tomb_ids = th ? tomb->as<uint64_t>() : nullptr;  // dense-id order
+    note_launch(), seed_chunks_kernel<<<(chunks + 127) / 128, 128, 0, ctx.stream>>>(sd, tomb_ids, n, partial);
+    note_launch(), seed_shares_kernel<<<max_blocks(4), 256, 0, ctx.stream>>>(sd, tomb_ids, (uint32_t)n, partial,
                                                              chunks, shares->as<double>(), s.err);
     s.shares = shares->as<double>();
+    if (local) {
+      WC_TRY(to_locality(v, ctx.stream, shares->as<double>(), shares->as<double>() + n));
+      s.shares = shares->as<double>() + n;
+    }
   }
   return cuda_status(cudaGetLastError(), ctx.detail, "pagerank setup");
 }
@@ -337,7 +369,8 @@ wc_status PageRankRun::run(Ctx& ctx) {
   wc_version* v = ctx.v;
   note_launch(), pr_init_kernel<<<grid, kPullThreads, 0, ctx.stream>>>(s);
   PullLaunch L;
-  WC_TRY(prepare_pull(ctx, v->rev, WC_PLUS_TIMES, opts.weighted, WC_F64, 1, L));
+  WC_TRY(prepare_pull(ctx, const_cast<DevCsr&>(csc(v)), WC_PLUS_TIMES, opts.weighted, WC_F64, 1, L));
+  if (local) L.hot = kHotNodes;
   // With a tolerance the solve usually stops well before max_iter: the
   // host keeps at most kAhead iterations queued beyond the last one the
   // device reported, and stops queueing once the device reports the stop,
@@ -350,6 +383,9 @@ wc_status PageRankRun::run(Ctx& ctx) {
   }
   ctx.phase_begin("iteration");
   for (uint32_t it = 0; it < opts.max_iter; it++) {
+    // A cancel stops the queueing (the kernels queued read the device's
+    // copy of the word, which finish() raises).
+    if (ctx.cancelled()) break;
     if (pace && s.has_tol) {
       bool stop = false;
       while (!(stop = pace[1] != 0) && it >= pace[0] + kAhead) {
@@ -371,7 +407,14 @@ wc_status PageRankRun::result(Ctx& ctx, double* ranks_dev_or_host, uint32_t* ite
   WC_CUDA(cudaMemcpy(&its, s.iterations, 4, cudaMemcpyDeviceToHost), ctx.detail);
   if (opts.max_iter == 0) its = 0;
   const double* final_x = s.x[its & 1];
-  WC_CUDA(cudaMemcpy(ranks_dev_or_host, final_x, ctx.v->n * 8, cudaMemcpyDefault), ctx.detail);
+  if (local) {
+    // Back to dense-id order, through the other rank buffer (free now).
+    WC_TRY(from_locality(ctx.v, ctx.stream, final_x, s.x[(its & 1) ^ 1]));
+    final_x = s.x[(its & 1) ^ 1];
+  }
+  WC_CUDA(cudaMemcpyAsync(ranks_dev_or_host, final_x, ctx.v->n * 8, cudaMemcpyDefault, ctx.stream),
+          ctx.detail);
+  WC_CUDA(cudaStreamSynchronize(ctx.stream), ctx.detail);
   if (iterations_out) *iterations_out = its;
   if (margin && its > 0) {
     double delta = 0.0;
@@ -396,7 +439,7 @@ wc_status wc_pagerank(wc_version* v, const wc_call* call, const wc_pagerank_opts
   if (ctx.cancelled()) return WC_CANCELLED;
   WC_TRY(ctx.begin());
   PageRankRun run;
-  WC_TRY(run.setup(ctx, o, tombstones, o->seed));
+  WC_TRY(run.setup(ctx, o, tombstones, o->seed, true));
   ctx.progress("iterating", 0, o->max_iter);
   WC_TRY(run.run(ctx));
   WC_TRY(ctx.finish());

@@ -32,16 +32,24 @@ struct PageRankRun {
   uint64_t live = 0;
   double nodes = 0.0;
   uint32_t grid = 1;
+  // The solve pulls over the version's locality-ordered CSC (v->loc), its
+  // vectors in that numbering; inputs are renumbered in by setup and the
+  // ranks out by result.  Off for callers that read the vectors themselves.
+  bool local = false;
   DevBuf *x = nullptr, *msg = nullptr, *out = nullptr, *shares = nullptr, *tomb = nullptr,
          *scalars = nullptr;
   PrState s;
 
   wc_status setup(Ctx& ctx, const wc_pagerank_opts* o, const uint64_t* tomb_host,
-                  const double* seed);
+                  const double* seed, bool in_locality_order = false);
+  // The CSC the iterations pull over and the grid for it.
+  const DevCsr& csc(const wc_version* v) const { return local ? v->loc.csc : v->rev; }
   wc_status run(Ctx& ctx);
   wc_status result(Ctx& ctx, double* ranks, uint32_t* iterations, double* margin);
 };
 
 uint64_t live_count(const uint64_t* tomb, uint64_t n);
+// Blocks of an iteration launch over `csc`.
+uint32_t pagerank_grid(const DevCsr& csc);
 
 }  // namespace wc

@@ -40,6 +40,7 @@ struct PullLaunch {
   DeviceError* err;
   wc_error_detail* detail;
   WriteArgs write;
+  uint32_t hot;  // over a locality-ordered CSC: gathers of j < hot kept in L1 (0: none)
 };
 
 wc_status launch_pull_f64(const PullLaunch& L, const void* x, void* y);

@@ -32,6 +32,9 @@ constexpr int kPullWarps = kPullThreads / 32;
 
 // One CSR orientation as the kernels read it.  W: double (f64 weights),
 // int32_t (the integral copy) or void (unweighted: every weight 1).
+// `hot`: over a locality-ordered CSC (nodes numbered by out-degree, largest
+// first), the gathers of x_j with j < hot are kept in L1 and the others
+// bypass it; 0 for a CSC in dense-id order (every gather as any other).
 template <class W> struct CsrView {
   const uint32_t* off;
   const uint32_t* tgt;
@@ -40,6 +43,7 @@ template <class W> struct CsrView {
   uint32_t unit_count;
   uint32_t* counters;
   void* carry;
+  uint32_t hot = 0;
 };
 template <> struct CsrView<void> {
   const uint32_t* off;
@@ -49,6 +53,7 @@ template <> struct CsrView<void> {
   uint32_t unit_count;
   uint32_t* counters;
   void* carry;
+  uint32_t hot = 0;
 };
 
 // An entry's weight as stored (WT), loaded apart from its product so the
@@ -84,6 +89,28 @@ template <class E, int S> struct EntryOf<E, S, void> {
 template <class E> __device__ inline E load_x(const E* x, uint32_t j) { return __ldg(x + j); }
 template <> __device__ inline bool8 load_x<bool8>(const bool8* x, uint32_t j) {
   return *(x + j);
+}
+
+// A gather over a locality-ordered CSC: the few most gathered values (j <
+// hot) are kept in L1, the rest are read past it so they do not evict those;
+// in L2 every value is kept ahead of the streamed CSR (`keep`: an
+// l2_evict_last_policy).  8-byte elements only; others take load_x.
+template <class E>
+__device__ inline E load_x_split(const E* x, uint32_t j, uint32_t hot, uint64_t keep) {
+  if constexpr (sizeof(E) == 8) {
+    unsigned long long b;
+    if (j < hot)
+      asm("ld.global.nc.L1::evict_last.L2::cache_hint.b64 %0, [%1], %2;"
+          : "=l"(b) : "l"(x + j), "l"(keep));
+    else
+      asm("ld.global.nc.L1::no_allocate.L2::cache_hint.b64 %0, [%1], %2;"
+          : "=l"(b) : "l"(x + j), "l"(keep));
+    E v;
+    memcpy(&v, &b, 8);
+    return v;
+  } else {
+    return load_x(x, j);
+  }
 }
 
 // An accumulator with a presence flag: the first entry sets the sum.
@@ -183,9 +210,11 @@ template <class E, class W> constexpr size_t pull_smem_bytes() {
 __device__ inline uint32_t unit_first(const Unit& d) { return (d.c >> 31) == 0 ? d.d : d.b; }
 __device__ inline uint32_t unit_count(const Unit& d) { return (d.c >> 31) == 0 ? d.c : d.d - d.b; }
 
-// Lane 0: fills buffer b with unit d.
+// Lane 0: fills buffer b with unit d, the CSR's spans streamed past L2's
+// kept lines (`stream`: an l2_evict_first_policy).
 template <class E, class W>
-__device__ inline void issue_unit(const CsrView<W>& A, PullRing<E, W>* ring, int b, const Unit& d) {
+__device__ inline void issue_unit(const CsrView<W>& A, PullRing<E, W>* ring, int b, const Unit& d,
+                                  uint64_t stream) {
   ring->desc[b] = d;
   const uint32_t e0 = unit_first(d), cnt = unit_count(d);
   const uint32_t ta = e0 & ~3u, tb = cnt ? (e0 + cnt + 3) & ~3u : ta;
@@ -204,11 +233,12 @@ __device__ inline void issue_unit(const CsrView<W>& A, PullRing<E, W>* ring, int
   const uint32_t oa = d.a & ~3u, ob = (d.b + 1 + 3) & ~3u;
   if (tile) bytes += (ob - oa) * 4;
   mbar_arrive_expect(&ring->bar[b], bytes);
-  if (tb > ta) bulk_load(ring->tgt[b], A.tgt + ta, (tb - ta) * 4, &ring->bar[b]);
+  if (tb > ta) bulk_load_hint(ring->tgt[b], A.tgt + ta, (tb - ta) * 4, &ring->bar[b], stream);
   if constexpr (WSize<W>::v != 0) {
-    if (wb > wa) bulk_load(ring->w[b].v, A.w + wa, (wb - wa) * WSize<W>::v, &ring->bar[b]);
+    if (wb > wa)
+      bulk_load_hint(ring->w[b].v, A.w + wa, (wb - wa) * WSize<W>::v, &ring->bar[b], stream);
   }
-  if (tile) bulk_load(ring->off[b], A.off + oa, (ob - oa) * 4, &ring->bar[b]);
+  if (tile) bulk_load_hint(ring->off[b], A.off + oa, (ob - oa) * 4, &ring->bar[b], stream);
 }
 
 // The weight of the k-th entry of the unit in buffer b.
@@ -223,18 +253,26 @@ __device__ inline typename EntryOf<E, S, W>::WT ring_weight(const PullRing<E, W>
 // Stages the products of the unit in buffer b (count <= 256 entries) in the
 // warp's stage: each lane gathers its (up to 8) x values at once, then forms
 // the products.
-template <class E, int S, class W>
+template <class E, int S, class W, bool SPLIT>
 __device__ inline void stage_products(const PullRing<E, W>* ring, int b, const E* __restrict__ x,
                                       uint32_t e0, uint32_t count, E* stage, DeviceError* err,
-                                      uint32_t row) {
+                                      uint32_t row, uint32_t hot, uint64_t keep) {
   const unsigned lane = threadIdx.x & 31;
   constexpr int Q = kTileEntries / 32;
   const uint32_t* tg = ring->tgt[b] + (e0 & 3u);
   E xv[Q];
+  if constexpr (SPLIT) {
 #pragma unroll
-  for (int q = 0; q < Q; q++) {
-    const uint32_t k = lane + 32 * q;
-    if (k < count) xv[q] = load_x(x, tg[k]);
+    for (int q = 0; q < Q; q++) {
+      const uint32_t k = lane + 32 * q;
+      if (k < count) xv[q] = load_x_split(x, tg[k], hot, keep);
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+      const uint32_t k = lane + 32 * q;
+      if (k < count) xv[q] = load_x(x, tg[k]);
+    }
   }
 #pragma unroll
   for (int q = 0; q < Q; q++) {
@@ -249,12 +287,13 @@ __device__ inline void stage_products(const PullRing<E, W>* ring, int b, const E
 }
 
 // Walks the schedule, a warp per unit, the units of a warp strided by the
-// grid's warp count, through the warp's staging ring.  The epilogue's
+// grid's warp count, through the warp's staging ring.  SPLIT: the CSC is in
+// locality order and A.hot splits the gathers (load_x_split).  The epilogue's
 // per-row operands (`epi.pre(row)`) are requested as a unit starts, so they
 // arrive with its gathers.  `epi.row(row, present, value, pre)` is called
 // exactly once per row, by one lane.  A ring wait that runs out (about 2 s)
 // raises WC_DEVICE_TIMEOUT and ends the walk after the copies in flight.
-template <class E, int S, class W, class Epi>
+template <class E, int S, class W, class Epi, bool SPLIT = false>
 __device__ inline void pull_units(const CsrView<W>& A, const E* __restrict__ x, Epi& epi,
                                   DeviceError* err, PullRing<E, W>* ring) {
   constexpr int R = PullRing<E, W>::R;
@@ -268,12 +307,15 @@ __device__ inline void pull_units(const CsrView<W>& A, const E* __restrict__ x, 
   if (lane == 0)
     for (int b = 0; b < R; b++) mbar_init(&ring->bar[b], 1);
   __syncwarp();
+  const uint64_t stream = l2_evict_first_policy();
+  uint64_t keep = 0;
+  if constexpr (SPLIT) keep = l2_evict_last_policy();
   Unit ahead{0u, 0u, 0u, 0u};  // lane 0: the next unit to issue
   uint32_t pending = 0;        // buffers with a copy in flight (uniform)
   for (int b = 0; b < R; b++) {
     const uint32_t u = warp + b * warps;
     if (u < A.unit_count) {
-      if (lane == 0) issue_unit(A, ring, b, A.units[u]);
+      if (lane == 0) issue_unit(A, ring, b, A.units[u], stream);
       pending |= 1u << b;
     }
   }
@@ -305,7 +347,7 @@ __device__ inline void pull_units(const CsrView<W>& A, const E* __restrict__ x, 
         hi = soff[lane + 1];
         pre = epi.pre(r0 + lane);
       }
-      stage_products<E, S, W>(ring, b, x, e0, count, ring->stage, err, r0);
+      stage_products<E, S, W, SPLIT>(ring, b, x, e0, count, ring->stage, err, r0, A.hot, keep);
       __syncwarp();
       if (lane < rows) {
         E sum{};
@@ -330,7 +372,7 @@ __device__ inline void pull_units(const CsrView<W>& A, const E* __restrict__ x, 
       const uint32_t row = unit.a, e0 = unit.b, e1 = unit.d;
       const uint32_t slot = unit.c & 0x7fffffffu;
       const uint32_t count = e1 - e0;
-      stage_products<E, S, W>(ring, b, x, e0, count, ring->stage, err, row);
+      stage_products<E, S, W, SPLIT>(ring, b, x, e0, count, ring->stage, err, row, A.hot, keep);
       __syncwarp();
       Partial<E, ADD> mine{Acc<E, ADD>::of(E{}), false};
       constexpr uint32_t per = kTileEntries / 32;
@@ -369,7 +411,7 @@ __device__ inline void pull_units(const CsrView<W>& A, const E* __restrict__ x, 
     const uint32_t un = u + R * warps;
     if (un < A.unit_count) {
       if (lane == 0) {
-        issue_unit(A, ring, b, ahead);
+        issue_unit(A, ring, b, ahead, stream);
         if (un + warps < A.unit_count) ahead = A.units[un + warps];
       }
       pending |= 1u << b;

@@ -216,6 +216,14 @@ struct DevCsr {
   uint32_t max_degree = 0;
 };
 
+// The reverse CSR in locality order (locality.cu): nodes renumbered by
+// out-degree, largest first; perm maps a dense id to its new number and
+// order a new number back to the dense id.
+struct Locality {
+  DevBuf perm, order;  // u32[n] each
+  DevCsr csc;
+};
+
 }  // namespace wc
 
 // The handle: one version's device copy, keyed by (graph, version).
@@ -230,6 +238,7 @@ struct wc_version {
   wc_budget* budget = nullptr;
   cudaStream_t stream = nullptr;
   wc::DevCsr fwd, rev;
+  wc::Locality loc;                    // rev renumbered for the pull solvers
   bool reverse_given = false;          // the caller uploaded a reverse CSR
   std::vector<uint64_t> host_offsets;  // forward offsets, for truncated-BFS stats
   std::vector<uint64_t> host_rev_offsets;
@@ -288,7 +297,9 @@ struct Ctx {
   wc_version* v;
   const wc_call* call;
   cudaStream_t stream;
-  wc_budget* budget;
+  wc_budget* budget;                  // the version's: the pool's device memory
+  wc_budget* call_budget = nullptr;   // the call's own (wc_call.memory), if any
+  uint64_t call_charged = 0;          // bytes charged to it by this call
   wc_error_detail* detail;
   bool async;
   uint32_t timeout_ms;
@@ -307,7 +318,7 @@ struct Ctx {
         async(false), timeout_ms(600000) {
     if (c) {
       if (c->stream) stream = (cudaStream_t)c->stream;
-      if (c->memory) budget = c->memory;
+      if (c->memory && c->memory != ver->budget) call_budget = c->memory;
       detail = c->detail;
       async = (c->flags & WC_CALL_ASYNC) != 0;
       timing = (c->flags & WC_CALL_TIMING) != 0;
@@ -315,6 +326,7 @@ struct Ctx {
     }
   }
   ~Ctx() {
+    if (call_budget && call_charged) uncharge(call_budget, call_charged);
     for (Timer& t : timers) {
       cudaEventDestroy(t.a);
       cudaEventDestroy(t.b);
@@ -411,11 +423,20 @@ struct Ctx {
   bool cancelled() const { return call && call->cancel && *call->cancel; }
 
   // Pooled scratch of at least `bytes` under `tag` (contents undefined).
+  // The device allocation belongs to the version's pool and is charged to
+  // the version's budget while the pool holds it.  A call given its own
+  // budget (wc_call.memory) is also charged the bytes it uses, for the
+  // call's duration, as the reference charges a call's ComputeMemory; a
+  // refusal there is WC_MEMORY_LIMIT before anything is allocated.
   wc_status scratch(int tag, uint64_t bytes, DevBuf** out) {
+    if (call_budget) {
+      WC_TRY(charge(call_budget, bytes, detail));
+      call_charged += bytes;
+    }
     DevBuf& b = v->pool[tag];
     if (b.bytes < bytes) {
       b.release();
-      WC_TRY(b.alloc(v->budget, bytes + bytes / 8, detail));
+      WC_TRY(b.alloc(budget, bytes + bytes / 8, detail));
     }
     *out = &b;
     return WC_OK;
@@ -455,6 +476,9 @@ struct Ctx {
       if (ms >= 2) std::this_thread::sleep_for(std::chrono::microseconds(20));
       else std::this_thread::yield();
     }
+    // A cancel raised while the call ran is reported even when the device
+    // finished first (the reference's last check before it returns).
+    if (!cancel && cancelled()) cancel = true;
     collect_timings();
     DeviceError e;
     WC_CUDA(cudaMemcpy(&e, v->error.ptr, sizeof e, cudaMemcpyDeviceToHost), detail);

@@ -3,6 +3,8 @@
 // segments).
 #pragma once
 
+#include <vector>
+
 #include "runtime.cuh"
 
 namespace wc {
@@ -18,7 +20,20 @@ wc_status device_weight_facts(wc_version* v, wc_error_detail* detail);
 // Whether the forward and reverse CSR are equal, weights included.
 wc_status device_symmetric(wc_version* v, wc_error_detail* detail);
 // With both orientations on the device: the weights' facts, the symmetry
-// test, the row-split schedules, the error word and the mapped words.
+// test, the row-split schedules, the locality-ordered reverse CSR, the error
+// word and the mapped words.
 wc_status finish_version(wc_version* v, wc_error_detail* detail);
+// The row-split schedule of one orientation from its host offsets.
+wc_status put_schedule(wc_version* v, DevCsr& d, const std::vector<uint64_t>& off,
+                       wc_error_detail* detail);
+// The reverse CSR in locality order (v->loc), after the weights' facts.
+wc_status device_locality(wc_version* v, wc_error_detail* detail);
+// Vectors between dense ids and the locality numbering, on `st`:
+// dst[perm[i]] = src[i] (in), dst[i] = src[perm[i]] (out), and a NodeSet's
+// bits renumbered (dst is cleared first).
+wc_status to_locality(const wc_version* v, cudaStream_t st, const double* src, double* dst);
+wc_status from_locality(const wc_version* v, cudaStream_t st, const double* src, double* dst);
+wc_status bits_to_locality(const wc_version* v, cudaStream_t st, const uint64_t* src,
+                           uint64_t* dst);
 
 }  // namespace wc

@@ -88,7 +88,7 @@ static wc_status put_csr(wc_version* v, DevCsr& d, const uint64_t* off, const ui
 }
 
 // The schedule of one orientation from its host offsets.
-static wc_status put_schedule(wc_version* v, DevCsr& d, const std::vector<uint64_t>& off,
+wc_status put_schedule(wc_version* v, DevCsr& d, const std::vector<uint64_t>& off,
                               wc_error_detail* detail) {
   std::vector<Unit> units;
   Schedule& s = d.schedule;
@@ -128,6 +128,7 @@ wc_status finish_version(wc_version* v, wc_error_detail* detail) {
   WC_TRY(device_symmetric(v, detail));
   WC_TRY(put_schedule(v, v->fwd, v->host_offsets, detail));
   WC_TRY(put_schedule(v, v->rev, v->host_rev_offsets, detail));
+  WC_TRY(device_locality(v, detail));
   WC_TRY(v->error.alloc(v->budget, sizeof(DeviceError), detail));
   WC_CUDA(cudaMemset(v->error.ptr, 0, sizeof(DeviceError)), detail);
   // Four mapped words: the cancel word, then the pacing words (iterations
@@ -272,10 +273,14 @@ wc_status wc_version_info_get(const wc_version* v, wc_version_info* info) {
   info->id_space = v->n;
   info->edges = v->m;
   uint64_t bytes = 0;
-  for (const DevCsr* d : {&v->fwd, &v->rev})
+  for (const DevCsr* d : {&v->fwd, &v->rev, &v->loc.csc})
     bytes += d->offsets.bytes + d->targets.bytes + d->weights.bytes + d->iweights.bytes +
              d->schedule.units.bytes + d->schedule.counters.bytes + d->schedule.carry.bytes;
+  bytes += v->loc.perm.bytes + v->loc.order.bytes;
   info->device_bytes = bytes;
+  uint64_t pooled = 0;
+  for (const auto& kv : v->pool) pooled += kv.second.bytes;
+  info->scratch_bytes = pooled;
   info->weighted = v->weighted;
   info->integral_weights = v->integral;
   info->device = v->device;

@@ -68,6 +68,42 @@ def test_bfs_batched_ragged_sizes_deep_caps_and_a_wide_hub(width, cap_hi):
     assert np.array_equal(e, eo)
 
 
+def path_version(n):
+    """The path 0 -> 1 -> ... -> n-1."""
+    offsets = np.minimum(np.arange(n + 1), n - 1).astype(np.uint64)
+    targets = np.arange(1, n).astype(np.uint32)
+    return O.Graph.from_csr(n, offsets, targets, reverse=False), W.GraphVersion(offsets, targets)
+
+
+def test_bfs_batched_caps_above_254_are_served_or_refused_never_cut_short():
+    # Depths are bytes (255: not reached), so a pass runs 254 levels at most.
+    # traversal/level.rs:119-123 and limits.rs:8: a cap is any u32.  A search
+    # that ends within 254 levels is served whatever its cap; one that still
+    # expands at depth 254 with a deeper cap is refused (Unsupported), so
+    # the adapter keeps the native search, rather than answered with 255s.
+    og, gv = path_version(300)
+    with pytest.raises(W.Unsupported):
+        W.bfs_batched(gv, [0], [300])
+    with pytest.raises(W.Unsupported):  # one offending source among many
+        src = np.arange(40, dtype=np.uint64) + 10
+        caps = np.full(40, 16, np.uint32)
+        caps[7] = 1000
+        src[7] = 0
+        W.bfs_batched(gv, src, caps)
+    # Cap 254 from 0 stops at node 254; from 50 and 100 the path ends at
+    # depths 249 and 199, below their caps of 300 and 2^32 - 1.
+    src = np.array([0, 0, 50, 100], np.uint64)
+    caps = np.array([254, 100, 300, 2**32 - 1], np.uint32)
+    d, e = W.bfs_batched(gv, src, caps)
+    do, eo = O.bfs_depths(og, src, caps)
+    assert np.array_equal(d, do) and np.array_equal(e, eo)
+    assert d[0, 254] == 254 and d[0, 255] == 255 and d[2, 299] == 249 and d[3, 299] == 199
+    og2, gv2 = path_version(200)
+    d, e = W.bfs_batched(gv2, [0], [2**32 - 1])
+    do, eo = O.bfs_depths(og2, np.array([0], np.uint64), np.array([2**32 - 1], np.uint32))
+    assert np.array_equal(d, do) and np.array_equal(e, eo) and d[0, 199] == 199
+
+
 def test_bfs_batched_autotuned_schedules_agree():
     g, og, gv = graph(15)
     rng = np.random.default_rng(3)
