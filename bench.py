@@ -362,6 +362,36 @@ def _spmv_sweep(W, O, torch, dev, stream, peak, g, cpu):
     return out
 
 
+def spmv_point(W, torch, dev, stream, peak, g):
+    """plus_times f64 over the reverse CSR (pull, the reference's transpose
+    product), R-MAT 22, 20 iterations from a 1% vector: spmv_pull_kernel's
+    fraction of the roofline, bytes 4(n+1) + 12m + 16n an iteration."""
+    n, m = g.id_space, g.edges
+    rng = np.random.default_rng(SEED)
+    w = 1.0 - rng.random(m)
+    gv = W.GraphVersion(g.offsets, g.targets, w)
+    x0 = torch.as_tensor(np.where(rng.random(n) < 0.01, 1.0, 0.0), device=dev)
+    prod = W.Product("plus_times", transpose=True)
+    x, y = x0.clone(), torch.empty_like(x0)
+    for _ in range(3):
+        W.spmv(gv, prod, x, y, stream=stream.cuda_stream, asynchronous=True)
+    torch.cuda.synchronize(dev)
+    a, b = _events(torch)
+    a.record(stream)
+    for _ in range(20):
+        W.spmv(gv, prod, x, y, stream=stream.cuda_stream, asynchronous=True)
+        x, y = y, x
+    b.record(stream)
+    b.synchronize()
+    W.load().wc_version_sync(gv.handle, None)
+    ms = a.elapsed_time(b) / 20
+    bytes_it = 4 * (n + 1) + 12 * m + 16 * n
+    gbs = bytes_it / (ms * 1e-3) / 1e9
+    return {"kernel": "spmv_pull_kernel", "semiring": "plus_times", "dtype": "f64",
+            "us_per_iteration": ms * 1e3, "bytes_per_iteration": bytes_it,
+            "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak}
+
+
 def leg_c2(W, O, torch, dev, stream, peak):
     """Semiring SpMV sweep: R-MAT 22 and G(n,m) of the same n and m."""
     g = W.rmat(22)
@@ -373,10 +403,10 @@ def leg_c2(W, O, torch, dev, stream, peak):
     return res
 
 
-def leg_c3(W, O, torch, dev, stream, peak):
+def leg_c3(W, O, torch, dev, stream, peak, g=None):
     """Batched min-plus (1,024 sources, int32 weights 1..100, caps U{1..16})
     and 256 personalised PageRank seed sets (sizes log-uniform 1..1000)."""
-    g = W.rmat(22)
+    g = g if g is not None else W.rmat(22)
     n, m = g.id_space, g.edges
     rng = np.random.default_rng(SEED)
     wi = rng.integers(1, 101, m).astype(np.float64)
@@ -429,6 +459,7 @@ def leg_c3(W, O, torch, dev, stream, peak):
     W.ppr_batched(gu, sets, W.PageRank(0.85, 1e-10, 100), ranks_out=r, iterations_out=pit)
     torch.cuda.synchronize(dev)
     ppr_s = time.perf_counter() - t0
+    del r
     seeds = []
     for q in range(8):
         seed = torch.zeros(n, dtype=torch.float64, device=dev)
@@ -908,6 +939,13 @@ def main():
                              "frac": pr_kernel_gbs / peak,
                              "bytes_per_iteration": pr_bytes}}
 
+    # ---- beside the headline: the SpMV's fraction, the batched min-plus
+    # and personalised PageRank against their plain per-source paths (the
+    # batched-traversal configuration's other two workloads)
+    spmv = spmv_point(W, torch, dev, stream, peak, g)
+    c3 = leg_c3(W, None, torch, dev, stream, peak, g=g)
+    torch.cuda.empty_cache()
+
     # ---- end to end through the public call, host buffers
     src_h = torch.from_numpy(src.view(np.int64)).pin_memory()
     caps_h = torch.from_numpy(caps.view(np.int32)).pin_memory()
@@ -977,6 +1015,9 @@ def main():
         "batched_vs_plain": batched_gteps_rank / plain_gteps,
         "pagerank_iters_per_s": pagerank["iters_per_s"],
         "pagerank": pagerank,
+        "spmv": spmv,
+        "minplus_batched": c3["minplus"],
+        "ppr_batched": c3["ppr"],
     }
     if rank == 0:
         print(json.dumps(line))

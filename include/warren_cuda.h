@@ -346,6 +346,49 @@ wc_status wc_pagerank_noalloc(wc_version* version, const wc_call* call,
                               const wc_pagerank_opts* opts, const uint64_t* tombstones,
                               double* ranks, uint32_t* iterations);
 
+/* No reference counterpart (warren-core solves on one host): one rank's part
+ * of a row-partitioned PageRank over several GPUs.  The solve's rows (the
+ * numbering wc_pagerank iterates in: nodes by out-degree, largest first) are
+ * cut into `parts` ranges of about equal entries; every rank holds the whole
+ * version and pulls its range each iteration, and between iterations the
+ * caller sums the parts' L1 changes and dangling ranks and gathers the
+ * parts' rows of the next message vector (one all-reduce of two scalars and
+ * one all-gather of 8·id_space bytes an iteration, over NCCL).  Results
+ * equal wc_pagerank's within the PageRank tolerance (the sums are grouped by
+ * part), with equal iteration counts.
+ *
+ * wc_pagerank_part_rows: the parts' first rows, row_bounds[parts + 1]. */
+wc_status wc_pagerank_part_rows(wc_version* version, uint32_t parts, uint64_t* row_bounds);
+
+typedef struct wc_pagerank_part_info {
+    uint64_t row_begin, row_end;  /* this part's rows in the solve's numbering */
+    uint64_t id_space;
+    uint64_t live;                /* live (untombstoned) nodes */
+    double dangling;              /* iteration 0's dangling rank (the same on every part) */
+    double threshold;             /* stop when the summed L1 change is below this (0: no tol) */
+} wc_pagerank_part_info;
+
+/* Sets up part `part` of `parts`: ranks2 and messages2 are the caller's
+ * device vectors, 2 × id_space doubles each (even and odd iterations, the
+ * solve's numbering); every row of ranks2[0..n) and messages2[0..n) gets
+ * the start vector and its messages.  Tombstones as wc_pagerank's;
+ * personalised solves are WC_UNSUPPORTED. */
+wc_status wc_pagerank_part_begin(wc_version* version, const wc_call* call,
+                                 const wc_pagerank_opts* opts, const uint64_t* tombstones,
+                                 uint32_t parts, uint32_t part, double* ranks2,
+                                 double* messages2, wc_pagerank_part_info* info);
+/* Iteration `iteration` over the part's rows, given that iteration's summed
+ * dangling rank: reads messages2[iteration & 1] (every row), writes the
+ * part's rows of ranks2 and messages2 [(iteration + 1) & 1], waits, and
+ * returns the part's L1 change and next dangling rank in sums[0], sums[1]. */
+wc_status wc_pagerank_part_step(wc_version* version, const wc_call* call, uint32_t iteration,
+                                double dangling, double* sums);
+/* After `iterations` iterations, with every part's rows of
+ * ranks2[iterations & 1] gathered by the caller: the ranks in dense-id
+ * order (host or device), as wc_pagerank returns them.  Ends the part. */
+wc_status wc_pagerank_part_end(wc_version* version, const wc_call* call, uint32_t iterations,
+                               double* ranks);
+
 /* The stop test's margin of the last iteration run: delta / (live × tol).
  * Available after wc_pagerank on the same version (diagnostics). */
 double wc_pagerank_last_margin(const wc_version* version);

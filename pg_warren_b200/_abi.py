@@ -105,6 +105,11 @@ class EigenStats(C.Structure):
     _fields_ = [("iterations", U64), ("components", U64), ("exact", U32), ("converged", I32)]
 
 
+class PageRankPartInfo(C.Structure):
+    _fields_ = [("row_begin", U64), ("row_end", U64), ("id_space", U64), ("live", U64),
+                ("dangling", D), ("threshold", D)]
+
+
 class HostCsr(C.Structure):
     _fields_ = [("id_space", U64), ("edges", U64), ("offsets", C.POINTER(U64)),
                 ("targets", C.POINTER(U32)), ("external_ids", C.POINTER(C.c_int64))]
@@ -134,6 +139,11 @@ SIGNATURES = [
     ("wc_pagerank_noalloc", I32, [P, C.POINTER(Call), C.POINTER(PageRankOpts), P, P,
                              C.POINTER(U32)]),
     ("wc_pagerank_last_margin", D, [P]),
+    ("wc_pagerank_part_rows", I32, [P, U32, P]),
+    ("wc_pagerank_part_begin", I32, [P, C.POINTER(Call), C.POINTER(PageRankOpts), P, U32, U32,
+                                     P, P, C.POINTER(PageRankPartInfo)]),
+    ("wc_pagerank_part_step", I32, [P, C.POINTER(Call), U32, D, C.POINTER(D)]),
+    ("wc_pagerank_part_end", I32, [P, C.POINTER(Call), U32, P]),
     ("wc_bfs", I32, [P, C.POINTER(Call), I32, P, U64, C.POINTER(Limits), P, P, P,
                      C.POINTER(TraversalStats)]),
     ("wc_bfs_visits", I32, [P, C.POINTER(Call), I32, P, U64, C.POINTER(Limits), P, P, U64,

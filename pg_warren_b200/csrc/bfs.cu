@@ -26,13 +26,37 @@ namespace wc {
 
 __device__ inline bool bit_at(const uint32_t* b, uint32_t i) { return (b[i >> 5] >> (i & 31)) & 1; }
 
-struct LevelCounters {
-  unsigned long long next_deg;   // Σ row length (search direction) over nodes admitted
-  unsigned long long next_rdeg;  // Σ row length (opposite direction) over nodes admitted
-  unsigned long long edges;      // row entries scanned by a pulled level
+// The device side of one level, indexed by the level within the chunk the
+// host queued: what the level's kernels read (its frontier and the switch's
+// choice) and what they add up for the next level.
+struct LevelState {
+  uint32_t count;                 // frontier nodes
+  uint32_t pull;                  // the level pulls
+  unsigned long long mf;          // Σ row length (search direction) of the frontier
+  unsigned long long visited_rdeg;  // Σ opposite-direction row length of the visited nodes
+  // Added up by the level's kernels:
+  unsigned long long next_deg;    // Σ row length (search direction) over nodes admitted
+  unsigned long long next_rdeg;   // Σ row length (opposite direction) over nodes admitted
+  unsigned long long edges;       // row entries scanned by a pulled level
   uint32_t next_count;
-  uint32_t pad;
+  uint32_t big_count;             // frontier rows deferred to push_big_kernel
 };
+
+// The switch (level.rs:19-29, 184-211 for the reference's; a GPU-tuned one
+// for bfs), evaluated where the level is planned.
+struct SwitchArgs {
+  uint32_t rule;  // SwitchRule
+  uint32_t reverse_allowed;
+  uint64_t n;
+  uint64_t total_rdeg;
+};
+
+__host__ __device__ inline bool level_pulls(const SwitchArgs& a, uint64_t count, uint64_t mf,
+                                            uint64_t visited_rdeg) {
+  const uint64_t mu = a.total_rdeg - visited_rdeg;
+  if (a.rule == REFERENCE_SWITCH) return a.reverse_allowed && count * 24 > a.n && mu < mf;
+  return count * 24 > a.n && mf * 14 > mu;
+}
 
 struct Rows {  // the rows read in one direction: one CSR, or two for Both
   const uint32_t* off0;
@@ -46,10 +70,10 @@ struct Rows {  // the rows read in one direction: one CSR, or two for Both
   }
 };
 
-// Appends v to the next frontier: one atomic per warp for the lanes that
-// admit a node this round.
-__device__ inline void admit(uint32_t v, bool take, uint32_t* next, LevelCounters* c,
-                             const Rows& adj, const Rows& radj) {
+// Appends v to the next frontier and marks it in the next frontier's
+// bitmap: one atomic per warp for the lanes that admit a node this round.
+__device__ inline void admit(uint32_t v, bool take, uint32_t* next, uint32_t* fnext,
+                             LevelState* c, const Rows& adj, const Rows& radj) {
   const unsigned mask = __ballot_sync(0xffffffffu, take);
   if (!mask) return;
   const unsigned lane = threadIdx.x & 31;
@@ -60,6 +84,7 @@ __device__ inline void admit(uint32_t v, bool take, uint32_t* next, LevelCounter
   unsigned long long d = 0, rd = 0;
   if (take) {
     next[base + __popc(mask & ((1u << lane) - 1))] = v;
+    atomicOr(fnext + (v >> 5), 1u << (v & 31));
     d = adj.degree(v);
     rd = radj.degree(v);
   }
@@ -73,19 +98,55 @@ __device__ inline void admit(uint32_t v, bool take, uint32_t* next, LevelCounter
   }
 }
 
-// Push: a warp per frontier node, lanes over its row entries.
-__global__ void __launch_bounds__(256) push_kernel(Rows adj, Rows radj, const uint32_t* frontier,
-                                                   uint32_t count, uint32_t depth_next,
-                                                   uint32_t* depth, unsigned long long* via,
-                                                   const uint64_t* filter, uint32_t* next,
-                                                   LevelCounters* c) {
+// What every kernel of a level is given.
+struct LevelArgs {
+  Rows adj, radj;
+  LevelState* st;        // this level's state (st + 1: the next level's)
+  const uint32_t* frontier;
+  uint32_t* next;
+  const uint32_t* fbits;  // this level's frontier as a bitmap
+  uint32_t* fnext;        // the next level's bitmap (cleared)
+  uint32_t* big;          // frontier rows too long for one warp
+  uint32_t depth_next;
+  uint32_t n;
+  uint32_t* depth;
+  unsigned long long* via;
+  const uint64_t* filter;
+};
+
+// Levels queued per round trip to the host.
+constexpr uint32_t kChunkLevels = 16;
+
+// Rows longer than this are pushed by the whole grid (push_big_kernel):
+// one warp per row would leave a hub's row to a single warp.
+constexpr uint32_t kBigRow = 2048;
+
+// One entry of a push: target v offered by frontier node u.
+__device__ inline bool offer(const LevelArgs& a, uint32_t u, uint32_t v) {
+  const bool allowed = !a.filter || ((a.filter[v >> 6] >> (v & 63)) & 1);
+  if (!allowed) return false;
+  const uint32_t d = a.depth[v];
+  if (d != WC_UNREACHED && d != a.depth_next) return false;
+  atomicMin(a.via + v, (unsigned long long)u);
+  return d == WC_UNREACHED && atomicCAS(a.depth + v, WC_UNREACHED, a.depth_next) == WC_UNREACHED;
+}
+
+// Push: a warp per frontier node, lanes over its row entries; rows longer
+// than kBigRow are listed for push_big_kernel instead.
+__global__ void __launch_bounds__(256) push_kernel(LevelArgs a) {
+  const LevelState& st = *a.st;
+  if (st.count == 0 || st.pull) return;
   const unsigned lane = threadIdx.x & 31;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; f < count; f += warps) {
-    const uint32_t u = frontier[f];
+  for (uint32_t f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; f < st.count; f += warps) {
+    const uint32_t u = a.frontier[f];
+    if (a.adj.degree(u) > kBigRow) {
+      if (lane == 0) a.big[atomicAdd(&a.st->big_count, 1u)] = u;
+      continue;
+    }
     for (int part = 0; part < 2; part++) {
-      const uint32_t* off = part == 0 ? adj.off0 : adj.off1;
-      const uint32_t* tgt = part == 0 ? adj.tgt0 : adj.tgt1;
+      const uint32_t* off = part == 0 ? a.adj.off0 : a.adj.off1;
+      const uint32_t* tgt = part == 0 ? a.adj.tgt0 : a.adj.tgt1;
       if (!off) break;
       const uint32_t lo = __ldg(off + u), hi = __ldg(off + u + 1);
       for (uint32_t e0 = lo; e0 < hi; e0 += 32) {
@@ -94,16 +155,38 @@ __global__ void __launch_bounds__(256) push_kernel(Rows adj, Rows radj, const ui
         uint32_t v = 0;
         if (e < hi) {
           v = __ldg(tgt + e);
-          bool allowed = !filter || ((filter[v >> 6] >> (v & 63)) & 1);
-          if (allowed) {
-            uint32_t d = depth[v];
-            if (d == WC_UNREACHED || d == depth_next) {
-              atomicMin(via + v, (unsigned long long)u);
-              if (d == WC_UNREACHED) take = atomicCAS(depth + v, WC_UNREACHED, depth_next) == WC_UNREACHED;
-            }
-          }
+          take = offer(a, u, v);
         }
-        admit(v, take, next, c, adj, radj);
+        admit(v, take, a.next, a.fnext, a.st, a.adj, a.radj);
+      }
+    }
+  }
+}
+
+// Push of the long rows: each row's entries spread over every warp of the
+// grid, the rows one after another.
+__global__ void __launch_bounds__(256) push_big_kernel(LevelArgs a) {
+  const LevelState& st = *a.st;
+  if (st.count == 0 || st.pull || st.big_count == 0) return;
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t b = 0; b < st.big_count; b++) {
+    const uint32_t u = a.big[b];
+    for (int part = 0; part < 2; part++) {
+      const uint32_t* off = part == 0 ? a.adj.off0 : a.adj.off1;
+      const uint32_t* tgt = part == 0 ? a.adj.tgt0 : a.adj.tgt1;
+      if (!off) break;
+      const uint32_t lo = __ldg(off + u), hi = __ldg(off + u + 1);
+      for (uint32_t e0 = lo + 32 * warp; e0 < hi; e0 += 32 * warps) {
+        const uint32_t e = e0 + lane;
+        bool take = false;
+        uint32_t v = 0;
+        if (e < hi) {
+          v = __ldg(tgt + e);
+          take = offer(a, u, v);
+        }
+        admit(v, take, a.next, a.fnext, a.st, a.adj, a.radj);
       }
     }
   }
@@ -114,29 +197,28 @@ __global__ void __launch_bounds__(256) push_kernel(Rows adj, Rows radj, const ui
 // smallest first hit of the two rows is `via` (what a push finds), while
 // `edges` counts entries as the reference's pull scans them: the first row
 // to its hit, or all of it and the second to its hit.
-__global__ void __launch_bounds__(256) pull_kernel(Rows adj, Rows radj, uint32_t n,
-                                                   const uint32_t* fbits, uint32_t depth_next,
-                                                   uint32_t* depth, unsigned long long* via,
-                                                   const uint64_t* filter, uint32_t* next,
-                                                   LevelCounters* c, int count_edges) {
+__global__ void __launch_bounds__(256) pull_kernel(LevelArgs a, int count_edges) {
+  const LevelState& st = *a.st;
+  if (st.count == 0 || !st.pull) return;
   unsigned long long scanned = 0;
+  const uint32_t n = a.n;
   const uint32_t stride = gridDim.x * blockDim.x;
   const uint32_t rounds = (n + stride - 1) / stride;
   for (uint32_t r = 0; r < rounds; r++) {
     const uint32_t v = r * stride + blockIdx.x * blockDim.x + threadIdx.x;
     bool take = false;
-    if (v < n && depth[v] == WC_UNREACHED && (!filter || ((filter[v >> 6] >> (v & 63)) & 1))) {
+    if (v < n && a.depth[v] == WC_UNREACHED && (!a.filter || ((a.filter[v >> 6] >> (v & 63)) & 1))) {
       uint64_t best = WC_NO_VIA;
       bool counting = true;
       for (int part = 0; part < 2; part++) {
-        const uint32_t* off = part == 0 ? radj.off0 : radj.off1;
-        const uint32_t* tgt = part == 0 ? radj.tgt0 : radj.tgt1;
+        const uint32_t* off = part == 0 ? a.radj.off0 : a.radj.off1;
+        const uint32_t* tgt = part == 0 ? a.radj.tgt0 : a.radj.tgt1;
         if (!off) break;
         const uint32_t lo = __ldg(off + v), hi = __ldg(off + v + 1);
         for (uint32_t e = lo; e < hi; e++) {
           const uint32_t u = __ldg(tgt + e);
           if (counting) scanned++;
-          if (bit_at(fbits, u)) {
+          if (bit_at(a.fbits, u)) {
             if (u < best) best = u;
             counting = false;
             break;
@@ -144,16 +226,34 @@ __global__ void __launch_bounds__(256) pull_kernel(Rows adj, Rows radj, uint32_t
         }
       }
       if (best != WC_NO_VIA) {
-        depth[v] = depth_next;
-        via[v] = best;
+        a.depth[v] = a.depth_next;
+        a.via[v] = best;
         take = true;
       }
     }
-    admit(v, take, next, c, adj, radj);
+    admit(v, take, a.next, a.fnext, a.st, a.adj, a.radj);
   }
   if (count_edges) {
     for (int o = 16; o > 0; o >>= 1) scanned += __shfl_down_sync(0xffffffffu, scanned, o);
-    if ((threadIdx.x & 31) == 0 && scanned) atomicAdd(&c->edges, scanned);
+    if ((threadIdx.x & 31) == 0 && scanned) atomicAdd(&a.st->edges, scanned);
+  }
+}
+
+// Closes a level: plans the next (its frontier, the switch's choice; an
+// empty frontier past the depth cap or once the call is cancelled) and
+// clears the bitmap the level after it will fill.
+__global__ void level_end_kernel(LevelState* st, SwitchArgs sw, uint32_t next_is_last,
+                                 uint32_t* fclear, uint32_t words, const int32_t* cancel) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += gridDim.x * blockDim.x)
+    fclear[i] = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const LevelState& cur = st[0];
+    LevelState& nx = st[1];
+    const bool stop = cur.count == 0 || next_is_last || *(volatile const int32_t*)cancel;
+    nx.count = stop ? 0u : cur.next_count;
+    nx.mf = cur.next_deg;
+    nx.visited_rdeg = cur.visited_rdeg + cur.next_rdeg;
+    nx.pull = nx.count && level_pulls(sw, nx.count, nx.mf, nx.visited_rdeg);
   }
 }
 
@@ -244,8 +344,10 @@ wc_status Search::run(Ctx& ctx, int dir, const uint64_t* starts_in, uint64_t sta
   WC_TRY(ctx.scratch(POOL_BFS_VIA, n * 8, &via));
   WC_TRY(ctx.scratch(POOL_BFS_Q0, std::max<uint64_t>(n, 1) * 4, &queue[0]));
   WC_TRY(ctx.scratch(POOL_BFS_Q1, std::max<uint64_t>(n, 1) * 4, &queue[1]));
-  WC_TRY(ctx.scratch(POOL_BFS_FBITS, ((n + 31) / 32) * 4, &fbits));
-  WC_TRY(ctx.scratch(POOL_BFS_COUNTERS, sizeof(LevelCounters), &counters));
+  const uint64_t words = (n + 31) / 32;
+  WC_TRY(ctx.scratch(POOL_BFS_FBITS, std::max<uint64_t>(words, 1) * 4 * 2, &fbits));
+  WC_TRY(ctx.scratch(POOL_BFS_COUNTERS, (kChunkLevels + 1) * sizeof(LevelState), &counters));
+  WC_TRY(ctx.scratch(POOL_BFS_BIG, (v->m / kBigRow + 2) * 4 * (dir == WC_BOTH ? 2 : 1), &big));
   const uint64_t* filter_dev = nullptr;
   if (filter_host) {
     WC_TRY(ctx.scratch(POOL_BFS_FILTER, ((n + 63) / 64) * 8, &filter));
@@ -255,12 +357,17 @@ wc_status Search::run(Ctx& ctx, int dir, const uint64_t* starts_in, uint64_t sta
   }
   WC_CUDA(cudaMemsetAsync(depth->ptr, 0xff, n * 4, ctx.stream), ctx.detail);
   WC_CUDA(cudaMemsetAsync(via->ptr, 0xff, n * 8, ctx.stream), ctx.detail);
+  WC_CUDA(cudaMemsetAsync(fbits->ptr, 0, std::max<uint64_t>(words, 1) * 4 * 2, ctx.stream),
+          ctx.detail);
   const uint32_t count0 = (uint32_t)seeds.size();
+  uint32_t* fb[2] = {fbits->as<uint32_t>(), fbits->as<uint32_t>() + std::max<uint64_t>(words, 1)};
   if (count0) {
     WC_CUDA(cudaMemcpyAsync(queue[0]->ptr, seeds.data(), count0 * 4, cudaMemcpyHostToDevice,
                             ctx.stream), ctx.detail);
     note_launch(), seed_kernel<<<(count0 + 255) / 256, 256, 0, ctx.stream>>>(queue[0]->as<uint32_t>(), count0,
                                                              depth->as<uint32_t>());
+    note_launch(), set_bits_kernel<<<(count0 + 255) / 256, 256, 0, ctx.stream>>>(
+        queue[0]->as<uint32_t>(), count0, fb[0]);
   }
   const Rows adj = rows_of(v, dir);
   const int rdir = dir == WC_OUT ? WC_IN : (dir == WC_IN ? WC_OUT : WC_BOTH);
@@ -273,49 +380,61 @@ wc_status Search::run(Ctx& ctx, int dir, const uint64_t* starts_in, uint64_t sta
     mf += host_degree(v, dir, s);
     visited_rdeg += host_degree(v, rdir, s);
   }
+  const SwitchArgs sw{(uint32_t)rule, (uint32_t)reverse_allowed, n, total_rdeg};
   stats = wc_traversal_stats{};
   stats.nodes_visited = count0;
   levels.clear();
-  uint32_t count = count0, cur = 0, d = 0;
+  // The levels are queued kChunkLevels at a time with no round trip: each
+  // level's kernels read its plan from the device (level_end_kernel writes
+  // it), and those of a level with no frontier return at once.  The host
+  // reads the chunk's plans back once, to go on or stop and for the stats.
+  LevelState first{};
+  first.count = max_depth > 0 ? count0 : 0;
+  first.mf = mf;
+  first.visited_rdeg = visited_rdeg;
+  first.pull = first.count && level_pulls(sw, first.count, mf, visited_rdeg);
+  LevelState* st = counters->as<LevelState>();
   const uint32_t blocks = max_blocks(8);
-  while (count > 0 && d < max_depth) {
+  const uint32_t pull_grid = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)((n + 255) / 256), blocks));
+  const uint32_t end_grid = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)((words + 255) / 256), blocks));
+  uint32_t d = 0;
+  std::vector<LevelState> plan(kChunkLevels + 1);
+  while (first.count > 0 && d < max_depth) {
     if (ctx.cancelled()) return WC_CANCELLED;
-    const uint64_t mu = total_rdeg - visited_rdeg;
-    bool pull;
-    if (rule == REFERENCE_SWITCH)
-      pull = reverse_allowed && (uint64_t)count * 24 > n && mu < mf;
-    else
-      pull = (uint64_t)count * 24 > n && mf * 14 > mu;
-    WC_CUDA(cudaMemsetAsync(counters->ptr, 0, sizeof(LevelCounters), ctx.stream), ctx.detail);
-    LevelCounters* c = counters->as<LevelCounters>();
-    uint32_t* frontier = queue[cur]->as<uint32_t>();
-    uint32_t* next = queue[cur ^ 1]->as<uint32_t>();
-    if (pull) {
-      WC_CUDA(cudaMemsetAsync(fbits->ptr, 0, ((n + 31) / 32) * 4, ctx.stream), ctx.detail);
-      note_launch(), set_bits_kernel<<<std::min<uint32_t>((count + 255) / 256, blocks), 256, 0, ctx.stream>>>(
-          frontier, count, fbits->as<uint32_t>());
-      note_launch(), pull_kernel<<<std::min<uint32_t>((uint32_t)((n + 255) / 256), blocks), 256, 0, ctx.stream>>>(
-          adj, radj, (uint32_t)n, fbits->as<uint32_t>(), d + 1, depth->as<uint32_t>(),
-          via->as<unsigned long long>(), filter_dev, next, c, 1);
-    } else {
-      note_launch(), push_kernel<<<std::min<uint32_t>((count + 7) / 8, blocks), 256, 0, ctx.stream>>>(
-          adj, radj, frontier, count, d + 1, depth->as<uint32_t>(), via->as<unsigned long long>(),
-          filter_dev, next, c);
+    WC_CUDA(cudaMemsetAsync(st, 0, (kChunkLevels + 1) * sizeof(LevelState), ctx.stream), ctx.detail);
+    WC_CUDA(cudaMemcpyAsync(st, &first, sizeof first, cudaMemcpyHostToDevice, ctx.stream), ctx.detail);
+    const uint32_t chunk = (uint32_t)std::min<uint64_t>(kChunkLevels, (uint64_t)max_depth - d);
+    for (uint32_t q = 0; q < chunk; q++) {
+      const uint32_t L = d + q;
+      LevelArgs a{adj, radj, st + q, queue[L & 1]->as<uint32_t>(), queue[(L + 1) & 1]->as<uint32_t>(),
+                  fb[L & 1], fb[(L + 1) & 1], big->as<uint32_t>(), L + 1, (uint32_t)n,
+                  depth->as<uint32_t>(), via->as<unsigned long long>(), filter_dev};
+      note_launch(), push_kernel<<<blocks, 256, 0, ctx.stream>>>(a);
+      note_launch(), push_big_kernel<<<blocks, 256, 0, ctx.stream>>>(a);
+      note_launch(), pull_kernel<<<pull_grid, 256, 0, ctx.stream>>>(a, 1);
+      // The bitmap of level L + 2 is level L's: clear it for the admits of L + 1.
+      note_launch(), level_end_kernel<<<end_grid, 256, 0, ctx.stream>>>(
+          st + q, sw, L + 1 >= max_depth ? 1u : 0u, fb[L & 1], (uint32_t)words, v->cancel_dev);
     }
     WC_CUDA(cudaGetLastError(), ctx.detail);
-    LevelCounters h;
-    WC_CUDA(cudaMemcpyAsync(&h, c, sizeof h, cudaMemcpyDeviceToHost, ctx.stream), ctx.detail);
+    WC_CUDA(cudaMemcpyAsync(plan.data(), st, (chunk + 1) * sizeof(LevelState), cudaMemcpyDeviceToHost,
+                            ctx.stream), ctx.detail);
     WC_CUDA(cudaStreamSynchronize(ctx.stream), ctx.detail);
-    levels.push_back(Level{pull, count, mf, pull ? (uint64_t)h.edges : mf, h.next_count});
-    stats.levels++;
-    if (pull) stats.pulled_levels++;
-    stats.edges_traversed += pull && rule == REFERENCE_SWITCH ? h.edges : mf;
-    stats.nodes_visited += h.next_count;
-    visited_rdeg += h.next_rdeg;
-    mf = h.next_deg;
-    count = h.next_count;
-    cur ^= 1;
-    d++;
+    for (uint32_t q = 0; q < chunk; q++) {
+      const LevelState& h = plan[q];
+      if (h.count == 0) break;
+      const bool pull = h.pull != 0;
+      levels.push_back(Level{pull, h.count, h.mf, pull ? (uint64_t)h.edges : h.mf, h.next_count});
+      stats.levels++;
+      if (pull) stats.pulled_levels++;
+      stats.edges_traversed += pull && rule == REFERENCE_SWITCH ? h.edges : h.mf;
+      stats.nodes_visited += h.next_count;
+      d++;
+    }
+    if (plan[chunk].count == 0) break;
+    first = plan[chunk];
+    first.next_deg = first.next_rdeg = first.edges = 0;
+    first.next_count = first.big_count = 0;
   }
   return WC_OK;
 }

@@ -22,7 +22,7 @@ struct Search {
   bool reverse_allowed = false;             // may a level be pulled (reachable_set)
   bool ordering_by_node_in_pulled = false;  // pulled levels list nodes ascending
   DevBuf *depth = nullptr, *via = nullptr, *queue[2] = {nullptr, nullptr}, *fbits = nullptr,
-         *counters = nullptr, *filter = nullptr;
+         *counters = nullptr, *filter = nullptr, *big = nullptr;
   std::vector<uint32_t> seeds;
   std::vector<Level> levels;
   wc_traversal_stats stats{};

@@ -28,10 +28,7 @@ namespace wc {
 
 constexpr uint64_t kChunk = 1 << 16;  // compute/reduce.rs:20
 
-// Over the locality-ordered CSC, the messages of the nodes numbered below
-// this (the most gathered) are kept in L1: 64 KB of them, what the SM's L1
-// holds beside four blocks' staging rings.
-constexpr uint32_t kHotNodes = 8192;
+
 
 __device__ inline bool tomb_at(const uint64_t* t, uint32_t i) {
   return t && ((t[i >> 6] >> (i & 63)) & 1);
@@ -254,6 +251,17 @@ wc_status prepare_pull(Ctx& ctx, DevCsr& csr, int semiring, int weighted_flag, i
                        uint32_t width, PullLaunch& L);
 wc_status launch_pull(const PullLaunch& L, int dtype, const void* x, void* y);
 
+wc_status launch_pr_init(const PrState& s, uint32_t grid, cudaStream_t stream) {
+  note_launch(), pr_init_kernel<<<grid, kPullThreads, 0, stream>>>(s);
+  return cuda_status(cudaGetLastError(), nullptr, "pagerank init");
+}
+
+wc_status launch_part_iteration(const PullLaunch& L, const PrState& s, uint32_t it,
+                                uint32_t blocks) {
+  if (L.weight_kind == WEIGHTS_F64) return launch_iter<double>(L, s, it, blocks);
+  return launch_iter<void>(L, s, it, blocks);
+}
+
 uint64_t live_count(const uint64_t* tomb, uint64_t n) {
   uint64_t dead = 0;
   if (tomb)
@@ -367,10 +375,10 @@ wc_status PageRankRun::setup(Ctx& ctx, const wc_pagerank_opts* o, const uint64_t
 
 wc_status PageRankRun::run(Ctx& ctx) {
   wc_version* v = ctx.v;
-  note_launch(), pr_init_kernel<<<grid, kPullThreads, 0, ctx.stream>>>(s);
+  WC_TRY(launch_pr_init(s, grid, ctx.stream));
   PullLaunch L;
   WC_TRY(prepare_pull(ctx, const_cast<DevCsr&>(csc(v)), WC_PLUS_TIMES, opts.weighted, WC_F64, 1, L));
-  if (local) L.hot = kHotNodes;
+  if (local) L.hot = kPageRankHotNodes;
   // With a tolerance the solve usually stops well before max_iter: the
   // host keeps at most kAhead iterations queued beyond the last one the
   // device reported, and stops queueing once the device reports the stop,

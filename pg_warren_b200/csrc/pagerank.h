@@ -48,7 +48,20 @@ struct PageRankRun {
   wc_status result(Ctx& ctx, double* ranks, uint32_t* iterations, double* margin);
 };
 
+// Over the locality-ordered CSC, the messages of the nodes numbered below
+// this (the most gathered) are kept in L1: 64 KB of them, what the SM's L1
+// holds beside four blocks' staging rings.
+constexpr uint32_t kPageRankHotNodes = 8192;
+
 uint64_t live_count(const uint64_t* tomb, uint64_t n);
+// pr_init_kernel: the start vector, its messages and dangling rank.
+wc_status launch_pr_init(const PrState& s, uint32_t grid, cudaStream_t stream);
+// One iteration (pr_iter_kernel) over L's units.
+struct PullLaunch;
+wc_status launch_part_iteration(const PullLaunch& L, const PrState& s, uint32_t it,
+                                uint32_t blocks);
+// Drops a version's partitioned solve (wc_pagerank_part_*) when it is released.
+void pagerank_part_forget(const wc_version* v);
 // Blocks of an iteration launch over `csc`.
 uint32_t pagerank_grid(const DevCsr& csc);
 

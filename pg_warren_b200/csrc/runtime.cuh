@@ -268,7 +268,7 @@ enum PoolTag {
   POOL_X = 1, POOL_Y, POOL_MASK, POOL_XCOPY, POOL_SEED,
   POOL_PR_X, POOL_PR_MSG, POOL_PR_OUT, POOL_PR_SHARES, POOL_PR_TOMB, POOL_PR_SCALARS,
   POOL_BFS_DEPTH, POOL_BFS_VIA, POOL_BFS_Q0, POOL_BFS_Q1, POOL_BFS_FBITS, POOL_BFS_COUNTERS,
-  POOL_BFS_FILTER, POOL_BFS_FLAGS,
+  POOL_BFS_FILTER, POOL_BFS_FLAGS, POOL_BFS_BIG = 30,
   POOL_BATCH_0 = 40, POOL_BATCH_1, POOL_BATCH_2, POOL_BATCH_3, POOL_BATCH_4, POOL_BATCH_5,
   POOL_BATCH_6, POOL_BATCH_7, POOL_BATCH_8, POOL_BATCH_9, POOL_BATCH_10, POOL_BATCH_11,
   POOL_EIG_0 = 60, POOL_EIG_1, POOL_EIG_2, POOL_EIG_3, POOL_EIG_4, POOL_EIG_5, POOL_EIG_6,

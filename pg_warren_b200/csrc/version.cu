@@ -6,6 +6,7 @@
 #include <memory>
 #include <thread>
 
+#include "pagerank.h"
 #include "product.h"
 #include "runtime.cuh"
 #include "upload.h"
@@ -264,6 +265,7 @@ wc_status wc_version_release(wc_version* v) {
     if (v->cancel_host) cudaFreeHost(v->cancel_host);
     if (v->stream) cudaStreamDestroy(v->stream);
   }
+  pagerank_part_forget(v);
   delete v;
   return WC_OK;
 }

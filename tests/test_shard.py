@@ -1,6 +1,7 @@
 """The sharded batched search's host side on two gloo ranks (CPU): each rank
 runs its share of the sources (here through the oracle's per-source BFS)
-and the gathered depths and edge counts equal the unsharded run."""
+into its rows of the output, the rows are broadcast from their owners, and
+every rank's output equals the unsharded run."""
 
 import os
 import socket
@@ -9,6 +10,8 @@ import numpy as np
 import pytest
 import torch.distributed as dist
 import torch.multiprocessing as mp
+
+import torch
 
 import oracle as O
 from pg_warren_b200.shard import run_sharded, shard_range
@@ -33,16 +36,27 @@ def _graph():
     return O.Graph.from_edges(n, edges, weighted=False, reverse=False)
 
 
+def _search_into(og, sources, caps, depths, edges):
+    def search(b, e):
+        d, x = O.bfs_depths(og, sources[b:e], caps[b:e])
+        depths[b:e] = torch.from_numpy(d)
+        edges[b:e] = torch.from_numpy(x.astype(np.int64))
+    return search
+
+
 def _rank(rank, world, port, sources, caps, out):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         og = _graph()
-        depths, edges = run_sharded(sources, caps, lambda s, c: O.bfs_depths(og, s, c))
-        if rank == 0:
-            np.save(out + "_d.npy", depths)
-            np.save(out + "_e.npy", edges)
+        depths = torch.full((len(sources), og.n), 7, dtype=torch.uint8)
+        edges = torch.full((len(sources),), -1, dtype=torch.int64)
+        b, e = run_sharded(len(sources), _search_into(og, sources, caps, depths, edges),
+                           [depths, edges])
+        np.save(out + f"_{rank}_d.npy", depths.numpy())
+        np.save(out + f"_{rank}_e.npy", edges.numpy())
+        np.save(out + f"_{rank}_share.npy", np.array([b, e]))
     finally:
         dist.destroy_process_group()
 
@@ -61,14 +75,18 @@ def test_two_gloo_ranks_gather_the_unsharded_result(tmp_path):
     mp.start_processes(_rank, args=(2, _free_port(), sources, caps, out), nprocs=2,
                        start_method="spawn")
     do, eo = O.bfs_depths(_graph(), sources, caps)
-    assert np.array_equal(np.load(out + "_d.npy"), do)
-    assert np.array_equal(np.load(out + "_e.npy"), eo)
+    for rank in range(2):
+        assert np.array_equal(np.load(out + f"_{rank}_d.npy"), do)
+        assert np.array_equal(np.load(out + f"_{rank}_e.npy"), eo.astype(np.int64))
+    assert [tuple(np.load(out + f"_{r}_share.npy")) for r in range(2)] == [(0, 19), (19, 37)]
 
 
 def test_without_a_process_group_the_call_is_unsharded():
     og = _graph()
     sources = np.array([1, 2, 3], np.uint64)
     caps = np.array([2, 3, 4], np.uint32)
-    d, e = run_sharded(sources, caps, lambda s, c: O.bfs_depths(og, s, c))
+    d = torch.zeros((3, og.n), dtype=torch.uint8)
+    e = torch.zeros(3, dtype=torch.int64)
+    assert run_sharded(3, _search_into(og, sources, caps, d, e), [d, e]) == (0, 3)
     do, eo = O.bfs_depths(og, sources, caps)
-    assert np.array_equal(d, do) and np.array_equal(e, eo)
+    assert np.array_equal(d.numpy(), do) and np.array_equal(e.numpy(), eo.astype(np.int64))
