@@ -109,14 +109,20 @@ struct MsLevel {
   uint64_t m;
   uint32_t* acc;      // n × W push accumulators, all zero between levels
   uint32_t* touched;  // rows with a push accumulator to settle, all zero between levels
-  const int32_t* cancel;  // the call's cancel word (host-mapped): a raised word ends the pass
 };
 
-// Whether level P.L runs at all: it has a frontier and the call is not
-// cancelled.  A level that does not run leaves the next level's count zero,
-// so every later level returns at once too.
-__device__ inline bool level_runs(const MsLevel& P) {
-  return P.counts[P.L] != 0 && !*(volatile const int32_t*)P.cancel;
+// Whether level P.L runs at all: it has a frontier.  A level that does not
+// run leaves the next level's count zero, so every later level returns at
+// once too.
+__device__ inline bool level_runs(const MsLevel& P) { return P.counts[P.L] != 0; }
+
+// Before each level's kernels: a raised cancel word (host-mapped, read here
+// by one thread) empties the level's frontier count, so all of the level's
+// kernels and every later level return at once.  The count changes only
+// between kernels, so a level runs whole or not at all, and the buffers kept
+// zero between calls stay zero.
+__global__ void msbfs_cancel_kernel(const int32_t* cancel, uint32_t* count) {
+  if (threadIdx.x == 0 && *(volatile const int32_t*)cancel) *count = 0;
 }
 
 // A level pushes (scatters the frontier rows over the forward CSR) while the
@@ -549,9 +555,7 @@ __global__ void __launch_bounds__(256) msbfs_push_kernel(MsLevel P) {
 // does (fresh = acc & ~V), clears the accumulator and its touched bit.
 template <int W>
 __global__ void __launch_bounds__(256) msbfs_settle_kernel(MsLevel P) {
-  // No cancel check here: a push that ran must be settled, which also
-  // leaves the accumulators and touched bits zero for the next call.
-  if (P.counts[P.L] == 0 || !level_pushes(P)) return;
+  if (!level_runs(P) || !level_pushes(P)) return;
   constexpr uint32_t G = 32 / W;
   const unsigned lane = threadIdx.x & 31;
   const unsigned sub = lane / W, w = lane % W;
@@ -1060,8 +1064,8 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
               F + L * fstride, F + (L + 1) * fstride, fbits + L * bitmap_words,
               fbits + (L + 1) * bitmap_words, wbits + (L + 1) * bitmap_words, masks, alive, L,
               counts, fedges, foff, fwd.targets.as<uint32_t>(), fwd.schedule.units.as<Unit>(),
-              fwd.schedule.count, v->m, b.acc->as<uint32_t>(), b.touched->as<uint32_t>(),
-              v->cancel_dev};
+              fwd.schedule.count, v->m, b.acc->as<uint32_t>(), b.touched->as<uint32_t>()};
+    note_launch(), msbfs_cancel_kernel<<<1, 32, 0, st>>>(v->cancel_dev, counts + L);
     note_launch(), msbfs_push_kernel<W><<<push_grid, 256, 0, st>>>(P);
     note_launch(), msbfs_settle_kernel<W><<<settle_grid, 256, 0, st>>>(P);
     note_launch(), msbfs_level_kernel<W><<<grid, 256, level_smem, st>>>(P);
