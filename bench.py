@@ -59,6 +59,13 @@ WIDTH = 1024
 PLAIN_SAMPLE = 32
 SEED = 1
 CPU_BUDGET_S = 12.0
+# DRAM bytes per algorithmic byte of a pull level, from the ncu capture of
+# msbfs_level_kernel on the same workload at R-MAT 20 (the full-size launch
+# is past the capture-size rule): traffic scales with the level's units.
+LEVEL_TRAFFIC_RATIO = 483.0 / 337.0
+LEVEL_TRAFFIC_SOURCE = ("dram__bytes_read.sum + dram__bytes_write.sum of one pull level at "
+                        "R-MAT 20 (profiles/msbfs_level_kernel_rmat20_1024src.md), scaled "
+                        "by the algorithmic bytes")
 
 
 def measured_peaks():
@@ -868,7 +875,7 @@ def main():
             batched()
         torch.cuda.synchronize(dev)
         barrier()
-        level_ms, level_launches, depth_ms = 0.0, 0, 0.0
+        level_ms, level_launches, depth_ms, pull_ms, pulled = 0.0, 0, 0.0, 0.0, 0
         step_ms = []
         launches0 = lib.wc_kernel_launches()
         with Clocks(local) as clocks:
@@ -885,6 +892,8 @@ def main():
                 level_ms += ms
                 level_launches += nl
                 depth_ms += gv.timing("depth")[0]
+                pull_ms += gv.timing("pull")[0]
+                pulled += gv.timing("pulled")[1]
         launches = lib.wc_kernel_launches() - launches0
         barrier()
     edges_step = int(edges_d.sum().item())
@@ -894,8 +903,11 @@ def main():
     batched_gteps_rank = edges_step * args.steps / (sum(step_ms) * 1e-3) / 1e9
     levels = executed_levels(depth_d, caps, columns)
     level_bytes = 4 * (n + 1) + 4 * m + n * columns // 4
-    level_avg_ms = level_ms / (levels * args.steps) if level_ms > 0 else None
-    achieved = level_bytes / (level_avg_ms * 1e-3) / 1e9 if level_avg_ms else None
+    # The roofline of msbfs_level_kernel: its launches timed alone, over the
+    # levels that pulled (the push levels' launches return at once).
+    pulled_per_step = pulled / args.steps
+    pull_avg_ms = pull_ms / pulled if pulled else None
+    achieved = level_bytes / (pull_avg_ms * 1e-3) / 1e9 if pull_avg_ms else None
 
     # ---- plain per-source GPU path, a sample of the same sources
     dpl = torch.empty(n, dtype=torch.int32, device=dev)
@@ -999,10 +1011,14 @@ def main():
         "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": WIDTH * 12,
                 "d2h_bytes_per_step": WIDTH * n + WIDTH * 8},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak if achieved else None, "traffic": None,
+                     "frac": achieved / peak if achieved else None,
+                     "traffic": level_bytes * LEVEL_TRAFFIC_RATIO,
+                     "traffic_source": LEVEL_TRAFFIC_SOURCE,
                      "kernel": "msbfs_level_kernel",
-                     "bytes_per_level": level_bytes, "levels_per_step": levels,
-                     "level_ms_avg": level_avg_ms, "peak_kind": peak_kind,
+                     "bytes_per_level": level_bytes, "pulled_levels_per_step": pulled_per_step,
+                     "levels_per_step": levels, "pull_ms_avg": pull_avg_ms,
+                     "peak_kind": peak_kind,
+                     "pull_ms_per_step": pull_ms / args.steps,
                      "level_ms_per_step": level_ms / args.steps,
                      "depth_ms_per_step": depth_ms / args.steps},
         "cpu_baseline": cpu,

@@ -10,6 +10,7 @@ namespace wc {
 struct BatchBuffers {
   DevBuf *V = nullptr, *F = nullptr, *bits = nullptr, *masks = nullptr, *counts = nullptr,
          *nacc = nullptr, *acc = nullptr, *touched = nullptr;
+  DevBuf* pulled = nullptr;  // u32: levels that pulled, in a timed call
   wc_status reserve(Ctx& ctx, uint32_t words, uint32_t levels);
 };
 

@@ -109,6 +109,7 @@ struct MsLevel {
   uint64_t m;
   uint32_t* acc;      // n × W push accumulators, all zero between levels
   uint32_t* touched;  // rows with a push accumulator to settle, all zero between levels
+  uint32_t* pulled;   // if set: counts the levels that pull (timed calls)
 };
 
 // Whether level P.L runs at all: it has a frontier.  A level that does not
@@ -228,6 +229,7 @@ template <int W>
 __global__ void __launch_bounds__(256, 4) msbfs_level_kernel(MsLevel P) {
   if (!level_runs(P)) return;  // nothing expands (or cancelled): F_{L+1} is not read
   if (level_pushes(P)) return;  // msbfs_push_kernel and msbfs_settle_kernel run it
+  if (P.pulled && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(P.pulled, 1u);
   constexpr uint32_t VEC = W >= 4 ? 4 : W;
   constexpr uint32_t LPR = W / VEC;
   constexpr uint32_t G = 32 / LPR;
@@ -1064,11 +1066,15 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
               F + L * fstride, F + (L + 1) * fstride, fbits + L * bitmap_words,
               fbits + (L + 1) * bitmap_words, wbits + (L + 1) * bitmap_words, masks, alive, L,
               counts, fedges, foff, fwd.targets.as<uint32_t>(), fwd.schedule.units.as<Unit>(),
-              fwd.schedule.count, v->m, b.acc->as<uint32_t>(), b.touched->as<uint32_t>()};
+              fwd.schedule.count, v->m, b.acc->as<uint32_t>(), b.touched->as<uint32_t>(),
+              b.pulled ? b.pulled->as<uint32_t>() : nullptr};
     note_launch(), msbfs_cancel_kernel<<<1, 32, 0, st>>>(v->cancel_dev, counts + L);
     note_launch(), msbfs_push_kernel<W><<<push_grid, 256, 0, st>>>(P);
     note_launch(), msbfs_settle_kernel<W><<<settle_grid, 256, 0, st>>>(P);
+    // The pull alone is timed too ("pull"), for its roofline.
+    ctx.phase_begin("pull");
     note_launch(), msbfs_level_kernel<W><<<grid, 256, level_smem, st>>>(P);
+    ctx.phase_end();
   }
   ctx.phase_end();
   if (clipped)
@@ -1173,6 +1179,10 @@ wc_status bfs_batched_run(Ctx& ctx, const wc_schedule& sched, const uint64_t* so
   for (uint32_t s = 0; s < width; s++) max_levels = std::max(max_levels, caps_host[s]);
   max_levels = std::min<uint32_t>(max_levels, kMaxLevels);
   WC_TRY(b.reserve(ctx, columns / 32, max_levels));
+  if (ctx.timing) {
+    WC_TRY(ctx.scratch(POOL_MSBFS_PULLED, 4, &b.pulled));
+    WC_CUDA(cudaMemsetAsync(b.pulled->ptr, 0, 4, ctx.stream), ctx.detail);
+  }
   WC_CUDA(cudaMemsetAsync(edges_dev, 0, width * 8, ctx.stream), ctx.detail);
   for (uint32_t s0 = 0; s0 < width; s0 += columns) {
     const uint32_t k = std::min(columns, width - s0);
@@ -1327,6 +1337,13 @@ wc_status wc_bfs_batched(wc_version* v, const wc_call* call, const uint64_t* sou
     WC_CUDA(cudaMemcpyAsync(edges_traversed_out, edges->ptr, width * 8, cudaMemcpyDefault,
                             ctx.stream), ctx.detail);
   const wc_status st = ctx.finish();
+  if (st == WC_OK && ctx.timing) {
+    // The levels that pulled, for the pull's roofline (wc_version_timing).
+    uint32_t pulled = 0;
+    WC_CUDA(cudaMemcpy(&pulled, v->pool[POOL_MSBFS_PULLED].ptr, 4, cudaMemcpyDeviceToHost),
+            ctx.detail);
+    v->timings["pulled"] = {0.0, pulled};
+  }
   if (st == WC_UNSUPPORTED)
     set_message(ctx.detail, "a search still expands at depth %u with a deeper cap; depths past %u "
                             "do not fit the byte output", kMaxLevels, kMaxLevels);

@@ -278,7 +278,7 @@ enum PoolTag {
   POOL_TOPK_0 = 100, POOL_TOPK_1,
   // Buffers the batched BFS keeps all-zero between calls; no other role
   // may share them.
-  POOL_MSBFS_NACC = 110, POOL_MSBFS_ACC, POOL_MSBFS_TOUCHED,
+  POOL_MSBFS_NACC = 110, POOL_MSBFS_ACC, POOL_MSBFS_TOUCHED, POOL_MSBFS_PULLED,
   // The 32-bit batched min-plus's long-row minima, kept at i32::MAX.
   POOL_MINPLUS32_NACC = 120,
   POOL_WCC_PARENT = 130, POOL_WCC_FLAG, POOL_WCC_LABELS,
@@ -312,6 +312,7 @@ struct Ctx {
     uint64_t launches;
   };
   std::vector<Timer> timers;
+  std::vector<size_t> open;  // timers begun and not yet ended (phases nest)
 
   Ctx(wc_version* ver, const wc_call* c)
       : v(ver), call(c), stream(ver->stream), budget(ver->budget), detail(nullptr),
@@ -340,11 +341,13 @@ struct Ctx {
     cudaEventCreate(&t.a);
     cudaEventCreate(&t.b);
     record(t.a);
+    open.push_back(timers.size());
     timers.push_back(t);
   }
   void phase_end() {
-    if (!timing || timers.empty()) return;
-    Timer& t = timers.back();
+    if (!timing || open.empty()) return;
+    Timer& t = timers[open.back()];
+    open.pop_back();
     record(t.b);
     t.launches = g_launches.load() - t.launches;
   }
