@@ -696,7 +696,8 @@ constexpr uint32_t kDepthNodes = 64;
 // The depth kernel's dynamic shared memory: the tile, the caps, the sums
 // and the tile's degrees.
 template <int W> constexpr size_t depth_smem_bytes() {
-  return (size_t)kDepthNodes * 8 * W * 4 + 32 * W * 4 + 32 * W * 8 + kDepthNodes * 4;
+  return (size_t)kDepthNodes * 8 * W * 4 + 32 * W * 4 + 32 * W * 8 + kDepthNodes * 4 +
+         (kDepthNodes / 4) * 16;
 }
 
 template <int W, int NB>
@@ -715,6 +716,9 @@ __global__ void __launch_bounds__(kDepthThreads, 2)
   uint32_t* cap4s = tile + TN * Q;                                              // [S]
   unsigned long long* esum = reinterpret_cast<unsigned long long*>(cap4s + S);  // [S]
   uint32_t* degs = reinterpret_cast<uint32_t*>(esum + S);                       // [TN]
+  // Per node quad: the degrees' low and high bytes as byte planes (for
+  // dp4a) and whether a degree is 2^16 or more (then the plain sum).
+  uint4* dplanes = reinterpret_cast<uint4*>(degs + TN);                         // [TN / 4]
   const uint32_t lane = threadIdx.x & 31;
   // The snapshots written: F_L exists for L < used (F_L is written only if
   // level L-1 had a frontier to expand).
@@ -746,9 +750,20 @@ __global__ void __launch_bounds__(kDepthThreads, 2)
         wl[c][b] = L < used && wi < bitmap_words ? wbits[(size_t)L * bitmap_words + wi] : 0u;
       }
     }
-    if (threadIdx.x < TN) {
+    if (threadIdx.x < TN) {  // two whole warps
       const uint32_t i = i0 + threadIdx.x;
-      degs[threadIdx.x] = i < n ? __ldg(off + i + 1) - __ldg(off + i) : 0u;
+      const uint32_t dg = i < n ? __ldg(off + i + 1) - __ldg(off + i) : 0u;
+      degs[threadIdx.x] = dg;
+      // Lanes 4q .. 4q + 3 hold quad q's degrees: OR their bytes together.
+      const uint32_t sh = 8 * (threadIdx.x & 3);
+      uint32_t p0 = (dg & 0xffu) << sh, p1 = ((dg >> 8) & 0xffu) << sh;
+      p0 |= __shfl_xor_sync(0xffffffffu, p0, 1);
+      p1 |= __shfl_xor_sync(0xffffffffu, p1, 1);
+      p0 |= __shfl_xor_sync(0xffffffffu, p0, 2);
+      p1 |= __shfl_xor_sync(0xffffffffu, p1, 2);
+      const uint32_t wq = __ballot_sync(0xffffffffu, (dg >> 16) != 0);
+      if ((threadIdx.x & 3) == 0)
+        dplanes[threadIdx.x >> 2] = make_uint4(p0, p1, (wq >> (threadIdx.x & 28)) & 0xfu, 0u);
     }
     // Phase 1a: every item's written levels 0..31 and the loads of its
     // first four, all in flight before any item is folded.
@@ -882,12 +897,11 @@ __global__ void __launch_bounds__(kDepthThreads, 2)
         for (uint32_t r = 0; r < 4; r++) o[h][r] = tile[(4 * q + r) * Q + col];
         // o[h][t]: source 4g + t at nodes 4q .. 4q + 3.
         byte_transpose4(o[h][0], o[h][1], o[h][2], o[h][3]);
-        const uint4 d = *reinterpret_cast<const uint4*>(degs + 4 * q);
         // The degrees' low two bytes as byte planes; a node of degree 2^16
         // or more takes the plain sum.
-        const bool wide = ((d.x | d.y | d.z | d.w) >> 16) != 0;
-        const uint32_t b0 = __byte_perm(__byte_perm(d.x, d.y, 0x0040), __byte_perm(d.z, d.w, 0x0040), 0x5410);
-        const uint32_t b1 = __byte_perm(__byte_perm(d.x, d.y, 0x0051), __byte_perm(d.z, d.w, 0x0051), 0x5410);
+        const uint4 dp = dplanes[q];
+        const bool wide = dp.z != 0;
+        const uint32_t b0 = dp.x, b1 = dp.y;
 #pragma unroll
         for (int t4 = 0; t4 < 4; t4++) {
           uint32_t lt;
@@ -901,9 +915,11 @@ __global__ void __launch_bounds__(kDepthThreads, 2)
           }
           if (!wide)
             part[t4] += __dp4a(lt, b0, 0u) + (__dp4a(lt, b1, 0u) << 8);
-          else
+          else {
+            const uint4 d = *reinterpret_cast<const uint4*>(degs + 4 * q);
             part[t4] += (lt & 1u ? d.x : 0u) + ((lt >> 8) & 1u ? d.y : 0u) +
                         ((lt >> 16) & 1u ? d.z : 0u) + ((lt >> 24) & 1u ? d.w : 0u);
+          }
         }
       }
       // Sum over the four lanes of the source quad: afterwards a lane holds
