@@ -283,6 +283,17 @@ __global__ void __launch_bounds__(256, 4) msbfs_level_kernel(MsLevel P) {
 #pragma unroll
         for (int i = 0; i < (int)VEC; i++) vrow[x].x[i] = 0xffffffffu;
     }
+    if (!tile && sub == 0) {
+      // A piece of a long row: the bits the row's other pieces have already
+      // gathered this level count as reached, so once the level has
+      // reached the row from every searching source its remaining pieces
+      // gather nothing (they still arrive, so the last one writes the row).
+      const uint32_t row_lo = __ldg(P.off + r0);
+      const uint32_t first = (unit.c & 0x7fffffffu) - (unit.b - row_lo) / kPieceEntries;
+      const uint32_t* na = P.nacc + (size_t)first * W + w0;
+#pragma unroll
+      for (int i = 0; i < (int)VEC; i++) vrow[0].x[i] |= __ldcg(na + i);
+    }
     uint32_t needy = 0;
 #pragma unroll
     for (uint32_t x = 0; x < VR; x++) {
