@@ -875,7 +875,6 @@ def main():
             batched()
         torch.cuda.synchronize(dev)
         barrier()
-        level_ms, level_launches, depth_ms, pull_ms, pulled = 0.0, 0, 0.0, 0.0, 0
         step_ms = []
         launches0 = lib.wc_kernel_launches()
         with Clocks(local) as clocks:
@@ -884,18 +883,25 @@ def main():
                 a = torch.cuda.Event(enable_timing=True)
                 b = torch.cuda.Event(enable_timing=True)
                 a.record(stream)
-                batched(timing=True)
+                batched()
                 b.record(stream)
                 b.synchronize()
                 step_ms.append(a.elapsed_time(b))
-                ms, nl = gv.timing("level")
-                level_ms += ms
-                level_launches += nl
-                depth_ms += gv.timing("depth")[0]
-                pull_ms += gv.timing("pull")[0]
-                pulled += gv.timing("pulled")[1]
         launches = lib.wc_kernel_launches() - launches0
         barrier()
+        # The kernel groups' times, from as many further steps made with the
+        # library's events (kept out of the timed steps above).
+        level_ms, level_launches, depth_ms, pull_ms, pulled = 0.0, 0, 0.0, 0.0, 0
+        for _ in range(args.steps):
+            flush.fill_(1)
+            batched(timing=True)
+            ms, nl = gv.timing("level")
+            level_ms += ms
+            level_launches += nl
+            depth_ms += gv.timing("depth")[0]
+            pull_ms += gv.timing("pull")[0]
+            pulled += gv.timing("pulled")[1]
+        torch.cuda.synchronize(dev)
     edges_step = int(edges_d.sum().item())
     total_ms = reduce(sum(step_ms), dist.ReduceOp.MAX if dist else None)
     edges_all = reduce(float(edges_step), dist.ReduceOp.SUM if dist else None)

@@ -152,6 +152,8 @@ typedef struct wc_version wc_version;   /* a version's device CSR + CSC */
 /* A budget of `limit` bytes of device memory (ComputeMemory::new,
  * compute/memory.rs).  Thread-safe. */
 wc_status wc_budget_create(uint64_t limit, wc_budget** out);
+/* Drops the caller's hold on the budget; a version charged to it keeps it
+ * until that version is released, so the two may go in either order. */
 void wc_budget_destroy(wc_budget* budget);
 uint64_t wc_budget_in_use(const wc_budget* budget);
 uint64_t wc_budget_peak(const wc_budget* budget);
@@ -240,7 +242,7 @@ typedef struct wc_version_info {
 /* Uploads `csr` for (graph_id, version) to the current device: the derived
  * device copy the seam keys by version (the reference's design document,
  * line 1240).  Charged to
- * `budget` (which must outlive the handle). */
+ * `budget` (the version holds it until wc_version_release). */
 wc_status wc_version_upload(uint64_t graph_id, uint64_t version, const wc_csr_host* csr,
                             wc_budget* budget, const wc_call* call, wc_version** out);
 wc_status wc_version_release(wc_version* version);

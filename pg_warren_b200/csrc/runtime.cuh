@@ -37,9 +37,35 @@ struct wc_budget {
   std::atomic<uint64_t> in_use{0};
   std::atomic<uint64_t> peak{0};
   std::mutex mu;
+  // The creator's reference and one per version charged to it: a version
+  // keeps its budget alive until its own buffers are freed, whatever order
+  // the caller releases them in.
+  std::atomic<int> refs{1};
 };
 
 namespace wc {
+
+inline void budget_retain(wc_budget* b) {
+  if (b) b->refs.fetch_add(1);
+}
+inline void budget_release(wc_budget* b) {
+  if (b && b->refs.fetch_sub(1) == 1) delete b;
+}
+
+// A version's reference to its budget, released after every other member
+// of the version (it is declared first), so its buffers uncharge a live one.
+struct BudgetRef {
+  wc_budget* b = nullptr;
+  BudgetRef() = default;
+  BudgetRef(const BudgetRef&) = delete;
+  BudgetRef& operator=(const BudgetRef&) = delete;
+  void hold(wc_budget* x) {
+    budget_retain(x);
+    budget_release(b);
+    b = x;
+  }
+  ~BudgetRef() { budget_release(b); }
+};
 
 inline void set_message(wc_error_detail* d, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
 inline void set_message(wc_error_detail* d, const char* fmt, ...) {
@@ -228,6 +254,7 @@ struct Locality {
 
 // The handle: one version's device copy, keyed by (graph, version).
 struct wc_version {
+  wc::BudgetRef budget_ref;  // first: released last
   uint64_t graph_id = 0, version = 0;
   uint64_t n = 0, m = 0;
   int device = 0;

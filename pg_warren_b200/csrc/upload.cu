@@ -388,6 +388,7 @@ wc_status wc_version_load_segments(uint64_t graph_id, uint64_t version, uint64_t
   v->n = n;
   v->m = m;
   v->budget = budget;
+  v->budget_ref.hold(budget);
   v->weighted = weights_segment != nullptr;
   WC_CUDA(cudaGetDevice(&v->device), d);
   WC_CUDA(cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking), d);

@@ -206,7 +206,7 @@ wc_status wc_budget_create(uint64_t limit, wc_budget** out) {
   return WC_OK;
 }
 
-void wc_budget_destroy(wc_budget* b) { delete b; }
+void wc_budget_destroy(wc_budget* b) { budget_release(b); }
 uint64_t wc_budget_in_use(const wc_budget* b) { return b ? b->in_use.load() : 0; }
 uint64_t wc_budget_peak(const wc_budget* b) { return b ? b->peak.load() : 0; }
 
@@ -235,6 +235,7 @@ wc_status wc_version_upload(uint64_t graph_id, uint64_t version, const wc_csr_ho
   v->n = n;
   v->m = m;
   v->budget = budget;
+  v->budget_ref.hold(budget);
   v->weighted = csr->weights != nullptr;
   WC_CUDA(cudaGetDevice(&v->device), detail);
   WC_CUDA(cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking), detail);

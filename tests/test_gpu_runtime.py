@@ -61,6 +61,22 @@ def test_a_version_budget_with_no_room_left_is_memory_limit():
     assert budget.in_use == held
 
 
+def test_a_version_keeps_its_budget_after_the_caller_drops_it():
+    # The caller may destroy a budget before the versions charged to it are
+    # released (a garbage collector finalises them in any order): the
+    # version holds the budget until its own buffers are freed.
+    budget = W.Budget()
+    g, gv = unweighted(12, budget=budget)
+    held = budget.in_use
+    handle, budget.handle = budget.handle, None
+    W.load().wc_budget_destroy(handle)  # the caller's hold goes first
+    r = W.pagerank(gv, None, W.PageRank())  # scratch charged to the budget
+    assert r.iterations > 0 and held > 0
+    gv.release()  # frees the buffers, uncharges, then lets the budget go
+    g2, gv2 = unweighted(12)
+    assert W.pagerank(gv2, None, W.PageRank()).iterations == r.iterations
+
+
 def test_cancel_from_another_thread_during_pagerank():
     # interrupts.rs:52-120: a flag raised on one thread while the work polls
     # it on another.  5,000 iterations without a tolerance: far longer than
