@@ -89,8 +89,9 @@ static wc_status static_setup(Ctx& ctx, PageRankRun& run, const wc_pagerank_opts
   if (o->has_tol && o->max_iter > 0)
     WC_TRY((wc_status)sql_float<F_MUL>(run.nodes, o->tol, &threshold));
   run.local = true;  // wc_pagerank's own numbering, so the results are its
-  const uint32_t blocks = pagerank_grid(run.csc(v));
-  run.grid = blocks;
+  run.grid = pagerank_grid(run.csc(v));
+  run.long_grid = pagerank_long_grid(run.csc(v));
+  const uint32_t blocks = pagerank_partial_blocks(run.csc(v));  // block sums kept
 
   unsigned char* p = base;
   auto take = [&](uint64_t bytes) {
@@ -219,7 +220,7 @@ wc_status wc_pagerank_noalloc(wc_version* v, const wc_call* call, const wc_pager
     set_message(detail, "a personalised PageRank needs per-call memory; use wc_pagerank");
     return WC_UNSUPPORTED;
   }
-  const uint32_t blocks = pagerank_grid(v->loc.csc);
+  const uint32_t blocks = pagerank_partial_blocks(v->loc.csc);
   const uint64_t need = static_bytes(v->n, o->max_iter, blocks, tombstones != nullptr);
   if (need > kStaticScratchBytes) {
     if (detail) {

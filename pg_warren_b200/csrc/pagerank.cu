@@ -65,12 +65,15 @@ __device__ inline void block_sum_two(double& a, double& b) {
 // of them, then the block in fixed order), so the totals do not depend on
 // which block arrives last.  Returns true in thread 0 of that block, with
 // the totals in a, b.
-__device__ inline bool reduce_two(double& a, double& b, double* partials, unsigned* counter) {
+// `before`: block partials an earlier kernel of the same step stored at
+// the front of `partials` (added in, first).
+__device__ inline bool reduce_two(double& a, double& b, double* partials, unsigned* counter,
+                                  unsigned before = 0) {
   __shared__ bool last;
   block_sum_two(a, b);
   if (threadIdx.x == 0) {
-    partials[2 * blockIdx.x] = a;
-    partials[2 * blockIdx.x + 1] = b;
+    partials[2 * (before + blockIdx.x)] = a;
+    partials[2 * (before + blockIdx.x) + 1] = b;
     __threadfence();
     last = atomicAdd(counter, 1u) == gridDim.x - 1;
   }
@@ -78,7 +81,7 @@ __device__ inline bool reduce_two(double& a, double& b, double* partials, unsign
   if (!last) return false;
   __threadfence();
   double ta = 0.0, tb = 0.0;
-  for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+  for (unsigned k = threadIdx.x; k < before + gridDim.x; k += blockDim.x) {
     ta += __ldcg(partials + 2 * k);
     tb += __ldcg(partials + 2 * k + 1);
   }
@@ -199,7 +202,31 @@ struct PrEpi {
 
 // Unweighted, four blocks an SM (64 registers) keep more gathers in flight;
 // with weights the extra registers would spill, so three.
-template <class W, bool SPLIT>
+// The step's close, by the last block of its last kernel: the stop test,
+// the cancel word and the progress words.
+__device__ inline void pr_close(const PrState& s, uint32_t it, double delta, double dangling) {
+  s.delta[it] = delta;
+  s.dangling[it + 1] = dangling;
+  *s.iterations = it + 1;
+  if (s.has_tol && sql_cmp_f(delta, s.threshold) < 0) *s.done = 1;
+  // The caller's cancel word (host memory, mapped) is read once per
+  // iteration, here; the next iteration then returns at once.
+  if (*(volatile const int32_t*)s.cancel) {
+    raise(s.err, WC_CANCELLED);
+    *s.done = 1;
+  }
+  // Tell the host how far the solve is, so it stops queueing iterations.
+  if (s.pace) {
+    volatile uint32_t* pace = s.pace;
+    pace[1] = *s.done;
+    pace[0] = it + 1;
+  }
+}
+
+// DEFER: the long rows' pieces only store their partials, and
+// pr_long_kernel finishes those rows and the step; each block here leaves
+// its sums at the front of the partials.
+template <class W, bool SPLIT, bool DEFER>
 __global__ void __launch_bounds__(kPullThreads, WSize<W>::v == 0 ? 4 : 3)
     pr_iter_kernel(CsrView<W> A, PrState s, uint32_t it) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -207,43 +234,79 @@ __global__ void __launch_bounds__(kPullThreads, WSize<W>::v == 0 ? 4 : 3)
   const int cur = it & 1;
   PrEpi epi{&s, cur, s.dangling[it], 0.0, 0.0};
   PullRing<double, W>* ring = reinterpret_cast<PullRing<double, W>*>(smem) + (threadIdx.x >> 5);
-  pull_units<double, WC_PLUS_TIMES, W, PrEpi, SPLIT>(A, s.msg[cur], epi, s.err, ring);
+  pull_units<double, WC_PLUS_TIMES, W, PrEpi, SPLIT, DEFER>(A, s.msg[cur], epi, s.err, ring);
   double delta = epi.delta, dangling = epi.dangling_out;
-  if (reduce_two(delta, dangling, s.partials, s.counter)) {
-    s.delta[it] = delta;
-    s.dangling[it + 1] = dangling;
-    *s.iterations = it + 1;
-    if (s.has_tol && sql_cmp_f(delta, s.threshold) < 0) *s.done = 1;
-    // The caller's cancel word (host memory, mapped) is read once per
-    // iteration, here; the next iteration then returns at once.
-    if (*(volatile const int32_t*)s.cancel) {
-      raise(s.err, WC_CANCELLED);
-      *s.done = 1;
+  if constexpr (DEFER) {
+    block_sum_two(delta, dangling);
+    if (threadIdx.x == 0) {
+      s.partials[2 * blockIdx.x] = delta;
+      s.partials[2 * blockIdx.x + 1] = dangling;
     }
-    // Tell the host how far the solve is, so it stops queueing iterations.
-    if (s.pace) {
-      volatile uint32_t* pace = s.pace;
-      pace[1] = *s.done;
-      pace[0] = it + 1;
-    }
+    return;
   }
+  if (reduce_two(delta, dangling, s.partials, s.counter)) pr_close(s, it, delta, dangling);
 }
 
+// The long rows of a step run with DEFER: a warp per row combines its
+// pieces' partials in piece order (as the last piece to arrive does
+// otherwise), then the row's advance and spread; the last block reduces
+// both kernels' block sums in a fixed order and closes the step.
+__global__ void __launch_bounds__(256)
+    pr_long_kernel(const uint4* longs, uint32_t long_count,
+                   const Partial<double, semiring_add(WC_PLUS_TIMES)>* carry, PrState s,
+                   uint32_t it, uint32_t first_blocks) {
+  if (*(volatile int32_t*)s.done) return;
+  const int cur = it & 1;
+  PrEpi epi{&s, cur, s.dangling[it], 0.0, 0.0};
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < long_count; r += warps) {
+    const uint4 L = longs[r];  // row, first slot, pieces
+    PrEpi::Pre pre{};
+    if (lane == 0) pre = epi.pre(L.x);
+    const auto total =
+        combine_pieces<double, semiring_add(WC_PLUS_TIMES), 1>(carry, L.y, L.z, 0, lane);
+    if (lane == 0) {
+      double v;
+      const int32_t st = total.acc.value(&v);
+      if (st) raise(s.err, st, L.x);
+      epi.row(L.x, true, v, pre);
+    }
+  }
+  double delta = epi.delta, dangling = epi.dangling_out;
+  if (reduce_two(delta, dangling, s.partials, s.counter, first_blocks))
+    pr_close(s, it, delta, dangling);
+}
+
+template <class W, bool SPLIT, bool DEFER>
+static wc_status set_iter_attributes(const PullLaunch& L) {
+  constexpr size_t smem = pull_smem_bytes<double, W>();
+  static const cudaError_t attr = cudaFuncSetAttribute(
+      pr_iter_kernel<W, SPLIT, DEFER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return cuda_status(attr, L.detail, "pagerank kernel attributes");
+}
+
+// One iteration: pr_iter_kernel over L's units, and with `longs` (the
+// schedule's long rows, DEFER) pr_long_kernel after it on `long_grid` blocks.
 template <class W>
-wc_status launch_iter(const PullLaunch& L, const PrState& s, uint32_t it, uint32_t blocks) {
+wc_status launch_iter(const PullLaunch& L, const PrState& s, uint32_t it, uint32_t blocks,
+                      const Schedule* longs = nullptr, uint32_t long_grid = 0) {
   CsrView<W> A{L.off, L.tgt, static_cast<const W*>(L.weights), L.units, L.unit_count, L.counters,
                L.carry, L.hot};
   constexpr size_t smem = pull_smem_bytes<double, W>();
-  static const cudaError_t attr = cudaFuncSetAttribute(
-      pr_iter_kernel<W, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  static const cudaError_t attr_split = cudaFuncSetAttribute(
-      pr_iter_kernel<W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (attr != cudaSuccess) return cuda_status(attr, L.detail, "pagerank kernel attributes");
-  if (attr_split != cudaSuccess) return cuda_status(attr_split, L.detail, "pagerank kernel attributes");
-  if (L.hot)
-    note_launch(), pr_iter_kernel<W, true><<<blocks, kPullThreads, smem, L.stream>>>(A, s, it);
-  else
-    note_launch(), pr_iter_kernel<W, false><<<blocks, kPullThreads, smem, L.stream>>>(A, s, it);
+  if (longs) {
+    WC_TRY((set_iter_attributes<W, true, true>(L)));
+    note_launch(), pr_iter_kernel<W, true, true><<<blocks, kPullThreads, smem, L.stream>>>(A, s, it);
+    note_launch(), pr_long_kernel<<<long_grid, 256, 0, L.stream>>>(
+        longs->long_list.as<uint4>(), longs->long_rows,
+        static_cast<const Partial<double, semiring_add(WC_PLUS_TIMES)>*>(L.carry), s, it, blocks);
+  } else if (L.hot) {
+    WC_TRY((set_iter_attributes<W, true, false>(L)));
+    note_launch(), pr_iter_kernel<W, true, false><<<blocks, kPullThreads, smem, L.stream>>>(A, s, it);
+  } else {
+    WC_TRY((set_iter_attributes<W, false, false>(L)));
+    note_launch(), pr_iter_kernel<W, false, false><<<blocks, kPullThreads, smem, L.stream>>>(A, s, it);
+  }
   return WC_OK;
 }
 
@@ -271,6 +334,14 @@ uint64_t live_count(const uint64_t* tomb, uint64_t n) {
       dead += __builtin_popcountll(word);
     }
   return n - dead;
+}
+
+uint32_t pagerank_long_grid(const DevCsr& csc) {
+  return std::max<uint32_t>(1, std::min<uint32_t>((csc.schedule.long_rows + 7) / 8, max_blocks(2)));
+}
+
+uint32_t pagerank_partial_blocks(const DevCsr& csc) {
+  return pagerank_grid(csc) + pagerank_long_grid(csc);
 }
 
 uint32_t pagerank_grid(const DevCsr& csc) {
@@ -304,10 +375,12 @@ wc_status PageRankRun::setup(Ctx& ctx, const wc_pagerank_opts* o, const uint64_t
   if (o->has_tol && o->max_iter > 0) WC_TRY((wc_status)sql_float<F_MUL>(nodes, o->tol, &threshold));
   const uint32_t blocks = pagerank_grid(csc(v));
   grid = blocks;
+  long_grid = pagerank_long_grid(csc(v));
+  const uint32_t partial_blocks = blocks + long_grid;
   WC_TRY(ctx.scratch(POOL_PR_X, 2 * n * 8, &x));
   WC_TRY(ctx.scratch(POOL_PR_MSG, 2 * n * 8, &msg));
   WC_TRY(ctx.scratch(POOL_PR_OUT, n * 8, &out));
-  const uint64_t scalar_bytes = (2 * (uint64_t)o->max_iter + 8) * 8 + 2 * blocks * 8 + 64;
+  const uint64_t scalar_bytes = (2 * (uint64_t)o->max_iter + 8) * 8 + 2 * partial_blocks * 8 + 64;
   WC_TRY(ctx.scratch(POOL_PR_SCALARS, scalar_bytes, &scalars));
   uint64_t* tomb_dev = nullptr;
   if (th) {
@@ -339,7 +412,7 @@ wc_status PageRankRun::setup(Ctx& ctx, const wc_pagerank_opts* o, const uint64_t
   s.delta = sc;
   s.dangling = sc + o->max_iter;
   s.partials = sc + 2 * (uint64_t)o->max_iter + 8;
-  unsigned char* tail = reinterpret_cast<unsigned char*>(s.partials + 2 * blocks);
+  unsigned char* tail = reinterpret_cast<unsigned char*>(s.partials + 2 * partial_blocks);
   s.counter = reinterpret_cast<unsigned*>(tail);
   s.iterations = reinterpret_cast<uint32_t*>(tail + 8);
   s.done = reinterpret_cast<int32_t*>(tail + 16);
@@ -402,8 +475,11 @@ wc_status PageRankRun::run(Ctx& ctx) {
       }
       if (stop) break;
     }
-    if (L.weight_kind == WEIGHTS_F64) WC_TRY(launch_iter<double>(L, s, it, grid));
-    else WC_TRY(launch_iter<void>(L, s, it, grid));
+    // In the locality order the long rows are finished by a pass of their
+    // own, after their pieces (no release/acquire arrival per piece).
+    const Schedule* longs = local ? &csc(v).schedule : nullptr;
+    if (L.weight_kind == WEIGHTS_F64) WC_TRY(launch_iter<double>(L, s, it, grid, longs, long_grid));
+    else WC_TRY(launch_iter<void>(L, s, it, grid, longs, long_grid));
   }
   ctx.phase_end();
   return cuda_status(cudaGetLastError(), ctx.detail, "pagerank iterations");

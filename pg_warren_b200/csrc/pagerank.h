@@ -32,6 +32,7 @@ struct PageRankRun {
   uint64_t live = 0;
   double nodes = 0.0;
   uint32_t grid = 1;
+  uint32_t long_grid = 1;  // pr_long_kernel's blocks (locality order)
   // The solve pulls over the version's locality-ordered CSC (v->loc), its
   // vectors in that numbering; inputs are renumbered in by setup and the
   // ranks out by result.  Off for callers that read the vectors themselves.
@@ -62,7 +63,10 @@ wc_status launch_part_iteration(const PullLaunch& L, const PrState& s, uint32_t 
                                 uint32_t blocks);
 // Drops a version's partitioned solve (wc_pagerank_part_*) when it is released.
 void pagerank_part_forget(const wc_version* v);
-// Blocks of an iteration launch over `csc`.
+// Blocks of an iteration launch over `csc`; of the long-row pass that
+// follows it in the locality order; and the block sums the step keeps.
 uint32_t pagerank_grid(const DevCsr& csc);
+uint32_t pagerank_long_grid(const DevCsr& csc);
+uint32_t pagerank_partial_blocks(const DevCsr& csc);
 
 }  // namespace wc

@@ -293,7 +293,7 @@ __device__ inline void stage_products(const PullRing<E, W>* ring, int b, const E
 // arrive with its gathers.  `epi.row(row, present, value, pre)` is called
 // exactly once per row, by one lane.  A ring wait that runs out (about 2 s)
 // raises WC_DEVICE_TIMEOUT and ends the walk after the copies in flight.
-template <class E, int S, class W, class Epi, bool SPLIT = false>
+template <class E, int S, class W, class Epi, bool SPLIT = false, bool DEFER = false>
 __device__ inline void pull_units(const CsrView<W>& A, const E* __restrict__ x, Epi& epi,
                                   DeviceError* err, PullRing<E, W>* ring) {
   constexpr int R = PullRing<E, W>::R;
@@ -382,27 +382,33 @@ __device__ inline void pull_units(const CsrView<W>& A, const E* __restrict__ x, 
         Partial<E, ADD> other = shfl_partial(mine, o);
         if ((lane & (2 * o - 1)) == 0) mine = join(mine, other);
       }
-      const uint32_t row_lo = __ldg(A.off + row);
-      const uint32_t deg = __ldg(A.off + row + 1) - row_lo;
-      const uint32_t pieces = (deg + kPieceEntries - 1) / kPieceEntries;
-      const uint32_t first = slot - (e0 - row_lo) / kPieceEntries;
-      uint32_t arrived = 0;
-      if (lane == 0) {
-        carry[slot] = mine;
-        arrived = arrive_acq_rel(A.counters + first);
-      }
-      arrived = __shfl_sync(0xffffffffu, arrived, 0);
-      if (arrived == pieces - 1) {
-        __threadfence();
-        typename Epi::Pre pre{};
-        if (lane == 0) pre = epi.pre(row);
-        Partial<E, ADD> total = combine_pieces<E, ADD, 1>(carry, first, pieces, 0, lane);
+      if constexpr (DEFER) {
+        // The piece's partial only: a later pass combines each long
+        // row's pieces in order (it starts after every piece is stored).
+        if (lane == 0) carry[slot] = mine;
+      } else {
+        const uint32_t row_lo = __ldg(A.off + row);
+        const uint32_t deg = __ldg(A.off + row + 1) - row_lo;
+        const uint32_t pieces = (deg + kPieceEntries - 1) / kPieceEntries;
+        const uint32_t first = slot - (e0 - row_lo) / kPieceEntries;
+        uint32_t arrived = 0;
         if (lane == 0) {
-          A.counters[first] = 0;
-          E v;
-          int32_t s = total.acc.value(&v);
-          if (s) raise(err, s, row);
-          epi.row(row, true, v, pre);
+          carry[slot] = mine;
+          arrived = arrive_acq_rel(A.counters + first);
+        }
+        arrived = __shfl_sync(0xffffffffu, arrived, 0);
+        if (arrived == pieces - 1) {
+          __threadfence();
+          typename Epi::Pre pre{};
+          if (lane == 0) pre = epi.pre(row);
+          Partial<E, ADD> total = combine_pieces<E, ADD, 1>(carry, first, pieces, 0, lane);
+          if (lane == 0) {
+            A.counters[first] = 0;
+            E v;
+            int32_t s = total.acc.value(&v);
+            if (s) raise(err, s, row);
+            epi.row(row, true, v, pre);
+          }
         }
       }
     }

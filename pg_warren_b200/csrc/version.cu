@@ -103,6 +103,21 @@ wc_status put_schedule(wc_version* v, DevCsr& d, const std::vector<uint64_t>& of
   WC_CUDA(cudaMemset(s.counters.ptr, 0, (uint64_t)std::max<uint32_t>(s.slots, 1) * 4), detail);
   WC_TRY(s.carry.alloc(v->budget, (uint64_t)std::max<uint32_t>(s.slots, 1) * kCarryBytesPerSlot,
                        detail));
+  // The long rows, for kernels that combine their pieces in a pass of their
+  // own: (row, first slot, pieces) in row order.
+  std::vector<uint32_t> longs;
+  longs.reserve(4 * (size_t)s.long_rows);
+  for (size_t u = 0; u < units.size(); u++) {
+    const Unit& d = units[u];
+    if ((d.c >> 31) == 0) continue;
+    if (u > 0 && (units[u - 1].c >> 31) != 0 && units[u - 1].a == d.a) continue;
+    const uint64_t deg = off[d.a + 1] - off[d.a];
+    longs.insert(longs.end(), {d.a, d.c & 0x7fffffffu, (uint32_t)((deg + kPieceEntries - 1) / kPieceEntries), 0u});
+  }
+  WC_TRY(s.long_list.alloc(v->budget, std::max<size_t>(longs.size(), 4) * 4, detail));
+  if (!longs.empty())
+    WC_CUDA(cudaMemcpy(s.long_list.ptr, longs.data(), longs.size() * 4, cudaMemcpyHostToDevice),
+            detail);
   return WC_OK;
 }
 
@@ -278,7 +293,8 @@ wc_status wc_version_info_get(const wc_version* v, wc_version_info* info) {
   uint64_t bytes = 0;
   for (const DevCsr* d : {&v->fwd, &v->rev, &v->loc.csc})
     bytes += d->offsets.bytes + d->targets.bytes + d->weights.bytes + d->iweights.bytes +
-             d->schedule.units.bytes + d->schedule.counters.bytes + d->schedule.carry.bytes;
+             d->schedule.units.bytes + d->schedule.counters.bytes + d->schedule.carry.bytes +
+             d->schedule.long_list.bytes;
   bytes += v->loc.perm.bytes + v->loc.order.bytes;
   info->device_bytes = bytes;
   uint64_t pooled = 0;
