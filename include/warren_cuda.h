@@ -439,6 +439,46 @@ wc_status wc_bfs_visits(wc_version* version, const wc_call* call, wc_direction d
                         const uint64_t* filter, uint64_t* visits_out, uint64_t capacity,
                         uint64_t* count, wc_traversal_stats* stats);
 
+/* traversal/bfs_cursor.rs:17-138 (BfsCursor): wc_bfs run one level per
+ * call, so a caller that stops asking (SQL LIMIT) stops the search.
+ * wc_bfs_cursor_open is BfsCursor::new (:40-73) — every argument is
+ * checked, the starts are admitted on the device, and later calls fail
+ * only when cancelled, timed out or out of memory — or, with
+ * reachable_set != 0, BfsCursor::reachable_set (:75-88): `filter` NULL and
+ * max_results unbounded, levels may be pulled (the reference's switch) and
+ * a pulled level lists its nodes ascending.  The cursor holds its own
+ * device buffers, charged to the version's budget, until
+ * wc_bfs_cursor_destroy; wc_version_release refuses (WC_INVALID_ARGUMENT)
+ * while a cursor over the version is open. */
+typedef struct wc_bfs_cursor wc_bfs_cursor;
+wc_status wc_bfs_cursor_open(wc_version* version, const wc_call* call, wc_direction direction,
+                             const uint64_t* starts, uint64_t start_count, const wc_limits* limits,
+                             const uint64_t* filter, int32_t reachable_set, wc_bfs_cursor** out);
+
+/* bfs_cursor.rs:90-126 (next_level): runs the next level (the starts the
+ * first time) and keeps its visits, in the order wc_bfs_visits lists them,
+ * for wc_bfs_cursor_read; *count gets how many.  *more (may be NULL) is 0
+ * once no level may follow: the search is exhausted, max_results was met
+ * (the level is cut there and the stats say truncated) or the cursor was
+ * stopped.  A finished cursor's calls return 0 visits. */
+wc_status wc_bfs_cursor_next(wc_bfs_cursor* cursor, const wc_call* call, uint64_t* count,
+                             int32_t* more);
+
+/* Visits [first, first + rows) of the last level: visits_out[3*r .. 3*r+2]
+ * = (node, depth, via), host or device memory. */
+wc_status wc_bfs_cursor_read(const wc_bfs_cursor* cursor, uint64_t first, uint64_t rows,
+                             uint64_t* visits_out);
+
+/* A visitor that breaks (bfs_cursor.rs:92-95, Admission::AdmitAndStop): the
+ * caller took `consumed` (1 .. the last level's count) visits of the last
+ * level and broke at the last of them.  The cursor finishes with the stats
+ * of a search that stopped there, not truncated. */
+wc_status wc_bfs_cursor_stop(wc_bfs_cursor* cursor, const wc_call* call, uint64_t consumed);
+
+/* bfs_cursor.rs:128-131 (stats): the work done so far. */
+wc_status wc_bfs_cursor_stats(const wc_bfs_cursor* cursor, wc_traversal_stats* stats);
+void wc_bfs_cursor_destroy(wc_bfs_cursor* cursor);
+
 /* traversal/reachable.rs:48-90 (reachable_set / reachable_set_each): the
  * nodes within max_depth of `starts` in the reference's order (by depth;
  * pushed levels in the order reached, pulled levels ascending), with the

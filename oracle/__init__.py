@@ -100,6 +100,8 @@ def _declare(L):
     L.wo_pagerank.argtypes = [P, P, D, I, D, I, U32, P, P, P, P, P]
     L.wo_bfs.restype = I32
     L.wo_bfs.argtypes = [P, I, P, U64, U32, U64, P, P, U64, P, P]
+    L.wo_level_search.restype = I32
+    L.wo_level_search.argtypes = [P, I, P, U64, U32, U64, P, I, P, U64, P, P]
     L.wo_reachable_set.restype = I32
     L.wo_reachable_set.argtypes = [P, I, P, U64, U32, P, U64, P, P]
     L.wo_bfs_depths.restype = I32
@@ -285,18 +287,22 @@ def tombstone_words(n, ids):
     return words
 
 
-def bfs(g, starts, direction=0, max_depth=None, max_results=None, filter_ids=None):
-    """traversal/bfs.rs:34-45: ([(node, depth, via)], stats dict)."""
+def bfs(g, starts, direction=0, max_depth=None, max_results=None, filter_ids=None,
+        pulling=False):
+    """traversal/bfs.rs:34-45: ([(node, depth, via)], stats dict).  With
+    `pulling`, levels may be pulled as reachable_set's are (level.rs:184-284),
+    the result limit applying to them too."""
     starts = np.ascontiguousarray(starts, dtype=np.uint64)
     cap = g.n + 1
     visits = np.zeros(3 * cap, np.uint64)
     count = np.zeros(1, np.uint64)
     stats = np.zeros(5, np.uint64)
     filt = tombstone_words(g.n, filter_ids) if filter_ids is not None else None
-    st = lib().wo_bfs(g.handle, direction, _ptr(starts), len(starts),
-                      0xFFFFFFFF if max_depth is None else max_depth,
-                      0xFFFFFFFFFFFFFFFF if max_results is None else max_results,
-                      _ptr(filt), _ptr(visits), cap, _ptr(count), _ptr(stats))
+    st = lib().wo_level_search(g.handle, direction, _ptr(starts), len(starts),
+                               0xFFFFFFFF if max_depth is None else max_depth,
+                               0xFFFFFFFFFFFFFFFF if max_results is None else max_results,
+                               _ptr(filt), 1 if pulling else 0, _ptr(visits), cap, _ptr(count),
+                               _ptr(stats))
     _check(st)
     c = int(count[0])
     v = visits[: 3 * c].reshape(-1, 3)

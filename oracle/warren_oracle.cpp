@@ -853,16 +853,21 @@ int32_t wo_pagerank(const wo_graph* gp, const uint64_t* tombstones, double dampi
   return pagerank(*(const Graph*)gp, tombstones, o, ranks, iterations, last_delta, threshold);
 }
 
-// traversal/bfs.rs:34-79 (bfs): visits (node, depth, via) in the reference's
-// order into `visits` (3 u64 per visit, `capacity` visits).
-int32_t wo_bfs(const wo_graph* gp, int direction, const uint64_t* starts, uint64_t nstarts,
-               uint32_t max_depth, uint64_t max_results, const uint64_t* filter, uint64_t* visits,
-               uint64_t capacity, uint64_t* count, uint64_t* stats) {
+// traversal/level.rs:88-337 (LevelSearch::run) with bfs.rs:96-110's
+// result limit: visits (node, depth, via) in the reference's order into
+// `visits` (3 u64 per visit, `capacity` visits).  `pulling` lets levels be
+// pulled (reachable_set's edges, with the reverse CSR); without it this is
+// traversal/bfs.rs:34-79 (bfs).
+int32_t wo_level_search(const wo_graph* gp, int direction, const uint64_t* starts,
+                        uint64_t nstarts, uint32_t max_depth, uint64_t max_results,
+                        const uint64_t* filter, int32_t pulling, uint64_t* visits,
+                        uint64_t capacity, uint64_t* count, uint64_t* stats) {
   const Graph& g = *(const Graph*)gp;
   if (direction != WC_OUT && !g.has_rev) return WC_REVERSE_CSR_MISSING;
   std::vector<Visit> v;
   Stats st;
-  Status s = level_search(g, direction, starts, nstarts, max_depth, max_results, filter, false, v, st);
+  Status s = level_search(g, direction, starts, nstarts, max_depth, max_results, filter,
+                          pulling && g.has_rev, v, st);
   if (s) return s;
   *count = v.size();
   for (uint64_t i = 0; i < v.size() && i < capacity; i++) {
@@ -878,6 +883,13 @@ int32_t wo_bfs(const wo_graph* gp, int direction, const uint64_t* starts, uint64
     stats[4] = st.pulled;
   }
   return WC_OK;
+}
+
+int32_t wo_bfs(const wo_graph* gp, int direction, const uint64_t* starts, uint64_t nstarts,
+               uint32_t max_depth, uint64_t max_results, const uint64_t* filter, uint64_t* visits,
+               uint64_t capacity, uint64_t* count, uint64_t* stats) {
+  return wo_level_search(gp, direction, starts, nstarts, max_depth, max_results, filter, 0,
+                         visits, capacity, count, stats);
 }
 
 // traversal/reachable.rs:79-90 (reachable_set_each): with the reverse CSR

@@ -150,6 +150,13 @@ SIGNATURES = [
                             C.POINTER(U64), C.POINTER(TraversalStats)]),
     ("wc_reachable_set", I32, [P, C.POINTER(Call), I32, P, U64, U32, P, U64, C.POINTER(U64),
                                C.POINTER(TraversalStats)]),
+    ("wc_bfs_cursor_open", I32, [P, C.POINTER(Call), I32, P, U64, C.POINTER(Limits), P, I32,
+                                 C.POINTER(P)]),
+    ("wc_bfs_cursor_next", I32, [P, C.POINTER(Call), C.POINTER(U64), C.POINTER(I32)]),
+    ("wc_bfs_cursor_read", I32, [P, U64, U64, P]),
+    ("wc_bfs_cursor_stop", I32, [P, C.POINTER(Call), U64]),
+    ("wc_bfs_cursor_stats", I32, [P, C.POINTER(TraversalStats)]),
+    ("wc_bfs_cursor_destroy", None, [P]),
     ("wc_reachable", I32, [P, C.POINTER(Call), I32, U64, U64, U32, C.POINTER(I32),
                            C.POINTER(TraversalStats)]),
     ("wc_components", I32, [P, C.POINTER(Call), P, C.POINTER(TraversalStats)]),

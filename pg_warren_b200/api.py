@@ -429,9 +429,11 @@ class GraphVersion:
         _raise(A.load().wc_version_sync(self.handle, C.byref(call)), detail)
 
     def release(self):
+        """Frees the device copy; refused (InvalidArgument) while a cursor
+        over it is open."""
         h = getattr(self, "handle", None)
         if h:
-            A.load().wc_version_release(h)
+            _raise(A.load().wc_version_release(h), A.ErrorDetail())
             self.handle = None
 
     def __del__(self):
@@ -747,6 +749,81 @@ def reachable_set(graph: GraphVersion, starts, max_depth=None, direction="out",
                                      _ptr(nodes), len(nodes), C.byref(count), C.byref(stats)),
            detail)
     return Traversed([int(v) for v in nodes[: count.value]], _stats(stats))
+
+
+class BfsCursor:
+    """traversal/bfs_cursor.rs:17-138: bfs (or, with `reachable=True`,
+    reachable_set) run one level per next_level call.  The cursor keeps
+    its graph alive and its own device buffers until close()."""
+
+    def __init__(self, graph: GraphVersion, starts, filter=None, limits: Limits = Limits(),
+                 direction: str = "out", reachable: bool = False, interrupts=None):
+        st = np.ascontiguousarray(np.asarray(starts, dtype=np.uint64))
+        filt = None
+        if filter is not None:
+            filt = node_set(graph.id_space, filter) if not isinstance(filter, np.ndarray) \
+                else filter
+        lim = _limits(limits)
+        call, detail = _call(interrupts)
+        handle = C.c_void_p()
+        _raise(A.load().wc_bfs_cursor_open(graph.handle, C.byref(call), _DIRECTIONS[direction],
+                                           _ptr(st), len(st), C.byref(lim), _ptr(filt),
+                                           1 if reachable else 0, C.byref(handle)), detail)
+        self.graph = graph
+        self.handle = handle.value
+
+    @classmethod
+    def reachable_set(cls, graph: GraphVersion, starts, max_depth=None, direction="out",
+                      interrupts=None) -> "BfsCursor":
+        """bfs_cursor.rs:75-88."""
+        return cls(graph, starts, None, Limits(max_depth, None), direction, True, interrupts)
+
+    def next_level(self, visitor=None, interrupts=None):
+        """bfs_cursor.rs:90-126: runs the next level and hands its visits
+        to `visitor` (a callable; a true return breaks, as
+        ControlFlow::Break) or returns them when no visitor is given.
+        Returns (visits, more) without a visitor, else `more`."""
+        if self.handle is None:
+            raise ValueError("cursor closed")
+        call, detail = _call(interrupts)
+        count = C.c_uint64(0)
+        more = C.c_int32(0)
+        lib = A.load()
+        _raise(lib.wc_bfs_cursor_next(self.handle, C.byref(call), C.byref(count),
+                                      C.byref(more)), detail)
+        rows = np.zeros((count.value, 3), np.uint64)
+        if count.value:
+            _raise(lib.wc_bfs_cursor_read(self.handle, 0, count.value, _ptr(rows)), detail)
+        visits = [Visit(int(a), int(b), None if int(c) == A.NO_VIA else int(c)) for a, b, c in rows]
+        if visitor is None:
+            return visits, bool(more.value)
+        for i, visit in enumerate(visits):
+            if visitor(visit):
+                _raise(lib.wc_bfs_cursor_stop(self.handle, C.byref(call), i + 1), detail)
+                return False
+        return bool(more.value)
+
+    def stats(self) -> TraversalStats:
+        stats = A.TraversalStats()
+        _raise(A.load().wc_bfs_cursor_stats(self.handle, C.byref(stats)), A.ErrorDetail())
+        return _stats(stats)
+
+    def close(self):
+        if self.handle is not None:
+            A.load().wc_bfs_cursor_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def components(graph: GraphVersion, labels_out=None, interrupts=None):

@@ -17,6 +17,7 @@
 // frontier's rows outweigh a fourteenth of the unvisited nodes').
 #include <algorithm>
 #include <numeric>
+#include <string>
 
 #include "bfs.h"
 #include "operand.h"
@@ -25,31 +26,6 @@
 namespace wc {
 
 __device__ inline bool bit_at(const uint32_t* b, uint32_t i) { return (b[i >> 5] >> (i & 31)) & 1; }
-
-// The device side of one level, indexed by the level within the chunk the
-// host queued: what the level's kernels read (its frontier and the switch's
-// choice) and what they add up for the next level.
-struct LevelState {
-  uint32_t count;                 // frontier nodes
-  uint32_t pull;                  // the level pulls
-  unsigned long long mf;          // Σ row length (search direction) of the frontier
-  unsigned long long visited_rdeg;  // Σ opposite-direction row length of the visited nodes
-  // Added up by the level's kernels:
-  unsigned long long next_deg;    // Σ row length (search direction) over nodes admitted
-  unsigned long long next_rdeg;   // Σ row length (opposite direction) over nodes admitted
-  unsigned long long edges;       // row entries scanned by a pulled level
-  uint32_t next_count;
-  uint32_t big_count;             // frontier rows deferred to push_big_kernel
-};
-
-// The switch (level.rs:19-29, 184-211 for the reference's; a GPU-tuned one
-// for bfs), evaluated where the level is planned.
-struct SwitchArgs {
-  uint32_t rule;  // SwitchRule
-  uint32_t reverse_allowed;
-  uint64_t n;
-  uint64_t total_rdeg;
-};
 
 __host__ __device__ inline bool level_pulls(const SwitchArgs& a, uint64_t count, uint64_t mf,
                                             uint64_t visited_rdeg) {
@@ -308,19 +284,40 @@ static uint64_t host_degree(const wc_version* v, int direction, uint64_t node) {
   return d;
 }
 
+wc_status Search::buffer(Ctx& ctx, int tag, uint64_t bytes, DevBuf** out) {
+  if (!owned) return ctx.scratch(tag, bytes, out);
+  DevBuf& b = (*owned)[tag];
+  if (b.bytes < bytes) WC_TRY(b.alloc(ctx.budget, bytes, ctx.detail));
+  *out = &b;
+  return WC_OK;
+}
+
 wc_status Search::run(Ctx& ctx, int dir, const uint64_t* starts_in, uint64_t start_count,
-                      uint32_t max_depth, const uint64_t* filter_host, SwitchRule rule) {
+                      uint32_t max_depth_in, const uint64_t* filter_host, SwitchRule rule) {
+  WC_TRY(start(ctx, dir, starts_in, start_count, max_depth_in, filter_host, rule));
+  return advance(ctx, UINT32_MAX);
+}
+
+wc_status Search::start(Ctx& ctx, int dir, const uint64_t* starts_in, uint64_t start_count,
+                        uint32_t max_depth_in, const uint64_t* filter_host, SwitchRule rule) {
   wc_version* v = ctx.v;
   const uint64_t n = v->n;
   direction = dir;
+  max_depth = max_depth_in;
   if (dir < WC_OUT || dir > WC_BOTH) return WC_INVALID_ARGUMENT;
   if (dir != WC_OUT && !v->reverse_given) return WC_REVERSE_CSR_MISSING;
   // The starts, repeats dropped, first occurrence kept (level.rs:125-147).
   std::vector<uint64_t> host_starts;
   if (start_count) {
     host_starts.resize(start_count);
-    WC_CUDA(cudaMemcpy(host_starts.data(), starts_in, start_count * 8, cudaMemcpyDefault),
-            ctx.detail);
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, starts_in) == cudaSuccess && pa.type == cudaMemoryTypeDevice) {
+      WC_CUDA(cudaMemcpy(host_starts.data(), starts_in, start_count * 8, cudaMemcpyDeviceToHost),
+              ctx.detail);
+    } else {
+      (void)cudaGetLastError();
+      std::memcpy(host_starts.data(), starts_in, start_count * 8);
+    }
   }
   for (uint64_t s : host_starts)
     if (s >= n) {
@@ -340,38 +337,25 @@ wc_status Search::run(Ctx& ctx, int dir, const uint64_t* starts_in, uint64_t sta
       }
     }
   }
-  WC_TRY(ctx.scratch(POOL_BFS_DEPTH, n * 4, &depth));
-  WC_TRY(ctx.scratch(POOL_BFS_VIA, n * 8, &via));
-  WC_TRY(ctx.scratch(POOL_BFS_Q0, std::max<uint64_t>(n, 1) * 4, &queue[0]));
-  WC_TRY(ctx.scratch(POOL_BFS_Q1, std::max<uint64_t>(n, 1) * 4, &queue[1]));
+  WC_TRY(buffer(ctx, POOL_BFS_DEPTH, n * 4, &depth));
+  WC_TRY(buffer(ctx, POOL_BFS_VIA, n * 8, &via));
+  WC_TRY(buffer(ctx, POOL_BFS_Q0, std::max<uint64_t>(n, 1) * 4, &queue[0]));
+  WC_TRY(buffer(ctx, POOL_BFS_Q1, std::max<uint64_t>(n, 1) * 4, &queue[1]));
   const uint64_t words = (n + 31) / 32;
-  WC_TRY(ctx.scratch(POOL_BFS_FBITS, std::max<uint64_t>(words, 1) * 4 * 2, &fbits));
-  WC_TRY(ctx.scratch(POOL_BFS_COUNTERS, (kChunkLevels + 1) * sizeof(LevelState), &counters));
-  WC_TRY(ctx.scratch(POOL_BFS_BIG, (v->m / kBigRow + 2) * 4 * (dir == WC_BOTH ? 2 : 1), &big));
-  const uint64_t* filter_dev = nullptr;
+  WC_TRY(buffer(ctx, POOL_BFS_FBITS, std::max<uint64_t>(words, 1) * 4 * 2, &fbits));
+  WC_TRY(buffer(ctx, POOL_BFS_COUNTERS, (kChunkLevels + 1) * sizeof(LevelState), &counters));
+  WC_TRY(buffer(ctx, POOL_BFS_BIG, (v->m / kBigRow + 2) * 4 * (dir == WC_BOTH ? 2 : 1), &big));
+  filter = nullptr;
   if (filter_host) {
-    WC_TRY(ctx.scratch(POOL_BFS_FILTER, ((n + 63) / 64) * 8, &filter));
+    WC_TRY(buffer(ctx, POOL_BFS_FILTER, ((n + 63) / 64) * 8, &filter));
     WC_CUDA(cudaMemcpyAsync(filter->ptr, filter_host, ((n + 63) / 64) * 8, cudaMemcpyDefault,
                             ctx.stream), ctx.detail);
-    filter_dev = filter->as<uint64_t>();
   }
-  WC_CUDA(cudaMemsetAsync(depth->ptr, 0xff, n * 4, ctx.stream), ctx.detail);
-  WC_CUDA(cudaMemsetAsync(via->ptr, 0xff, n * 8, ctx.stream), ctx.detail);
-  WC_CUDA(cudaMemsetAsync(fbits->ptr, 0, std::max<uint64_t>(words, 1) * 4 * 2, ctx.stream),
-          ctx.detail);
+  // The device state (depths, vias, bitmaps, the seeds) is set up with the
+  // first levels queued, in the same graph (enqueue_init).
+  init_pending = true;
   const uint32_t count0 = (uint32_t)seeds.size();
-  uint32_t* fb[2] = {fbits->as<uint32_t>(), fbits->as<uint32_t>() + std::max<uint64_t>(words, 1)};
-  if (count0) {
-    WC_CUDA(cudaMemcpyAsync(queue[0]->ptr, seeds.data(), count0 * 4, cudaMemcpyHostToDevice,
-                            ctx.stream), ctx.detail);
-    note_launch(), seed_kernel<<<(count0 + 255) / 256, 256, 0, ctx.stream>>>(queue[0]->as<uint32_t>(), count0,
-                                                             depth->as<uint32_t>());
-    note_launch(), set_bits_kernel<<<(count0 + 255) / 256, 256, 0, ctx.stream>>>(
-        queue[0]->as<uint32_t>(), count0, fb[0]);
-  }
-  const Rows adj = rows_of(v, dir);
   const int rdir = dir == WC_OUT ? WC_IN : (dir == WC_IN ? WC_OUT : WC_BOTH);
-  const Rows radj = rows_of(v, rdir);
   // Row lengths of the frontier (search direction) and of every node in
   // the opposite direction: what Beamer's switch compares.
   uint64_t mf = 0, visited_rdeg = 0;
@@ -380,45 +364,127 @@ wc_status Search::run(Ctx& ctx, int dir, const uint64_t* starts_in, uint64_t sta
     mf += host_degree(v, dir, s);
     visited_rdeg += host_degree(v, rdir, s);
   }
-  const SwitchArgs sw{(uint32_t)rule, (uint32_t)reverse_allowed, n, total_rdeg};
+  sw = SwitchArgs{(uint32_t)rule, (uint32_t)reverse_allowed, n, total_rdeg};
   stats = wc_traversal_stats{};
   stats.nodes_visited = count0;
   levels.clear();
+  depth_reached = 0;
+  last_admitted = count0;
+  next_plan = LevelState{};
+  next_plan.count = max_depth > 0 ? count0 : 0;
+  next_plan.mf = mf;
+  next_plan.visited_rdeg = visited_rdeg;
+  next_plan.pull = next_plan.count && level_pulls(sw, next_plan.count, mf, visited_rdeg);
+  return WC_OK;
+}
+
+// Sets the device state up: every depth unreached, every via none, the
+// bitmaps clear, the seeds at depth 0 in the first queue and bitmap.  The
+// seeds come from the pinned staging area when they fit (so that the
+// sequence can be captured and replayed), else from host memory.
+wc_status Search::enqueue_init(Ctx& ctx, bool staged) {
+  const uint64_t n = ctx.v->n;
+  const uint64_t words = std::max<uint64_t>((n + 31) / 32, 1);
+  const uint32_t count0 = (uint32_t)seeds.size();
+  WC_CUDA(cudaMemsetAsync(depth->ptr, 0xff, n * 4, ctx.stream), ctx.detail);
+  WC_CUDA(cudaMemsetAsync(via->ptr, 0xff, n * 8, ctx.stream), ctx.detail);
+  WC_CUDA(cudaMemsetAsync(fbits->ptr, 0, words * 4 * 2, ctx.stream), ctx.detail);
+  if (count0) {
+    const void* src = staged ? (const void*)(ctx.v->stage_host + kStagePayload)
+                             : (const void*)seeds.data();
+    WC_CUDA(cudaMemcpyAsync(queue[0]->ptr, src, count0 * 4, cudaMemcpyHostToDevice, ctx.stream),
+            ctx.detail);
+    note_launch(), seed_kernel<<<(count0 + 255) / 256, 256, 0, ctx.stream>>>(
+        queue[0]->as<uint32_t>(), count0, depth->as<uint32_t>());
+    note_launch(), set_bits_kernel<<<(count0 + 255) / 256, 256, 0, ctx.stream>>>(
+        queue[0]->as<uint32_t>(), count0, fbits->as<uint32_t>());
+  }
+  return cuda_status(cudaGetLastError(), ctx.detail, "bfs init");
+}
+
+wc_status Search::advance(Ctx& ctx, uint32_t max_levels) {
+  wc_version* v = ctx.v;
+  const uint64_t n = v->n;
+  const uint64_t words = (n + 31) / 32;
+  const int dir = direction;
+  const int rdir = dir == WC_OUT ? WC_IN : (dir == WC_IN ? WC_OUT : WC_BOTH);
+  const Rows adj = rows_of(v, dir);
+  const Rows radj = rows_of(v, rdir);
+  uint32_t* fb[2] = {fbits->as<uint32_t>(), fbits->as<uint32_t>() + std::max<uint64_t>(words, 1)};
+  const uint64_t* filter_dev = filter ? filter->as<uint64_t>() : nullptr;
+  LevelState* st = counters->as<LevelState>();
+  const uint32_t blocks = max_blocks(8);
+  // A warp per frontier node; rows longer than kBigRow go to push_big_kernel.
+  const uint32_t push_grid = max_blocks(2);
+  const uint32_t pull_grid = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)((n + 255) / 256), blocks));
+  const uint32_t end_grid = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)((words + 255) / 256), blocks));
+  uint32_t& d = depth_reached;
+  const uint32_t stop_at = (uint32_t)std::min<uint64_t>(max_depth, (uint64_t)d + max_levels);
+  static_assert((kChunkLevels + 1) * sizeof(LevelState) <= kStagePlanBytes, "plan staging");
+  LevelState* plan = reinterpret_cast<LevelState*>(v->stage_host + kStagePlan);
+  const bool seeds_fit = seeds.size() * 4 <= kStageBytes - kStagePayload;
+  if (init_pending && (!seeds_fit || !(next_plan.count > 0 && d < stop_at))) {
+    // No level follows, or the seeds do not fit the staging area: set the
+    // state up on its own.
+    init_pending = false;
+    WC_TRY(enqueue_init(ctx, false));
+  }
   // The levels are queued kChunkLevels at a time with no round trip: each
   // level's kernels read its plan from the device (level_end_kernel writes
   // it), and those of a level with no frontier return at once.  The host
   // reads the chunk's plans back once, to go on or stop and for the stats.
-  LevelState first{};
-  first.count = max_depth > 0 ? count0 : 0;
-  first.mf = mf;
-  first.visited_rdeg = visited_rdeg;
-  first.pull = first.count && level_pulls(sw, first.count, mf, visited_rdeg);
-  LevelState* st = counters->as<LevelState>();
-  const uint32_t blocks = max_blocks(8);
-  const uint32_t pull_grid = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)((n + 255) / 256), blocks));
-  const uint32_t end_grid = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)((words + 255) / 256), blocks));
-  uint32_t d = 0;
-  std::vector<LevelState> plan(kChunkLevels + 1);
-  while (first.count > 0 && d < max_depth) {
+  while (next_plan.count > 0 && d < stop_at) {
     if (ctx.cancelled()) return WC_CANCELLED;
-    WC_CUDA(cudaMemsetAsync(st, 0, (kChunkLevels + 1) * sizeof(LevelState), ctx.stream), ctx.detail);
-    WC_CUDA(cudaMemcpyAsync(st, &first, sizeof first, cudaMemcpyHostToDevice, ctx.stream), ctx.detail);
-    const uint32_t chunk = (uint32_t)std::min<uint64_t>(kChunkLevels, (uint64_t)max_depth - d);
-    for (uint32_t q = 0; q < chunk; q++) {
-      const uint32_t L = d + q;
-      LevelArgs a{adj, radj, st + q, queue[L & 1]->as<uint32_t>(), queue[(L + 1) & 1]->as<uint32_t>(),
-                  fb[L & 1], fb[(L + 1) & 1], big->as<uint32_t>(), L + 1, (uint32_t)n,
-                  depth->as<uint32_t>(), via->as<unsigned long long>(), filter_dev};
-      note_launch(), push_kernel<<<blocks, 256, 0, ctx.stream>>>(a);
-      note_launch(), push_big_kernel<<<blocks, 256, 0, ctx.stream>>>(a);
-      note_launch(), pull_kernel<<<pull_grid, 256, 0, ctx.stream>>>(a, 1);
-      // The bitmap of level L + 2 is level L's: clear it for the admits of L + 1.
-      note_launch(), level_end_kernel<<<end_grid, 256, 0, ctx.stream>>>(
-          st + q, sw, L + 1 >= max_depth ? 1u : 0u, fb[L & 1], (uint32_t)words, v->cancel_dev);
-    }
-    WC_CUDA(cudaGetLastError(), ctx.detail);
-    WC_CUDA(cudaMemcpyAsync(plan.data(), st, (chunk + 1) * sizeof(LevelState), cudaMemcpyDeviceToHost,
-                            ctx.stream), ctx.detail);
+    const uint32_t chunk = std::min<uint32_t>(kChunkLevels, stop_at - d);
+    const uint32_t d0 = d;
+    const bool init = init_pending;
+    init_pending = false;
+    // What varies from call to call goes through the pinned staging area:
+    // the first level's plan and the seeds.
+    plan[0] = next_plan;
+    if (init && !seeds.empty())
+      std::memcpy(v->stage_host + kStagePayload, seeds.data(), seeds.size() * 4);
+    // Every argument of the chunk's launches, so that a repeat of the same
+    // shape replays the graph without capturing it.
+    std::string args;
+    auto put = [&](const void* p, size_t bytes) { args.append((const char*)p, bytes); };
+    const uint64_t head[] = {chunk, d0, max_depth, init ? seeds.size() : UINT64_MAX, n,
+                             (uint64_t)(uintptr_t)st, (uint64_t)(uintptr_t)v->cancel_dev,
+                             (uint64_t)(uintptr_t)depth->ptr, (uint64_t)(uintptr_t)via->ptr,
+                             (uint64_t)(uintptr_t)fbits->ptr, (uint64_t)(uintptr_t)queue[0]->ptr,
+                             (uint64_t)(uintptr_t)queue[1]->ptr, (uint64_t)(uintptr_t)big->ptr,
+                             (uint64_t)(uintptr_t)filter_dev, (uint64_t)(uintptr_t)adj.off0,
+                             (uint64_t)(uintptr_t)adj.off1, (uint64_t)(uintptr_t)radj.off0,
+                             (uint64_t)(uintptr_t)radj.off1, push_grid, pull_grid, end_grid, blocks,
+                             (uint64_t)(uintptr_t)v->stage_host};
+    put(head, sizeof head);
+    put(&sw, sizeof sw);
+    // The chunk's launches go out as one graph: a search of a few levels
+    // costs one launch's latency, and a repeat of the same shape (the same
+    // buffers, depth cap and seed count) no capture either.
+    WC_TRY(ctx.run_cached("plainbfs/" + std::to_string(chunk), args, [&]() -> wc_status {
+      if (init) WC_TRY(enqueue_init(ctx, true));
+      WC_CUDA(cudaMemsetAsync(st, 0, (kChunkLevels + 1) * sizeof(LevelState), ctx.stream),
+              ctx.detail);
+      WC_CUDA(cudaMemcpyAsync(st, plan, sizeof(LevelState), cudaMemcpyHostToDevice, ctx.stream),
+              ctx.detail);
+      for (uint32_t q = 0; q < chunk; q++) {
+        const uint32_t L = d0 + q;
+        LevelArgs a{adj, radj, st + q, queue[L & 1]->as<uint32_t>(),
+                    queue[(L + 1) & 1]->as<uint32_t>(), fb[L & 1], fb[(L + 1) & 1],
+                    big->as<uint32_t>(), L + 1, (uint32_t)n, depth->as<uint32_t>(),
+                    via->as<unsigned long long>(), filter_dev};
+        note_launch(), push_kernel<<<push_grid, 256, 0, ctx.stream>>>(a);
+        note_launch(), push_big_kernel<<<blocks, 256, 0, ctx.stream>>>(a);
+        note_launch(), pull_kernel<<<pull_grid, 256, 0, ctx.stream>>>(a, 1);
+        // The bitmap of level L + 2 is level L's: clear it for the admits of L + 1.
+        note_launch(), level_end_kernel<<<end_grid, 256, 0, ctx.stream>>>(
+            st + q, sw, L + 1 >= max_depth ? 1u : 0u, fb[L & 1], (uint32_t)words, v->cancel_dev);
+      }
+      WC_CUDA(cudaMemcpyAsync(plan, st, (kChunkLevels + 1) * sizeof(LevelState),
+                              cudaMemcpyDeviceToHost, ctx.stream), ctx.detail);
+      return cuda_status(cudaGetLastError(), ctx.detail, "bfs levels");
+    }));
     WC_CUDA(cudaStreamSynchronize(ctx.stream), ctx.detail);
     for (uint32_t q = 0; q < chunk; q++) {
       const LevelState& h = plan[q];
@@ -427,14 +493,19 @@ wc_status Search::run(Ctx& ctx, int dir, const uint64_t* starts_in, uint64_t sta
       levels.push_back(Level{pull, h.count, h.mf, pull ? (uint64_t)h.edges : h.mf, h.next_count});
       stats.levels++;
       if (pull) stats.pulled_levels++;
-      stats.edges_traversed += pull && rule == REFERENCE_SWITCH ? h.edges : h.mf;
+      stats.edges_traversed += pull && sw.rule == REFERENCE_SWITCH ? h.edges : h.mf;
       stats.nodes_visited += h.next_count;
+      last_admitted = h.next_count;
       d++;
     }
-    if (plan[chunk].count == 0) break;
-    first = plan[chunk];
-    first.next_deg = first.next_rdeg = first.edges = 0;
-    first.next_count = first.big_count = 0;
+    const bool more = plan[chunk].count != 0;
+    next_plan = plan[chunk];
+    // A chunk cut short by max_levels leaves the next level planned; the
+    // depth cap or an empty frontier leaves nothing to plan.
+    if (d >= max_depth) next_plan.count = 0;
+    next_plan.next_deg = next_plan.next_rdeg = next_plan.edges = 0;
+    next_plan.next_count = next_plan.big_count = 0;
+    if (!more) break;
   }
   return WC_OK;
 }
@@ -485,53 +556,241 @@ wc_status Search::ordered(Ctx& ctx, std::vector<uint64_t>& rows, bool with_via) 
   return WC_OK;
 }
 
+// The row entries a pushed level scans up to and including the entry that
+// offers `node` from `via`: the rows of the frontier nodes (ascending)
+// before `via`, then `via`'s rows up to the node.
+static wc_status push_scan(Ctx& ctx, int direction, const std::vector<uint64_t>& frontier_sorted,
+                           uint64_t node, uint64_t via, uint64_t* edges_out) {
+  wc_version* v = ctx.v;
+  uint64_t edges = 0;
+  for (uint64_t f : frontier_sorted) {
+    if (f == via) break;
+    edges += host_degree(v, direction, f);
+  }
+  uint64_t pos = 0;
+  bool found = false;
+  for (int part = 0; part < 2 && !found; part++) {
+    const bool use_fwd = part == 0 && direction != WC_IN;
+    const bool use_rev = part == 0 ? direction == WC_IN : direction == WC_BOTH;
+    if (!use_fwd && !use_rev) continue;
+    const DevCsr& csr = use_fwd ? v->fwd : v->rev;
+    const std::vector<uint64_t>& ho = use_fwd ? v->host_offsets : v->host_rev_offsets;
+    const uint64_t lo = ho[via], hi = ho[via + 1];
+    std::vector<uint32_t> row(hi - lo);
+    if (hi > lo)
+      WC_CUDA(cudaMemcpy(row.data(), csr.targets.as<uint32_t>() + lo, (hi - lo) * 4,
+                         cudaMemcpyDeviceToHost), ctx.detail);
+    for (uint64_t k = 0; k < row.size(); k++)
+      if (row[k] == node) {
+        pos += k + 1;
+        found = true;
+        break;
+      }
+    if (!found) pos += row.size();
+  }
+  *edges_out = edges + pos;
+  return WC_OK;
+}
+
 // The row entries a push-only search scans up to and including the entry
 // that offers visit `index` of `rows` (the reference's order): every row of
 // the levels before it, then in its level the rows of the frontier nodes
 // before its `via`, and `via`'s rows up to the visit's node.
 static wc_status scan_through(Ctx& ctx, const Search& s, const std::vector<uint64_t>& rows,
                               uint64_t index, uint64_t* edges_out) {
-  wc_version* v = ctx.v;
-  const int direction = s.direction;
   const uint64_t total = rows.size() / 3;
   const uint64_t node = rows[3 * index];
   const uint32_t d = (uint32_t)rows[3 * index + 1];
   uint64_t edges = 0;
   if (d > 0) {
     for (uint32_t l = 0; l + 1 < d; l++) edges += s.levels[l].frontier_entries;
-    const uint64_t via = rows[3 * index + 2];
     std::vector<uint64_t> frontier;
     for (uint64_t r = 0; r < total; r++)
       if (rows[3 * r + 1] == d - 1) frontier.push_back(rows[3 * r]);
     std::sort(frontier.begin(), frontier.end());
-    for (uint64_t f : frontier) {
-      if (f == via) break;
-      edges += host_degree(v, direction, f);
-    }
-    uint64_t pos = 0;
-    bool found = false;
-    for (int part = 0; part < 2 && !found; part++) {
-      const bool use_fwd = part == 0 && direction != WC_IN;
-      const bool use_rev = part == 0 ? direction == WC_IN : direction == WC_BOTH;
-      if (!use_fwd && !use_rev) continue;
-      const DevCsr& csr = use_fwd ? v->fwd : v->rev;
-      const std::vector<uint64_t>& ho = use_fwd ? v->host_offsets : v->host_rev_offsets;
-      const uint64_t lo = ho[via], hi = ho[via + 1];
-      std::vector<uint32_t> row(hi - lo);
-      if (hi > lo)
-        WC_CUDA(cudaMemcpy(row.data(), csr.targets.as<uint32_t>() + lo, (hi - lo) * 4,
-                           cudaMemcpyDeviceToHost), ctx.detail);
-      for (uint64_t k = 0; k < row.size(); k++)
-        if (row[k] == node) {
-          pos += k + 1;
-          found = true;
-          break;
-        }
-      if (!found) pos += row.size();
-    }
-    edges += pos;
+    uint64_t within = 0;
+    WC_TRY(push_scan(ctx, s.direction, frontier, node, rows[3 * index + 2], &within));
+    edges += within;
   }
   *edges_out = edges;
+  return WC_OK;
+}
+
+// The rows of one level's admitted nodes, for ordering on the host:
+// (node, via, 1 if the node is not in via's forward row (Both only)).
+__global__ void level_rows_kernel(const uint32_t* nodes, uint32_t count,
+                                  const unsigned long long* via, const uint32_t* off,
+                                  const uint32_t* tgt, int both, unsigned long long* out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const uint32_t v = nodes[i];
+    const unsigned long long w = via[v];
+    unsigned long long second = 0;
+    if (both && w != WC_NO_VIA) {
+      second = 1;
+      uint32_t lo = off[w], hi = off[w + 1];
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) / 2;
+        const uint32_t t = tgt[mid];
+        if (t == v) {
+          second = 0;
+          break;
+        }
+        if (t < v) lo = mid + 1;
+        else hi = mid;
+      }
+    }
+    out[3 * (uint64_t)i] = v;
+    out[3 * (uint64_t)i + 1] = w;
+    out[3 * (uint64_t)i + 2] = second;
+  }
+}
+
+// The row entries a pulled level (level.rs:243-282) scans through node
+// `last`: each node not visited before the level (depth unreached, or the
+// level's own `depth`), ascending, scans its opposite-direction rows in
+// order up to its first frontier node (depth - 1), or all of them.
+__global__ void pulled_scan_kernel(Rows radj, const uint32_t* depth, uint32_t level_depth,
+                                   uint32_t last, unsigned long long* out) {
+  unsigned long long sum = 0;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t v = blockIdx.x * blockDim.x + threadIdx.x; v <= last; v += stride) {
+    const uint32_t dv = depth[v];
+    if (dv != WC_UNREACHED && dv != level_depth) continue;
+    bool hit = false;
+    for (int part = 0; part < 2 && !hit; part++) {
+      const uint32_t* off = part == 0 ? radj.off0 : radj.off1;
+      const uint32_t* tgt = part == 0 ? radj.tgt0 : radj.tgt1;
+      if (!off) break;
+      const uint32_t lo = __ldg(off + v), hi = __ldg(off + v + 1);
+      for (uint32_t e = lo; e < hi; e++) {
+        sum++;
+        if (depth[__ldg(tgt + e)] == level_depth - 1) {
+          hit = true;
+          break;
+        }
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
+  if ((threadIdx.x & 31) == 0 && sum) atomicAdd(out, sum);
+}
+
+}  // namespace wc
+
+// traversal/bfs_cursor.rs:17-138 (BfsCursor): a search that lives across
+// calls, one level per wc_bfs_cursor_next, with its own device buffers.
+struct wc_bfs_cursor {
+  wc_version* v = nullptr;
+  wc::Search search;
+  std::map<int, wc::DevBuf> bufs;  // the search's buffers, charged to the version's budget
+  bool reachable = false;          // reachable_set's form: levels may be pulled
+  uint64_t max_results = UINT64_MAX;
+  uint64_t emitted = 0;            // visits handed out so far
+  bool seeded = false, finished = false;
+  std::vector<uint64_t> rows;      // the last level's visits: (node, depth, via)
+  std::vector<uint64_t> frontier;  // the frontier it expanded, ascending
+  bool pulled_order = false;       // the last level came in ascending node order
+  wc_traversal_stats before{};     // the stats before the last level
+  wc_traversal_stats stats{};
+};
+
+namespace wc {
+
+// The stats of a search cut inside the cursor's last level: the visit at
+// `index` of the level is the last one scanned (the refused one of a
+// truncation, or the one a visitor broke at), `nodes` visits of the level
+// were admitted.
+static wc_status cut_stats(Ctx& ctx, wc_bfs_cursor* c, uint64_t index, uint64_t nodes,
+                           bool truncated) {
+  wc_traversal_stats st = c->stats;
+  st.nodes_visited = c->before.nodes_visited + nodes;
+  st.truncated = truncated ? 1 : 0;
+  st.edges_traversed = c->before.edges_traversed;
+  const uint64_t node = c->rows[3 * index];
+  const uint32_t d = (uint32_t)c->rows[3 * index + 1];
+  if (d > 0) {
+    uint64_t within = 0;
+    if (c->pulled_order) {
+      const int dir = c->search.direction;
+      const int rdir = dir == WC_OUT ? WC_IN : (dir == WC_IN ? WC_OUT : WC_BOTH);
+      DevBuf* sum;
+      WC_TRY(ctx.scratch(POOL_BFS_SCAN, 8, &sum));
+      WC_CUDA(cudaMemsetAsync(sum->ptr, 0, 8, ctx.stream), ctx.detail);
+      note_launch(), pulled_scan_kernel<<<max_blocks(8), 256, 0, ctx.stream>>>(
+          rows_of(ctx.v, rdir), c->search.depth->as<uint32_t>(), d, (uint32_t)node,
+          sum->as<unsigned long long>());
+      WC_CUDA(cudaMemcpyAsync(&within, sum->ptr, 8, cudaMemcpyDeviceToHost, ctx.stream),
+              ctx.detail);
+      WC_CUDA(cudaStreamSynchronize(ctx.stream), ctx.detail);
+    } else {
+      WC_TRY(push_scan(ctx, c->search.direction, c->frontier, node, c->rows[3 * index + 2],
+                       &within));
+    }
+    st.edges_traversed += within;
+  }
+  c->stats = st;
+  return WC_OK;
+}
+
+// Expands the cursor's next level into c->rows, in the reference's order.
+static wc_status cursor_level(Ctx& ctx, wc_bfs_cursor* c) {
+  Search& s = c->search;
+  c->pulled_order = false;
+  if (!c->seeded) {
+    c->seeded = true;
+    c->rows.clear();
+    c->frontier.clear();
+    for (uint32_t x : s.seeds) c->rows.insert(c->rows.end(), {(uint64_t)x, 0, WC_NO_VIA});
+    c->stats = s.stats;
+    return WC_OK;
+  }
+  // The frontier this level expands: the last level's nodes, ascending.
+  c->frontier.clear();
+  for (size_t r = 0; r < c->rows.size(); r += 3) c->frontier.push_back(c->rows[r]);
+  std::sort(c->frontier.begin(), c->frontier.end());
+  c->rows.clear();
+  const size_t had = s.levels.size();
+  const uint32_t L = s.depth_reached;
+  WC_TRY(s.advance(ctx, 1));
+  WC_TRY(ctx.finish());
+  c->stats = s.stats;
+  if (s.levels.size() == had) return WC_OK;
+  const Level& lv = s.levels.back();
+  // bfs reports its levels as pushed whichever form ran; reachable_set
+  // lists a pulled level by node.
+  c->pulled_order = lv.pulled && c->reachable;
+  const uint32_t k = lv.admitted;
+  if (k == 0) return WC_OK;
+  DevBuf* out;
+  WC_TRY(ctx.scratch(POOL_BFS_ROWS, (uint64_t)k * 24, &out));
+  const bool both = s.direction == WC_BOTH;
+  note_launch(), level_rows_kernel<<<std::min<uint32_t>((k + 255) / 256, max_blocks(4)), 256, 0,
+                                     ctx.stream>>>(
+      s.queue[(L + 1) & 1]->as<uint32_t>(), k, s.via->as<unsigned long long>(),
+      ctx.v->fwd.offsets.as<uint32_t>(), ctx.v->fwd.targets.as<uint32_t>(), both ? 1 : 0,
+      out->as<unsigned long long>());
+  std::vector<uint64_t> raw((uint64_t)k * 3);
+  WC_CUDA(cudaMemcpyAsync(raw.data(), out->ptr, (uint64_t)k * 24, cudaMemcpyDeviceToHost,
+                          ctx.stream), ctx.detail);
+  WC_CUDA(cudaStreamSynchronize(ctx.stream), ctx.detail);
+  // A pushed level in the order reached: by via (frontier rows ascending),
+  // then the forward row's nodes before the reverse row's (Both), then by
+  // position in the row (rows are ascending); a pulled one by node.
+  std::vector<uint32_t> idx(k);
+  std::iota(idx.begin(), idx.end(), 0u);
+  const bool by_node = c->pulled_order;
+  std::sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) {
+    const uint64_t* x = &raw[3 * (uint64_t)a];
+    const uint64_t* y = &raw[3 * (uint64_t)b];
+    if (!by_node) {
+      if (x[1] != y[1]) return x[1] < y[1];
+      if (x[2] != y[2]) return x[2] < y[2];
+    }
+    return x[0] < y[0];
+  });
+  c->rows.reserve((uint64_t)k * 3);
+  for (uint32_t i : idx)
+    c->rows.insert(c->rows.end(), {raw[3 * (uint64_t)i], (uint64_t)L + 1, raw[3 * (uint64_t)i + 1]});
   return WC_OK;
 }
 
@@ -674,6 +933,124 @@ wc_status wc_reachable(wc_version* v, const wc_call* call, wc_direction directio
     }
   if (stats) *stats = st;
   return WC_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+wc_status wc_bfs_cursor_open(wc_version* v, const wc_call* call, wc_direction direction,
+                             const uint64_t* starts, uint64_t start_count, const wc_limits* limits,
+                             const uint64_t* filter, int32_t reachable_set, wc_bfs_cursor** out) {
+  if (!v || !out || (start_count && !starts)) return WC_INVALID_ARGUMENT;
+  *out = nullptr;
+  const uint32_t max_depth = limits ? limits->max_depth : WC_UNREACHED;
+  const uint64_t max_results = limits ? limits->max_results : UINT64_MAX;
+  // reachable_set takes no filter and no result limit (reachable.rs:48-58).
+  if (reachable_set && (filter || max_results != UINT64_MAX)) return WC_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lock(v->mu);
+  WC_CUDA(cudaSetDevice(v->device), call ? call->detail : nullptr);
+  std::unique_ptr<wc_bfs_cursor> c(new wc_bfs_cursor);
+  c->v = v;
+  c->reachable = reachable_set != 0;
+  c->max_results = max_results;
+  c->search.owned = &c->bufs;
+  if (c->reachable) {
+    c->search.reverse_allowed = v->reverse_given;
+    c->search.ordering_by_node_in_pulled = true;
+  }
+  Ctx ctx(v, call);
+  if (ctx.cancelled()) return WC_CANCELLED;
+  WC_TRY(ctx.begin());
+  WC_TRY(c->search.start(ctx, direction, starts, start_count, max_depth, filter,
+                         c->reachable ? REFERENCE_SWITCH : GPU_SWITCH));
+  WC_TRY(ctx.finish());
+  v->cursors.fetch_add(1);
+  *out = c.release();
+  return WC_OK;
+}
+
+wc_status wc_bfs_cursor_next(wc_bfs_cursor* c, const wc_call* call, uint64_t* count,
+                             int32_t* more) {
+  if (!c || !count) return WC_INVALID_ARGUMENT;
+  *count = 0;
+  if (more) *more = 0;
+  if (c->finished) {
+    c->rows.clear();
+    return WC_OK;
+  }
+  wc_version* v = c->v;
+  std::lock_guard<std::recursive_mutex> lock(v->mu);
+  WC_CUDA(cudaSetDevice(v->device), call ? call->detail : nullptr);
+  Ctx ctx(v, call);
+  // Interrupts are polled before any work (interrupts.rs; the seed's first
+  // admission polls, and so does each expansion).
+  if (ctx.cancelled()) return WC_CANCELLED;
+  WC_TRY(ctx.begin());
+  c->before = c->stats;
+  WC_TRY(cursor_level(ctx, c));
+  const uint64_t k = c->rows.size() / 3;
+  if (c->max_results - c->emitted < k) {
+    // bfs.rs:96-110: the visit past max_results is refused and the search
+    // stops there.
+    const uint64_t keep = c->max_results - c->emitted;
+    WC_TRY(cut_stats(ctx, c, keep, keep, true));
+    c->rows.resize(3 * keep);
+    c->finished = true;
+  } else {
+    c->finished = c->search.exhausted();
+  }
+  c->emitted += c->rows.size() / 3;
+  *count = c->rows.size() / 3;
+  if (more) *more = c->finished ? 0 : 1;
+  return WC_OK;
+}
+
+wc_status wc_bfs_cursor_read(const wc_bfs_cursor* c, uint64_t first, uint64_t rows,
+                             uint64_t* visits_out) {
+  if (!c || (rows && !visits_out)) return WC_INVALID_ARGUMENT;
+  const uint64_t have = c->rows.size() / 3;
+  if (first > have || rows > have - first) return WC_INVALID_ARGUMENT;
+  if (rows)
+    WC_CUDA(cudaMemcpy(visits_out, c->rows.data() + 3 * first, rows * 24, cudaMemcpyDefault),
+            nullptr);
+  return WC_OK;
+}
+
+wc_status wc_bfs_cursor_stop(wc_bfs_cursor* c, const wc_call* call, uint64_t consumed) {
+  if (!c) return WC_INVALID_ARGUMENT;
+  const uint64_t have = c->rows.size() / 3;
+  if (consumed == 0 || consumed > have) return WC_INVALID_ARGUMENT;
+  wc_version* v = c->v;
+  std::lock_guard<std::recursive_mutex> lock(v->mu);
+  WC_CUDA(cudaSetDevice(v->device), call ? call->detail : nullptr);
+  Ctx ctx(v, call);
+  // A visitor that breaks admits the visit it broke at (Admission::
+  // AdmitAndStop, level.rs:304-324): the search stops there, not truncated.
+  WC_TRY(cut_stats(ctx, c, consumed - 1, consumed, false));
+  c->rows.resize(3 * consumed);
+  c->emitted = c->emitted - have + consumed;
+  c->finished = true;
+  return WC_OK;
+}
+
+wc_status wc_bfs_cursor_stats(const wc_bfs_cursor* c, wc_traversal_stats* stats) {
+  if (!c || !stats) return WC_INVALID_ARGUMENT;
+  *stats = c->stats;
+  return WC_OK;
+}
+
+void wc_bfs_cursor_destroy(wc_bfs_cursor* c) {
+  if (!c) return;
+  wc_version* v = c->v;
+  {
+    std::lock_guard<std::recursive_mutex> lock(v->mu);
+    cudaSetDevice(v->device);
+    if (v->stream) cudaStreamSynchronize(v->stream);
+    c->bufs.clear();
+  }
+  v->cursors.fetch_sub(1);
+  delete c;
 }
 
 }  // extern "C"

@@ -203,6 +203,14 @@ struct DeviceError {
   uint64_t aux;
 };
 
+// The version's pinned staging area: the device error word's read-back,
+// then a small plan area, then a payload area.
+constexpr uint64_t kStageBytes = 65536;
+constexpr uint64_t kStageError = 0;
+constexpr uint64_t kStagePlan = 64;
+constexpr uint64_t kStagePlanBytes = 4032;
+constexpr uint64_t kStagePayload = kStagePlan + kStagePlanBytes;
+
 // ------------------------------------------------------------------ schedule
 // The row-split schedule of one CSR orientation for the pull kernels: rows
 // grouped into warp tiles (at most kTileRows consecutive rows, at most
@@ -275,6 +283,9 @@ struct wc_version {
   int32_t* cancel_dev = nullptr;
   volatile uint32_t* pace_host = nullptr;  // mapped: [0] iterations done, [1] stopped
   uint32_t* pace_dev = nullptr;
+  // Pinned host staging (wc::kStage*): small per-call uploads and
+  // read-backs, which captured graphs may also copy from and to.
+  uint8_t* stage_host = nullptr;
   std::recursive_mutex mu;             // calls on one handle run one at a time
   double last_margin = 0.0;
   std::map<uint64_t, wc_schedule> tuned;  // (kind << 32 | width) -> schedule
@@ -287,6 +298,11 @@ struct wc_version {
   // Executable CUDA graphs of fixed launch sequences, by shape (see
   // Ctx::run_captured); destroyed with the version.
   std::map<std::string, cudaGraphExec_t> graphs;
+  // The launch arguments each of those graphs was captured with (run_cached).
+  std::map<std::string, std::string> graph_args;
+  // Cursors open over the version (wc_bfs_cursor): it is not released
+  // while any is.
+  std::atomic<uint32_t> cursors{0};
 };
 
 namespace wc {
@@ -296,7 +312,7 @@ enum PoolTag {
   POOL_X = 1, POOL_Y, POOL_MASK, POOL_XCOPY, POOL_SEED,
   POOL_PR_X, POOL_PR_MSG, POOL_PR_OUT, POOL_PR_SHARES, POOL_PR_TOMB, POOL_PR_SCALARS,
   POOL_BFS_DEPTH, POOL_BFS_VIA, POOL_BFS_Q0, POOL_BFS_Q1, POOL_BFS_FBITS, POOL_BFS_COUNTERS,
-  POOL_BFS_FILTER, POOL_BFS_FLAGS, POOL_BFS_BIG = 30,
+  POOL_BFS_FILTER, POOL_BFS_FLAGS, POOL_BFS_BIG = 30, POOL_BFS_ROWS, POOL_BFS_SCAN,
   POOL_BATCH_0 = 40, POOL_BATCH_1, POOL_BATCH_2, POOL_BATCH_3, POOL_BATCH_4, POOL_BATCH_5,
   POOL_BATCH_6, POOL_BATCH_7, POOL_BATCH_8, POOL_BATCH_9, POOL_BATCH_10, POOL_BATCH_11,
   POOL_EIG_0 = 60, POOL_EIG_1, POOL_EIG_2, POOL_EIG_3, POOL_EIG_4, POOL_EIG_5, POOL_EIG_6,
@@ -334,6 +350,7 @@ struct Ctx {
 
   bool timing = false;
   bool capturing = false;  // the stream is being captured by run_captured
+  bool device_error = false;  // finish() returned a status a kernel raised
   struct Timer {
     std::string name;
     cudaEvent_t a, b;
@@ -397,7 +414,30 @@ struct Ctx {
         cs != cudaStreamCaptureStatusNone)
       return enqueue();
     cudaGraphExec_t exec = nullptr;
+    v->graph_args.erase(key);
     WC_TRY(capture(key, enqueue, &exec));
+    return cuda_status(cudaGraphLaunch(exec, stream), detail, "cudaGraphLaunch");
+  }
+
+  // run_captured for a sequence whose launches are fully described by
+  // `args` (every kernel argument, copy and size, flattened): when the
+  // version's graph for `key` was captured with the same `args` it is
+  // launched as it stands, with no capture.  What changes from call to call
+  // must then come through memory (a pinned staging copy in the graph).
+  template <class F> wc_status run_cached(const std::string& key, const std::string& args,
+                                          F&& enqueue) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (!stream || cudaStreamIsCapturing(stream, &cs) != cudaSuccess ||
+        cs != cudaStreamCaptureStatusNone)
+      return enqueue();
+    auto it = v->graphs.find(key);
+    auto at = v->graph_args.find(key);
+    if (it != v->graphs.end() && it->second && at != v->graph_args.end() && at->second == args)
+      return cuda_status(cudaGraphLaunch(it->second, stream), detail, "cudaGraphLaunch");
+    v->graph_args.erase(key);
+    cudaGraphExec_t exec = nullptr;
+    WC_TRY(capture(key, enqueue, &exec));
+    v->graph_args[key] = args;
     return cuda_status(cudaGraphLaunch(exec, stream), detail, "cudaGraphLaunch");
   }
 
@@ -512,11 +552,15 @@ struct Ctx {
     if (!cancel && cancelled()) cancel = true;
     collect_timings();
     DeviceError e;
-    WC_CUDA(cudaMemcpy(&e, v->error.ptr, sizeof e, cudaMemcpyDeviceToHost), detail);
+    WC_CUDA(cudaMemcpyAsync(v->stage_host + kStageError, v->error.ptr, sizeof e,
+                            cudaMemcpyDeviceToHost, stream), detail);
+    WC_CUDA(cudaStreamSynchronize(stream), detail);
+    std::memcpy(&e, v->stage_host + kStageError, sizeof e);
     if (cancel) return WC_CANCELLED;
     if (timed_out) return WC_DEVICE_TIMEOUT;
     if (e.status != 0) {
       if (detail) detail->node = e.aux;
+      device_error = true;
       return (wc_status)e.status;
     }
     return WC_OK;

@@ -154,6 +154,7 @@ wc_status finish_version(wc_version* v, wc_error_detail* detail) {
   WC_CUDA(cudaHostGetDevicePointer((void**)&v->cancel_dev, v->cancel_host, 0), detail);
   v->pace_host = reinterpret_cast<volatile uint32_t*>(v->cancel_host + 1);
   v->pace_dev = reinterpret_cast<uint32_t*>(v->cancel_dev + 1);
+  WC_CUDA(cudaHostAlloc((void**)&v->stage_host, kStageBytes, cudaHostAllocDefault), detail);
   return WC_OK;
 }
 
@@ -272,13 +273,14 @@ wc_status wc_version_upload(uint64_t graph_id, uint64_t version, const wc_csr_ho
 }
 
 wc_status wc_version_release(wc_version* v) {
-  if (!v) return WC_INVALID_ARGUMENT;
+  if (!v || v->cursors.load() != 0) return WC_INVALID_ARGUMENT;
   {
     std::lock_guard<std::recursive_mutex> lock(v->mu);
     if (v->stream) cudaStreamSynchronize(v->stream);
     for (auto& g : v->graphs)
       if (g.second) cudaGraphExecDestroy(g.second);
     if (v->cancel_host) cudaFreeHost(v->cancel_host);
+    if (v->stage_host) cudaFreeHost(v->stage_host);
     if (v->stream) cudaStreamDestroy(v->stream);
   }
   pagerank_part_forget(v);
