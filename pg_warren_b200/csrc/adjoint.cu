@@ -18,6 +18,7 @@
 #include "columns.cuh"
 #include "operand.h"
 #include "pagerank.h"
+#include "pull32.cuh"
 #include "pull_multi.cuh"
 
 namespace wc {
@@ -125,6 +126,88 @@ __global__ void __launch_bounds__(256) adj_rows_kernel(CsrView<W> A, AdjState s,
   pull_multi<double, WC_PLUS_TIMES, W, P>(A, s.lam[cur], epi, s.err, carry);
 }
 
+// The same iteration and final pass over pull32_units (cp.async gathers
+// into a per-warp ring, small blocks, as many warps an SM as the registers
+// allow): a lane is a loss; a loss that has stopped gathers nothing and
+// keeps its λ.
+struct AdjEpi32 {
+  struct Row {
+    double out;
+  };
+  const AdjState* s;
+  int cur;
+  uint32_t run_bits;
+  double pi;
+  double delta = 0.0, total = 0.0;
+  bool final_pass;
+  bool active;
+  __device__ Row row(uint32_t i) const { return Row{s->out[i]}; }
+  __device__ Row shfl(const Row& r, uint32_t src) const {
+    return Row{__shfl_sync(0xffffffffu, r.out, src)};
+  }
+  __device__ void emit(uint32_t i, const Partial<double, WC_OP_PLUS>& acc, const Row& r) {
+    const AdjState& st = *s;
+    const unsigned c = threadIdx.x & 31;
+    const size_t at = (size_t)i * 32 + c;
+    double z = 0.0;
+    if (acc.present) acc.acc.value(&z);
+    const double o = r.out;
+    const double si = (acc.present && o > 0.0) ? z / o : 0.0;
+    if (final_pass) {
+      st.S[at] = si;
+      return;
+    }
+    const double old = st.lam[cur][at];
+    if (!((run_bits >> c) & 1)) {
+      st.lam[cur ^ 1][at] = old;
+      total += old;
+      return;
+    }
+    const double next = st.damping * (si + (o > 0.0 ? 0.0 : pi)) + st.C[at];
+    delta += fabs(next - old);
+    total += next;
+    st.lam[cur ^ 1][at] = next;
+  }
+};
+
+template <class W>
+__global__ void __launch_bounds__(kPull32Warps * 32, 5)
+    adj_iter32_kernel(CsrView<W> A, AdjState s, uint32_t it, Partial<double, WC_OP_PLUS>* carry,
+                      uint32_t max_iter) {
+  const uint32_t run = *(volatile uint32_t*)s.running;
+  if (!run) return;
+  extern __shared__ __align__(16) double adj_smem[];
+  const unsigned c = threadIdx.x & 31;
+  AdjEpi32 epi{&s, (int)(it & 1), run, s.pi[c]};
+  epi.final_pass = false;
+  epi.active = (run >> c) & 1;
+  pull32_units<W>(A, s.lam[it & 1], epi, s.err, carry,
+                  adj_smem + (threadIdx.x >> 5) * kPull32WarpDoubles);
+  double delta = epi.delta, total = epi.total;
+  if (reduce_columns<32>(delta, total, s.partials, s.counter)) {
+    const uint32_t q = threadIdx.x;
+    if (q < 32 && ((run >> q) & 1)) {
+      s.pi[q] = s.p * total;
+      s.iterations[q] = it + 1;
+      if (it + 1 >= max_iter || delta < s.tol) atomicAnd(s.running, ~(1u << q));
+    }
+    if (q == 0) *s.executed = it + 1;
+  }
+}
+
+template <class W>
+__global__ void __launch_bounds__(kPull32Warps * 32, 5)
+    adj_rows32_kernel(CsrView<W> A, AdjState s, Partial<double, WC_OP_PLUS>* carry) {
+  extern __shared__ __align__(16) double adj_smem[];
+  const int cur = *s.executed & 1;
+  const unsigned c = threadIdx.x & 31;
+  AdjEpi32 epi{&s, cur, 0, 0.0};
+  epi.final_pass = true;
+  epi.active = c < s.k;
+  pull32_units<W>(A, s.lam[cur], epi, s.err, carry,
+                  adj_smem + (threadIdx.x >> 5) * kPull32WarpDoubles);
+}
+
 // grad[c][e] = d · x_i / out_i · (λ_j − S_i) for e = (i → j), a warp per
 // unit of the forward schedule; consecutive lanes take consecutive entries
 // so each loss's row of the gradient is written coalesced.
@@ -178,6 +261,13 @@ __global__ void adj_targets_kernel(const uint64_t* targets, const uint64_t* offs
     atomicAdd(C + (size_t)targets[q] * kAdjP + c, 1.0);
 }
 
+// The iterations' blocks: kPull32Warps warps, at most one warp a unit.
+static uint32_t adjoint_grid32(const DevCsr& fwd) {
+  return std::max<uint32_t>(1, std::min<uint32_t>(max_blocks(5),
+                                                  (fwd.schedule.count + kPull32Warps - 1) /
+                                                      kPull32Warps));
+}
+
 template <class W>
 static wc_status adjoint_pass(Ctx& ctx, AdjState& s, const DevCsr& fwd, const void* weights,
                               uint32_t max_iter, Partial<double, WC_OP_PLUS>* carry, double* grad,
@@ -185,10 +275,17 @@ static wc_status adjoint_pass(Ctx& ctx, AdjState& s, const DevCsr& fwd, const vo
   CsrView<W> A{fwd.offsets.as<uint32_t>(), fwd.targets.as<uint32_t>(),
                static_cast<const W*>(weights), fwd.schedule.units.as<Unit>(), fwd.schedule.count,
                fwd.schedule.counters.as<uint32_t>(), nullptr};
+  const uint32_t grid32 = adjoint_grid32(fwd);
+  WC_CUDA(cudaFuncSetAttribute(adj_iter32_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kPull32Smem), ctx.detail);
+  WC_CUDA(cudaFuncSetAttribute(adj_rows32_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kPull32Smem), ctx.detail);
   note_launch(), adj_init_kernel<kAdjP><<<grid, 256, 0, ctx.stream>>>(s);
   for (uint32_t it = 0; it < max_iter; it++)
-    note_launch(), adj_iter_kernel<kAdjP, W><<<grid, 256, 0, ctx.stream>>>(A, s, it, carry, max_iter);
-  note_launch(), adj_rows_kernel<kAdjP, W><<<grid, 256, 0, ctx.stream>>>(A, s, carry);
+    note_launch(), adj_iter32_kernel<W><<<grid32, kPull32Warps * 32, kPull32Smem, ctx.stream>>>(
+        A, s, it, carry, max_iter);
+  note_launch(), adj_rows32_kernel<W><<<grid32, kPull32Warps * 32, kPull32Smem, ctx.stream>>>(
+      A, s, carry);
   note_launch(), adj_scatter_kernel<kAdjP><<<max_blocks(8), 256, 0, ctx.stream>>>(
       fwd.offsets.as<uint32_t>(), fwd.targets.as<uint32_t>(), fwd.schedule.units.as<Unit>(),
       fwd.schedule.count, s, grad);
@@ -240,7 +337,8 @@ wc_status wc_pagerank_adjoint(wc_version* v, const wc_call* call, const wc_pager
   WC_TRY(ctx.scratch(POOL_ADJ_3, n * P * 8 * 2, &lam));
   WC_TRY(ctx.scratch(POOL_ADJ_4, n * P * 8, &Sb));
   WC_TRY(ctx.scratch(POOL_ADJ_5, n * P * 8, &Cb));
-  WC_TRY(ctx.scratch(POOL_ADJ_6, 4096 + (uint64_t)grid * P * 16, &sc));
+  WC_TRY(ctx.scratch(POOL_ADJ_6,
+                     4096 + (uint64_t)std::max(grid, adjoint_grid32(v->fwd)) * P * 16, &sc));
   WC_TRY(ctx.scratch(POOL_ADJ_7, (uint64_t)std::max<uint32_t>(v->fwd.schedule.slots, 1) * P *
                                      sizeof(Partial<double, WC_OP_PLUS>), &carry));
   WC_TRY(ctx.scratch(POOL_ADJ_8, (uint64_t)losses * 4 + 64, &itb));

@@ -30,8 +30,10 @@
 #include "columns.cuh"
 #include "operand.h"
 #include "pagerank.h"
+#include "pull32.cuh"
 #include "pull_multi.cuh"
 #include "sqlfloat.cuh"
+#include "upload.h"
 
 namespace wc {
 
@@ -52,16 +54,20 @@ struct PprCtl {
   double d0;  // the start vector's dangling mass (the same for every set)
 };
 
+// The per-node state (x, msg, out, member, tomb) is kept in the version's
+// locality order (locality.cu), the order of the CSC the iterations pull
+// over; the sets come in and the ranks go out in dense ids.
 struct PprStream {
   uint32_t n, width, max_iter;
   double* x[2];    // n × P
   double* msg[2];  // n × P
   const double* out;       // out-weights
-  uint32_t* member;        // n: bit c set if node i is in slot c's set
+  uint32_t* member;        // n: bit c set if row k's node is in slot c's set
   const double* shares;    // per set: 1 / |set|
   const uint64_t* nodes;   // the sets, CSR
   const uint64_t* offsets;
   const uint64_t* tomb;
+  const uint32_t* perm;    // dense id -> row of the locality order
   double start, damping, teleport, threshold;
   bool has_tol;
   PprCtl* ctl;
@@ -228,48 +234,57 @@ __global__ void __launch_bounds__(256) ppr_iter_kernel(CsrView<W> A, PprStream s
 }
 
 // ------------------------------------------------------ the 32-slot pull
-// With 32 slots a row of the msg operand is 256 bytes and one lane owns one
-// column.  The iteration is bound by the latency of the row gathers, not by
-// bandwidth, so the warp keeps them in flight with asynchronous copies
-// (cp.async) into shared memory instead of registers: a unit's gathers go
-// out 16 entries at a time, two groups in flight, and the tile's old ranks
-// (the R rows of x, contiguous) arrive the same way while the targets,
-// row ends and per-row values load into lanes.  Entries are folded in
-// ascending order per row, as pull_multi folds them, so the ranks are the
-// same to the bit.
+// With 32 slots the iteration is pull32_units (pull32.cuh) with the rank
+// update as its epilogue; it is bound by instruction issue, not bandwidth.
 
-constexpr uint32_t kPpr32Warps = 4;          // warps a block
-constexpr uint32_t kPpr32Chunk = 16;         // entries a gather group
-constexpr uint32_t kPpr32WarpDoubles = 2048;  // old ranks (32 × 32) + ring (2 × 16 × 32)
-
-__device__ inline void cp_async8(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src)
-               : "memory");
-}
-__device__ inline void cp_async16(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src)
-               : "memory");
-}
-__device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N> __device__ inline void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// v[i] for a register array and a run-time i (selects, no local memory).
-template <class T> __device__ inline T pick8(const T (&v)[8], uint32_t i) {
-  T r = v[0];
-#pragma unroll
-  for (uint32_t q = 1; q < 8; q++)
-    if (i == q) r = v[q];
-  return r;
-}
+// The rank update of row i for this lane's slot (pagerank/mod.rs:201-282).
+struct PprEpi32 {
+  struct Row {
+    uint32_t mem;
+    double out;
+    bool dead;
+  };
+  const PprStream* s;
+  const double* XO;
+  double* XN;
+  double* MN;
+  double dangling_in, share;
+  double delta = 0.0, dangling_out = 0.0;
+  bool active;
+  __device__ Row row(uint32_t i) const {
+    return Row{s->member[i], s->out[i], tomb_bit(s->tomb, i)};
+  }
+  __device__ Row shfl(const Row& r, uint32_t src) const {
+    return Row{__shfl_sync(0xffffffffu, r.mem, src), __shfl_sync(0xffffffffu, r.out, src),
+               __shfl_sync(0xffffffffu, r.dead, src) != 0};
+  }
+  __device__ void emit(uint32_t i, const Partial<double, WC_OP_PLUS>& acc, const Row& r) {
+    if (!active) return;
+    const unsigned lane = threadIdx.x & 31;
+    const PprStream& st = *s;
+    const double old = XO[(size_t)i * 32 + lane];
+    double y = 0.0;
+    if (acc.present) acc.acc.value(&y);
+    double next = 0.0;
+    if (!r.dead) {
+      const double p = ((r.mem >> lane) & 1) ? share : 0.0;
+      double dp, flowed, a, b;
+      int32_t e = sql_float<F_MUL>(dangling_in, p, &dp);
+      if (!e) e = sql_float<F_ADD>(y, dp, &flowed);
+      if (!e) e = sql_float<F_MUL>(st.damping, flowed, &a);
+      if (!e) e = sql_float<F_MUL>(st.teleport, p, &b);
+      if (!e) e = sql_float<F_ADD>(a, b, &next);
+      if (e) raise(st.err, e, i);
+    }
+    delta += fabs(next - old);
+    XN[(size_t)i * 32 + lane] = next;
+    dangling_out += ppr_spread(next, r.out, &MN[(size_t)i * 32 + lane], st.err, i);
+  }
+};
 
 template <class W>
-__global__ void __launch_bounds__(kPpr32Warps * 32)
+__global__ void __launch_bounds__(kPull32Warps * 32, 5)
     ppr_iter32_kernel(CsrView<W> A, PprStream s, Partial<double, WC_OP_PLUS>* carry) {
-  constexpr int ADD = WC_OP_PLUS;
-  typedef EntryOf<double, WC_PLUS_TIMES, W> Ent;
-  typedef Partial<double, ADD> Part;
   PprCtl* ctl = s.ctl;
   const uint32_t run = *(volatile uint32_t*)&ctl->running;
   if (!run) {
@@ -283,162 +298,11 @@ __global__ void __launch_bounds__(kPpr32Warps * 32)
   const uint32_t g = *(volatile uint32_t*)&ctl->g;
   const int cur = g & 1;
   const unsigned lane = threadIdx.x & 31;
-  double* xold = ppr_smem + (threadIdx.x >> 5) * kPpr32WarpDoubles;  // [row][column]
-  double* ring = xold + 32 * 32;                                      // [slot][column]
-  const bool active = (run >> lane) & 1;
-  const double dangling_in = ctl->dangling[lane], share = ctl->share[lane];
-  double delta = 0.0, dangling_out = 0.0;
-  const double* __restrict__ X = s.msg[cur];
-  const double* XO = s.x[cur];
-  double* XN = s.x[cur ^ 1];
-  double* MN = s.msg[cur ^ 1];
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-
-  // The rank update of row i for this lane's column (pagerank/mod.rs:201-282).
-  auto emit = [&](uint32_t i, const Part& acc, double old, uint32_t mem, double outw, bool dead) {
-    if (!active) return;
-    double y = 0.0;
-    if (acc.present) acc.acc.value(&y);
-    double next = 0.0;
-    if (!dead) {
-      const double p = ((mem >> lane) & 1) ? share : 0.0;
-      double dp, flowed, a, b;
-      int32_t e = sql_float<F_MUL>(dangling_in, p, &dp);
-      if (!e) e = sql_float<F_ADD>(y, dp, &flowed);
-      if (!e) e = sql_float<F_MUL>(s.damping, flowed, &a);
-      if (!e) e = sql_float<F_MUL>(s.teleport, p, &b);
-      if (!e) e = sql_float<F_ADD>(a, b, &next);
-      if (e) raise(s.err, e, i);
-    }
-    delta += fabs(next - old);
-    XN[(size_t)i * 32 + lane] = next;
-    dangling_out += ppr_spread(next, outw, &MN[(size_t)i * 32 + lane], s.err, i);
-  };
-  // Folds entry `e` (its gathered value in ring slot `slot`) into `acc`.
-  auto fold = [&](Part& acc, uint32_t slot, typename Ent::WT wv, uint32_t row) {
-    if (!active) return;
-    const double xv = ring[slot * 32 + lane];
-    double p;
-    int32_t st = Ent::product(wv, xv, &p);
-    if (st) raise(s.err, st, row);
-    if (acc.present) {
-      double sum;
-      acc.acc.value(&sum);
-      st = Apply<double, ADD>::go(sum, p, &sum);
-      if (st) raise(s.err, st, row);
-      acc.acc = Acc<double, ADD>::of(sum);
-    } else {
-      acc.acc = Acc<double, ADD>::of(p);
-      acc.present = true;
-    }
-  };
-
-  for (uint32_t u = warp; u < A.unit_count; u += warps) {
-    const Unit unit = A.units[u];
-    const bool tile = (unit.c >> 31) == 0;
-    const uint32_t a = unit.a;
-    const uint32_t R = tile ? unit.b - unit.a : 1;
-    const uint32_t base = tile ? unit.d : unit.b;
-    const uint32_t count = tile ? unit.c : unit.d - unit.b;
-    __syncwarp();  // every lane is done with the last unit's old ranks
-    if (tile) {
-      const double* src = XO + (size_t)a * 32;
-      for (uint32_t ch = lane; ch < R * 16; ch += 32) cp_async16(xold + ch * 2, src + ch * 2);
-    }
-    cp_async_commit();
-    // Targets and weights of the unit (≤ 256 entries): entry 32·q + lane in
-    // register q; per-row values of the tile: row `lane` in each lane.
-    uint32_t jr[8];
-    typename Ent::WT wr[8];
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-      const uint32_t k = 32 * q + lane;
-      jr[q] = k < count ? __ldg(A.tgt + base + k) : 0u;
-      wr[q] = k < count ? Ent::load(A, base + k) : typename Ent::WT{};
-    }
-    uint32_t hi_l = count, mem_l = 0;
-    double out_l = 0.0;
-    bool dead_l = false;
-    if (tile && lane < R) {
-      hi_l = __ldg(A.off + a + lane + 1) - base;
-      mem_l = s.member[a + lane];
-      out_l = s.out[a + lane];
-      dead_l = tomb_bit(s.tomb, a + lane);
-    }
-    const uint32_t chunks = (count + kPpr32Chunk - 1) / kPpr32Chunk;
-    // Gather group q into ring half q & 1.
-    auto issue = [&](uint32_t q) {
-      const uint32_t jw = pick8(jr, q >> 1), off = (q & 1) * kPpr32Chunk;
-      double* dst = ring + off * 32 + lane;
-#pragma unroll
-      for (uint32_t t = 0; t < kPpr32Chunk; t++) {
-        const uint32_t j = __shfl_sync(0xffffffffu, jw, off + t);
-        if (active && q * kPpr32Chunk + t < count) cp_async8(dst + t * 32, X + (size_t)j * 32 + lane);
-      }
-      cp_async_commit();
-    };
-    if (chunks > 0) issue(0);
-    Part acc{Acc<double, ADD>::of(0.0), false};
-    uint32_t r = 0;
-    uint32_t hi_r = __shfl_sync(0xffffffffu, hi_l, 0);
-    for (uint32_t q = 0; q < chunks; q++) {
-      if (q + 1 < chunks) {
-        issue(q + 1);
-        cp_async_wait<1>();
-      } else {
-        cp_async_wait<0>();
-      }
-      __syncwarp();
-      const uint32_t n_q = min(kPpr32Chunk, count - q * kPpr32Chunk);
-      const typename Ent::WT ww = pick8(wr, q >> 1);
-      for (uint32_t t = 0; t < n_q; t++) {
-        const uint32_t k = q * kPpr32Chunk + t;
-        while (k >= hi_r) {  // rows ending before entry k (tiles only)
-          emit(a + r, acc, xold[r * 32 + lane], __shfl_sync(0xffffffffu, mem_l, r),
-               __shfl_sync(0xffffffffu, out_l, r), __shfl_sync(0xffffffffu, dead_l, r));
-          acc = Part{Acc<double, ADD>::of(0.0), false};
-          r++;
-          hi_r = __shfl_sync(0xffffffffu, hi_l, r);
-        }
-        const typename Ent::WT wv = (typename Ent::WT)__shfl_sync(0xffffffffu, ww, k & 31);
-        fold(acc, (q & 1) * kPpr32Chunk + t, wv, tile ? a + r : a);
-      }
-    }
-    if (chunks == 0) {
-      cp_async_wait<0>();
-      __syncwarp();
-    }
-    if (tile) {
-      for (; r < R; r++) {
-        emit(a + r, acc, xold[r * 32 + lane], __shfl_sync(0xffffffffu, mem_l, r),
-             __shfl_sync(0xffffffffu, out_l, r), __shfl_sync(0xffffffffu, dead_l, r));
-        acc = Part{Acc<double, ADD>::of(0.0), false};
-      }
-      continue;
-    }
-    // A piece of a long row: its partial in the carry slot; the warp that
-    // brings the row's last piece combines the pieces in order and emits.
-    const uint32_t row = a, slot = unit.c & 0x7fffffffu;
-    const uint32_t row_lo = __ldg(A.off + row);
-    const uint32_t deg = __ldg(A.off + row + 1) - row_lo;
-    const uint32_t pieces = (deg + kPieceEntries - 1) / kPieceEntries;
-    const uint32_t first = slot - (base - row_lo) / kPieceEntries;
-    carry[(size_t)slot * 32 + lane] = acc;
-    __threadfence();
-    __syncwarp();
-    uint32_t arrived = 0;
-    if (lane == 0) arrived = atomicAdd(A.counters + first, 1u);
-    arrived = __shfl_sync(0xffffffffu, arrived, 0);
-    if (arrived == pieces - 1) {
-      __threadfence();
-      const Part total = combine_pieces<double, ADD, 32>(carry, first, pieces, lane, 0);
-      emit(row, total, XO[(size_t)row * 32 + lane], s.member[row], s.out[row],
-           tomb_bit(s.tomb, row));
-      __syncwarp();
-      if (lane == 0) A.counters[first] = 0;
-    }
-  }
+  PprEpi32 epi{&s, s.x[cur], s.x[cur ^ 1], s.msg[cur ^ 1], ctl->dangling[lane], ctl->share[lane]};
+  epi.active = (run >> lane) & 1;
+  pull32_units<W>(A, s.msg[cur], epi, s.err, carry,
+                  ppr_smem + (threadIdx.x >> 5) * kPull32WarpDoubles);
+  double delta = epi.delta, dangling_out = epi.dangling_out;
   if (reduce_columns<32>(delta, dangling_out, s.partials, &ctl->counter))
     ppr_control<32>(s, run, g, delta, dangling_out);
 }
@@ -453,21 +317,24 @@ __global__ void ppr_rows_kernel(PprStream s) {
   if (!F) return;
   const uint32_t R = *(volatile const uint32_t*)&ctl->refilled;
   const int nb = ctl->g & 1;  // the buffer the last iteration wrote
+  // A thread per dense id i (the ranks leave in dense-id order), its state
+  // at row k of the locality order.
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += gridDim.x * blockDim.x) {
-    const uint32_t m = s.member[i];
-    if (m & F) s.member[i] = m & ~F;
+    const uint32_t k = s.perm[i];
+    const uint32_t m = s.member[k];
+    if (m & F) s.member[k] = m & ~F;
     for (uint32_t b = F; b; b &= b - 1) {
       const uint32_t c = __ffs(b) - 1;
-      s.ranks[(size_t)ctl->fin_set[c] * s.n + i] = s.x[nb][(size_t)i * P + c];
+      s.ranks[(size_t)ctl->fin_set[c] * s.n + i] = s.x[nb][(size_t)k * P + c];
     }
     if (R) {
-      const double x0 = tomb_bit(s.tomb, i) ? 0.0 : s.start;
+      const double x0 = tomb_bit(s.tomb, k) ? 0.0 : s.start;
       double m0;
-      ppr_spread(x0, s.out[i], &m0, s.err, i);
+      ppr_spread(x0, s.out[k], &m0, s.err, i);
       for (uint32_t b = R; b; b &= b - 1) {
         const uint32_t c = __ffs(b) - 1;
-        s.x[nb][(size_t)i * P + c] = x0;
-        s.msg[nb][(size_t)i * P + c] = m0;
+        s.x[nb][(size_t)k * P + c] = x0;
+        s.msg[nb][(size_t)k * P + c] = m0;
       }
     }
   }
@@ -480,7 +347,7 @@ __global__ void ppr_members_kernel(PprStream s) {
   if (!((*(volatile const uint32_t*)&ctl->refilled >> c) & 1)) return;
   const uint32_t set = ctl->slot_set[c];
   for (uint64_t q = s.offsets[set] + threadIdx.x; q < s.offsets[set + 1]; q += blockDim.x)
-    atomicOr(s.member + s.nodes[q], 1u << c);
+    atomicOr(s.member + s.perm[s.nodes[q]], 1u << c);
 }
 
 // max_iter = 0: every set's ranks are the start vector.
@@ -488,17 +355,17 @@ __global__ void ppr_start_out_kernel(PprStream s) {
   for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < (uint64_t)s.width * s.n;
        q += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t i = (uint32_t)(q % s.n);
-    s.ranks[q] = tomb_bit(s.tomb, i) ? 0.0 : s.start;
+    s.ranks[q] = tomb_bit(s.tomb, s.perm[i]) ? 0.0 : s.start;
   }
   for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < s.width; q += gridDim.x * blockDim.x)
     s.iterations[q] = 0;
 }
 
-// Blocks of 8 warps (P = 8, 16) or kPpr32Warps (P = 32), at most one warp a unit.
+// Blocks of 8 warps (P = 8, 16) or kPull32Warps (P = 32), at most one warp a unit.
 static uint32_t ppr_grid(const wc_version* v, uint32_t P, uint32_t blocks_per_sm) {
-  const uint32_t warps = P == 32 ? kPpr32Warps : 8;
+  const uint32_t warps = P == 32 ? kPull32Warps : 8;
   return std::max<uint32_t>(1, std::min<uint32_t>(max_blocks((int)blocks_per_sm),
-                                                  (v->rev.schedule.count + warps - 1) / warps));
+                                                  (v->loc.csc.schedule.count + warps - 1) / warps));
 }
 
 // The run's scratch, acquired before anything is queued or captured.
@@ -512,7 +379,7 @@ static wc_status ppr_reserve(Ctx& ctx, uint32_t P, uint32_t blocks_per_sm) {
   WC_TRY(ctx.scratch(POOL_BATCH_2, n * 4, &b));
   WC_TRY(ctx.scratch(POOL_BATCH_3, 4096 + (uint64_t)grid * P * 16, &b));
   return ctx.scratch(POOL_BATCH_4,
-                     (uint64_t)std::max<uint32_t>(v->rev.schedule.slots, 1) * P *
+                     (uint64_t)std::max<uint32_t>(v->loc.csc.schedule.slots, 1) * P *
                          sizeof(Partial<double, WC_OP_PLUS>), &b);
 }
 
@@ -521,20 +388,20 @@ static void ppr_queue_iteration(Ctx& ctx, const PprStream& s, uint32_t grid, boo
                                 Partial<double, WC_OP_PLUS>* carry) {
   wc_version* v = ctx.v;
   if constexpr (P == 32) {
-    constexpr size_t smem32 = kPpr32Warps * kPpr32WarpDoubles * sizeof(double);
+    constexpr size_t smem32 = kPull32Smem;
     if (weighted)
-      note_launch(), ppr_iter32_kernel<double><<<grid, kPpr32Warps * 32, smem32, ctx.stream>>>(
-          view_of<double>(v->rev, v->rev.weights.ptr), s, carry);
+      note_launch(), ppr_iter32_kernel<double><<<grid, kPull32Warps * 32, smem32, ctx.stream>>>(
+          view_of<double>(v->loc.csc, v->loc.csc.weights.ptr), s, carry);
     else
-      note_launch(), ppr_iter32_kernel<void><<<grid, kPpr32Warps * 32, smem32, ctx.stream>>>(
-          view_of<void>(v->rev, nullptr), s, carry);
+      note_launch(), ppr_iter32_kernel<void><<<grid, kPull32Warps * 32, smem32, ctx.stream>>>(
+          view_of<void>(v->loc.csc, nullptr), s, carry);
   } else {
     if (weighted)
       note_launch(), ppr_iter_kernel<P, double><<<grid, 256, 0, ctx.stream>>>(
-          view_of<double>(v->rev, v->rev.weights.ptr), s, carry);
+          view_of<double>(v->loc.csc, v->loc.csc.weights.ptr), s, carry);
     else
       note_launch(), ppr_iter_kernel<P, void><<<grid, 256, 0, ctx.stream>>>(
-          view_of<void>(v->rev, nullptr), s, carry);
+          view_of<void>(v->loc.csc, nullptr), s, carry);
   }
   note_launch(), ppr_rows_kernel<P><<<max_blocks(4), 256, 0, ctx.stream>>>(s);
   note_launch(), ppr_members_kernel<<<P, 128, 0, ctx.stream>>>(s);
@@ -557,7 +424,7 @@ wc_status ppr_stream(Ctx& ctx, const PageRankRun& base, const uint64_t* nodes,
   WC_TRY(ctx.scratch(POOL_BATCH_2, (uint64_t)n * 4, &memb));
   WC_TRY(ctx.scratch(POOL_BATCH_3, 4096 + (uint64_t)grid * P * 16, &sb));
   WC_TRY(ctx.scratch(POOL_BATCH_4,
-                     (uint64_t)std::max<uint32_t>(v->rev.schedule.slots, 1) * P *
+                     (uint64_t)std::max<uint32_t>(v->loc.csc.schedule.slots, 1) * P *
                          sizeof(Partial<double, WC_OP_PLUS>), &cb));
   static_assert(sizeof(PprCtl) <= 4096, "the control block fits its page");
   PprStream s{};
@@ -574,6 +441,7 @@ wc_status ppr_stream(Ctx& ctx, const PageRankRun& base, const uint64_t* nodes,
   s.nodes = nodes;
   s.offsets = offsets;
   s.tomb = base.s.tomb;
+  s.perm = v->loc.perm.as<uint32_t>();
   s.start = base.s.start;
   s.damping = base.s.damping;
   s.teleport = base.s.teleport;
@@ -591,7 +459,7 @@ wc_status ppr_stream(Ctx& ctx, const PageRankRun& base, const uint64_t* nodes,
   const bool weighted = base.opts.weighted != 0 && v->weighted;
   auto* carry = cb->as<Partial<double, WC_OP_PLUS>>();
   if constexpr (P == 32) {
-    constexpr int smem32 = kPpr32Warps * kPpr32WarpDoubles * sizeof(double);
+    constexpr int smem32 = (int)kPull32Smem;
     WC_CUDA(cudaFuncSetAttribute(ppr_iter32_kernel<double>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smem32), ctx.detail);
     WC_CUDA(cudaFuncSetAttribute(ppr_iter32_kernel<void>,
@@ -682,13 +550,15 @@ wc_status tune_ppr(Ctx& ctx, uint32_t width, wc_schedule* best) {
   WC_CUDA(cudaMemcpyAsync(F->ptr, offs.data(), (sample + 1) * 8, cudaMemcpyHostToDevice, ctx.stream), ctx.detail);
   wc_pagerank_opts o{0.85, 1e-10, 1, -1, 10, nullptr};
   PageRankRun base;
-  WC_TRY(base.setup(ctx, &o, nullptr, nullptr));
+  WC_TRY(base.setup(ctx, &o, nullptr, nullptr, true));
   cudaEvent_t a, b;
   WC_CUDA(cudaEventCreate(&a), ctx.detail);
   WC_CUDA(cudaEventCreate(&b), ctx.detail);
   float best_ms = 1e30f;
   for (uint32_t P : {8u, 16u, 32u})
-    for (uint32_t bps : {2u, 3u, 4u}) {
+    for (uint32_t bps : {2u, 3u, 4u, 5u, 6u}) {
+      // The 32-slot kernel's 4-warp blocks fit more an SM than the others'.
+      if (P == 32 ? bps < 3 : bps > 4) continue;
       float ms = 0;
       for (int rep = 0; rep < 2; rep++) {
         WC_CUDA(cudaEventRecord(a, ctx.stream), ctx.detail);
@@ -731,7 +601,7 @@ wc_status wc_ppr_batched(wc_version* v, const wc_call* call, const wc_pagerank_o
     WC_CUDA(cudaMemcpy(nodes.data(), seed_nodes, nodes.size() * 8, cudaMemcpyDefault), ctx.detail);
   WC_TRY(ctx.begin());
   PageRankRun base;
-  WC_TRY(base.setup(ctx, o, nullptr, nullptr));
+  WC_TRY(base.setup(ctx, o, nullptr, nullptr, true));
   // Each set's personalisation (pagerank/mod.rs:155-199 with a seed of 1
   // on the set): the set's size summed in the reference's order is exact
   // (integers), then 1 / size, then 1 × that share.
@@ -757,9 +627,9 @@ wc_status wc_ppr_batched(wc_version* v, const wc_call* call, const wc_pagerank_o
   DevBuf* its;
   WC_TRY(ctx.scratch(POOL_BATCH_9, (uint64_t)width * 4, &its));
   const auto key = ((uint64_t)WC_BATCH_PPR << 32) | width;
-  const wc_schedule sched = v->tuned.count(key) ? v->tuned[key] : wc_schedule{32, 1, 3, 0};
+  const wc_schedule sched = v->tuned.count(key) ? v->tuned[key] : wc_schedule{32, 1, 5, 0};
   const uint32_t P = sched.columns_per_pass <= 8 ? 8 : sched.columns_per_pass <= 16 ? 16 : 32;
-  const uint32_t bps = sched.blocks_per_sm ? sched.blocks_per_sm : 3;
+  const uint32_t bps = sched.blocks_per_sm ? sched.blocks_per_sm : 5;
   DevBuf* sh;
   WC_TRY(ctx.scratch(POOL_BATCH_11, (uint64_t)width * 8, &sh));
   WC_CUDA(cudaMemcpyAsync(sh->ptr, shares.data(), (uint64_t)width * 8, cudaMemcpyHostToDevice,
@@ -771,7 +641,7 @@ wc_status wc_ppr_batched(wc_version* v, const wc_call* call, const wc_pagerank_o
   if (iterations_out)
     WC_CUDA(cudaMemcpyAsync(iterations_out, its->ptr, width * 4, cudaMemcpyDefault, ctx.stream),
             ctx.detail);
-  return ctx.finish();
+  return locality_status(ctx, ctx.finish());
 }
 
 }  // extern "C"

@@ -109,9 +109,8 @@ __device__ inline bool offer(const LevelArgs& a, uint32_t u, uint32_t v) {
 
 // Push: a warp per frontier node, lanes over its row entries; rows longer
 // than kBigRow are listed for push_big_kernel instead.
-__global__ void __launch_bounds__(256) push_kernel(LevelArgs a) {
+__device__ inline void push_level(const LevelArgs& a) {
   const LevelState& st = *a.st;
-  if (st.count == 0 || st.pull) return;
   const unsigned lane = threadIdx.x & 31;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; f < st.count; f += warps) {
@@ -173,9 +172,7 @@ __global__ void __launch_bounds__(256) push_big_kernel(LevelArgs a) {
 // smallest first hit of the two rows is `via` (what a push finds), while
 // `edges` counts entries as the reference's pull scans them: the first row
 // to its hit, or all of it and the second to its hit.
-__global__ void __launch_bounds__(256) pull_kernel(LevelArgs a, int count_edges) {
-  const LevelState& st = *a.st;
-  if (st.count == 0 || !st.pull) return;
+__device__ inline void pull_level(const LevelArgs& a) {
   unsigned long long scanned = 0;
   const uint32_t n = a.n;
   const uint32_t stride = gridDim.x * blockDim.x;
@@ -209,10 +206,17 @@ __global__ void __launch_bounds__(256) pull_kernel(LevelArgs a, int count_edges)
     }
     admit(v, take, a.next, a.fnext, a.st, a.adj, a.radj);
   }
-  if (count_edges) {
-    for (int o = 16; o > 0; o >>= 1) scanned += __shfl_down_sync(0xffffffffu, scanned, o);
-    if ((threadIdx.x & 31) == 0 && scanned) atomicAdd(&a.st->edges, scanned);
-  }
+  for (int o = 16; o > 0; o >>= 1) scanned += __shfl_down_sync(0xffffffffu, scanned, o);
+  if ((threadIdx.x & 31) == 0 && scanned) atomicAdd(&a.st->edges, scanned);
+}
+
+// One launch a level: it pushes or pulls as the level's plan says (every
+// block reads the same plan), and returns at once past the last frontier.
+__global__ void __launch_bounds__(256) level_kernel(LevelArgs a) {
+  const LevelState& st = *a.st;
+  if (st.count == 0) return;
+  if (st.pull) pull_level(a);
+  else push_level(a);
 }
 
 // Closes a level: plans the next (its frontier, the switch's choice; an
@@ -231,11 +235,6 @@ __global__ void level_end_kernel(LevelState* st, SwitchArgs sw, uint32_t next_is
     nx.visited_rdeg = cur.visited_rdeg + cur.next_rdeg;
     nx.pull = nx.count && level_pulls(sw, nx.count, nx.mf, nx.visited_rdeg);
   }
-}
-
-__global__ void set_bits_kernel(const uint32_t* nodes, uint32_t count, uint32_t* bits) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
-    atomicOr(bits + (nodes[i] >> 5), 1u << (nodes[i] & 31));
 }
 
 // For Both: whether node v sits in its via's forward row (a binary search;
@@ -263,9 +262,33 @@ __global__ void in_forward_row_kernel(uint32_t n, const uint32_t* depth,
   }
 }
 
-__global__ void seed_kernel(const uint32_t* starts, uint32_t count, uint32_t* depth) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
-    depth[starts[i]] = 0;
+// A search's state before its seeds: every depth unreached, every via
+// none, both frontier bitmaps clear.
+__global__ void bfs_fill_kernel(uint32_t* depth, unsigned long long* via, uint32_t n,
+                                uint32_t* fbits, uint32_t fwords) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    depth[i] = WC_UNREACHED;
+    via[i] = WC_NO_VIA;
+  }
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < fwords; i += stride) fbits[i] = 0;
+}
+
+// The seeds (from the host's staging memory, read in place): depth 0, in
+// the first queue and the first bitmap.
+__global__ void bfs_seed_kernel(const uint32_t* seeds, uint32_t count, uint32_t* queue,
+                                uint32_t* depth, uint32_t* fbits) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const uint32_t s = seeds[i];
+    queue[i] = s;
+    depth[s] = 0;
+    atomicOr(fbits + (s >> 5), 1u << (s & 31));
+  }
+}
+
+// A chunk's plans: the first from the host's staging memory, the rest zero.
+__global__ void bfs_plan_kernel(const LevelState* first, LevelState* st, uint32_t count) {
+  for (uint32_t i = threadIdx.x; i < count; i += blockDim.x) st[i] = i == 0 ? *first : LevelState{};
 }
 
 static Rows rows_of(wc_version* v, int direction) {
@@ -337,8 +360,14 @@ wc_status Search::start(Ctx& ctx, int dir, const uint64_t* starts_in, uint64_t s
       }
     }
   }
-  WC_TRY(buffer(ctx, POOL_BFS_DEPTH, n * 4, &depth));
-  WC_TRY(buffer(ctx, POOL_BFS_VIA, n * 8, &via));
+  if (!depth_p) {
+    WC_TRY(buffer(ctx, POOL_BFS_DEPTH, n * 4, &depth));
+    depth_p = depth->as<uint32_t>();
+  }
+  if (!via_p) {
+    WC_TRY(buffer(ctx, POOL_BFS_VIA, n * 8, &via));
+    via_p = via->as<unsigned long long>();
+  }
   WC_TRY(buffer(ctx, POOL_BFS_Q0, std::max<uint64_t>(n, 1) * 4, &queue[0]));
   WC_TRY(buffer(ctx, POOL_BFS_Q1, std::max<uint64_t>(n, 1) * 4, &queue[1]));
   const uint64_t words = (n + 31) / 32;
@@ -386,23 +415,24 @@ wc_status Search::enqueue_init(Ctx& ctx, bool staged) {
   const uint64_t n = ctx.v->n;
   const uint64_t words = std::max<uint64_t>((n + 31) / 32, 1);
   const uint32_t count0 = (uint32_t)seeds.size();
-  WC_CUDA(cudaMemsetAsync(depth->ptr, 0xff, n * 4, ctx.stream), ctx.detail);
-  WC_CUDA(cudaMemsetAsync(via->ptr, 0xff, n * 8, ctx.stream), ctx.detail);
-  WC_CUDA(cudaMemsetAsync(fbits->ptr, 0, words * 4 * 2, ctx.stream), ctx.detail);
+  const uint64_t items = std::max<uint64_t>(n, 2 * words);
+  const uint32_t fill_grid = (uint32_t)std::min<uint64_t>((items + 255) / 256, max_blocks(8));
+  note_launch(), bfs_fill_kernel<<<fill_grid, 256, 0, ctx.stream>>>(
+      depth_p, via_p, (uint32_t)n, fbits->as<uint32_t>(), (uint32_t)(2 * words));
   if (count0) {
-    const void* src = staged ? (const void*)(ctx.v->stage_host + kStagePayload)
-                             : (const void*)seeds.data();
-    WC_CUDA(cudaMemcpyAsync(queue[0]->ptr, src, count0 * 4, cudaMemcpyHostToDevice, ctx.stream),
-            ctx.detail);
-    note_launch(), seed_kernel<<<(count0 + 255) / 256, 256, 0, ctx.stream>>>(
-        queue[0]->as<uint32_t>(), count0, depth->as<uint32_t>());
-    note_launch(), set_bits_kernel<<<(count0 + 255) / 256, 256, 0, ctx.stream>>>(
-        queue[0]->as<uint32_t>(), count0, fbits->as<uint32_t>());
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(ctx.v->stage_dev + kStagePayload);
+    if (!staged) {
+      WC_CUDA(cudaMemcpyAsync(queue[1]->ptr, seeds.data(), count0 * 4, cudaMemcpyHostToDevice,
+                              ctx.stream), ctx.detail);
+      src = queue[1]->as<uint32_t>();
+    }
+    note_launch(), bfs_seed_kernel<<<(count0 + 255) / 256, 256, 0, ctx.stream>>>(
+        src, count0, queue[0]->as<uint32_t>(), depth_p, fbits->as<uint32_t>());
   }
   return cuda_status(cudaGetLastError(), ctx.detail, "bfs init");
 }
 
-wc_status Search::advance(Ctx& ctx, uint32_t max_levels) {
+wc_status Search::advance(Ctx& ctx, uint32_t max_levels, bool defer_last) {
   wc_version* v = ctx.v;
   const uint64_t n = v->n;
   const uint64_t words = (n + 31) / 32;
@@ -414,9 +444,10 @@ wc_status Search::advance(Ctx& ctx, uint32_t max_levels) {
   const uint64_t* filter_dev = filter ? filter->as<uint64_t>() : nullptr;
   LevelState* st = counters->as<LevelState>();
   const uint32_t blocks = max_blocks(8);
-  // A warp per frontier node; rows longer than kBigRow go to push_big_kernel.
-  const uint32_t push_grid = max_blocks(2);
-  const uint32_t pull_grid = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)((n + 255) / 256), blocks));
+  // A push takes a warp per frontier node (rows longer than kBigRow go to
+  // push_big_kernel), a pull a thread per node.
+  const uint32_t level_grid = std::max<uint32_t>(
+      max_blocks(2), std::min<uint32_t>((uint32_t)((n + 255) / 256), blocks));
   const uint32_t end_grid = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)((words + 255) / 256), blocks));
   uint32_t& d = depth_reached;
   const uint32_t stop_at = (uint32_t)std::min<uint64_t>(max_depth, (uint64_t)d + max_levels);
@@ -427,7 +458,9 @@ wc_status Search::advance(Ctx& ctx, uint32_t max_levels) {
     // No level follows, or the seeds do not fit the staging area: set the
     // state up on its own.
     init_pending = false;
-    WC_TRY(enqueue_init(ctx, false));
+    if (seeds_fit && !seeds.empty())
+      std::memcpy(v->stage_host + kStagePayload, seeds.data(), seeds.size() * 4);
+    WC_TRY(enqueue_init(ctx, seeds_fit));
   }
   // The levels are queued kChunkLevels at a time with no round trip: each
   // level's kernels read its plan from the device (level_end_kernel writes
@@ -450,12 +483,12 @@ wc_status Search::advance(Ctx& ctx, uint32_t max_levels) {
     auto put = [&](const void* p, size_t bytes) { args.append((const char*)p, bytes); };
     const uint64_t head[] = {chunk, d0, max_depth, init ? seeds.size() : UINT64_MAX, n,
                              (uint64_t)(uintptr_t)st, (uint64_t)(uintptr_t)v->cancel_dev,
-                             (uint64_t)(uintptr_t)depth->ptr, (uint64_t)(uintptr_t)via->ptr,
+                             (uint64_t)(uintptr_t)depth_p, (uint64_t)(uintptr_t)via_p,
                              (uint64_t)(uintptr_t)fbits->ptr, (uint64_t)(uintptr_t)queue[0]->ptr,
                              (uint64_t)(uintptr_t)queue[1]->ptr, (uint64_t)(uintptr_t)big->ptr,
                              (uint64_t)(uintptr_t)filter_dev, (uint64_t)(uintptr_t)adj.off0,
                              (uint64_t)(uintptr_t)adj.off1, (uint64_t)(uintptr_t)radj.off0,
-                             (uint64_t)(uintptr_t)radj.off1, push_grid, pull_grid, end_grid, blocks,
+                             (uint64_t)(uintptr_t)radj.off1, level_grid, end_grid, blocks,
                              (uint64_t)(uintptr_t)v->stage_host};
     put(head, sizeof head);
     put(&sw, sizeof sw);
@@ -464,19 +497,15 @@ wc_status Search::advance(Ctx& ctx, uint32_t max_levels) {
     // buffers, depth cap and seed count) no capture either.
     WC_TRY(ctx.run_cached("plainbfs/" + std::to_string(chunk), args, [&]() -> wc_status {
       if (init) WC_TRY(enqueue_init(ctx, true));
-      WC_CUDA(cudaMemsetAsync(st, 0, (kChunkLevels + 1) * sizeof(LevelState), ctx.stream),
-              ctx.detail);
-      WC_CUDA(cudaMemcpyAsync(st, plan, sizeof(LevelState), cudaMemcpyHostToDevice, ctx.stream),
-              ctx.detail);
+      note_launch(), bfs_plan_kernel<<<1, 32, 0, ctx.stream>>>(
+          reinterpret_cast<const LevelState*>(v->stage_dev + kStagePlan), st, kChunkLevels + 1);
       for (uint32_t q = 0; q < chunk; q++) {
         const uint32_t L = d0 + q;
         LevelArgs a{adj, radj, st + q, queue[L & 1]->as<uint32_t>(),
                     queue[(L + 1) & 1]->as<uint32_t>(), fb[L & 1], fb[(L + 1) & 1],
-                    big->as<uint32_t>(), L + 1, (uint32_t)n, depth->as<uint32_t>(),
-                    via->as<unsigned long long>(), filter_dev};
-        note_launch(), push_kernel<<<push_grid, 256, 0, ctx.stream>>>(a);
+                    big->as<uint32_t>(), L + 1, (uint32_t)n, depth_p, via_p, filter_dev};
+        note_launch(), level_kernel<<<level_grid, 256, 0, ctx.stream>>>(a);
         note_launch(), push_big_kernel<<<blocks, 256, 0, ctx.stream>>>(a);
-        note_launch(), pull_kernel<<<pull_grid, 256, 0, ctx.stream>>>(a, 1);
         // The bitmap of level L + 2 is level L's: clear it for the admits of L + 1.
         note_launch(), level_end_kernel<<<end_grid, 256, 0, ctx.stream>>>(
             st + q, sw, L + 1 >= max_depth ? 1u : 0u, fb[L & 1], (uint32_t)words, v->cancel_dev);
@@ -485,29 +514,47 @@ wc_status Search::advance(Ctx& ctx, uint32_t max_levels) {
                               cudaMemcpyDeviceToHost, ctx.stream), ctx.detail);
       return cuda_status(cudaGetLastError(), ctx.detail, "bfs levels");
     }));
-    WC_CUDA(cudaStreamSynchronize(ctx.stream), ctx.detail);
-    for (uint32_t q = 0; q < chunk; q++) {
-      const LevelState& h = plan[q];
-      if (h.count == 0) break;
-      const bool pull = h.pull != 0;
-      levels.push_back(Level{pull, h.count, h.mf, pull ? (uint64_t)h.edges : h.mf, h.next_count});
-      stats.levels++;
-      if (pull) stats.pulled_levels++;
-      stats.edges_traversed += pull && sw.rule == REFERENCE_SWITCH ? h.edges : h.mf;
-      stats.nodes_visited += h.next_count;
-      last_admitted = h.next_count;
-      d++;
+    if (defer_last && d0 + chunk == stop_at) {
+      // The last chunk there can be: the caller queues its own copies
+      // behind it and waits once, then reads the plans (collect).
+      pending_chunk = chunk;
+      return WC_OK;
     }
-    const bool more = plan[chunk].count != 0;
-    next_plan = plan[chunk];
-    // A chunk cut short by max_levels leaves the next level planned; the
-    // depth cap or an empty frontier leaves nothing to plan.
-    if (d >= max_depth) next_plan.count = 0;
-    next_plan.next_deg = next_plan.next_rdeg = next_plan.edges = 0;
-    next_plan.next_count = next_plan.big_count = 0;
-    if (!more) break;
+    WC_CUDA(cudaStreamSynchronize(ctx.stream), ctx.detail);
+    if (!absorb(plan, chunk)) break;
   }
   return WC_OK;
+}
+
+// Reads a chunk's plans back into the stats; whether the search goes on.
+bool Search::absorb(const LevelState* plan, uint32_t chunk) {
+  uint32_t& d = depth_reached;
+  for (uint32_t q = 0; q < chunk; q++) {
+    const LevelState& h = plan[q];
+    if (h.count == 0) break;
+    const bool pull = h.pull != 0;
+    levels.push_back(Level{pull, h.count, h.mf, pull ? (uint64_t)h.edges : h.mf, h.next_count});
+    stats.levels++;
+    if (pull) stats.pulled_levels++;
+    stats.edges_traversed += pull && sw.rule == REFERENCE_SWITCH ? h.edges : h.mf;
+    stats.nodes_visited += h.next_count;
+    last_admitted = h.next_count;
+    d++;
+  }
+  const bool more = plan[chunk].count != 0;
+  next_plan = plan[chunk];
+  // A chunk cut short by max_levels leaves the next level planned; the
+  // depth cap or an empty frontier leaves nothing to plan.
+  if (d >= max_depth) next_plan.count = 0;
+  next_plan.next_deg = next_plan.next_rdeg = next_plan.edges = 0;
+  next_plan.next_count = next_plan.big_count = 0;
+  return more;
+}
+
+void Search::collect(Ctx& ctx) {
+  if (!pending_chunk) return;
+  absorb(reinterpret_cast<const LevelState*>(ctx.v->stage_host + kStagePlan), pending_chunk);
+  pending_chunk = 0;
 }
 
 // The visits in the reference's order: starts first (as given, repeats
@@ -517,8 +564,8 @@ wc_status Search::ordered(Ctx& ctx, std::vector<uint64_t>& rows, bool with_via) 
   const uint64_t n = ctx.v->n;
   std::vector<uint32_t> dh(n);
   std::vector<uint64_t> vh(n);
-  WC_CUDA(cudaMemcpy(dh.data(), depth->ptr, n * 4, cudaMemcpyDeviceToHost), ctx.detail);
-  WC_CUDA(cudaMemcpy(vh.data(), via->ptr, n * 8, cudaMemcpyDeviceToHost), ctx.detail);
+  WC_CUDA(cudaMemcpy(dh.data(), depth_p, n * 4, cudaMemcpyDeviceToHost), ctx.detail);
+  WC_CUDA(cudaMemcpy(vh.data(), via_p, n * 8, cudaMemcpyDeviceToHost), ctx.detail);
   // Within a pushed level, nodes come by via, then by position in via's
   // rows: ascending for one CSR; for Both, the forward row's nodes first.
   std::vector<uint8_t> second_row(n, 0);
@@ -526,7 +573,7 @@ wc_status Search::ordered(Ctx& ctx, std::vector<uint64_t>& rows, bool with_via) 
     DevBuf* flags;
     WC_TRY(ctx.scratch(POOL_BFS_FLAGS, n, &flags));
     note_launch(), in_forward_row_kernel<<<max_blocks(4), 256, 0, ctx.stream>>>(
-        (uint32_t)n, depth->as<uint32_t>(), via->as<unsigned long long>(),
+        (uint32_t)n, depth_p, via_p,
         ctx.v->fwd.offsets.as<uint32_t>(), ctx.v->fwd.targets.as<uint32_t>(), flags->as<uint8_t>());
     WC_CUDA(cudaMemcpyAsync(second_row.data(), flags->ptr, n, cudaMemcpyDeviceToHost, ctx.stream),
             ctx.detail);
@@ -717,7 +764,7 @@ static wc_status cut_stats(Ctx& ctx, wc_bfs_cursor* c, uint64_t index, uint64_t 
       WC_TRY(ctx.scratch(POOL_BFS_SCAN, 8, &sum));
       WC_CUDA(cudaMemsetAsync(sum->ptr, 0, 8, ctx.stream), ctx.detail);
       note_launch(), pulled_scan_kernel<<<max_blocks(8), 256, 0, ctx.stream>>>(
-          rows_of(ctx.v, rdir), c->search.depth->as<uint32_t>(), d, (uint32_t)node,
+          rows_of(ctx.v, rdir), c->search.depth_p, d, (uint32_t)node,
           sum->as<unsigned long long>());
       WC_CUDA(cudaMemcpyAsync(&within, sum->ptr, 8, cudaMemcpyDeviceToHost, ctx.stream),
               ctx.detail);
@@ -766,7 +813,7 @@ static wc_status cursor_level(Ctx& ctx, wc_bfs_cursor* c) {
   const bool both = s.direction == WC_BOTH;
   note_launch(), level_rows_kernel<<<std::min<uint32_t>((k + 255) / 256, max_blocks(4)), 256, 0,
                                      ctx.stream>>>(
-      s.queue[(L + 1) & 1]->as<uint32_t>(), k, s.via->as<unsigned long long>(),
+      s.queue[(L + 1) & 1]->as<uint32_t>(), k, s.via_p,
       ctx.v->fwd.offsets.as<uint32_t>(), ctx.v->fwd.targets.as<uint32_t>(), both ? 1 : 0,
       out->as<unsigned long long>());
   std::vector<uint64_t> raw((uint64_t)k * 3);
@@ -828,15 +875,23 @@ wc_status wc_bfs(wc_version* v, const wc_call* call, wc_direction direction, con
     return WC_OK;
   }
   Search s;
-  WC_TRY(s.run(ctx, direction, starts, start_count, max_depth, filter, GPU_SWITCH));
+  // Device outputs are searched in place (no copies out).
+  const bool depth_dev = depth_out && is_device_pointer(depth_out);
+  const bool via_dev = via_out && is_device_pointer(via_out);
+  if (depth_dev) s.depth_p = depth_out;
+  if (via_dev) s.via_p = reinterpret_cast<unsigned long long*>(via_out);
+  WC_TRY(s.start(ctx, direction, starts, start_count, max_depth, filter, GPU_SWITCH));
+  // The last chunk of levels, the copies out and the error word are waited
+  // for once.
+  WC_TRY(s.advance(ctx, UINT32_MAX, true));
+  if (depth_out && !depth_dev)
+    WC_CUDA(cudaMemcpyAsync(depth_out, s.depth_p, v->n * 4, cudaMemcpyDefault, ctx.stream),
+            ctx.detail);
+  if (via_out && !via_dev)
+    WC_CUDA(cudaMemcpyAsync(via_out, s.via_p, v->n * 8, cudaMemcpyDefault, ctx.stream),
+            ctx.detail);
   WC_TRY(ctx.finish());
-  if (depth_out)
-    WC_CUDA(cudaMemcpyAsync(depth_out, s.depth->ptr, v->n * 4, cudaMemcpyDefault, ctx.stream),
-            ctx.detail);
-  if (via_out)
-    WC_CUDA(cudaMemcpyAsync(via_out, s.via->ptr, v->n * 8, cudaMemcpyDefault, ctx.stream),
-            ctx.detail);
-  WC_CUDA(cudaStreamSynchronize(ctx.stream), ctx.detail);
+  s.collect(ctx);
   if (stats) *stats = s.stats;
   return WC_OK;
 }

@@ -54,6 +54,10 @@ struct Search {
   DevBuf *depth = nullptr, *via = nullptr, *queue[2] = {nullptr, nullptr}, *fbits = nullptr,
          *counters = nullptr, *filter = nullptr, *big = nullptr;
   std::map<int, DevBuf>* owned = nullptr;   // buffers by pool tag, if not the pool's
+  // The per-node depths and vias the search writes: the caller's device
+  // arrays when set before start(), else the search's own buffers.
+  uint32_t* depth_p = nullptr;
+  unsigned long long* via_p = nullptr;
   std::vector<uint32_t> seeds;
   std::vector<Level> levels;
   wc_traversal_stats stats{};
@@ -64,20 +68,25 @@ struct Search {
   LevelState next_plan{};      // the plan of the next level (count 0: exhausted)
   uint32_t last_admitted = 0;  // nodes admitted by the last level expanded
   bool init_pending = false;   // the device state is set up with the first levels
+  uint32_t pending_chunk = 0;  // levels of a deferred chunk not yet read back
 
   wc_status run(Ctx& ctx, int direction, const uint64_t* starts, uint64_t start_count,
                 uint32_t max_depth, const uint64_t* filter, SwitchRule rule);
   wc_status start(Ctx& ctx, int direction, const uint64_t* starts, uint64_t start_count,
                   uint32_t max_depth, const uint64_t* filter, SwitchRule rule);
   // Expands up to `max_levels` more levels (fewer once the frontier empties
-  // or the depth cap is met).
-  wc_status advance(Ctx& ctx, uint32_t max_levels);
+  // or the depth cap is met).  With `defer_last` the last chunk the cap
+  // allows is queued without waiting for it: the caller waits (after
+  // queueing its own work) and then calls collect() for the stats.
+  wc_status advance(Ctx& ctx, uint32_t max_levels, bool defer_last = false);
+  void collect(Ctx& ctx);
   bool exhausted() const { return next_plan.count == 0; }
   wc_status ordered(Ctx& ctx, std::vector<uint64_t>& rows, bool with_via);
 
  private:
   wc_status buffer(Ctx& ctx, int tag, uint64_t bytes, DevBuf** out);
   wc_status enqueue_init(Ctx& ctx, bool staged);
+  bool absorb(const LevelState* plan, uint32_t chunk);
 };
 
 }  // namespace wc

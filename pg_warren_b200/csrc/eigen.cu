@@ -657,7 +657,7 @@ struct Eigensolver {
       Search s;
       WC_TRY(s.run(ctx, WC_BOTH, roots.data(), roots.size(), WC_UNREACHED, nullptr, GPU_SWITCH));
       std::vector<uint32_t> depth(n);
-      WC_CUDA(cudaMemcpy(depth.data(), s.depth->ptr, (uint64_t)n * 4, cudaMemcpyDeviceToHost), ctx.detail);
+      WC_CUDA(cudaMemcpy(depth.data(), s.depth_p, (uint64_t)n * 4, cudaMemcpyDeviceToHost), ctx.detail);
       std::vector<uint8_t> col(n, 0);
       for (uint32_t i = 0; i < n; i++) col[i] = act[i] && depth[i] != WC_UNREACHED ? (depth[i] & 1) : 0;
       std::vector<uint64_t> off(v->host_offsets);

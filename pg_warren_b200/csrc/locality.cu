@@ -176,4 +176,13 @@ wc_status bits_to_locality(const wc_version* v, cudaStream_t st, const uint64_t*
   return cuda_status(cudaGetLastError(), nullptr, "renumber bits");
 }
 
+wc_status locality_status(Ctx& ctx, wc_status st) {
+  if (st == WC_OK || !ctx.device_error || !ctx.detail || ctx.detail->node >= ctx.v->n) return st;
+  uint32_t id = 0;
+  if (cudaMemcpy(&id, ctx.v->loc.order.as<uint32_t>() + ctx.detail->node, 4,
+                 cudaMemcpyDeviceToHost) == cudaSuccess)
+    ctx.detail->node = id;
+  return st;
+}
+
 }  // namespace wc

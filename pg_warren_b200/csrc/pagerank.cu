@@ -526,7 +526,7 @@ wc_status wc_pagerank(wc_version* v, const wc_call* call, const wc_pagerank_opts
   WC_TRY(run.setup(ctx, o, tombstones, o->seed, true));
   ctx.progress("iterating", 0, o->max_iter);
   WC_TRY(run.run(ctx));
-  WC_TRY(ctx.finish());
+  WC_TRY(locality_status(ctx, ctx.finish()));
   double margin = 0.0;
   WC_TRY(run.result(ctx, ranks, iterations, &margin));
   v->last_margin = margin;

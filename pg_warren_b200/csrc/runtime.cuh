@@ -286,6 +286,7 @@ struct wc_version {
   // Pinned host staging (wc::kStage*): small per-call uploads and
   // read-backs, which captured graphs may also copy from and to.
   uint8_t* stage_host = nullptr;
+  uint8_t* stage_dev = nullptr;  // the same memory, mapped for kernels
   std::recursive_mutex mu;             // calls on one handle run one at a time
   double last_margin = 0.0;
   std::map<uint64_t, wc_schedule> tuned;  // (kind << 32 | width) -> schedule
@@ -528,6 +529,10 @@ struct Ctx {
   // passing it on to the device (kernels that loop read it and stop).  Then
   // reads the device error word.
   wc_status finish() {
+    // The device error word comes back behind the call's work, so one wait
+    // covers both.
+    WC_CUDA(cudaMemcpyAsync(v->stage_host + kStageError, v->error.ptr, sizeof(DeviceError),
+                            cudaMemcpyDeviceToHost, stream), detail);
     auto start = std::chrono::steady_clock::now();
     bool cancel = false, timed_out = false;
     for (;;) {
@@ -552,9 +557,6 @@ struct Ctx {
     if (!cancel && cancelled()) cancel = true;
     collect_timings();
     DeviceError e;
-    WC_CUDA(cudaMemcpyAsync(v->stage_host + kStageError, v->error.ptr, sizeof e,
-                            cudaMemcpyDeviceToHost, stream), detail);
-    WC_CUDA(cudaStreamSynchronize(stream), detail);
     std::memcpy(&e, v->stage_host + kStageError, sizeof e);
     if (cancel) return WC_CANCELLED;
     if (timed_out) return WC_DEVICE_TIMEOUT;

@@ -32,6 +32,9 @@ wc_status device_locality(wc_version* v, wc_error_detail* detail);
 // dst[perm[i]] = src[i] (in), dst[i] = src[perm[i]] (out), and a NodeSet's
 // bits renumbered (dst is cleared first).
 wc_status to_locality(const wc_version* v, cudaStream_t st, const double* src, double* dst);
+// A status from ctx.finish() of a solve in the locality order: a node a
+// kernel reported (a row of that order) is renamed to its dense id.
+wc_status locality_status(Ctx& ctx, wc_status st);
 wc_status from_locality(const wc_version* v, cudaStream_t st, const double* src, double* dst);
 wc_status bits_to_locality(const wc_version* v, cudaStream_t st, const uint64_t* src,
                            uint64_t* dst);

@@ -154,7 +154,8 @@ wc_status finish_version(wc_version* v, wc_error_detail* detail) {
   WC_CUDA(cudaHostGetDevicePointer((void**)&v->cancel_dev, v->cancel_host, 0), detail);
   v->pace_host = reinterpret_cast<volatile uint32_t*>(v->cancel_host + 1);
   v->pace_dev = reinterpret_cast<uint32_t*>(v->cancel_dev + 1);
-  WC_CUDA(cudaHostAlloc((void**)&v->stage_host, kStageBytes, cudaHostAllocDefault), detail);
+  WC_CUDA(cudaHostAlloc((void**)&v->stage_host, kStageBytes, cudaHostAllocMapped), detail);
+  WC_CUDA(cudaHostGetDevicePointer((void**)&v->stage_dev, v->stage_host, 0), detail);
   return WC_OK;
 }
 
