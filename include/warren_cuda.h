@@ -253,7 +253,7 @@ wc_status wc_version_sync(wc_version* version, const wc_call* call);
 /* The device time (ms, CUDA events on the call's stream) of kernel group
  * `phase` in the last call made with WC_CALL_TIMING, and in *launches the
  * kernels it launched in that group (may be NULL); 0 if not recorded.
- * Groups: "iteration" (PageRank); "level" (a batched search's levels: push,
+ * Groups: "setup", "iteration" (PageRank); "level" (a batched search's levels: push,
  * settle and pull launches), "pull" (the pull launches alone), "depth";
  * "pulled" has no time and counts the levels that pulled. */
 double wc_version_timing(const wc_version* version, const char* phase, uint32_t* launches);

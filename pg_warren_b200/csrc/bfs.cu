@@ -82,6 +82,8 @@ struct LevelArgs {
   uint32_t* next;
   const uint32_t* fbits;  // this level's frontier as a bitmap
   uint32_t* fnext;        // the next level's bitmap (cleared)
+  uint32_t* fclear;       // the previous level's bitmap, cleared here for the level after
+  uint32_t fwords;
   uint32_t* big;          // frontier rows too long for one warp
   uint32_t depth_next;
   uint32_t n;
@@ -138,15 +140,32 @@ __device__ inline void push_level(const LevelArgs& a) {
   }
 }
 
+// Plans the level after st[0] in st[1]: its frontier (none past the depth
+// cap or once the call is cancelled) and the switch's choice.
+__device__ inline void plan_next(LevelState* st, const SwitchArgs& sw, uint32_t next_is_last,
+                                 const int32_t* cancel) {
+  const volatile LevelState& cur = st[0];
+  LevelState& nx = st[1];
+  const bool stop = cur.count == 0 || next_is_last || *(volatile const int32_t*)cancel;
+  nx.count = stop ? 0u : cur.next_count;
+  nx.mf = cur.next_deg;
+  nx.visited_rdeg = cur.visited_rdeg + cur.next_rdeg;
+  nx.pull = nx.count && level_pulls(sw, nx.count, nx.mf, nx.visited_rdeg);
+}
+
 // Push of the long rows: each row's entries spread over every warp of the
-// grid, the rows one after another.
-__global__ void __launch_bounds__(256) push_big_kernel(LevelArgs a) {
+// grid, the rows one after another.  Then the block that finishes last
+// closes the level: it plans the next one.
+__global__ void __launch_bounds__(256) push_big_kernel(LevelArgs a, SwitchArgs sw,
+                                                       uint32_t next_is_last,
+                                                       const int32_t* cancel) {
   const LevelState& st = *a.st;
-  if (st.count == 0 || st.pull || st.big_count == 0) return;
+  if (st.count == 0) return;  // no frontier: every later plan stays empty
   const unsigned lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t b = 0; b < st.big_count; b++) {
+  const uint32_t big = st.pull ? 0u : st.big_count;
+  for (uint32_t b = 0; b < big; b++) {
     const uint32_t u = a.big[b];
     for (int part = 0; part < 2; part++) {
       const uint32_t* off = part == 0 ? a.adj.off0 : a.adj.off1;
@@ -164,6 +183,17 @@ __global__ void __launch_bounds__(256) push_big_kernel(LevelArgs a) {
         admit(v, take, a.next, a.fnext, a.st, a.adj, a.radj);
       }
     }
+  }
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(&a.st->done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    plan_next(a.st, sw, next_is_last, cancel);
   }
 }
 
@@ -215,26 +245,10 @@ __device__ inline void pull_level(const LevelArgs& a) {
 __global__ void __launch_bounds__(256) level_kernel(LevelArgs a) {
   const LevelState& st = *a.st;
   if (st.count == 0) return;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.fwords; i += gridDim.x * blockDim.x)
+    a.fclear[i] = 0;
   if (st.pull) pull_level(a);
   else push_level(a);
-}
-
-// Closes a level: plans the next (its frontier, the switch's choice; an
-// empty frontier past the depth cap or once the call is cancelled) and
-// clears the bitmap the level after it will fill.
-__global__ void level_end_kernel(LevelState* st, SwitchArgs sw, uint32_t next_is_last,
-                                 uint32_t* fclear, uint32_t words, const int32_t* cancel) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += gridDim.x * blockDim.x)
-    fclear[i] = 0;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    const LevelState& cur = st[0];
-    LevelState& nx = st[1];
-    const bool stop = cur.count == 0 || next_is_last || *(volatile const int32_t*)cancel;
-    nx.count = stop ? 0u : cur.next_count;
-    nx.mf = cur.next_deg;
-    nx.visited_rdeg = cur.visited_rdeg + cur.next_rdeg;
-    nx.pull = nx.count && level_pulls(sw, nx.count, nx.mf, nx.visited_rdeg);
-  }
 }
 
 // For Both: whether node v sits in its via's forward row (a binary search;
@@ -371,7 +385,7 @@ wc_status Search::start(Ctx& ctx, int dir, const uint64_t* starts_in, uint64_t s
   WC_TRY(buffer(ctx, POOL_BFS_Q0, std::max<uint64_t>(n, 1) * 4, &queue[0]));
   WC_TRY(buffer(ctx, POOL_BFS_Q1, std::max<uint64_t>(n, 1) * 4, &queue[1]));
   const uint64_t words = (n + 31) / 32;
-  WC_TRY(buffer(ctx, POOL_BFS_FBITS, std::max<uint64_t>(words, 1) * 4 * 2, &fbits));
+  WC_TRY(buffer(ctx, POOL_BFS_FBITS, std::max<uint64_t>(words, 1) * 4 * 3, &fbits));
   WC_TRY(buffer(ctx, POOL_BFS_COUNTERS, (kChunkLevels + 1) * sizeof(LevelState), &counters));
   WC_TRY(buffer(ctx, POOL_BFS_BIG, (v->m / kBigRow + 2) * 4 * (dir == WC_BOTH ? 2 : 1), &big));
   filter = nullptr;
@@ -415,10 +429,10 @@ wc_status Search::enqueue_init(Ctx& ctx, bool staged) {
   const uint64_t n = ctx.v->n;
   const uint64_t words = std::max<uint64_t>((n + 31) / 32, 1);
   const uint32_t count0 = (uint32_t)seeds.size();
-  const uint64_t items = std::max<uint64_t>(n, 2 * words);
+  const uint64_t items = std::max<uint64_t>(n, 3 * words);
   const uint32_t fill_grid = (uint32_t)std::min<uint64_t>((items + 255) / 256, max_blocks(8));
   note_launch(), bfs_fill_kernel<<<fill_grid, 256, 0, ctx.stream>>>(
-      depth_p, via_p, (uint32_t)n, fbits->as<uint32_t>(), (uint32_t)(2 * words));
+      depth_p, via_p, (uint32_t)n, fbits->as<uint32_t>(), (uint32_t)(3 * words));
   if (count0) {
     const uint32_t* src = reinterpret_cast<const uint32_t*>(ctx.v->stage_dev + kStagePayload);
     if (!staged) {
@@ -440,7 +454,11 @@ wc_status Search::advance(Ctx& ctx, uint32_t max_levels, bool defer_last) {
   const int rdir = dir == WC_OUT ? WC_IN : (dir == WC_IN ? WC_OUT : WC_BOTH);
   const Rows adj = rows_of(v, dir);
   const Rows radj = rows_of(v, rdir);
-  uint32_t* fb[2] = {fbits->as<uint32_t>(), fbits->as<uint32_t>() + std::max<uint64_t>(words, 1)};
+  // Three frontier bitmaps in turn: level L reads L % 3, fills (L + 1) % 3
+  // and clears (L + 2) % 3, which the level before it read.
+  const uint64_t fw = std::max<uint64_t>(words, 1);
+  uint32_t* fb[3] = {fbits->as<uint32_t>(), fbits->as<uint32_t>() + fw,
+                     fbits->as<uint32_t>() + 2 * fw};
   const uint64_t* filter_dev = filter ? filter->as<uint64_t>() : nullptr;
   LevelState* st = counters->as<LevelState>();
   const uint32_t blocks = max_blocks(8);
@@ -448,7 +466,6 @@ wc_status Search::advance(Ctx& ctx, uint32_t max_levels, bool defer_last) {
   // push_big_kernel), a pull a thread per node.
   const uint32_t level_grid = std::max<uint32_t>(
       max_blocks(2), std::min<uint32_t>((uint32_t)((n + 255) / 256), blocks));
-  const uint32_t end_grid = std::max<uint32_t>(1, std::min<uint32_t>((uint32_t)((words + 255) / 256), blocks));
   uint32_t& d = depth_reached;
   const uint32_t stop_at = (uint32_t)std::min<uint64_t>(max_depth, (uint64_t)d + max_levels);
   static_assert((kChunkLevels + 1) * sizeof(LevelState) <= kStagePlanBytes, "plan staging");
@@ -463,7 +480,7 @@ wc_status Search::advance(Ctx& ctx, uint32_t max_levels, bool defer_last) {
     WC_TRY(enqueue_init(ctx, seeds_fit));
   }
   // The levels are queued kChunkLevels at a time with no round trip: each
-  // level's kernels read its plan from the device (level_end_kernel writes
+  // level's kernels read its plan from the device (push_big_kernel writes
   // it), and those of a level with no frontier return at once.  The host
   // reads the chunk's plans back once, to go on or stop and for the stats.
   while (next_plan.count > 0 && d < stop_at) {
@@ -488,7 +505,7 @@ wc_status Search::advance(Ctx& ctx, uint32_t max_levels, bool defer_last) {
                              (uint64_t)(uintptr_t)queue[1]->ptr, (uint64_t)(uintptr_t)big->ptr,
                              (uint64_t)(uintptr_t)filter_dev, (uint64_t)(uintptr_t)adj.off0,
                              (uint64_t)(uintptr_t)adj.off1, (uint64_t)(uintptr_t)radj.off0,
-                             (uint64_t)(uintptr_t)radj.off1, level_grid, end_grid, blocks,
+                             (uint64_t)(uintptr_t)radj.off1, level_grid, blocks,
                              (uint64_t)(uintptr_t)v->stage_host};
     put(head, sizeof head);
     put(&sw, sizeof sw);
@@ -502,13 +519,12 @@ wc_status Search::advance(Ctx& ctx, uint32_t max_levels, bool defer_last) {
       for (uint32_t q = 0; q < chunk; q++) {
         const uint32_t L = d0 + q;
         LevelArgs a{adj, radj, st + q, queue[L & 1]->as<uint32_t>(),
-                    queue[(L + 1) & 1]->as<uint32_t>(), fb[L & 1], fb[(L + 1) & 1],
-                    big->as<uint32_t>(), L + 1, (uint32_t)n, depth_p, via_p, filter_dev};
+                    queue[(L + 1) & 1]->as<uint32_t>(), fb[L % 3], fb[(L + 1) % 3],
+                    fb[(L + 2) % 3], (uint32_t)fw, big->as<uint32_t>(), L + 1, (uint32_t)n,
+                    depth_p, via_p, filter_dev};
         note_launch(), level_kernel<<<level_grid, 256, 0, ctx.stream>>>(a);
-        note_launch(), push_big_kernel<<<blocks, 256, 0, ctx.stream>>>(a);
-        // The bitmap of level L + 2 is level L's: clear it for the admits of L + 1.
-        note_launch(), level_end_kernel<<<end_grid, 256, 0, ctx.stream>>>(
-            st + q, sw, L + 1 >= max_depth ? 1u : 0u, fb[L & 1], (uint32_t)words, v->cancel_dev);
+        note_launch(), push_big_kernel<<<blocks, 256, 0, ctx.stream>>>(
+            a, sw, L + 1 >= max_depth ? 1u : 0u, v->cancel_dev);
       }
       WC_CUDA(cudaMemcpyAsync(plan, st, (kChunkLevels + 1) * sizeof(LevelState),
                               cudaMemcpyDeviceToHost, ctx.stream), ctx.detail);

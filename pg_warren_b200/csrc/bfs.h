@@ -32,6 +32,7 @@ struct LevelState {
   unsigned long long edges;       // row entries scanned by a pulled level
   uint32_t next_count;
   uint32_t big_count;             // frontier rows deferred to push_big_kernel
+  uint32_t done;                  // push_big_kernel's blocks finished
 };
 
 // The switch (level.rs:19-29, 184-211 for the reference's; a GPU-tuned one

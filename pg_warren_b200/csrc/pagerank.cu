@@ -95,16 +95,39 @@ __device__ inline bool reduce_two(double& a, double& b, double* partials, unsign
 
 // The reference's sum of a seed over live rows (reduce.rs:137-153, 266-279):
 // each 65536-element chunk folded sequentially from +0.
-__global__ void seed_chunks_kernel(const double* seed, const uint64_t* tomb, uint64_t n,
-                                   double* partial) {
-  uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  uint64_t lo = c * kChunk;
-  if (lo >= n) return;
-  uint64_t hi = min(n, lo + kChunk);
-  double s = 0.0;
-  for (uint64_t i = lo; i < hi; i++)
-    if (!tomb_at(tomb, (uint32_t)i)) s = s + seed[i];
-  partial[c] = s;
+// Block c sums chunk c of the live seed values in index order: warps 1..
+// stage the next 2,048 terms in shared memory while thread 0 adds the
+// current ones.  A tombstoned row's term is +0.0, which leaves a sum that
+// starts at +0.0 unchanged, as skipping it does.
+constexpr uint32_t kSeedStage = 2048;
+
+__global__ void __launch_bounds__(256) seed_chunks_kernel(const double* seed, const uint64_t* tomb,
+                                                          uint64_t n, double* partial) {
+  __shared__ double stage[2][kSeedStage];
+  const uint64_t c0 = (uint64_t)blockIdx.x * kChunk;
+  const uint64_t c1 = min(n, c0 + kChunk);
+  const uint32_t rounds = (uint32_t)((c1 - c0 + kSeedStage - 1) / kSeedStage);
+  auto fill = [&](uint32_t r, uint32_t first) {
+    double* st = stage[r & 1];
+    for (uint32_t q = threadIdx.x - first; q < kSeedStage; q += blockDim.x - first) {
+      const uint64_t i = c0 + (uint64_t)r * kSeedStage + q;
+      st[q] = (i < c1 && !tomb_at(tomb, (uint32_t)i)) ? seed[i] : 0.0;
+    }
+  };
+  double sum = 0.0;
+  fill(0, 0);
+  __syncthreads();
+  for (uint32_t r = 0; r < rounds; r++) {
+    if (threadIdx.x == 0) {
+      const double* st = stage[r & 1];
+#pragma unroll 16
+      for (uint32_t q = 0; q < kSeedStage; q++) sum = sum + st[q];
+    } else if (threadIdx.x >= 32 && r + 1 < rounds) {
+      fill(r + 1, 32);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sum;
 }
 
 __global__ void seed_shares_kernel(const double* seed, const uint64_t* tomb, uint32_t n,
@@ -434,7 +457,8 @@ wc_status PageRankRun::setup(Ctx& ctx, const wc_pagerank_opts* o, const uint64_t
     WC_TRY(ctx.scratch(POOL_PR_SHARES, n * 8 * (local ? 2 : 1) + (uint64_t)chunks * 8, &shares));
     double* partial = shares->as<double>() + n * (local ? 2 : 1);
     const uint64_t* tomb_ids = th ? tomb->as<uint64_t>() : nullptr;  // dense-id order
-    note_launch(), seed_chunks_kernel<<<(chunks + 127) / 128, 128, 0, ctx.stream>>>(sd, tomb_ids, n, partial);
+    if (chunks)
+      note_launch(), seed_chunks_kernel<<<chunks, 256, 0, ctx.stream>>>(sd, tomb_ids, n, partial);
     note_launch(), seed_shares_kernel<<<max_blocks(4), 256, 0, ctx.stream>>>(sd, tomb_ids, (uint32_t)n, partial,
                                                              chunks, shares->as<double>(), s.err);
     s.shares = shares->as<double>();
@@ -523,7 +547,9 @@ wc_status wc_pagerank(wc_version* v, const wc_call* call, const wc_pagerank_opts
   if (ctx.cancelled()) return WC_CANCELLED;
   WC_TRY(ctx.begin());
   PageRankRun run;
+  ctx.phase_begin("setup");
   WC_TRY(run.setup(ctx, o, tombstones, o->seed, true));
+  ctx.phase_end();
   ctx.progress("iterating", 0, o->max_iter);
   WC_TRY(run.run(ctx));
   WC_TRY(locality_status(ctx, ctx.finish()));

@@ -149,3 +149,36 @@ def test_rmat_largest_component_normalised_laplacian_smallest():
     assert e.components == 1 and e.exact == 1
     assert np.abs(e.values - lam).max() < 1e-10
     assert e.residuals.max() <= 1e-8
+
+
+def _largest_component(scale):
+    from scipy.sparse import csr_matrix
+    from scipy.sparse.csgraph import connected_components
+    g = W.rmat(scale, undirected=True)
+    n = g.id_space
+    rows = np.repeat(np.arange(n), np.diff(g.offsets).astype(np.int64))
+    a = csr_matrix((np.ones(g.edges), (rows, g.targets)), shape=(n, n))
+    _, labels = connected_components(a, directed=False)
+    keep = np.where(labels == np.bincount(labels).argmax())[0]
+    sub = a[keep][:, keep].tocsr()
+    sub.sort_indices()
+    return sub
+
+
+def test_rmat16_largest_component_matches_an_independent_solver():
+    # The C4 variant's shape at R-MAT 16 (46,777 nodes): the 16 smallest
+    # eigenvalues of the normalised Laplacian against ARPACK (scipy's
+    # eigsh) on 2I - L, whose largest eigenvalues are 2 minus those.
+    from scipy.sparse import diags, identity
+    from scipy.sparse.linalg import eigsh
+    sub = _largest_component(16)
+    gv = W.GraphVersion(sub.indptr.astype(np.uint64), sub.indices.astype(np.uint32))
+    e = W.eigen(gv, W.EigenOptions(16, which="smallest", operator="normalized_laplacian",
+                                   tol=1e-13, max_iter=100000, seed=3))
+    inv = diags(1.0 / np.sqrt(np.asarray(sub.sum(axis=1)).ravel()))
+    m = identity(sub.shape[0]) + inv @ sub @ inv
+    lam = np.sort(2.0 - eigsh(m, k=16, which="LA", ncv=96, tol=1e-14, maxiter=100000,
+                              return_eigenvectors=False))
+    assert e.components == 1 and e.exact == 1
+    assert np.abs(np.sort(e.values) - lam).max() < 1e-10
+    assert e.residuals.max() <= 1e-8
