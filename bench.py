@@ -729,7 +729,7 @@ def profile_case(args):
         rng = np.random.default_rng(SEED)
         sizes = np.exp(rng.uniform(0, np.log(1000), 32)).astype(np.int64)
         sets = [rng.choice(n, int(s), replace=False) for s in sizes]
-        W.set_schedule(gv, "ppr", 32, columns_per_pass=32, blocks_per_sm=3)
+        W.set_schedule(gv, "ppr", 32, columns_per_pass=32, blocks_per_sm=5)
         r = torch.empty((32, n), dtype=torch.float64, device="cuda")
         it = torch.empty(32, dtype=torch.int32, device="cuda")
         for _ in range(2):

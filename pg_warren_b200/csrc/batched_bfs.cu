@@ -110,6 +110,7 @@ struct MsLevel {
   uint32_t* acc;      // n × W push accumulators, all zero between levels
   uint32_t* touched;  // rows with a push accumulator to settle, all zero between levels
   uint32_t* pulled;   // if set: counts the levels that pull (timed calls)
+  const uint32_t* unit_rows;  // per unit of `units`: its rows that hold entries
 };
 
 // Whether level P.L runs at all: it has a frontier.  A level that does not
@@ -211,11 +212,12 @@ __device__ inline void prefetch_l2(const void* p) {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 template <int W>
-__device__ inline void prefetch_unit(const MsLevel& P, const Unit& d, unsigned lane) {
+__device__ inline void prefetch_unit(const MsLevel& P, const Unit& d, uint32_t held,
+                                     unsigned lane) {
   const bool tile = (d.c >> 31) == 0;
   const uint32_t r0 = d.a, R = tile ? d.b - d.a : 1;
   const uint32_t e0 = tile ? d.d : d.b, cnt = tile ? d.c : d.d - d.b;
-  if (lane < R) prefetch_l2(P.V + (size_t)(r0 + lane) * W);
+  if (lane < R && ((held >> lane) & 1)) prefetch_l2(P.V + (size_t)(r0 + lane) * W);
   if (32 * lane < cnt) prefetch_l2(P.tgt + e0 + 32 * lane);
   if (tile && lane == 31) prefetch_l2(P.off + r0);
 }
@@ -261,12 +263,22 @@ __global__ void __launch_bounds__(256, 4) msbfs_level_kernel(MsLevel P) {
   V4 live = {};                // this warp's fresh bits, for the next level's live set
 
   Unit nxt{};
-  if (warp + warps < P.unit_count) nxt = P.units[warp + warps];
+  uint32_t nxt_held = 0;
+  if (warp + warps < P.unit_count) {
+    nxt = P.units[warp + warps];
+    nxt_held = P.unit_rows[warp + warps];
+  }
   for (uint32_t u = warp; u < P.unit_count; u += warps) {
     const Unit unit = P.units[u];  // loaded a unit earlier as `nxt`: a cache hit
+    // The rows that hold entries: a row with none (about half of an R-MAT
+    // graph's) can gain no bits, so its visited words are not read.
+    const uint32_t held = P.unit_rows[u];
     if (u + warps < P.unit_count) {
-      prefetch_unit<W>(P, nxt, lane);
-      if (u + 2 * warps < P.unit_count) nxt = P.units[u + 2 * warps];
+      prefetch_unit<W>(P, nxt, nxt_held, lane);
+      if (u + 2 * warps < P.unit_count) {
+        nxt = P.units[u + 2 * warps];
+        nxt_held = P.unit_rows[u + 2 * warps];
+      }
     }
     const bool tile = (unit.c >> 31) == 0;
     const uint32_t r0 = unit.a;
@@ -278,7 +290,7 @@ __global__ void __launch_bounds__(256, 4) msbfs_level_kernel(MsLevel P) {
 #pragma unroll
     for (uint32_t x = 0; x < VR; x++) {
       const uint32_t r = x * G + sub;
-      if (r < R) vrow[x] = load_words<VEC>(P.V + (size_t)(r0 + r) * W + w0);
+      if (r < R && ((held >> r) & 1)) vrow[x] = load_words<VEC>(P.V + (size_t)(r0 + r) * W + w0);
       else
 #pragma unroll
         for (int i = 0; i < (int)VEC; i++) vrow[x].x[i] = 0xffffffffu;
@@ -1094,7 +1106,8 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
               fbits + (L + 1) * bitmap_words, wbits + (L + 1) * bitmap_words, masks, alive, L,
               counts, fedges, foff, fwd.targets.as<uint32_t>(), fwd.schedule.units.as<Unit>(),
               fwd.schedule.count, v->m, b.acc->as<uint32_t>(), b.touched->as<uint32_t>(),
-              b.pulled ? b.pulled->as<uint32_t>() : nullptr};
+              b.pulled ? b.pulled->as<uint32_t>() : nullptr,
+              csc.schedule.row_masks.as<uint32_t>()};
     note_launch(), msbfs_cancel_kernel<<<1, 32, 0, st>>>(v->cancel_dev, counts + L);
     note_launch(), msbfs_push_kernel<W><<<push_grid, 256, 0, st>>>(P);
     note_launch(), msbfs_settle_kernel<W><<<settle_grid, 256, 0, st>>>(P);

@@ -236,6 +236,7 @@ struct Schedule {
   DevBuf counters;    // u32[slots]: arrivals per long row (indexed by its first slot)
   DevBuf carry;       // the pieces' partial results, kCarryBytesPerSlot per slot
   DevBuf long_list;   // uint4[long_rows]: each long row, its first slot and piece count
+  DevBuf row_masks;   // u32[count]: a tile's rows that hold entries (bit r: row a + r)
   uint32_t count = 0;
   uint32_t slots = 0;
   uint32_t long_rows = 0;

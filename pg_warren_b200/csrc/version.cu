@@ -118,6 +118,20 @@ wc_status put_schedule(wc_version* v, DevCsr& d, const std::vector<uint64_t>& of
   if (!longs.empty())
     WC_CUDA(cudaMemcpy(s.long_list.ptr, longs.data(), longs.size() * 4, cudaMemcpyHostToDevice),
             detail);
+  // Per tile, its rows that hold entries (a piece's row always does).
+  std::vector<uint32_t> masks(units.size(), 1u);
+  for (size_t u = 0; u < units.size(); u++) {
+    const Unit& d = units[u];
+    if ((d.c >> 31) != 0) continue;
+    uint32_t m = 0;
+    for (uint32_t r = d.a; r < d.b; r++)
+      if (off[r + 1] > off[r]) m |= 1u << (r - d.a);
+    masks[u] = m;
+  }
+  WC_TRY(s.row_masks.alloc(v->budget, std::max<size_t>(masks.size(), 1) * 4, detail));
+  if (!masks.empty())
+    WC_CUDA(cudaMemcpy(s.row_masks.ptr, masks.data(), masks.size() * 4, cudaMemcpyHostToDevice),
+            detail);
   return WC_OK;
 }
 
@@ -297,7 +311,7 @@ wc_status wc_version_info_get(const wc_version* v, wc_version_info* info) {
   for (const DevCsr* d : {&v->fwd, &v->rev, &v->loc.csc})
     bytes += d->offsets.bytes + d->targets.bytes + d->weights.bytes + d->iweights.bytes +
              d->schedule.units.bytes + d->schedule.counters.bytes + d->schedule.carry.bytes +
-             d->schedule.long_list.bytes;
+             d->schedule.long_list.bytes + d->schedule.row_masks.bytes;
   bytes += v->loc.perm.bytes + v->loc.order.bytes;
   info->device_bytes = bytes;
   uint64_t pooled = 0;
