@@ -4,8 +4,9 @@
 //
 // A row of the gathered operand is 256 bytes and one lane owns one column.
 // A warp keeps its gathers in flight as asynchronous copies (cp.async) into
-// a ring in shared memory instead of registers: a unit's entries go out 16
-// at a time, two groups in flight, while the targets, row ends and per-row
+// a ring in shared memory instead of registers (16 bytes a lane, a
+// half-warp an entry): a unit's entries go out 16 at a time, two groups in
+// flight, while the targets, row ends and per-row
 // values load into lanes.  A warp's shared memory is only its ring (8 KB),
 // so as many warps fit an SM as the registers allow.  Entries are folded in
 // ascending order per row, as pull_multi folds them, so each row's sum is
@@ -34,6 +35,10 @@ __device__ inline void cp_async8(void* dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src)
                : "memory");
 }
+__device__ inline void cp_async16_ca(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src)
+               : "memory");
+}
 __device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N> __device__ inline void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
@@ -60,6 +65,7 @@ __device__ inline void pull32_units(const CsrView<W>& A, const double* __restric
   typedef typename Epi::Row Row;
   const unsigned lane = threadIdx.x & 31;
   const bool active = epi.active;
+  const unsigned amask = __ballot_sync(0xffffffffu, active);  // the running columns
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
 
@@ -107,14 +113,20 @@ __device__ inline void pull32_units(const CsrView<W>& A, const double* __restric
       row_l = epi.row(a + lane);
     }
     const uint32_t chunks = (count + kPull32Chunk - 1) / kPull32Chunk;
-    // Gather group q into ring half q & 1.
+    // Gather group q into ring half q & 1: each half-warp copies one
+    // entry's row, 16 bytes (two columns) a lane, skipping column pairs
+    // that do not run.
+    const uint32_t half = lane >> 4, c2 = 2 * (lane & 15);
+    const bool pair_runs = ((amask >> c2) & 3u) != 0;
     auto issue = [&](uint32_t q) {
       const uint32_t jw = pick8(jr, q >> 1), off = (q & 1) * kPull32Chunk;
-      double* dst = ring + off * 32 + lane;
+      double* dst = ring + off * 32 + c2;
 #pragma unroll
-      for (uint32_t t = 0; t < kPull32Chunk; t++) {
-        const uint32_t j = __shfl_sync(0xffffffffu, jw, off + t);
-        if (active && q * kPull32Chunk + t < count) cp_async8(dst + t * 32, X + (size_t)j * 32 + lane);
+      for (uint32_t t = 0; t < kPull32Chunk; t += 2) {
+        const uint32_t tt = t + half;
+        const uint32_t j = __shfl_sync(0xffffffffu, jw, off + tt);
+        if (pair_runs && q * kPull32Chunk + tt < count)
+          cp_async16_ca(dst + tt * 32, X + (size_t)j * 32 + c2);
       }
       cp_async_commit();
     };
@@ -123,6 +135,9 @@ __device__ inline void pull32_units(const CsrView<W>& A, const double* __restric
     uint32_t r = 0;
     uint32_t hi_r = __shfl_sync(0xffffffffu, hi_l, 0);
     for (uint32_t q = 0; q < chunks; q++) {
+      // A lane's copies fill other lanes' columns: every lane is done with
+      // the half that group q + 1 refills (group q - 1's) before it is.
+      __syncwarp();
       if (q + 1 < chunks) {
         issue(q + 1);
         cp_async_wait<1>();
