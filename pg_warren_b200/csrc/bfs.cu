@@ -85,6 +85,7 @@ struct LevelArgs {
   uint32_t* fclear;       // the previous level's bitmap, cleared here for the level after
   uint32_t fwords;
   uint32_t* big;          // frontier rows too long for one warp
+  uint32_t big_cap;       // its entries: long rows from the front, huge ones from the back
   uint32_t depth_next;
   uint32_t n;
   uint32_t* depth;
@@ -95,9 +96,17 @@ struct LevelArgs {
 // Levels queued per round trip to the host.
 constexpr uint32_t kChunkLevels = 16;
 
-// Rows longer than this are pushed by the whole grid (push_big_kernel):
-// one warp per row would leave a hub's row to a single warp.
+// Rows longer than this are pushed by a block each (push_big_kernel): one
+// warp per row would leave a hub's row to a single warp.  Rows longer than
+// kHugeRow are pushed by the whole grid, one after another.
 constexpr uint32_t kBigRow = 2048;
+constexpr uint32_t kHugeRow = 32768;
+
+// The long-row list's entries: at most one per kBigRow entries of the rows
+// read (both CSRs for Both).
+inline uint32_t big_entries(uint64_t m, int dir) {
+  return (uint32_t)((m / kBigRow + 2) * (dir == WC_BOTH ? 2 : 1));
+}
 
 // One entry of a push: target v offered by frontier node u.
 __device__ inline bool offer(const LevelArgs& a, uint32_t u, uint32_t v) {
@@ -117,8 +126,12 @@ __device__ inline void push_level(const LevelArgs& a) {
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; f < st.count; f += warps) {
     const uint32_t u = a.frontier[f];
-    if (a.adj.degree(u) > kBigRow) {
-      if (lane == 0) a.big[atomicAdd(&a.st->big_count, 1u)] = u;
+    const uint32_t deg = a.adj.degree(u);
+    if (deg > kBigRow) {
+      if (lane == 0) {
+        if (deg > kHugeRow) a.big[a.big_cap - 1 - atomicAdd(&a.st->huge_count, 1u)] = u;
+        else a.big[atomicAdd(&a.st->big_count, 1u)] = u;
+      }
       continue;
     }
     for (int part = 0; part < 2; part++) {
@@ -153,37 +166,43 @@ __device__ inline void plan_next(LevelState* st, const SwitchArgs& sw, uint32_t 
   nx.pull = nx.count && level_pulls(sw, nx.count, nx.mf, nx.visited_rdeg);
 }
 
-// Push of the long rows: each row's entries spread over every warp of the
-// grid, the rows one after another.  Then the block that finishes last
-// closes the level: it plans the next one.
+// Push of the long rows: a huge row's entries spread over every warp of the
+// grid, the huge rows one after another; then each long row over the warps
+// of one block, the blocks taking the long rows in turn.  Then the block
+// that finishes last closes the level: it plans the next one.
+__device__ inline void push_row_part(const LevelArgs& a, uint32_t u, uint32_t first_warp,
+                                     uint32_t warp_stride) {
+  const unsigned lane = threadIdx.x & 31;
+  for (int part = 0; part < 2; part++) {
+    const uint32_t* off = part == 0 ? a.adj.off0 : a.adj.off1;
+    const uint32_t* tgt = part == 0 ? a.adj.tgt0 : a.adj.tgt1;
+    if (!off) break;
+    const uint32_t lo = __ldg(off + u), hi = __ldg(off + u + 1);
+    for (uint32_t e0 = lo + 32 * first_warp; e0 < hi; e0 += 32 * warp_stride) {
+      const uint32_t e = e0 + lane;
+      bool take = false;
+      uint32_t v = 0;
+      if (e < hi) {
+        v = __ldg(tgt + e);
+        take = offer(a, u, v);
+      }
+      admit(v, take, a.next, a.fnext, a.st, a.adj, a.radj);
+    }
+  }
+}
+
 __global__ void __launch_bounds__(256) push_big_kernel(LevelArgs a, SwitchArgs sw,
                                                        uint32_t next_is_last,
                                                        const int32_t* cancel) {
   const LevelState& st = *a.st;
   if (st.count == 0) return;  // no frontier: every later plan stays empty
-  const unsigned lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t huge = st.pull ? 0u : st.huge_count;
+  for (uint32_t h = 0; h < huge; h++) push_row_part(a, a.big[a.big_cap - 1 - h], warp, warps);
   const uint32_t big = st.pull ? 0u : st.big_count;
-  for (uint32_t b = 0; b < big; b++) {
-    const uint32_t u = a.big[b];
-    for (int part = 0; part < 2; part++) {
-      const uint32_t* off = part == 0 ? a.adj.off0 : a.adj.off1;
-      const uint32_t* tgt = part == 0 ? a.adj.tgt0 : a.adj.tgt1;
-      if (!off) break;
-      const uint32_t lo = __ldg(off + u), hi = __ldg(off + u + 1);
-      for (uint32_t e0 = lo + 32 * warp; e0 < hi; e0 += 32 * warps) {
-        const uint32_t e = e0 + lane;
-        bool take = false;
-        uint32_t v = 0;
-        if (e < hi) {
-          v = __ldg(tgt + e);
-          take = offer(a, u, v);
-        }
-        admit(v, take, a.next, a.fnext, a.st, a.adj, a.radj);
-      }
-    }
-  }
+  for (uint32_t b = blockIdx.x; b < big; b += gridDim.x)
+    push_row_part(a, a.big[b], threadIdx.x >> 5, blockDim.x >> 5);
   __shared__ bool last;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -387,7 +406,7 @@ wc_status Search::start(Ctx& ctx, int dir, const uint64_t* starts_in, uint64_t s
   const uint64_t words = (n + 31) / 32;
   WC_TRY(buffer(ctx, POOL_BFS_FBITS, std::max<uint64_t>(words, 1) * 4 * 3, &fbits));
   WC_TRY(buffer(ctx, POOL_BFS_COUNTERS, (kChunkLevels + 1) * sizeof(LevelState), &counters));
-  WC_TRY(buffer(ctx, POOL_BFS_BIG, (v->m / kBigRow + 2) * 4 * (dir == WC_BOTH ? 2 : 1), &big));
+  WC_TRY(buffer(ctx, POOL_BFS_BIG, big_entries(v->m, dir) * 4, &big));
   filter = nullptr;
   if (filter_host) {
     WC_TRY(buffer(ctx, POOL_BFS_FILTER, ((n + 63) / 64) * 8, &filter));
@@ -464,6 +483,7 @@ wc_status Search::advance(Ctx& ctx, uint32_t max_levels, bool defer_last) {
   const uint32_t blocks = max_blocks(8);
   // A push takes a warp per frontier node (rows longer than kBigRow go to
   // push_big_kernel), a pull a thread per node.
+  const uint32_t big_cap = big_entries(v->m, dir);
   const uint32_t level_grid = std::max<uint32_t>(
       max_blocks(2), std::min<uint32_t>((uint32_t)((n + 255) / 256), blocks));
   uint32_t& d = depth_reached;
@@ -505,7 +525,7 @@ wc_status Search::advance(Ctx& ctx, uint32_t max_levels, bool defer_last) {
                              (uint64_t)(uintptr_t)queue[1]->ptr, (uint64_t)(uintptr_t)big->ptr,
                              (uint64_t)(uintptr_t)filter_dev, (uint64_t)(uintptr_t)adj.off0,
                              (uint64_t)(uintptr_t)adj.off1, (uint64_t)(uintptr_t)radj.off0,
-                             (uint64_t)(uintptr_t)radj.off1, level_grid, blocks,
+                             (uint64_t)(uintptr_t)radj.off1, level_grid, blocks, big_cap,
                              (uint64_t)(uintptr_t)v->stage_host};
     put(head, sizeof head);
     put(&sw, sizeof sw);
@@ -520,7 +540,7 @@ wc_status Search::advance(Ctx& ctx, uint32_t max_levels, bool defer_last) {
         const uint32_t L = d0 + q;
         LevelArgs a{adj, radj, st + q, queue[L & 1]->as<uint32_t>(),
                     queue[(L + 1) & 1]->as<uint32_t>(), fb[L % 3], fb[(L + 1) % 3],
-                    fb[(L + 2) % 3], (uint32_t)fw, big->as<uint32_t>(), L + 1, (uint32_t)n,
+                    fb[(L + 2) % 3], (uint32_t)fw, big->as<uint32_t>(), big_cap, L + 1, (uint32_t)n,
                     depth_p, via_p, filter_dev};
         note_launch(), level_kernel<<<level_grid, 256, 0, ctx.stream>>>(a);
         note_launch(), push_big_kernel<<<blocks, 256, 0, ctx.stream>>>(

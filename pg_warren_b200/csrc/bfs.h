@@ -32,6 +32,7 @@ struct LevelState {
   unsigned long long edges;       // row entries scanned by a pulled level
   uint32_t next_count;
   uint32_t big_count;             // frontier rows deferred to push_big_kernel
+  uint32_t huge_count;            // of which pushed by the whole grid (listed from the end)
   uint32_t done;                  // push_big_kernel's blocks finished
 };
 

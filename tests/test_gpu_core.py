@@ -362,3 +362,25 @@ def test_spmm_hub_rows_every_width(width):
                               replace=True, accumulate="plus", transpose=True)
     assert so == sg == 0
     assert yg.tobytes() == yo.tobytes()
+
+
+def test_bfs_long_and_huge_rows_match_the_oracle():
+    # Rows over 2,048 entries go to the long-row push (a block each) and
+    # rows over 32,768 to the whole-grid push: two hubs of 40,000 and
+    # 5,000 out-edges beside random edges, every direction, seeds that
+    # reach the hubs at different levels.
+    rng = np.random.default_rng(21)
+    n = 50000
+    pairs = set()
+    for t in rng.choice(n, 40000, replace=False):
+        pairs.add((7, int(t)))
+    for t in rng.choice(n, 5000, replace=False):
+        pairs.add((11, int(t)))
+    for _ in range(3 * n):
+        pairs.add((int(rng.integers(0, n)), int(rng.integers(0, n))))
+    pairs.add((3, 7))
+    og, gv = directed(n, sorted(pairs))
+    for starts in ([7], [3], [11, 40000], [int(rng.integers(0, n))]):
+        for direction in ("out", "in", "both"):
+            compare_bfs(og, gv, starts, direction=direction)
+            compare_bfs(og, gv, starts, direction=direction, max_depth=2)
