@@ -460,7 +460,8 @@ wc_status wc_bfs_cursor_open(wc_version* version, const wc_call* call, wc_direct
  * for wc_bfs_cursor_read; *count gets how many.  *more (may be NULL) is 0
  * once no level may follow: the search is exhausted, max_results was met
  * (the level is cut there and the stats say truncated) or the cursor was
- * stopped.  A finished cursor's calls return 0 visits. */
+ * stopped.  A finished cursor's calls return 0 visits; a call that fails
+ * (cancelled, timed out, out of memory) finishes the cursor. */
 wc_status wc_bfs_cursor_next(wc_bfs_cursor* cursor, const wc_call* call, uint64_t* count,
                              int32_t* more);
 

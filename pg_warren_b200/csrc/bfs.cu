@@ -1074,12 +1074,19 @@ wc_status wc_bfs_cursor_next(wc_bfs_cursor* c, const wc_call* call, uint64_t* co
   std::lock_guard<std::recursive_mutex> lock(v->mu);
   WC_CUDA(cudaSetDevice(v->device), call ? call->detail : nullptr);
   Ctx ctx(v, call);
+  // A level that fails (cancelled, timed out, out of memory) ends the
+  // cursor: its device state is no longer one the search can go on from.
+  auto fail = [&](wc_status st) {
+    c->finished = true;
+    c->rows.clear();
+    return st;
+  };
   // Interrupts are polled before any work (interrupts.rs; the seed's first
   // admission polls, and so does each expansion).
-  if (ctx.cancelled()) return WC_CANCELLED;
-  WC_TRY(ctx.begin());
+  if (ctx.cancelled()) return fail(WC_CANCELLED);
+  if (const wc_status st = ctx.begin(); st != WC_OK) return fail(st);
   c->before = c->stats;
-  WC_TRY(cursor_level(ctx, c));
+  if (const wc_status st = cursor_level(ctx, c); st != WC_OK) return fail(st);
   const uint64_t k = c->rows.size() / 3;
   if (c->max_results - c->emitted < k) {
     // bfs.rs:96-110: the visit past max_results is refused and the search

@@ -86,6 +86,8 @@ def test_a_raised_cancellation_stops_the_cursor():
         intr.cancel()
         with pytest.raises(W.api.Cancelled):
             c.next_level(interrupts=intr)
+        # the cancelled cursor is finished
+        assert c.next_level() == ([], False)
 
 
 def test_a_version_is_not_released_under_an_open_cursor():
@@ -192,3 +194,22 @@ def test_cursor_rmat16_with_pulled_levels():
             assert [v[0] for v in sum(levels(c), [])] == nodes
             assert c.stats().pulled_levels == ost["pulled_levels"]
             assert c.stats().edges_traversed == ost["edges_traversed"]
+
+
+def test_a_cursor_keeps_its_state_across_other_calls_on_the_version():
+    # The cursor's buffers are its own: searches run on the same version
+    # between its levels change nothing it hands out.
+    g = W.rmat(14, seed=3)
+    og = O.Graph.from_csr(g.id_space, g.offsets, g.targets)
+    gv = W.GraphVersion(g.offsets, g.targets)
+    expected, st = O.bfs(og, [5])
+    with W.BfsCursor(gv, [5]) as c, W.BfsCursor.reachable_set(gv, [9]) as other:
+        found = []
+        more = True
+        while more:
+            visits, more = c.next_level()
+            found += [(v.node, v.depth, v.via) for v in visits]
+            W.bfs(gv, [int(len(found) % g.id_space)], limits=W.Limits(3, None))
+            other.next_level()
+        assert found == expected
+        assert c.stats().edges_traversed == st["edges_traversed"]
