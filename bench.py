@@ -365,6 +365,16 @@ def _spmv_sweep(W, O, torch, dev, stream, peak, g, cpu):
             sec = time.perf_counter() - t0
             out[f"{sr}/cpu"] = {"ge_per_s": m / sec / 1e9, "threads": int(O.lib().wo_threads()),
                                 "sample": "one iteration over the CSC"}
+            # Parity at this size: the same product on the device.
+            yg = torch.empty_like(x0)
+            W.spmv(gv, W.Product(sr, transpose=True), x0.clone(), yg)
+            yg = yg.cpu().numpy()
+            if sr == "plus_times":
+                rel = np.abs(yg - ys) / np.maximum(np.abs(ys), 1e-300)
+                out[f"{sr}/parity"] = {"max_rel_vs_oracle": float(rel.max()),
+                                       "rows_bit_exact": float(np.mean(yg == ys))}
+            else:
+                out[f"{sr}/parity"] = {"bit_exact_vs_oracle": bool(np.array_equal(yg, ys))}
         del gv
     return out
 
@@ -429,6 +439,18 @@ def leg_c3(W, O, torch, dev, stream, peak, g=None):
     torch.cuda.synchronize(dev)
     mp_s = time.perf_counter() - t0
     iters = int(it.sum().item())
+    # Parity at this size (the suite's leg; the default line leaves it to
+    # the tests): the oracle's sssp_vector loop on 8 sources.
+    mp_parity = None
+    if O is not None:
+        og = O.Graph.from_csr(n, g.offsets, g.targets, wi)
+        pick = np.arange(0, 1024, 128)
+        do, ito = O.sssp_i64(og, src[pick], caps[pick])
+        got = d[torch.as_tensor(pick, device=dev)].cpu().numpy()
+        mp_parity = {"checked_sources": int(len(pick)),
+                     "bit_exact": bool(np.array_equal(got, do) and np.array_equal(
+                         it.cpu().numpy()[pick], ito.astype(np.int32)))}
+        del og
     del d
     # The plain per-source path: the sssp_vector loop, one SpMV a step
     # (min_plus over the reverse CSR, accumulate min) on a sample of the
@@ -466,6 +488,21 @@ def leg_c3(W, O, torch, dev, stream, peak, g=None):
     W.ppr_batched(gu, sets, W.PageRank(0.85, 1e-10, 100), ranks_out=r, iterations_out=pit)
     torch.cuda.synchronize(dev)
     ppr_s = time.perf_counter() - t0
+    # Parity at this size (the suite's leg): the oracle's seeded PageRank on
+    # 3 of the sets.
+    ppr_parity = None
+    if O is not None:
+        ogu = O.Graph.from_csr(n, g.offsets, g.targets)
+        rels, its_equal = [], True
+        for q in (0, 100, 200):
+            seed = np.zeros(n)
+            seed[sets[q]] = 1.0
+            ro, ito, _, _ = O.pagerank(ogu, 0.85, 1e-10, 100, seed=seed)
+            rels.append(float(np.abs(r[q].cpu().numpy() - ro).sum() / np.abs(ro).sum()))
+            its_equal &= int(pit[q].item()) == ito
+        ppr_parity = {"checked_sets": 3, "max_rel_l1_vs_oracle": max(rels),
+                      "iterations_equal": bool(its_equal)}
+        del ogu
     del r
     seeds = []
     for q in range(8):
@@ -484,12 +521,14 @@ def leg_c3(W, O, torch, dev, stream, peak, g=None):
                         "gteps_relaxations": iters * m / mp_s / 1e9,
                         "plain_per_source_ms": plain_per_source * 1e3,
                         "plain_sample": f"{plain_cols} sources, {plain_iters} loop steps",
-                        "batched_vs_plain": plain_per_source * 1024 / mp_s},
+                        "batched_vs_plain": plain_per_source * 1024 / mp_s,
+                        "parity": mp_parity},
             "ppr": {"seed_sets": 256, "seconds": ppr_s, "iterations_max": int(pit.max().item()),
                     "columns_per_pass": psched.columns_per_pass,
                     "per_set_ms": ppr_s / 256 * 1e3,
                     "plain_per_set_ms": plain_ppr_s * 1e3,
-                    "batched_vs_plain": plain_ppr_s * 256 / ppr_s}}
+                    "batched_vs_plain": plain_ppr_s * 256 / ppr_s,
+                    "parity": ppr_parity}}
 
 
 def leg_c4(W, O, torch, dev, stream, peak):
@@ -558,6 +597,15 @@ def leg_c5(W, O, torch, dev, stream, peak):
     _, ranks, its = W.pagerank_adjoint(gv, losses, pr, adjoint_tol=1e-14, grad_out=grad)
     torch.cuda.synchronize(dev)
     adj_s = time.perf_counter() - t0
+    # Parity at this size: the oracle's FP64 CPU adjoint for the first loss.
+    og = O.Graph.from_csr(n, g.offsets, g.targets, w)
+    go, ro, ito = O.pagerank_adjoint(og, losses[:1], 0.85, None, 100, 1e-14)
+    del og
+    g0 = grad[0].cpu().numpy()
+    adj_parity = {"checked_losses": 1,
+                  "max_abs_diff_over_max_abs": float(np.abs(g0 - go[0]).max() / np.abs(go[0]).max()),
+                  "ranks_rel_l1": float(np.abs(ranks - ro).sum() / ro.sum()),
+                  "iterations_equal": bool(int(its[0]) == int(ito[0]) and int(its[1]) >= 1)}
     h = 1e-6
     checks = []
     for e in rng.choice(m, 3, replace=False):
@@ -575,7 +623,7 @@ def leg_c5(W, O, torch, dev, stream, peak):
                        "rel": abs(fd - gd) / max(abs(gd), 1e-300), "fd_floor": floor})
     return {"graph": {"scale": 22, "nodes": n, "edges": m}, "losses": 64,
             "targets_per_loss": 1000, "seconds": adj_s, "forward_iterations": int(its[0]),
-            "adjoint_iterations": int(its[1]), "fd_checks": checks}
+            "adjoint_iterations": int(its[1]), "fd_checks": checks, "parity": adj_parity}
 
 
 def leg_cent(W, O, torch, dev, stream, peak):
