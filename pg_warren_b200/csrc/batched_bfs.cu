@@ -713,18 +713,39 @@ __device__ inline uint32_t written_levels(const uint32_t (&wl)[2], uint32_t x, u
   return valid ? lm : 0u;
 }
 
-constexpr uint32_t kDepthThreads = 512;
+// A depth block is two teams of 512 threads: the producers fold a tile's
+// levels into depth bytes (phase 1) while the consumers store the tile
+// before it (phase 2), the tile double-buffered in shared memory and handed
+// over through named barriers, so the stores of one tile run beside the
+// folds of the next instead of after them.
+constexpr uint32_t kDepthThreads = 512;    // producers
+constexpr uint32_t kDepthConsumers = 512;
+constexpr uint32_t kDepthBlock = kDepthThreads + kDepthConsumers;
 constexpr uint32_t kDepthNodes = 64;
+
+// Named barriers of the depth block: 1 + b (tile buffer b full), 3 + b
+// (buffer b free), 5 (the consumers alone).
+// Every warp of a team reaches each of them converged; each team's
+// arrivals are matched one for one by the other team's waits, so at most
+// one generation of a barrier is ever open.
+__device__ inline void depth_bar_sync(uint32_t id, uint32_t count) {
+  __syncwarp();
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+__device__ inline void depth_bar_arrive(uint32_t id, uint32_t count) {
+  __syncwarp();
+  asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
 
 // The depth kernel's dynamic shared memory: the tile, the caps, the sums
 // and the tile's degrees.
 template <int W> constexpr size_t depth_smem_bytes() {
-  return (size_t)kDepthNodes * 8 * W * 4 + 32 * W * 4 + 32 * W * 8 + kDepthNodes * 4 +
-         (kDepthNodes / 4) * 16;
+  return 2 * (size_t)kDepthNodes * 8 * W * 4 + 32 * W * 4 + 32 * W * 8 + 2 * kDepthNodes * 4 +
+         2 * (kDepthNodes / 4) * 16;
 }
 
 template <int W, int NB>
-__global__ void __launch_bounds__(kDepthThreads, 2)
+__global__ void __launch_bounds__(kDepthBlock, 1)
     msbfs_depth_kernel(uint32_t n, uint32_t k, uint32_t levels, const uint32_t* F, uint64_t fstride,
                        const uint32_t* wbits, uint32_t bitmap_words, const uint32_t* caps,
                        const uint32_t* off, const uint32_t* counts, uint8_t* depth_out,
@@ -735,13 +756,14 @@ __global__ void __launch_bounds__(kDepthThreads, 2)
   constexpr uint32_t IT = (TN * W + kDepthThreads - 1) / kDepthThreads;  // phase-1 items a thread takes
   constexpr uint32_t LC = NB == 5 ? 1 : 8;  // 32-level chunks of the written levels
   extern __shared__ __align__(16) unsigned char depth_smem[];
-  uint32_t* tile = reinterpret_cast<uint32_t*>(depth_smem);                    // [TN][Q]
-  uint32_t* cap4s = tile + TN * Q;                                              // [S]
+  uint32_t* tiles2 = reinterpret_cast<uint32_t*>(depth_smem);                  // [2][TN][Q]
+  uint32_t* cap4s = tiles2 + 2 * TN * Q;                                        // [S]
   unsigned long long* esum = reinterpret_cast<unsigned long long*>(cap4s + S);  // [S]
-  uint32_t* degs = reinterpret_cast<uint32_t*>(esum + S);                       // [TN]
+  uint32_t* degs2 = reinterpret_cast<uint32_t*>(esum + S);                      // [2][TN]
   // Per node quad: the degrees' low and high bytes as byte planes (for
   // dp4a) and whether a degree is 2^16 or more (then the plain sum).
-  uint4* dplanes = reinterpret_cast<uint4*>(degs + TN);                         // [TN / 4]
+  uint4* dplanes2 = reinterpret_cast<uint4*>(degs2 + 2 * TN);                   // [2][TN / 4]
+  const bool producer = threadIdx.x < kDepthThreads;
   const uint32_t lane = threadIdx.x & 31;
   // The snapshots written: F_L exists for L < used (F_L is written only if
   // level L-1 had a frontier to expand).
@@ -760,8 +782,16 @@ __global__ void __launch_bounds__(kDepthThreads, 2)
   const bool aligned = (n & 3u) == 0 && (base & 3u) == 0;
   const bool aligned16 = (n & 15u) == 0 && (base & 15u) == 0;
   const uint32_t tiles = (n + TN - 1) / TN;
-  for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+  __syncthreads();  // the caps and sums, before the teams part
+  for (uint32_t t = blockIdx.x, li = 0; t < tiles; t += gridDim.x, li++) {
     const uint32_t i0 = t * TN;
+    const uint32_t buf = li & 1;
+    uint32_t* tile = tiles2 + buf * TN * Q;     // [TN][Q]
+    uint32_t* degs = degs2 + buf * TN;          // [TN]
+    uint4* dplanes = dplanes2 + buf * (TN / 4);  // [TN / 4]
+    if (producer) {
+    // The consumers are done with this buffer's tile before last.
+    if (li >= 2) depth_bar_sync(3 + buf, kDepthBlock);
     // Lane L holds level 32c + L's written-row words of the tile's nodes.
     uint32_t wl[LC][2];
 #pragma unroll
@@ -903,10 +933,12 @@ __global__ void __launch_bounds__(kDepthThreads, 2)
       *grp0 = make_uint4(lo[0], hi[0], lo[1], hi[1]);
       *grp1 = make_uint4(lo[2], hi[2], lo[3], hi[3]);
     }
-    __syncthreads();
+    depth_bar_arrive(1 + buf, kDepthBlock);
+    } else {
+    depth_bar_sync(1 + buf, kDepthBlock);
     // Phase 2: lanes 4h .. 4h + 3 of a warp take source quad g, lane p of
     // them nodes 16p .. 16p + 15 (node quads 4p .. 4p + 3).
-    for (uint32_t y = threadIdx.x; y < Q * 4; y += blockDim.x) {
+    for (uint32_t y = threadIdx.x - kDepthThreads; y < Q * 4; y += kDepthConsumers) {
       const uint32_t g = y >> 2, p = y & 3;
       const uint4 c4 = *reinterpret_cast<const uint4*>(cap4s + 4 * g);
       const uint32_t cap[4] = {c4.x, c4.y, c4.z, c4.w};
@@ -974,9 +1006,18 @@ __global__ void __launch_bounds__(kDepthThreads, 2)
         }
       }
     }
-    __syncthreads();
+    depth_bar_arrive(3 + buf, kDepthBlock);
+    }
   }
-  for (uint32_t x = threadIdx.x; x < k; x += blockDim.x)
+  if (producer) {
+    // Match the consumers' frees of the last two tiles, then leave.
+    const uint32_t mine = blockIdx.x < tiles ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0u;
+    for (uint32_t li = mine >= 2 ? mine - 2 : 0u; li < mine; li++)
+      depth_bar_sync(3 + (li & 1), kDepthBlock);
+    return;
+  }
+  depth_bar_sync(5, kDepthConsumers);
+  for (uint32_t x = threadIdx.x - kDepthThreads; x < k; x += kDepthConsumers)
     if (esum[x]) atomicAdd(edges + x, esum[x]);
 }
 
@@ -1133,21 +1174,22 @@ wc_status run_pass(Ctx& ctx, BatchBuffers& b, const uint64_t* sources_dev, const
       return WC_INVALID_ARGUMENT;
     }
   }
-  // Depths: persistent blocks of 64-node tiles, two blocks an SM.
-  const uint32_t depth_grid = max_blocks(2);
+  // Depths: persistent blocks of 64-node tiles (a producer and a consumer
+  // team each), one block an SM.
+  const uint32_t depth_grid = max_blocks(1);
   constexpr size_t depth_smem = depth_smem_bytes<W>();
   ctx.phase_begin("depth");
   // Depths fit five bit planes up to level 31.
   if (levels + 1 <= 32) {
     WC_CUDA(cudaFuncSetAttribute(msbfs_depth_kernel<W, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)depth_smem), ctx.detail);
-    note_launch(), msbfs_depth_kernel<W, 5><<<depth_grid, kDepthThreads, depth_smem, st>>>(
+    note_launch(), msbfs_depth_kernel<W, 5><<<depth_grid, kDepthBlock, depth_smem, st>>>(
         n, k, levels + 1, F, fstride, wbits, (uint32_t)bitmap_words, caps_dev,
         v->fwd.offsets.as<uint32_t>(), counts, depth_dev, edges_dev);
   } else {
     WC_CUDA(cudaFuncSetAttribute(msbfs_depth_kernel<W, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)depth_smem), ctx.detail);
-    note_launch(), msbfs_depth_kernel<W, 8><<<depth_grid, kDepthThreads, depth_smem, st>>>(
+    note_launch(), msbfs_depth_kernel<W, 8><<<depth_grid, kDepthBlock, depth_smem, st>>>(
         n, k, levels + 1, F, fstride, wbits, (uint32_t)bitmap_words, caps_dev,
         v->fwd.offsets.as<uint32_t>(), counts, depth_dev, edges_dev);
   }
