@@ -168,7 +168,7 @@ __device__ inline void plan_next(LevelState* st, const SwitchArgs& sw, uint32_t 
 
 // Push of the long rows: a huge row's entries spread over every warp of the
 // grid, the huge rows one after another; then each long row over the warps
-// of one block, the blocks taking the long rows in turn.  Then the block
+// of a team of blocks, the teams taking the long rows in turn.  Then the block
 // that finishes last closes the level: it plans the next one.
 __device__ inline void push_row_part(const LevelArgs& a, uint32_t u, uint32_t first_warp,
                                      uint32_t warp_stride) {
@@ -200,9 +200,18 @@ __global__ void __launch_bounds__(256) push_big_kernel(LevelArgs a, SwitchArgs s
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t huge = st.pull ? 0u : st.huge_count;
   for (uint32_t h = 0; h < huge; h++) push_row_part(a, a.big[a.big_cap - 1 - h], warp, warps);
+  // Each long row gets a team of blocks: one when there are more rows than
+  // blocks, else as many as share the grid evenly.
   const uint32_t big = st.pull ? 0u : st.big_count;
-  for (uint32_t b = blockIdx.x; b < big; b += gridDim.x)
-    push_row_part(a, a.big[b], threadIdx.x >> 5, blockDim.x >> 5);
+  if (big) {
+    const uint32_t team = max(1u, gridDim.x / big);
+    const uint32_t rows_at_once = gridDim.x / team;
+    const uint32_t slot = blockIdx.x / team;
+    const uint32_t wpb = blockDim.x >> 5;
+    if (slot < rows_at_once)
+      for (uint32_t b = slot; b < big; b += rows_at_once)
+        push_row_part(a, a.big[b], (blockIdx.x % team) * wpb + (threadIdx.x >> 5), team * wpb);
+  }
   __shared__ bool last;
   __syncthreads();
   if (threadIdx.x == 0) {
