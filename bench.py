@@ -62,7 +62,7 @@ CPU_BUDGET_S = 12.0
 # DRAM bytes per algorithmic byte of a pull level, from the ncu capture of
 # msbfs_level_kernel on the same workload at R-MAT 20 (the full-size launch
 # is past the capture-size rule): traffic scales with the level's units.
-LEVEL_TRAFFIC_RATIO = 474.05 / 337.0
+LEVEL_TRAFFIC_RATIO = (256.51 + 113.99) / 337.0
 LEVEL_TRAFFIC_SOURCE = ("dram__bytes_read.sum + dram__bytes_write.sum of one pull level at "
                         "R-MAT 20 (profiles/msbfs_level_kernel_rmat20_1024src.md), scaled "
                         "by the algorithmic bytes")
