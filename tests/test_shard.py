@@ -90,3 +90,49 @@ def test_without_a_process_group_the_call_is_unsharded():
     assert run_sharded(3, _search_into(og, sources, caps, d, e), [d, e]) == (0, 3)
     do, eo = O.bfs_depths(og, sources, caps)
     assert np.array_equal(d.numpy(), do) and np.array_equal(e.numpy(), eo.astype(np.int64))
+
+
+def _wgraph():
+    rng = np.random.default_rng(12)
+    n = 200
+    edges = [(0, int(a), int(b), float(rng.integers(1, 9)))
+             for a, b in rng.integers(0, n, (1500, 2)) if a != b]
+    return O.Graph.from_edges(n, edges, weighted=True, reverse=True)
+
+
+def _rank_minplus(rank, world, port, sources, hops, out):
+    # The min-plus shape of the sharded call (i64 distances and i32
+    # iteration counts, two outputs of other widths), with the oracle's
+    # sssp_vector loop as each rank's search; some ranks may own no rows.
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        og = _wgraph()
+        dist_out = torch.full((len(sources), og.n), -7, dtype=torch.int64)
+        its = torch.full((len(sources),), -1, dtype=torch.int32)
+
+        def search(b, e):
+            d, it = O.sssp_i64(og, sources[b:e], hops[b:e])
+            dist_out[b:e] = torch.from_numpy(d)
+            its[b:e] = torch.from_numpy(it.astype(np.int32))
+
+        run_sharded(len(sources), search, [dist_out, its])
+        np.save(out + f"_{rank}_d.npy", dist_out.numpy())
+        np.save(out + f"_{rank}_i.npy", its.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("count", [2, 5])
+def test_three_gloo_ranks_gather_minplus_rows_even_when_a_rank_owns_none(tmp_path, count):
+    rng = np.random.default_rng(count)
+    sources = rng.integers(0, 200, count).astype(np.uint64)
+    hops = rng.integers(0, 12, count).astype(np.uint32)
+    out = str(tmp_path / "m")
+    mp.start_processes(_rank_minplus, args=(3, _free_port(), sources, hops, out), nprocs=3,
+                       start_method="spawn")
+    do, ito = O.sssp_i64(_wgraph(), sources, hops)
+    for rank in range(3):
+        assert np.array_equal(np.load(out + f"_{rank}_d.npy"), do)
+        assert np.array_equal(np.load(out + f"_{rank}_i.npy"), ito.astype(np.int32))
