@@ -1072,7 +1072,8 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic",
-        "config": config(n, m, columns_per_pass=columns, blocks_per_sm=sched.blocks_per_sm),
+        "config": config(n, m),
+        "schedule": {"columns_per_pass": columns, "blocks_per_sm": sched.blocks_per_sm},
         "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": WIDTH * 12,
                 "d2h_bytes_per_step": WIDTH * n + WIDTH * 8},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
