@@ -394,6 +394,21 @@ wc_status wc_pagerank_part_step(wc_version* version, const wc_call* call, uint32
 wc_status wc_pagerank_part_end(wc_version* version, const wc_call* call, uint32_t iterations,
                                double* ranks);
 
+/* No reference counterpart (warren-core multiplies on one host): one rank's
+ * part of a row-partitioned wc_spmv over several GPUs.  The rows of the
+ * product's CSR (forward, or reverse with `transpose`) are cut into `parts`
+ * ranges of about equal entries, at unit boundaries of its schedule; every
+ * rank holds the whole version and the whole x, and computes its range of
+ * y, which the caller then gathers (one all-gather of y's rows a product).
+ * The part's rows equal wc_spmv's bit for bit (the same kernel folds each
+ * row the same way); y's other rows are left as given.
+ *
+ * wc_spmv_part_rows: the parts' first rows, row_bounds[parts + 1]. */
+wc_status wc_spmv_part_rows(wc_version* version, int32_t transpose, uint32_t parts,
+                            uint64_t* row_bounds);
+wc_status wc_spmv_part(wc_version* version, const wc_call* call, const wc_product* product,
+                       wc_dtype dtype, uint32_t parts, uint32_t part, const void* x, void* y);
+
 /* The stop test's margin of the last iteration run: delta / (live × tol).
  * Available after wc_pagerank on the same version (diagnostics). */
 double wc_pagerank_last_margin(const wc_version* version);
@@ -489,6 +504,53 @@ wc_status wc_reachable_set(wc_version* version, const wc_call* call, wc_directio
                            const uint64_t* starts, uint64_t start_count, uint32_t max_depth,
                            uint64_t* nodes_out, uint64_t capacity, uint64_t* count,
                            wc_traversal_stats* stats);
+
+/* No reference counterpart (warren-core searches on one host): one rank's
+ * part of a row-partitioned level search (traversal/level.rs, LevelSearch)
+ * over several GPUs.  The rows are cut into `parts` ranges (multiples of 64
+ * rows, about equal pull entries); every rank holds the whole version and
+ * the whole frontier bitmap, and owns the visited bits and depths of its
+ * range.  Each level every rank reaches its range's rows (pulled, or pushed
+ * from the whole frontier: the same choice on every rank), and between
+ * levels the caller sums the parts' next-frontier counts and out-edges and
+ * gathers the parts' words of the next frontier bitmap (one all-reduce of
+ * two integers and one all-gather of id_space/8 bytes a level).  The
+ * depths equal wc_bfs's depth_out over the same starts, direction and
+ * max_depth (no filter, no max_results).
+ *
+ * wc_bfs_part_rows: the parts' first rows, row_bounds[parts + 1]. */
+wc_status wc_bfs_part_rows(wc_version* version, wc_direction direction, uint32_t parts,
+                           uint64_t* row_bounds);
+
+typedef struct wc_bfs_part_info {
+    uint64_t row_begin, row_end;  /* this part's rows */
+    uint64_t id_space;
+    uint64_t words;               /* 64-bit words of one frontier bitmap */
+    uint64_t frontier;            /* level 0's frontier: the distinct starts */
+    uint64_t frontier_edges;      /* and their out-edges in the search direction */
+} wc_bfs_part_info;
+
+/* Sets up part `part` of `parts`: frontier2 is the caller's device memory,
+ * 2 × words 64-bit words (the frontiers of even and odd levels; bit i of
+ * word i/64 is node i); every start's bit is set in frontier2[0..words).
+ * Starts outside the id space are WC_NODE_OUTSIDE_ID_SPACE.  The part's
+ * visited bits and depths are device buffers of its own, charged to the
+ * version's budget until wc_bfs_part_end. */
+wc_status wc_bfs_part_begin(wc_version* version, const wc_call* call, wc_direction direction,
+                            const uint64_t* starts, uint64_t start_count, uint32_t max_depth,
+                            uint32_t parts, uint32_t part, uint64_t* frontier2,
+                            wc_bfs_part_info* info);
+/* Level `level` (< max_depth) over the part's rows, given the level's
+ * frontier (every part's words of frontier2[level & 1], gathered) and its
+ * summed out-edges: writes the part's words of frontier2[(level + 1) & 1],
+ * waits, and returns the part's next-frontier nodes and their out-edges in
+ * sums[0], sums[1]. */
+wc_status wc_bfs_part_step(wc_version* version, const wc_call* call, uint32_t level,
+                           uint64_t frontier_edges, uint64_t* sums);
+/* The part's rows of the depths (WC_UNREACHED where not reached) into
+ * depth_out[row_begin .. row_end) (host or device, id_space entries).  Ends
+ * the part. */
+wc_status wc_bfs_part_end(wc_version* version, const wc_call* call, uint32_t* depth_out);
 
 /* traversal/reachable.rs:18-43 (reachable). */
 wc_status wc_reachable(wc_version* version, const wc_call* call, wc_direction direction,

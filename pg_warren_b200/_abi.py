@@ -110,6 +110,11 @@ class PageRankPartInfo(C.Structure):
                 ("dangling", D), ("threshold", D)]
 
 
+class BfsPartInfo(C.Structure):
+    _fields_ = [("row_begin", U64), ("row_end", U64), ("id_space", U64), ("words", U64),
+                ("frontier", U64), ("frontier_edges", U64)]
+
+
 class HostCsr(C.Structure):
     _fields_ = [("id_space", U64), ("edges", U64), ("offsets", C.POINTER(U64)),
                 ("targets", C.POINTER(U32)), ("external_ids", C.POINTER(C.c_int64))]
@@ -144,6 +149,13 @@ SIGNATURES = [
                                      P, P, C.POINTER(PageRankPartInfo)]),
     ("wc_pagerank_part_step", I32, [P, C.POINTER(Call), U32, D, C.POINTER(D)]),
     ("wc_pagerank_part_end", I32, [P, C.POINTER(Call), U32, P]),
+    ("wc_spmv_part_rows", I32, [P, I32, U32, P]),
+    ("wc_spmv_part", I32, [P, C.POINTER(Call), C.POINTER(ProductC), I32, U32, U32, P, P]),
+    ("wc_bfs_part_rows", I32, [P, I32, U32, P]),
+    ("wc_bfs_part_begin", I32, [P, C.POINTER(Call), I32, P, U64, U32, U32, U32, P,
+                                C.POINTER(BfsPartInfo)]),
+    ("wc_bfs_part_step", I32, [P, C.POINTER(Call), U32, U64, P]),
+    ("wc_bfs_part_end", I32, [P, C.POINTER(Call), P]),
     ("wc_bfs", I32, [P, C.POINTER(Call), I32, P, U64, C.POINTER(Limits), P, P, P,
                      C.POINTER(TraversalStats)]),
     ("wc_bfs_visits", I32, [P, C.POINTER(Call), I32, P, U64, C.POINTER(Limits), P, P, U64,

@@ -63,6 +63,9 @@ wc_status launch_part_iteration(const PullLaunch& L, const PrState& s, uint32_t 
                                 uint32_t blocks);
 // Drops a version's partitioned solve (wc_pagerank_part_*) when it is released.
 void pagerank_part_forget(const wc_version* v);
+// The row-partitioned search's and product's state kept with a version
+// (bfs_part.cu), dropped when the version is released.
+void bfs_part_forget(const wc_version* v);
 // Blocks of an iteration launch over `csc`; of the long-row pass that
 // follows it in the locality order; and the block sums the step keeps.
 uint32_t pagerank_grid(const DevCsr& csc);

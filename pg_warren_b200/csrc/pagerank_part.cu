@@ -22,12 +22,13 @@ namespace wc {
 wc_status prepare_pull(Ctx& ctx, DevCsr& csr, int semiring, int weighted_flag, int dtype,
                        uint32_t width, PullLaunch& L);
 
-// The parts' first units and first rows: units are taken in order and a
-// part is closed at the first row boundary at or past its share of the
-// entries; a long row's pieces stay in one part.
-static wc_status part_cuts(wc_version* v, uint32_t parts, std::vector<uint32_t>& unit_cut,
-                           std::vector<uint64_t>& row_cut, wc_error_detail* detail) {
-  const Schedule& sc = v->loc.csc.schedule;
+// The parts' first units and first rows over `csr`'s schedule: units are
+// taken in order and a part is closed at the first row boundary at or past
+// its share of the entries; a long row's pieces stay in one part.
+wc_status schedule_part_cuts(const wc_version* v, const DevCsr& csr, uint32_t parts,
+                             std::vector<uint32_t>& unit_cut, std::vector<uint64_t>& row_cut,
+                             wc_error_detail* detail) {
+  const Schedule& sc = csr.schedule;
   std::vector<Unit> units(sc.count);
   if (sc.count)
     WC_CUDA(cudaMemcpy(units.data(), sc.units.ptr, sc.count * sizeof(Unit), cudaMemcpyDeviceToHost),
@@ -54,6 +55,11 @@ static wc_status part_cuts(wc_version* v, uint32_t parts, std::vector<uint32_t>&
     row_cut[p] = v->n;
   }
   return WC_OK;
+}
+
+static wc_status part_cuts(wc_version* v, uint32_t parts, std::vector<uint32_t>& unit_cut,
+                           std::vector<uint64_t>& row_cut, wc_error_detail* detail) {
+  return schedule_part_cuts(v, v->loc.csc, parts, unit_cut, row_cut, detail);
 }
 
 // The state of a part kept with the version between its calls.

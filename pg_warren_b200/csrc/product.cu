@@ -2,6 +2,9 @@
 // device.  Aᵀ is always pulled over the device's reverse CSR; the reference
 // pushes only where it has no reverse CSR, and its push and pull agree bit
 // for bit (product/mod.rs:8-12), so the result is the same.
+#include <algorithm>
+#include <vector>
+
 #include "operand.h"
 #include "product.h"
 #include "semiring.cuh"
@@ -73,9 +76,13 @@ wc_status launch_pull(const PullLaunch& L, int dtype, const void* x, void* y) {
   return WC_DTYPE_MISMATCH;
 }
 
+// `parts` > 0: only part `part` of the rows (schedule_part_cuts over the
+// product's CSR) is computed and written; y's other rows are left as given.
 static wc_status product(wc_version* v, const wc_call* call, const wc_product* p, wc_dtype dtype,
-                         uint32_t width, const void* x, void* y) {
+                         uint32_t width, const void* x, void* y, uint32_t parts = 0,
+                         uint32_t part = 0) {
   if (!v || !p || !x || !y) return WC_INVALID_ARGUMENT;
+  if (parts && part >= parts) return WC_INVALID_ARGUMENT;
   if (p->semiring < 0 || p->semiring > WC_MAX_SECOND) return WC_UNKNOWN_SEMIRING;
   if (dtype < WC_F32 || dtype > WC_BOOL) return WC_DTYPE_MISMATCH;
   if (width == 0) return WC_ZERO_WIDTH;
@@ -107,6 +114,13 @@ static wc_status product(wc_version* v, const wc_call* call, const wc_product* p
   PullLaunch L;
   DevCsr& csr = p->transpose ? v->rev : v->fwd;
   WC_TRY(prepare_pull(ctx, csr, p->semiring, p->weighted, dtype, width, L));
+  if (parts) {
+    std::vector<uint32_t> uc;
+    std::vector<uint64_t> rc;
+    WC_TRY(schedule_part_cuts(v, csr, parts, uc, rc, ctx.detail));
+    L.units += uc[part];
+    L.unit_count = uc[part + 1] - uc[part];
+  }
   if (width > 1) {
     DevBuf* mc;
     WC_TRY(ctx.scratch(POOL_SPMM_CARRY,
@@ -117,7 +131,7 @@ static wc_status product(wc_version* v, const wc_call* call, const wc_product* p
   if (p->mask) L.write = WriteArgs{M.dev, (int32_t)p->mask->dtype, p->mask->complement, p->replace,
                                    (int32_t)p->accumulate};
   else L.write = WriteArgs{nullptr, WC_F64, 0, p->replace, (int32_t)p->accumulate};
-  WC_TRY(launch_pull(L, dtype, xd, Y.dev));
+  if (L.unit_count) WC_TRY(launch_pull(L, dtype, xd, Y.dev));
   WC_TRY(Y.out(ctx));
   // Asynchronous only where every operand is the caller's device memory.
   if (ctx.async && X.is_device && Y.is_device && (!p->mask || M.is_device)) return WC_OK;
@@ -136,6 +150,24 @@ wc_status wc_spmv(wc_version* v, const wc_call* call, const wc_product* p, wc_dt
 wc_status wc_spmm(wc_version* v, const wc_call* call, const wc_product* p, wc_dtype dtype,
                   uint32_t width, const void* x, void* y) {
   return wc::product(v, call, p, dtype, width, x, y);
+}
+
+wc_status wc_spmv_part_rows(wc_version* v, int32_t transpose, uint32_t parts,
+                            uint64_t* row_bounds) {
+  if (!v || parts == 0 || !row_bounds) return WC_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lock(v->mu);
+  WC_CUDA(cudaSetDevice(v->device), nullptr);
+  std::vector<uint32_t> uc;
+  std::vector<uint64_t> rc;
+  WC_TRY(wc::schedule_part_cuts(v, transpose ? v->rev : v->fwd, parts, uc, rc, nullptr));
+  std::copy(rc.begin(), rc.end(), row_bounds);
+  return WC_OK;
+}
+
+wc_status wc_spmv_part(wc_version* v, const wc_call* call, const wc_product* p, wc_dtype dtype,
+                       uint32_t parts, uint32_t part, const void* x, void* y) {
+  if (parts == 0) return WC_INVALID_ARGUMENT;
+  return wc::product(v, call, p, dtype, 1, x, y, parts, part);
 }
 
 }  // extern "C"

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <vector>
 
 #include "runtime.cuh"
 
@@ -42,6 +43,13 @@ struct PullLaunch {
   WriteArgs write;
   uint32_t hot;  // over a locality-ordered CSC: gathers of j < hot kept in L1 (0: none)
 };
+
+// Cuts `csr`'s schedule into `parts` ranges of about equal entries at unit
+// boundaries (a long row's pieces in one range): unit_cut and row_cut get
+// parts + 1 entries, the parts' first units and first rows.
+wc_status schedule_part_cuts(const wc_version* v, const DevCsr& csr, uint32_t parts,
+                             std::vector<uint32_t>& unit_cut, std::vector<uint64_t>& row_cut,
+                             wc_error_detail* detail);
 
 wc_status launch_pull_f64(const PullLaunch& L, const void* x, void* y);
 wc_status launch_pull_f32(const PullLaunch& L, const void* x, void* y);

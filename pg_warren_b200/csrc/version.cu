@@ -299,6 +299,7 @@ wc_status wc_version_release(wc_version* v) {
     if (v->stream) cudaStreamDestroy(v->stream);
   }
   pagerank_part_forget(v);
+  bfs_part_forget(v);
   delete v;
   return WC_OK;
 }
