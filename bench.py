@@ -439,8 +439,7 @@ def leg_c3(W, O, torch, dev, stream, peak, g=None):
     torch.cuda.synchronize(dev)
     mp_s = time.perf_counter() - t0
     iters = int(it.sum().item())
-    # Parity at this size (the suite's leg; the default line leaves it to
-    # the tests): the oracle's sssp_vector loop on 8 sources.
+    # Parity at this size: the oracle's sssp_vector loop on 8 sources.
     mp_parity = None
     if O is not None:
         og = O.Graph.from_csr(n, g.offsets, g.targets, wi)
@@ -488,8 +487,7 @@ def leg_c3(W, O, torch, dev, stream, peak, g=None):
     W.ppr_batched(gu, sets, W.PageRank(0.85, 1e-10, 100), ranks_out=r, iterations_out=pit)
     torch.cuda.synchronize(dev)
     ppr_s = time.perf_counter() - t0
-    # Parity at this size (the suite's leg): the oracle's seeded PageRank on
-    # 3 of the sets.
+    # Parity at this size: the oracle's seeded PageRank on 3 of the sets.
     ppr_parity = None
     if O is not None:
         ogu = O.Graph.from_csr(n, g.offsets, g.targets)
@@ -746,7 +744,7 @@ def suite(args):
 
 
 # --------------------------------------------------------------- profiler cases
-# `python bench.py --case batched|spmv|ppr|minplus|eigen|adjoint --scale S`: one
+# `python bench.py --case batched|spmv|ppr|minplus|eigen|adjoint|bfspart --scale S`: one
 # small workload per kernel family, for ncu captures (a few GB on the device
 # at most).
 
@@ -849,6 +847,23 @@ def profile_case(args):
             seconds = time.perf_counter() - t0
         print(json.dumps({"case": "adjoint", "nodes": n, "edges": g.edges, "seconds": seconds,
                           "iterations": [int(i) for i in its]}))
+    elif args.case == "bfspart":
+        # The row-partitioned level search as one part (its pull, push and
+        # settle kernels), from one seed, two calls; then one part of a
+        # two-part product over the reverse CSR.
+        from pg_warren_b200.partition import bfs_partitioned, SpmvDeviceParts
+        seed = [int(np.random.default_rng(SEED).integers(0, n))]
+        for _ in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            depth, levels = bfs_partitioned(gv, seed)
+            seconds = time.perf_counter() - t0
+        x = torch.rand(n, dtype=torch.float64, device="cuda")
+        y = torch.zeros(n, dtype=torch.float64, device="cuda")
+        SpmvDeviceParts(gv, W.Product("plus_times", transpose=True)).apply(2, 0, x, y)
+        torch.cuda.synchronize()
+        print(json.dumps({"case": "bfspart", "nodes": n, "edges": g.edges, "levels": levels,
+                          "reached": int((depth != 0xFFFFFFFF).sum()), "seconds": seconds}))
     else:
         # SpMV plus_times (f64, unweighted) over the forward CSR three
         # times, then a PageRank of three iterations.
@@ -871,7 +886,8 @@ def main():
     ap.add_argument("--impl", default="warren")
     ap.add_argument("--suite", default=None,
                     help="comma-separated configurations to measure instead: c1,c2,c3,c4,c5,cent,load")
-    ap.add_argument("--case", default=None, choices=["batched", "spmv", "ppr", "minplus", "eigen", "adjoint"],
+    ap.add_argument("--case", default=None, choices=["batched", "spmv", "ppr", "minplus", "eigen", "adjoint",
+                                                       "bfspart"],
                     help="a small workload for profilers instead")
     ap.add_argument("--scale", type=int, default=20)
     args = ap.parse_args()
@@ -1020,7 +1036,14 @@ def main():
     # and personalised PageRank against their plain per-source paths (the
     # batched-traversal configuration's other two workloads)
     spmv = spmv_point(W, torch, dev, stream, peak, g)
-    c3 = leg_c3(W, None, torch, dev, stream, peak, g=g)
+    # The oracle checks the batched min-plus (8 sources) and personalised
+    # PageRank (3 sets) outputs at this size, outside their timed calls, on
+    # rank 0 of a one-GPU run (as the CPU baseline below checks the depths).
+    checker = None
+    if rank == 0 and world == 1:
+        import oracle as checker
+        checker.build()
+    c3 = leg_c3(W, checker, torch, dev, stream, peak, g=g)
     torch.cuda.empty_cache()
 
     # ---- end to end through the public call, host buffers
