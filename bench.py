@@ -744,7 +744,7 @@ def suite(args):
 
 
 # --------------------------------------------------------------- profiler cases
-# `python bench.py --case batched|spmv|ppr|minplus|eigen|adjoint|bfspart --scale S`: one
+# `python bench.py --case batched|spmv|ppr|minplus|eigen|adjoint|bfspart|all --scale S`: one
 # small workload per kernel family, for ncu captures (a few GB on the device
 # at most).
 
@@ -847,6 +847,69 @@ def profile_case(args):
             seconds = time.perf_counter() - t0
         print(json.dumps({"case": "adjoint", "nodes": n, "edges": g.edges, "seconds": seconds,
                           "iterations": [int(i) for i in its]}))
+    elif args.case == "all":
+        # Every kernel family once on the same graph, for a launch list with
+        # each kernel's DRAM bytes: products in every element type, PageRank
+        # (plain, seeded, no-allocation), the traversals (plain, visits,
+        # reachable set, cursor, components), the batched searches, the
+        # eigensolver, the adjoint, top-k, the vector map and reductions,
+        # the centralities, the version load from segments and the
+        # partitioned parts.
+        from pg_warren_b200 import expr as X
+        from pg_warren_b200.partition import bfs_partitioned, SpmvDeviceParts
+        rng = np.random.default_rng(SEED)
+        xf = torch.rand(n, dtype=torch.float64, device="cuda")
+        for sr, dt in (("plus_times", torch.float64), ("plus_times", torch.float32),
+                       ("min_plus", torch.int64), ("lor_land", torch.bool)):
+            xx = (xf * 100).to(dt) if dt != torch.bool else xf < 0.1
+            yy = torch.zeros(n, dtype=dt, device="cuda")
+            W.spmv(gv, W.Product(sr, transpose=True), xx, yy)
+        W.spmm(gv, W.Product("plus_times"), torch.rand((n, 8), dtype=torch.float64, device="cuda"),
+               torch.zeros((n, 8), dtype=torch.float64, device="cuda"))
+        W.pagerank(gv, None, W.PageRank(0.85, 1e-10, 100))
+        seed = np.zeros(n)
+        seed[rng.choice(n, 100, replace=False)] = 1.0
+        W.pagerank(gv, None, W.PageRank(0.85, 1e-10, 100, seed=seed))
+        W.pagerank_noalloc(gv, None, W.PageRank(0.85, 1e-10, 100))
+        starts = [int(v) for v in rng.integers(0, n, 4)]
+        W.bfs_depths(gv, starts)
+        W.bfs(gv, starts[:1], limits=W.Limits(3, None))
+        W.reachable_set(gv, starts, None, "both")
+        cur = W.BfsCursor(gv, starts[:1])
+        for _ in range(4):
+            cur.next_level()
+        cur.close()
+        W.components(gv)
+        src = torch.as_tensor(rng.integers(0, n, 256).astype(np.int64), device="cuda")
+        caps = torch.full((256,), 16, dtype=torch.int32, device="cuda")
+        W.bfs_batched(gv, src, caps)
+        wi = rng.integers(1, 101, g.edges).astype(np.float64)
+        gw = W.GraphVersion(g.offsets, g.targets, wi)
+        W.minplus_batched(gw, rng.integers(0, n, 64).astype(np.uint64),
+                          np.full(64, 8, np.uint32))
+        sets = [rng.choice(n, int(k), replace=False) for k in rng.integers(1, 300, 32)]
+        W.ppr_batched(gv, sets, W.PageRank(0.85, 1e-10, 100))
+        gs = W.rmat(16, undirected=True).upload()
+        W.eigen(gs, W.EigenOptions(4, which="smallest", operator="normalized_laplacian",
+                                   tol=1e-8, max_iter=400, seed=7))
+        gl = W.GraphVersion(g.offsets, g.targets, W.edge_weights(g, "lognormal"))
+        W.pagerank_adjoint(gl, [rng.choice(n, 100, replace=False) for _ in range(4)],
+                           W.PageRank(0.85, None, 20))
+        W.top_k(gv, xf, 100)
+        W.vector_map(gv, X.Arithmetic("+", X.Call("sqrt", X.Vector("f64", 0)),
+                                      X.Literal("f64", 1.0)), [xf])
+        W.vector_reduce(gv, xf, "sum")
+        W.vector_norm_diff(gv, xf, xf * 0.5, "l1")
+        W.closeness_centrality(gv, W.Sampling(k=64, seed=3))
+        W.betweenness_centrality(gv, W.Sampling(k=16, seed=3))
+        rows, offs, tgts, wts = W.api.csr_segments(g.offsets, g.targets)
+        W.GraphVersion.from_segments(n, offs, tgts, wts, rows)
+        bfs_partitioned(gv, starts[:1])
+        SpmvDeviceParts(gv, W.Product("plus_times", transpose=True)).apply(
+            2, 1, xf, torch.zeros_like(xf))
+        torch.cuda.synchronize()
+        print(json.dumps({"case": "all", "nodes": n, "edges": g.edges,
+                          "launches": int(W.load().wc_kernel_launches())}))
     elif args.case == "bfspart":
         # The row-partitioned level search as one part (its pull, push and
         # settle kernels), from one seed, two calls; then one part of a
@@ -887,7 +950,7 @@ def main():
     ap.add_argument("--suite", default=None,
                     help="comma-separated configurations to measure instead: c1,c2,c3,c4,c5,cent,load")
     ap.add_argument("--case", default=None, choices=["batched", "spmv", "ppr", "minplus", "eigen", "adjoint",
-                                                       "bfspart"],
+                                                       "bfspart", "all"],
                     help="a small workload for profilers instead")
     ap.add_argument("--scale", type=int, default=20)
     args = ap.parse_args()

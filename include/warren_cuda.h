@@ -534,8 +534,8 @@ typedef struct wc_bfs_part_info {
  * 2 × words 64-bit words (the frontiers of even and odd levels; bit i of
  * word i/64 is node i); every start's bit is set in frontier2[0..words).
  * Starts outside the id space are WC_NODE_OUTSIDE_ID_SPACE.  The part's
- * visited bits and depths are device buffers of its own, charged to the
- * version's budget until wc_bfs_part_end. */
+ * visited bits and depths are the version's pooled scratch (charged to its
+ * budget while the pool holds them), kept between searches. */
 wc_status wc_bfs_part_begin(wc_version* version, const wc_call* call, wc_direction direction,
                             const uint64_t* starts, uint64_t start_count, uint32_t max_depth,
                             uint32_t parts, uint32_t part, uint64_t* frontier2,

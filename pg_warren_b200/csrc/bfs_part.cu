@@ -19,6 +19,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "operand.h"
@@ -225,9 +226,34 @@ uint32_t grid_for(uint64_t items, uint32_t per_block) {
 
 // The parts' first rows for a search in `dir`: each part takes about an
 // equal share of the rows' pull entries plus one per row, cut at multiples
-// of 64 rows so that every 64-bit word of a bitmap has one owner.
+// of 64 rows so that every 64-bit word of a bitmap has one owner.  Kept per
+// (version, direction, parts): the offsets are read back only the first
+// time.
+static std::map<std::tuple<const wc_version*, int, uint32_t>, std::vector<uint64_t>> g_cuts;
+static std::mutex g_cuts_mu;
+
+static wc_status compute_bfs_part_cuts(wc_version* v, int dir, uint32_t parts,
+                                       std::vector<uint64_t>& cut, wc_error_detail* detail);
+
 static wc_status bfs_part_cuts(wc_version* v, int dir, uint32_t parts, std::vector<uint64_t>& cut,
                                wc_error_detail* detail) {
+  const auto key = std::make_tuple((const wc_version*)v, dir, parts);
+  {
+    std::lock_guard<std::mutex> lock(g_cuts_mu);
+    auto it = g_cuts.find(key);
+    if (it != g_cuts.end()) {
+      cut = it->second;
+      return WC_OK;
+    }
+  }
+  WC_TRY(compute_bfs_part_cuts(v, dir, parts, cut, detail));
+  std::lock_guard<std::mutex> lock(g_cuts_mu);
+  g_cuts[key] = cut;
+  return WC_OK;
+}
+
+static wc_status compute_bfs_part_cuts(wc_version* v, int dir, uint32_t parts,
+                                       std::vector<uint64_t>& cut, wc_error_detail* detail) {
   const uint64_t n = v->n;
   std::vector<uint64_t> work(n + 1, 0);
   std::vector<uint32_t> off(n + 1);
@@ -258,7 +284,7 @@ struct PartSearch {
   uint32_t max_depth = 0;
   uint64_t* frontier2 = nullptr;  // the caller's: 2 × words
   uint64_t words = 0;
-  DevBuf visited, depth, sums;
+  DevBuf *visited = nullptr, *depth = nullptr, *sums = nullptr;  // the version's pool
 };
 
 std::map<const wc_version*, std::unique_ptr<PartSearch>> g_searches;
@@ -277,8 +303,13 @@ uint32_t* frontier_half(PartSearch* ps, uint32_t level) {
 }  // namespace
 
 void bfs_part_forget(const wc_version* v) {
-  std::lock_guard<std::mutex> lock(g_searches_mu);
-  g_searches.erase(v);
+  {
+    std::lock_guard<std::mutex> lock(g_searches_mu);
+    g_searches.erase(v);
+  }
+  std::lock_guard<std::mutex> lock(g_cuts_mu);
+  for (auto it = g_cuts.begin(); it != g_cuts.end();)
+    it = std::get<0>(it->first) == v ? g_cuts.erase(it) : std::next(it);
 }
 
 }  // namespace wc
@@ -336,35 +367,36 @@ wc_status wc_bfs_part_begin(wc_version* v, const wc_call* call, wc_direction dir
   ps->frontier2 = frontier2;
   ps->words = (n + 63) / 64;
   const uint64_t words32 = 2 * ps->words;
-  WC_TRY(ps->visited.alloc(v->budget, std::max<uint64_t>(words32, 1) * 4, ctx.detail));
-  WC_TRY(ps->depth.alloc(v->budget, std::max<uint64_t>(n, 1) * 4, ctx.detail));
-  WC_TRY(ps->sums.alloc(v->budget, 64, ctx.detail));
+  // Pooled with the version (kept between searches), so a search allocates
+  // only when it needs more than the last one did.
+  WC_TRY(ctx.scratch(POOL_PART_VISITED, std::max<uint64_t>(words32, 1) * 4, &ps->visited));
+  WC_TRY(ctx.scratch(POOL_PART_DEPTH, std::max<uint64_t>(n, 1) * 4, &ps->depth));
+  WC_TRY(ctx.scratch(POOL_PART_SUMS, 64, &ps->sums));
+  DevBuf* starts_dev = nullptr;
+  if (start_count) WC_TRY(ctx.scratch(POOL_PART_STARTS, start_count * 8, &starts_dev));
   WC_TRY(ctx.begin());
-  DevBuf starts_dev;
-  if (start_count) {
-    WC_TRY(starts_dev.alloc(v->budget, start_count * 8, ctx.detail));
-    WC_CUDA(cudaMemcpyAsync(starts_dev.ptr, host.data(), start_count * 8, cudaMemcpyHostToDevice,
+  if (start_count)
+    WC_CUDA(cudaMemcpyAsync(starts_dev->ptr, host.data(), start_count * 8, cudaMemcpyHostToDevice,
                             ctx.stream), ctx.detail);
-  }
   WC_CUDA(cudaMemsetAsync(frontier2, 0, 2 * ps->words * 8, ctx.stream), ctx.detail);
-  WC_CUDA(cudaMemsetAsync(ps->visited.ptr, 0, std::max<uint64_t>(words32, 1) * 4, ctx.stream),
+  WC_CUDA(cudaMemsetAsync(ps->visited->ptr, 0, std::max<uint64_t>(words32, 1) * 4, ctx.stream),
           ctx.detail);
-  WC_CUDA(cudaMemsetAsync(ps->sums.ptr, 0, 64, ctx.stream), ctx.detail);
+  WC_CUDA(cudaMemsetAsync(ps->sums->ptr, 0, 64, ctx.stream), ctx.detail);
   if (ps->hi > ps->lo)
     note_launch(), bpart_fill_kernel<<<grid_for(ps->hi - ps->lo, 256), 256, 0, ctx.stream>>>(
-        ps->depth.as<uint32_t>(), ps->lo, ps->hi, WC_UNREACHED);
+        ps->depth->as<uint32_t>(), ps->lo, ps->hi, WC_UNREACHED);
   uint32_t* F = frontier_half(ps.get(), 0);
   if (start_count)
     note_launch(), bpart_seed_kernel<<<grid_for(start_count, 256), 256, 0, ctx.stream>>>(
-        starts_dev.as<uint64_t>(), start_count, ps->lo, ps->hi, F, ps->visited.as<uint32_t>(),
-        ps->depth.as<uint32_t>());
+        starts_dev->as<uint64_t>(), start_count, ps->lo, ps->hi, F, ps->visited->as<uint32_t>(),
+        ps->depth->as<uint32_t>());
   // Level 0's frontier, counted over the whole bitmap (the same on every part).
   note_launch(), bpart_count_kernel<<<grid_for(words32, 256), 256, 0, ctx.stream>>>(
-      F, 0, (uint32_t)words32, push_adj(v, direction), ps->sums.as<unsigned long long>());
+      F, 0, (uint32_t)words32, push_adj(v, direction), ps->sums->as<unsigned long long>());
   WC_CUDA(cudaGetLastError(), ctx.detail);
   WC_TRY(ctx.finish());
   unsigned long long sums[2];
-  WC_CUDA(cudaMemcpy(sums, ps->sums.ptr, 16, cudaMemcpyDeviceToHost), ctx.detail);
+  WC_CUDA(cudaMemcpy(sums, ps->sums->ptr, 16, cudaMemcpyDeviceToHost), ctx.detail);
   info->row_begin = ps->lo;
   info->row_end = ps->hi;
   info->id_space = n;
@@ -393,13 +425,13 @@ wc_status wc_bfs_part_step(wc_version* v, const wc_call* call, uint32_t level,
   WC_TRY(ctx.begin());
   const uint32_t* F = frontier_half(ps, level);
   uint32_t* N = frontier_half(ps, level + 1);
-  unsigned long long* acc = ps->sums.as<unsigned long long>();
+  unsigned long long* acc = ps->sums->as<unsigned long long>();
   WC_CUDA(cudaMemsetAsync(acc, 0, 16, ctx.stream), ctx.detail);
   if (ps->hi > ps->lo) {
     const uint32_t w_lo = ps->lo / 32, w_hi = (ps->hi + 31) / 32;
     const uint64_t scanned = (ps->dir == WC_BOTH ? 2 : 1) * v->m;
     const bool push = frontier_edges * kPartPushDivisor < scanned;
-    uint32_t* visited = ps->visited.as<uint32_t>();
+    uint32_t* visited = ps->visited->as<uint32_t>();
     if (push) {
       WC_CUDA(cudaMemsetAsync(N + w_lo, 0, (uint64_t)(w_hi - w_lo) * 4, ctx.stream), ctx.detail);
       note_launch(), bpart_push_kernel<<<grid_for(2 * ps->words * 32, 256), 256, 0, ctx.stream>>>(
@@ -410,7 +442,7 @@ wc_status wc_bfs_part_step(wc_version* v, const wc_call* call, uint32_t level,
                                                        ps->hi, N);
     }
     note_launch(), bpart_settle_kernel<<<grid_for(w_hi - w_lo, 256), 256, 0, ctx.stream>>>(
-        N, visited, ps->depth.as<uint32_t>(), ps->lo, ps->hi, level + 1, push_adj(v, ps->dir), acc);
+        N, visited, ps->depth->as<uint32_t>(), ps->lo, ps->hi, level + 1, push_adj(v, ps->dir), acc);
     WC_CUDA(cudaGetLastError(), ctx.detail);
   }
   WC_TRY(ctx.finish());
@@ -429,11 +461,14 @@ wc_status wc_bfs_part_end(wc_version* v, const wc_call* call, uint32_t* depth_ou
   WC_CUDA(cudaSetDevice(v->device), call ? call->detail : nullptr);
   Ctx ctx(v, call);
   if (ps->hi > ps->lo)
-    WC_CUDA(cudaMemcpyAsync(depth_out + ps->lo, ps->depth.as<uint32_t>() + ps->lo,
+    WC_CUDA(cudaMemcpyAsync(depth_out + ps->lo, ps->depth->as<uint32_t>() + ps->lo,
                             (uint64_t)(ps->hi - ps->lo) * 4, cudaMemcpyDefault, ctx.stream),
             ctx.detail);
   const wc_status st = ctx.finish();
-  bfs_part_forget(v);
+  {
+    std::lock_guard<std::mutex> slock(g_searches_mu);
+    g_searches.erase(v);  // the cuts stay with the version
+  }
   return st;
 }
 

@@ -8,7 +8,10 @@
 // iteration is wc_pagerank's own kernel over the part's units, with the stop
 // test left to the caller, who has the summed change.
 #include <algorithm>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "operand.h"
@@ -25,9 +28,41 @@ wc_status prepare_pull(Ctx& ctx, DevCsr& csr, int semiring, int weighted_flag, i
 // The parts' first units and first rows over `csr`'s schedule: units are
 // taken in order and a part is closed at the first row boundary at or past
 // its share of the entries; a long row's pieces stay in one part.
+// The cuts are kept per (version, CSR, parts): a version never changes, and
+// the schedule's units are read back from the device only the first time.
+struct Cuts {
+  std::vector<uint32_t> units;
+  std::vector<uint64_t> rows;
+};
+static std::map<std::tuple<const wc_version*, const DevCsr*, uint32_t>, Cuts> g_cuts;
+static std::mutex g_cuts_mu;
+
+static wc_status compute_part_cuts(const wc_version* v, const DevCsr& csr, uint32_t parts,
+                                   std::vector<uint32_t>& unit_cut,
+                                   std::vector<uint64_t>& row_cut, wc_error_detail* detail);
+
 wc_status schedule_part_cuts(const wc_version* v, const DevCsr& csr, uint32_t parts,
                              std::vector<uint32_t>& unit_cut, std::vector<uint64_t>& row_cut,
                              wc_error_detail* detail) {
+  const auto key = std::make_tuple(v, &csr, parts);
+  {
+    std::lock_guard<std::mutex> lock(g_cuts_mu);
+    auto it = g_cuts.find(key);
+    if (it != g_cuts.end()) {
+      unit_cut = it->second.units;
+      row_cut = it->second.rows;
+      return WC_OK;
+    }
+  }
+  WC_TRY(compute_part_cuts(v, csr, parts, unit_cut, row_cut, detail));
+  std::lock_guard<std::mutex> lock(g_cuts_mu);
+  g_cuts[key] = Cuts{unit_cut, row_cut};
+  return WC_OK;
+}
+
+static wc_status compute_part_cuts(const wc_version* v, const DevCsr& csr, uint32_t parts,
+                                   std::vector<uint32_t>& unit_cut,
+                                   std::vector<uint64_t>& row_cut, wc_error_detail* detail) {
   const Schedule& sc = csr.schedule;
   std::vector<Unit> units(sc.count);
   if (sc.count)
@@ -78,8 +113,13 @@ static PartSolve* part_of(const wc_version* v) {
 }
 
 void pagerank_part_forget(const wc_version* v) {
-  std::lock_guard<std::mutex> lock(g_parts_mu);
-  g_parts.erase(v);
+  {
+    std::lock_guard<std::mutex> lock(g_parts_mu);
+    g_parts.erase(v);
+  }
+  std::lock_guard<std::mutex> lock(g_cuts_mu);
+  for (auto it = g_cuts.begin(); it != g_cuts.end();)
+    it = std::get<0>(it->first) == v ? g_cuts.erase(it) : std::next(it);
 }
 
 }  // namespace wc

@@ -336,6 +336,8 @@ enum PoolTag {
   POOL_MAP_OPERAND_0 = 180,  // .. 195: one per operand
   POOL_BC_SIGMA = 200, POOL_BC_DELTA, POOL_BC_TOTAL, POOL_BC_REACHED, POOL_BC_FLAG,
   POOL_BC_SOURCES, POOL_BC_CAPS, POOL_BC_LIST, POOL_BC_TOMB, POOL_BC_VALUES, POOL_BC_CARRY,
+  // A row-partitioned search's part: held from its begin to its end.
+  POOL_PART_VISITED = 220, POOL_PART_DEPTH, POOL_PART_SUMS, POOL_PART_STARTS,
 };
 
 // A call's context: the stream, the caller's detail and cancellation.
