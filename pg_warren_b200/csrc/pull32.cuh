@@ -147,6 +147,18 @@ __device__ inline void pull32_units(const CsrView<W>& A, const double* __restric
       __syncwarp();
       const uint32_t n_q = min(kPull32Chunk, count - q * kPull32Chunk);
       const typename Ent::WT ww = pick8(wr, q >> 1);
+      const uint32_t k0 = q * kPull32Chunk;
+      if (n_q == kPull32Chunk && k0 + kPull32Chunk <= hi_r) {
+        // No row ends inside this chunk: its entries all fold into the
+        // current row, in order, with no boundary test between them.
+        const uint32_t row = tile ? a + r : a;
+#pragma unroll
+        for (uint32_t t = 0; t < kPull32Chunk; t++) {
+          const typename Ent::WT wv = (typename Ent::WT)__shfl_sync(0xffffffffu, ww, (k0 + t) & 31);
+          fold(acc, (q & 1) * kPull32Chunk + t, wv, row);
+        }
+        continue;
+      }
       for (uint32_t t = 0; t < n_q; t++) {
         const uint32_t k = q * kPull32Chunk + t;
         while (k >= hi_r) {  // rows ending before entry k (tiles only)
