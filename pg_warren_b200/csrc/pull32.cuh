@@ -159,16 +159,21 @@ __device__ inline void pull32_units(const CsrView<W>& A, const double* __restric
         }
         continue;
       }
-      for (uint32_t t = 0; t < n_q; t++) {
-        const uint32_t k = q * kPull32Chunk + t;
-        while (k >= hi_r) {  // rows ending before entry k (tiles only)
+      // Otherwise row by row: emit the rows that end before entry t, then
+      // fold the chunk's entries of the current row with no test between.
+      for (uint32_t t = 0; t < n_q;) {
+        while (k0 + t >= hi_r) {  // rows ending before entry k0 + t (tiles only)
           epi.emit(a + r, acc, epi.shfl(row_l, r));
           acc = Part{Acc<double, ADD>::of(0.0), false};
           r++;
           hi_r = __shfl_sync(0xffffffffu, hi_l, r);
         }
-        const typename Ent::WT wv = (typename Ent::WT)__shfl_sync(0xffffffffu, ww, k & 31);
-        fold(acc, (q & 1) * kPull32Chunk + t, wv, tile ? a + r : a);
+        const uint32_t end = min(n_q, hi_r - k0);
+        const uint32_t row = tile ? a + r : a;
+        for (; t < end; t++) {
+          const typename Ent::WT wv = (typename Ent::WT)__shfl_sync(0xffffffffu, ww, (k0 + t) & 31);
+          fold(acc, (q & 1) * kPull32Chunk + t, wv, row);
+        }
       }
     }
     if (chunks == 0) {
