@@ -62,14 +62,23 @@ __global__ void sum_partial_kernel(uint32_t n, F f, double* partial) {
   }
 }
 
-__global__ void sum_final_kernel(const double* partial, uint32_t count, uint32_t columns,
-                                 double* out) {
-  // out[c] = Σ_b partial[b * columns + c], b in order.
-  const uint32_t c = threadIdx.x + blockIdx.x * blockDim.x;
-  if (c >= columns) return;
-  double t = 0.0;
-  for (uint32_t b = 0; b < count; b++) t += partial[(size_t)b * columns + c];
-  out[c] = t;
+// out[c] = Σ_b partial[b * columns + c], b in order.  One block: the
+// partials are first brought into shared memory by every thread (coalesced
+// loads, all in flight at once), then each column is added up in block
+// order by one thread from there, so the dependent chain of additions waits
+// on shared memory rather than on L2.
+constexpr uint32_t kSumFinalMaxValues = kRedBlocks * 8;  // count × columns
+__global__ void __launch_bounds__(256) sum_final_kernel(const double* partial, uint32_t count,
+                                                        uint32_t columns, double* out) {
+  __shared__ double sp[kSumFinalMaxValues];
+  const uint32_t total = count * columns;
+  for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) sp[i] = partial[i];
+  __syncthreads();
+  for (uint32_t c = threadIdx.x; c < columns; c += blockDim.x) {
+    double t = 0.0;
+    for (uint32_t b = 0; b < count; b++) t += sp[b * columns + c];
+    out[c] = t;
+  }
 }
 
 // Qᵀw for vectors [j0, j0 + 8) of Q (column-major, n rows each), with an
@@ -516,7 +525,8 @@ struct Eigensolver {
   cudaStream_t st() const { return ctx.stream; }
 
   wc_status sum_final(uint32_t count, uint32_t columns, double* out_host) {
-    note_launch(), sum_final_kernel<<<(columns + 63) / 64, 64, 0, st()>>>(partial->as<double>(), count, columns,
+    if ((uint64_t)count * columns > kSumFinalMaxValues) return WC_INVALID_ARGUMENT;
+    note_launch(), sum_final_kernel<<<1, 256, 0, st()>>>(partial->as<double>(), count, columns,
                                                          coefbuf->as<double>());
     WC_CUDA(cudaMemcpyAsync(out_host, coefbuf->ptr, columns * 8, cudaMemcpyDeviceToHost, st()),
             ctx.detail);
