@@ -20,6 +20,7 @@
 // the reference calls nalgebra's SymmetricEigen (spectral/ritz.rs:34-52).
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <numeric>
 
 #include "bfs.h"
@@ -71,6 +72,10 @@ constexpr uint32_t kSumFinalMaxValues = kRedBlocks * 8;  // count × columns
 __global__ void __launch_bounds__(256) sum_final_kernel(const double* partial, uint32_t count,
                                                         uint32_t columns, double* out) {
   __shared__ double sp[kSumFinalMaxValues];
+  // Block b combines the b-th run of count × columns partials into
+  // out[b·columns ..): several projections' partials in one launch.
+  partial += (size_t)blockIdx.x * count * columns;
+  out += (size_t)blockIdx.x * columns;
   const uint32_t total = count * columns;
   for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) sp[i] = partial[i];
   __syncthreads();
@@ -756,31 +761,47 @@ struct Eigensolver {
 
   // ---------------------------------------------------------- the basis
   uint32_t size = 0, len = 0;
+  uint32_t held_chunks = 1;  // projection chunks the partial and coefficient buffers hold
 
   double* col(uint32_t j) { return Q->as<double>() + (size_t)j * n; }
 
-  // Qᵀw (after w -= c·q_p for pending p >= 0).
-  wc_status project(double* w, int pending, double c, std::vector<double>& out) {
-    out.assign(len, 0.0);
-    for (uint32_t j0 = 0; j0 < len || (j0 == 0 && pending >= 0); j0 += 8) {
-      note_launch(), project_kernel<<<grid, 256, 0, st()>>>(n, Q->as<double>(), len, j0, w, pending, c,
-                                             partial->as<double>());
-      std::vector<double> part(8);
-      WC_TRY(sum_final(grid, 8, part.data()));
-      for (uint32_t q = 0; q < 8 && j0 + q < len; q++) out[j0 + q] = part[q];
-      if (len == 0) break;
+  // Qᵀw (after w -= c·q_p for pending p >= 0) into coefbuf[0 .. len) on the
+  // device: every 8-column chunk's projection, then one launch combining
+  // each chunk's partials in block order, then the coefficients' copy into
+  // the pinned staging, all queued without a wait; subtract_projected, which
+  // follows, waits once for all of it.
+  wc_status project(double* w, int pending, double c) {
+    if (len == 0 && pending < 0) return WC_OK;
+    const uint32_t chunks = std::max<uint32_t>(1, (len + 7) / 8);
+    if ((uint64_t)chunks * 8 * 8 > kStageBytes - kStagePayload) return WC_UNSUPPORTED;
+    if (chunks > held_chunks) {  // grown once per solve, not charged again each step
+      WC_TRY(ctx.scratch(POOL_EIG_7, (uint64_t)chunks * grid * 8 * 8, &partial));
+      WC_TRY(ctx.scratch(POOL_EIG_8, (uint64_t)std::max<uint32_t>(64, chunks * 8) * 8, &coefbuf));
+      held_chunks = chunks;
     }
+    for (uint32_t b = 0; b < chunks; b++)
+      note_launch(), project_kernel<<<grid, 256, 0, st()>>>(n, Q->as<double>(), len, 8 * b, w,
+                                                            pending, c,
+                                                            partial->as<double>() +
+                                                                (size_t)b * grid * 8);
+    note_launch(), sum_final_kernel<<<chunks, 256, 0, st()>>>(partial->as<double>(), grid, 8,
+                                                              coefbuf->as<double>());
+    if (len)
+      WC_CUDA(cudaMemcpyAsync(v->stage_host + kStagePayload, coefbuf->ptr, len * 8,
+                              cudaMemcpyDeviceToHost, st()),
+              ctx.detail);
     return WC_OK;
   }
 
-  wc_status subtract(double* w, const std::vector<double>& c, double* norm) {
-    if (!c.empty())
-      WC_CUDA(cudaMemcpyAsync(coefbuf->ptr, c.data(), c.size() * 8, cudaMemcpyHostToDevice, st()),
-              ctx.detail);
+  // w -= Σ_j c_j q_j with the coefficients project left in coefbuf, then
+  // ‖w‖; waits for the stream, after which `c` gets those coefficients.
+  wc_status subtract_projected(double* w, std::vector<double>& c, double* norm) {
     note_launch(), subtract_kernel<<<grid, 256, 0, st()>>>(n, Q->as<double>(), coefbuf->as<double>(), len, w,
                                             partial->as<double>());
     double s;
     WC_TRY(sum_final(grid, 1, &s));
+    c.assign(len, 0.0);
+    if (len) std::memcpy(c.data(), v->stage_host + kStagePayload, len * 8);
     *norm = std::sqrt(s);
     return WC_OK;
   }
@@ -803,14 +824,14 @@ struct Eigensolver {
       pending_c = alpha;
     } else {
       std::vector<double> first;
-      WC_TRY(project(w, -1, 0.0, first));
+      WC_TRY(project(w, -1, 0.0));
       double ignored;
-      WC_TRY(subtract(w, first, &ignored));
+      WC_TRY(subtract_projected(w, first, &ignored));
       for (uint32_t j = 0; j < len; j++) coefficients[j] += first[j];
     }
     std::vector<double> correction;
-    WC_TRY(project(w, pending, pending_c, correction));
-    WC_TRY(subtract(w, correction, norm));
+    WC_TRY(project(w, pending, pending_c));
+    WC_TRY(subtract_projected(w, correction, norm));
     for (uint32_t j = 0; j < len; j++) coefficients[j] += correction[j];
     return WC_OK;
   }
