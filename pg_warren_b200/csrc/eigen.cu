@@ -310,11 +310,9 @@ __global__ void deflate_coef_kernel(uint32_t n, const uint8_t* active, const uin
     val[s][0] = val[s][1] = 0.0;
   }
   __syncthreads();
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    if (!active[i]) continue;
-    const uint32_t c = comp[i];
-    const double a = unit[i] * x[i];
-    const double b = (colour && colour[i]) ? -a : a;
+  // Adds (a, b) for component c into the block's table, or into coef when
+  // the table's slot holds another component.
+  auto add = [&](uint32_t c, double a, double b) {
     const uint32_t slot = c & 63;
     uint32_t prev = atomicCAS(&key[slot], 0xffffffffu, c);
     if (prev == 0xffffffffu || prev == c) {
@@ -323,6 +321,35 @@ __global__ void deflate_coef_kernel(uint32_t n, const uint8_t* active, const uin
     } else {
       atomicAdd(coef + 2 * (size_t)c, a);
       atomicAdd(coef + 2 * (size_t)c + 1, b);
+    }
+  };
+  // A warp takes 32 consecutive nodes a step.  When every active node among
+  // them lies in one component (the common case: a large component's nodes
+  // are numbered together), the warp sums them with shuffles and one lane
+  // adds the sums; otherwise each active lane adds its own.
+  const unsigned lane = threadIdx.x & 31;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); i0 < n; i0 += stride) {
+    const uint32_t i = i0 + lane;
+    const bool live = i < n && active[i];
+    uint32_t c = 0xffffffffu;
+    double a = 0.0, b = 0.0;
+    if (live) {
+      c = comp[i];
+      a = unit[i] * x[i];
+      b = (colour && colour[i]) ? -a : a;
+    }
+    const unsigned lm = __ballot_sync(0xffffffffu, live);
+    if (!lm) continue;
+    const uint32_t c_first = __shfl_sync(0xffffffffu, c, __ffs(lm) - 1);
+    if (__all_sync(0xffffffffu, !live || c == c_first)) {
+      for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+      }
+      if (lane == 0) add(c_first, a, b);
+    } else if (live) {
+      add(c, a, b);
     }
   }
   __syncthreads();
