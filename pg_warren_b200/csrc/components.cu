@@ -25,6 +25,7 @@ __global__ void wcc_hook_kernel(const uint32_t* off, const uint32_t* tgt, uint32
                                 uint32_t* parent, int* changed) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  bool hooked = false;
   for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += warps) {
     const uint32_t lo = off[u], hi = off[u + 1];
     for (uint32_t e = lo + lane; e < hi; e += 32) {
@@ -33,10 +34,13 @@ __global__ void wcc_hook_kernel(const uint32_t* off, const uint32_t* tgt, uint32
       while (b != parent[b]) b = parent[b];
       if (a != b) {
         atomicMin(parent + max(a, b), min(a, b));
-        *changed = 1;
+        hooked = true;
       }
     }
   }
+  // One write of the flag a warp (every edge writing it contended on one
+  // address).
+  if (__any_sync(0xffffffffu, hooked) && lane == 0) *changed = 1;
 }
 
 __global__ void wcc_compress_kernel(uint32_t* parent, uint32_t n) {

@@ -253,6 +253,7 @@ __global__ void cc_hook_kernel(const uint32_t* off, const uint32_t* tgt, const u
                                uint32_t n, uint32_t* parent, int* changed) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  bool hooked = false;
   for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += warps) {
     if (!active[u]) continue;
     const uint32_t lo = off[u], hi = off[u + 1];
@@ -264,10 +265,13 @@ __global__ void cc_hook_kernel(const uint32_t* off, const uint32_t* tgt, const u
       while (b != parent[b]) b = parent[b];
       if (a != b) {
         atomicMin(parent + max(a, b), min(a, b));
-        *changed = 1;
+        hooked = true;
       }
     }
   }
+  // One write of the flag a warp (every edge writing it contended on one
+  // address).
+  if (__any_sync(0xffffffffu, hooked) && lane == 0) *changed = 1;
 }
 
 __global__ void cc_compress_kernel(uint32_t* parent, uint32_t n) {
